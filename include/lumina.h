@@ -1,0 +1,158 @@
+/* lumina.h -- C ABI of liblumina.so, the B200 render path.
+ *
+ * Plain C: pointers, sizes and POD structs only.  Every call returns LG_OK (0)
+ * or a negative LG_ERR_* status and never exits the process (the reference
+ * calls exit(1) on any CUDA error, pathtracer.cu:17-20); lg_last_error()
+ * returns the calling thread's last message.
+ *
+ * Record layouts match the reference's C++ structs byte for byte
+ * (include/scene.h:6-56, include/bvh.h:7-16), so a Scene's vectors can be
+ * passed straight through.
+ *
+ * Entry points and the reference interface each one replaces:
+ *   lg_scene_load_json      LoadSceneJSON                 src/scene_loader.cpp:26-138
+ *   lg_build_bvh            BuildBVH                      src/bvh.cpp:164-211
+ *   lg_build_bvh_device     BuildBVH, device-resident in/out
+ *   lg_renderer_*, lg_render RenderSceneCUDA              src/pathtracer.cu:581-757
+ *   lg_render_batch         cuda_ref --batch job loop     src/main.cpp:158-190
+ *   lg_tonemap_device       tonemap_kernel                src/pathtracer.cu:413-429
+ *   lg_look_at              overwrite_camera              src/main.cpp:29-59
+ *   lg_write_png            stbi_write_png call sites     src/main.cpp:214-226
+ *   lg_unet_*               ml/train.py:37-75 UNet and its Adam/L1 step (ml/train.py:184-201)
+ */
+#ifndef LUMINA_H
+#define LUMINA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LG_OK 0
+#define LG_ERR_INVALID (-1)     /* bad argument or scene content */
+#define LG_ERR_CUDA (-2)        /* CUDA runtime error (message in lg_last_error) */
+#define LG_ERR_IO (-3)          /* file could not be opened / written */
+#define LG_ERR_PARSE (-4)       /* malformed scene.json */
+#define LG_ERR_NOMEM (-5)       /* host or device allocation failed */
+#define LG_ERR_DEVICE (-6)      /* a kernel reported an error flag (stack or queue overflow, wait limit) */
+#define LG_ERR_CAPACITY (-7)    /* output buffer too small */
+
+typedef struct { float v[3][3]; float n[3][3]; float uv[3][2]; int32_t material; } lg_triangle;   /* 100 B */
+typedef struct { float bbMin[3]; float bbMax[3]; int32_t left, right, firstTri, triCount; } lg_bvh_node; /* 40 B */
+typedef struct { float pos[3]; float color[3]; float intensity; float radius; } lg_point_light;
+typedef struct { float dir[3]; float color[3]; float intensity; } lg_dir_light;
+typedef struct {
+    float pos[3];
+    float camera_to_world[16]; /* rows 0/1/2 = forward/left/up, row 3 = position */
+    float fov_y_deg, aspect, near_z, far_z;
+    int32_t width, height;
+} lg_camera;
+
+/* A scene as plain arrays (host memory unless a call says otherwise). */
+typedef struct {
+    lg_camera camera;
+    lg_dir_light sun;
+    const lg_triangle* tris;
+    int32_t n_tris;
+    const float* mat_albedo;   /* 3 floats per material */
+    const float* mat_emissive; /* 3 floats per material, may be NULL */
+    int32_t n_mats;
+    const lg_point_light* points;
+    int32_t n_points;
+    const lg_dir_light* directionals; /* parsed and kept; not used for shading (as in the reference) */
+    int32_t n_directionals;
+} lg_scene_desc;
+
+const char* lg_last_error(void);
+int lg_version(void);
+
+/* ---- scene.json (drop-in for LoadSceneJSON) ---- */
+typedef struct lg_scene lg_scene;
+/* flags: bit0 = print the reference's "[scene] loaded ..." summary to stdout.
+ * threads: host threads for parsing the triangle array (<= 0: all cores). */
+int lg_scene_load_json(const char* path, int flags, int threads, lg_scene** out);
+int lg_scene_create(const lg_scene_desc* desc, lg_scene** out); /* deep copy */
+int lg_scene_describe(const lg_scene* s, lg_scene_desc* out);   /* pointers stay owned by s */
+int lg_scene_set_camera(lg_scene* s, const lg_camera* cam);
+int lg_scene_save_json(const lg_scene* s, const char* path);
+/* Material texture path (may be ""), owned by s. */
+const char* lg_scene_texture(const lg_scene* s, int material);
+void lg_scene_destroy(lg_scene* s);
+
+/* overwrite_camera (src/main.cpp:29-59): forward = normalize(target-pos),
+ * left = normalize(-fy, fx, 0) (fallback +Y), up = forward x left.
+ * Leaves cam unchanged when |target-pos| < 1e-8. */
+void lg_look_at(lg_camera* cam, const float pos[3], const float target[3]);
+
+/* ---- BVH (drop-in for BuildBVH) ----
+ * Builds on the current CUDA device.  nodes_out must hold max(2*n_tris-1, 1)
+ * nodes.  perm_out[i] (optional) = input index of the triangle placed at i;
+ * tris_out (optional, may equal tris) receives the reordered triangles.
+ * n_tris == 0 gives *n_nodes_out = 0. */
+int lg_build_bvh(const lg_triangle* tris, int32_t n_tris, lg_bvh_node* nodes_out, int32_t* n_nodes_out,
+                 int32_t* perm_out, lg_triangle* tris_out);
+/* Same with device pointers on `stream` (a cudaStream_t, may be NULL).
+ * d_tris_out may be NULL.  Scratch is taken from a per-device pool that
+ * grows on demand. */
+int lg_build_bvh_device(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* d_nodes_out, int32_t* n_nodes_out,
+                        int32_t* d_perm_out, lg_triangle* d_tris_out, void* stream);
+
+/* ---- path tracer ---- */
+typedef struct lg_renderer lg_renderer;
+
+#define LG_RENDER_ACCUM64 1u   /* keep an FP64 per-pixel accumulator (judge images) */
+
+typedef struct {
+    int32_t spp;           /* samples per pixel (chunks of 8 share one RNG stream, as in the reference) */
+    int32_t max_bounces;
+    int32_t sample_base;   /* first sample index (continues a progressive render); normally 0 */
+    uint32_t flags;        /* LG_RENDER_* */
+} lg_render_opts;
+
+typedef struct {
+    float kernel_ms;       /* device time of the trace + tonemap launches */
+    /* The rest is filled only while counting is on (lg_renderer_set_counting). */
+    uint64_t closest_rays; /* closest-hit rays traced (camera + bounce) */
+    uint64_t shadow_rays;  /* shadow rays traced */
+    uint64_t node_fetches; /* 64-byte two-child BVH records read */
+    uint64_t tri_tests;    /* ray/triangle tests (48 bytes of vertex data each) */
+    uint64_t leaf_fetches; /* 8-byte leaf-table entries read */
+} lg_render_stats;
+
+int lg_renderer_create(int device, lg_renderer** out);
+void lg_renderer_destroy(lg_renderer* r);
+/* Upload a scene and build its BVH on the device (triangles are reordered on
+ * the device; host arrays are not modified). */
+int lg_renderer_set_scene(lg_renderer* r, const lg_scene_desc* scene);
+/* Upload a scene whose triangles are already in BVH order with its node array. */
+int lg_renderer_set_scene_bvh(lg_renderer* r, const lg_scene_desc* scene, const lg_bvh_node* nodes, int32_t n_nodes);
+/* Copy back the device BVH (nodes_out may be NULL to query the count). */
+int lg_renderer_get_bvh(lg_renderer* r, lg_bvh_node* nodes_out, int32_t* n_nodes, lg_triangle* tris_out);
+int lg_renderer_set_counting(lg_renderer* r, int enable);
+/* Render one frame.  rgb8 (W*H*3 bytes) and accum (W*H*3 floats, sum over
+ * samples as RenderSceneCUDA's accumulator) are host buffers; either may be
+ * NULL.  accum64 (W*H*3 doubles) requires LG_RENDER_ACCUM64. */
+int lg_render(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, uint8_t* rgb8, float* accum,
+              double* accum64, lg_render_stats* stats);
+/* Device-output variant: results stay in device buffers owned by the
+ * renderer until the next call; pointers are returned (any may be NULL). */
+int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, void* stream,
+                     const uint8_t** d_rgb8, const float** d_accum, const double** d_accum64);
+/* n_jobs frames with per-job cameras and spp, tonemapped into rgb8_out
+ * (n_jobs * W*H*3 bytes, host). */
+int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts* opts, int32_t n_jobs,
+                    uint8_t* rgb8_out, float* ms_per_job);
+
+/* tonemap_kernel: rgb8 = (u8)(sqrt(clamp(accum*inv_spp, 0, 1)) * 255). */
+int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, float inv_spp, void* stream);
+
+/* ---- image output ---- */
+int lg_write_png(const char* path, int32_t w, int32_t h, const uint8_t* rgb8);
+int lg_write_hdr(const char* path, int32_t w, int32_t h, const float* rgb32);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,761 @@
+// capi.cu -- the extern "C" boundary (include/lumina.h) and the C++ drop-ins
+// BuildBVH (include/bvh.h) and RenderSceneCUDA (reference pathtracer.cu:581-757).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "bvh.h"
+#include "common.h"
+#include "lbvh.cuh"
+#include "scene.h"
+#include "trace.cuh"
+
+namespace lg
+{
+bool load_scene_file(const std::string& path, Scene& out, bool verbose, int threads, std::string& err);
+bool save_scene_file(const Scene& sc, const std::string& path, int threads);
+bool write_png(const char* path, int w, int h, const uint8_t* rgb);
+bool write_hdr(const char* path, int w, int h, const float* rgb);
+
+namespace
+{
+thread_local std::string g_err;
+}
+
+int set_error(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+void clear_error() { g_err.clear(); }
+
+// Growable device buffer.
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t b)
+    {
+        if (b <= bytes) return LG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess)
+        {
+            p = nullptr;
+            return set_error(LG_ERR_NOMEM, "cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return LG_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return (T*)p; }
+};
+
+// Per-device scratch for the pointer-level BVH entry points.
+struct DeviceScratch
+{
+    std::mutex mu;
+    DevBuf buf;
+};
+DeviceScratch& device_scratch(int dev)
+{
+    static DeviceScratch pool[64];
+    return pool[dev & 63];
+}
+
+}  // namespace lg
+
+using namespace lg;
+
+struct lg_scene
+{
+    Scene s;
+    std::vector<float> albedo, emissive;  // flattened views for lg_scene_describe
+};
+
+struct lg_renderer
+{
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool counting = false;
+    // scene
+    int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0;
+    lg_dir_light sun{};
+    DevBuf tris, tris_in, nodes, wide, leaves, tv, mats, points, scratch;
+    // frame
+    DevBuf accum, accum64, rgb, work, counters;
+    int fw = 0, fh = 0;
+};
+
+namespace
+{
+struct DeviceGuard
+{
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int validate_scene(const lg_scene_desc* d)
+{
+    if (!d) return set_error(LG_ERR_INVALID, "scene is NULL");
+    if (d->n_tris < 0 || d->n_mats < 0 || d->n_points < 0) return set_error(LG_ERR_INVALID, "negative count");
+    if (d->n_tris > 0 && !d->tris) return set_error(LG_ERR_INVALID, "tris is NULL");
+    if (d->n_mats > 0 && !d->mat_albedo) return set_error(LG_ERR_INVALID, "mat_albedo is NULL");
+    if (d->n_points > 0 && !d->points) return set_error(LG_ERR_INVALID, "points is NULL");
+    for (int i = 0; i < d->n_tris; ++i)
+    {
+        const int m = d->tris[i].material;
+        if (m < 0 || m >= d->n_mats)
+            return set_error(LG_ERR_INVALID, "triangle %d has material %d outside [0,%d)", i, m, d->n_mats);
+    }
+    return LG_OK;
+}
+
+int upload_common(lg_renderer* r, const lg_scene_desc* d)
+{
+    r->n_mats = d->n_mats;
+    r->n_points = d->n_points;
+    r->sun = d->sun;
+    std::vector<float4> m((size_t)std::max(d->n_mats, 1));
+    for (int i = 0; i < d->n_mats; ++i)
+        m[(size_t)i] = make_float4(d->mat_albedo[3 * i], d->mat_albedo[3 * i + 1], d->mat_albedo[3 * i + 2], 0.0f);
+    LG_TRY(r->mats.reserve(m.size() * sizeof(float4)));
+    LG_TRY_CUDA(cudaMemcpyAsync(r->mats.p, m.data(), m.size() * sizeof(float4), cudaMemcpyHostToDevice, r->stream));
+    LG_TRY(r->points.reserve((size_t)std::max(d->n_points, 1) * sizeof(lg_point_light)));
+    if (d->n_points)
+        LG_TRY_CUDA(cudaMemcpyAsync(r->points.p, d->points, (size_t)d->n_points * sizeof(lg_point_light),
+                                    cudaMemcpyHostToDevice, r->stream));
+    return LG_OK;
+}
+
+// Wide nodes + intersection records from the device node/triangle arrays.
+int finish_scene(lg_renderer* r)
+{
+    if (r->n_nodes == 0) { r->root = 0; return LG_OK; }
+    LG_TRY(r->wide.reserve((size_t)r->n_nodes * sizeof(WideNode)));
+    LG_TRY(r->leaves.reserve((size_t)r->n_nodes * sizeof(int2)));
+    LG_TRY(r->tv.reserve((size_t)r->n_tris * 3 * sizeof(float4)));
+    size_t need = ((size_t)r->n_nodes * 2 + (size_t)r->n_nodes / 1024 + 8) * sizeof(int);
+    LG_TRY(r->scratch.reserve(need));
+    int root = 0, ni = 0, nl = 0;
+    LG_TRY_CUDA(build_wide_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide.as<WideNode>(),
+                                 r->leaves.as<int2>(), r->scratch.as<int>(), &root, &ni, &nl, r->stream));
+    LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    r->root = root;
+    return LG_OK;
+}
+
+int ensure_frame(lg_renderer* r, int w, int h, bool acc64)
+{
+    const size_t n = (size_t)w * h * 3;
+    LG_TRY(r->accum.reserve(n * sizeof(float)));
+    LG_TRY(r->rgb.reserve(n));
+    if (acc64) LG_TRY(r->accum64.reserve(n * sizeof(double)));
+    LG_TRY(r->work.reserve(256));
+    LG_TRY(r->counters.reserve(sizeof(RenderCounters)));
+    r->fw = w;
+    r->fh = h;
+    return LG_OK;
+}
+
+int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* o, lg_render_stats* stats)
+{
+    if (!r || !cam || !o) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (cam->width <= 0 || cam->height <= 0) return set_error(LG_ERR_INVALID, "image size %dx%d", cam->width, cam->height);
+    if (o->spp < 0 || o->max_bounces < 0) return set_error(LG_ERR_INVALID, "spp/bounces must be >= 0");
+    const bool acc64 = (o->flags & LG_RENDER_ACCUM64) != 0;
+    LG_TRY(ensure_frame(r, cam->width, cam->height, acc64));
+    const long long nval = (long long)cam->width * cam->height * 3;
+    LG_TRY_CUDA(cudaMemsetAsync(r->accum.p, 0, (size_t)nval * sizeof(float), r->stream));
+    if (acc64) LG_TRY_CUDA(cudaMemsetAsync(r->accum64.p, 0, (size_t)nval * sizeof(double), r->stream));
+    if (r->counting) LG_TRY_CUDA(cudaMemsetAsync(r->counters.p, 0, sizeof(RenderCounters), r->stream));
+    LG_TRY_CUDA(cudaEventRecord(r->ev0, r->stream));
+    if (o->spp > 0 && r->n_nodes > 0)
+    {
+        DevScene s;
+        s.nodes = r->wide.as<WideNode>();
+        s.leaves = r->leaves.as<int2>();
+        s.tv = r->tv.as<float4>();
+        s.tris = r->tris.as<lg_triangle>();
+        s.mats = r->mats.as<float4>();
+        s.points = r->points.as<lg_point_light>();
+        s.n_points = r->n_points;
+        s.root = r->root;
+        s.sun = r->sun;
+        TraceJob job;
+        job.spp = o->spp;
+        job.max_bounces = o->max_bounces;
+        job.sample_base = o->sample_base;
+        job.n_chunks = (o->spp + 7) / 8;
+        job.tiles_x = (cam->width + 7) / 8;
+        job.n_tiles = job.tiles_x * ((cam->height + 3) / 4);
+        job.accum = r->accum.as<float>();
+        job.accum64 = acc64 ? r->accum64.as<double>() : nullptr;
+        job.work = r->work.as<unsigned>();
+        job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
+        LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->stream));
+    }
+    const float inv = 1.0f / (float)o->spp;
+    LG_TRY_CUDA(launch_tonemap(r->accum.as<float>(), r->rgb.as<uint8_t>(), nval, inv, r->stream));
+    LG_TRY_CUDA(cudaEventRecord(r->ev1, r->stream));
+    if (stats)
+    {
+        LG_TRY_CUDA(cudaEventSynchronize(r->ev1));
+        float ms = 0.0f;
+        LG_TRY_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
+        stats->kernel_ms = ms;
+        stats->closest_rays = stats->shadow_rays = 0;
+        stats->node_fetches = stats->tri_tests = stats->leaf_fetches = 0;
+        if (r->counting)
+        {
+            RenderCounters c;
+            LG_TRY_CUDA(cudaMemcpy(&c, r->counters.p, sizeof c, cudaMemcpyDeviceToHost));
+            stats->closest_rays = c.closest_rays;
+            stats->shadow_rays = c.shadow_rays;
+            stats->node_fetches = c.node_fetches;
+            stats->tri_tests = c.tri_tests;
+            stats->leaf_fetches = c.leaf_fetches;
+            if (c.stack_overflows)
+                return set_error(LG_ERR_DEVICE, "traversal stack overflowed %llu times", c.stack_overflows);
+        }
+    }
+    return LG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+const char* lg_last_error(void) { return g_err.c_str(); }
+int lg_version(void) { return 100; }
+
+// ---- scene ----
+int lg_scene_load_json(const char* path, int flags, int threads, lg_scene** out)
+{
+    if (!path || !out) return set_error(LG_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    lg_scene* s = new (std::nothrow) lg_scene();
+    if (!s) return set_error(LG_ERR_NOMEM, "out of memory");
+    std::string err;
+    if (!load_scene_file(path, s->s, (flags & 1) != 0, threads, err))
+    {
+        delete s;
+        return g_err.find("failed to open") != std::string::npos ? LG_ERR_IO : LG_ERR_PARSE;
+    }
+    *out = s;
+    return LG_OK;
+}
+
+int lg_scene_create(const lg_scene_desc* d, lg_scene** out)
+{
+    if (!d || !out) return set_error(LG_ERR_INVALID, "NULL argument");
+    lg_scene* s = new (std::nothrow) lg_scene();
+    if (!s) return set_error(LG_ERR_NOMEM, "out of memory");
+    CameraDesc& c = s->s.camera;
+    std::memcpy(c.pos, d->camera.pos, sizeof c.pos);
+    std::memcpy(c.cameraToWorld, d->camera.camera_to_world, sizeof c.cameraToWorld);
+    c.fovYDeg = d->camera.fov_y_deg;
+    c.aspect = d->camera.aspect;
+    c.nearZ = d->camera.near_z;
+    c.farZ = d->camera.far_z;
+    c.imageWidth = d->camera.width;
+    c.imageHeight = d->camera.height;
+    std::memcpy(&s->s.sun, &d->sun, sizeof(lg_dir_light));
+    s->s.triangles.resize((size_t)std::max(d->n_tris, 0));
+    if (d->n_tris > 0) std::memcpy(s->s.triangles.data(), d->tris, (size_t)d->n_tris * sizeof(Triangle));
+    for (int i = 0; i < d->n_mats; ++i)
+    {
+        Material m;
+        for (int k = 0; k < 3; ++k)
+        {
+            m.albedo[k] = d->mat_albedo[3 * i + k];
+            m.emissive[k] = d->mat_emissive ? d->mat_emissive[3 * i + k] : 0.0f;
+        }
+        s->s.materials.push_back(m);
+    }
+    s->s.points.resize((size_t)std::max(d->n_points, 0));
+    if (d->n_points > 0) std::memcpy(s->s.points.data(), d->points, (size_t)d->n_points * sizeof(PointLight));
+    s->s.directionals.resize((size_t)std::max(d->n_directionals, 0));
+    if (d->n_directionals > 0)
+        std::memcpy(s->s.directionals.data(), d->directionals, (size_t)d->n_directionals * sizeof(DirectionalLight));
+    *out = s;
+    return LG_OK;
+}
+
+int lg_scene_describe(const lg_scene* cs, lg_scene_desc* d)
+{
+    if (!cs || !d) return set_error(LG_ERR_INVALID, "NULL argument");
+    lg_scene* s = const_cast<lg_scene*>(cs);
+    const CameraDesc& c = s->s.camera;
+    std::memcpy(d->camera.pos, c.pos, sizeof c.pos);
+    std::memcpy(d->camera.camera_to_world, c.cameraToWorld, sizeof c.cameraToWorld);
+    d->camera.fov_y_deg = c.fovYDeg;
+    d->camera.aspect = c.aspect;
+    d->camera.near_z = c.nearZ;
+    d->camera.far_z = c.farZ;
+    d->camera.width = c.imageWidth;
+    d->camera.height = c.imageHeight;
+    std::memcpy(&d->sun, &s->s.sun, sizeof(lg_dir_light));
+    d->tris = reinterpret_cast<const lg_triangle*>(s->s.triangles.data());
+    d->n_tris = (int32_t)s->s.triangles.size();
+    s->albedo.resize(s->s.materials.size() * 3);
+    s->emissive.resize(s->s.materials.size() * 3);
+    for (size_t i = 0; i < s->s.materials.size(); ++i)
+        for (int k = 0; k < 3; ++k)
+        {
+            s->albedo[3 * i + k] = s->s.materials[i].albedo[k];
+            s->emissive[3 * i + k] = s->s.materials[i].emissive[k];
+        }
+    d->mat_albedo = s->albedo.data();
+    d->mat_emissive = s->emissive.data();
+    d->n_mats = (int32_t)s->s.materials.size();
+    d->points = reinterpret_cast<const lg_point_light*>(s->s.points.data());
+    d->n_points = (int32_t)s->s.points.size();
+    d->directionals = reinterpret_cast<const lg_dir_light*>(s->s.directionals.data());
+    d->n_directionals = (int32_t)s->s.directionals.size();
+    return LG_OK;
+}
+
+int lg_scene_set_camera(lg_scene* s, const lg_camera* cam)
+{
+    if (!s || !cam) return set_error(LG_ERR_INVALID, "NULL argument");
+    CameraDesc& c = s->s.camera;
+    std::memcpy(c.pos, cam->pos, sizeof c.pos);
+    std::memcpy(c.cameraToWorld, cam->camera_to_world, sizeof c.cameraToWorld);
+    c.fovYDeg = cam->fov_y_deg;
+    c.aspect = cam->aspect;
+    c.nearZ = cam->near_z;
+    c.farZ = cam->far_z;
+    c.imageWidth = cam->width;
+    c.imageHeight = cam->height;
+    return LG_OK;
+}
+
+int lg_scene_save_json(const lg_scene* s, const char* path)
+{
+    if (!s || !path) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (!save_scene_file(s->s, path, 0)) return set_error(LG_ERR_IO, "cannot write %s", path);
+    return LG_OK;
+}
+
+const char* lg_scene_texture(const lg_scene* s, int material)
+{
+    if (!s || material < 0 || material >= (int)s->s.materials.size()) return "";
+    return s->s.materials[(size_t)material].diffuseTex.c_str();
+}
+
+void lg_scene_destroy(lg_scene* s) { delete s; }
+
+// overwrite_camera (reference main.cpp:29-59).
+void lg_look_at(lg_camera* cam, const float pos[3], const float tgt[3])
+{
+    float fx = tgt[0] - pos[0];
+    float fy = tgt[1] - pos[1];
+    float fz = tgt[2] - pos[2];
+    float fl = std::sqrt(fx * fx + fy * fy + fz * fz);
+    if (fl < 1e-8f) return;
+    fx /= fl;
+    fy /= fl;
+    fz /= fl;
+    float lx = -fy, ly = fx, lz = 0.0f;
+    float ll = std::sqrt(lx * lx + ly * ly + lz * lz);
+    if (ll < 1e-6f) { lx = 0; ly = 1; lz = 0; ll = 1; }
+    lx /= ll;
+    ly /= ll;
+    lz /= ll;
+    float ux = fy * lz - fz * ly;
+    float uy = fz * lx - fx * lz;
+    float uz = fx * ly - fy * lx;
+    float* m = cam->camera_to_world;
+    m[0] = fx; m[1] = fy; m[2] = fz; m[3] = 0;
+    m[4] = lx; m[5] = ly; m[6] = lz; m[7] = 0;
+    m[8] = ux; m[9] = uy; m[10] = uz; m[11] = 0;
+    m[12] = pos[0]; m[13] = pos[1]; m[14] = pos[2]; m[15] = 1;
+    cam->pos[0] = pos[0];
+    cam->pos[1] = pos[1];
+    cam->pos[2] = pos[2];
+}
+
+// ---- BVH ----
+int lg_build_bvh_device(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* d_nodes_out, int32_t* n_nodes_out,
+                        int32_t* d_perm_out, lg_triangle* d_tris_out, void* stream)
+{
+    if (!n_nodes_out || (n_tris > 0 && (!d_tris || !d_nodes_out))) return set_error(LG_ERR_INVALID, "NULL argument");
+    int dev = 0;
+    LG_TRY_CUDA(cudaGetDevice(&dev));
+    DeviceScratch& ds = device_scratch(dev);
+    std::lock_guard<std::mutex> lk(ds.mu);
+    const bool tmp = d_tris_out == nullptr || d_tris_out == d_tris;
+    LG_TRY(ds.buf.reserve(lbvh_scratch_bytes(n_tris, tmp)));
+    int count = 0;
+    LG_TRY(lbvh_build(d_tris, n_tris, d_nodes_out, &count, d_perm_out, d_tris_out, ds.buf.p, ds.buf.bytes,
+                      (cudaStream_t)stream));
+    *n_nodes_out = count;
+    return LG_OK;
+}
+
+int lg_build_bvh(const lg_triangle* tris, int32_t n, lg_bvh_node* nodes_out, int32_t* n_nodes_out, int32_t* perm_out,
+                 lg_triangle* tris_out)
+{
+    if (!n_nodes_out || n < 0 || (n > 0 && (!tris || !nodes_out))) return set_error(LG_ERR_INVALID, "bad argument");
+    if (n == 0) { *n_nodes_out = 0; return LG_OK; }
+    lg_triangle* d_in = nullptr;
+    lg_triangle* d_out = nullptr;
+    lg_bvh_node* d_nodes = nullptr;
+    int32_t* d_perm = nullptr;
+    int rc = LG_OK;
+    int32_t count = 0;
+    const size_t tb = (size_t)n * sizeof(lg_triangle);
+    cudaStream_t st = nullptr;
+    auto fail = [&](cudaError_t e, const char* what) {
+        rc = set_error(LG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) { fail(e, "stream"); goto done; }
+    if ((e = cudaMalloc(&d_in, tb)) != cudaSuccess) { fail(e, "cudaMalloc"); goto done; }
+    if ((e = cudaMalloc(&d_out, tb)) != cudaSuccess) { fail(e, "cudaMalloc"); goto done; }
+    if ((e = cudaMalloc(&d_nodes, (size_t)(2 * n - 1) * sizeof(lg_bvh_node))) != cudaSuccess) { fail(e, "cudaMalloc"); goto done; }
+    if ((e = cudaMalloc(&d_perm, (size_t)n * sizeof(int32_t))) != cudaSuccess) { fail(e, "cudaMalloc"); goto done; }
+    if ((e = cudaMemcpyAsync(d_in, tris, tb, cudaMemcpyHostToDevice, st)) != cudaSuccess) { fail(e, "H2D"); goto done; }
+    rc = lg_build_bvh_device(d_in, n, d_nodes, &count, d_perm, d_out, st);
+    if (rc != LG_OK) goto done;
+    if ((e = cudaMemcpyAsync(nodes_out, d_nodes, (size_t)count * sizeof(lg_bvh_node), cudaMemcpyDeviceToHost, st)) != cudaSuccess) { fail(e, "D2H"); goto done; }
+    if (perm_out && (e = cudaMemcpyAsync(perm_out, d_perm, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, st)) != cudaSuccess) { fail(e, "D2H"); goto done; }
+    if (tris_out && (e = cudaMemcpyAsync(tris_out, d_out, tb, cudaMemcpyDeviceToHost, st)) != cudaSuccess) { fail(e, "D2H"); goto done; }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) { fail(e, "sync"); goto done; }
+    *n_nodes_out = count;
+done:
+    cudaFree(d_in);
+    cudaFree(d_out);
+    cudaFree(d_nodes);
+    cudaFree(d_perm);
+    if (st) cudaStreamDestroy(st);
+    return rc;
+}
+
+// ---- renderer ----
+int lg_renderer_create(int device, lg_renderer** out)
+{
+    if (!out) return set_error(LG_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_error(LG_ERR_CUDA, "no CUDA device: %s", e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
+    if (device < 0 || device >= ndev) return set_error(LG_ERR_INVALID, "device %d out of range", device);
+    DeviceGuard g(device);
+    lg_renderer* r = new (std::nothrow) lg_renderer();
+    if (!r) return set_error(LG_ERR_NOMEM, "out of memory");
+    r->device = device;
+    cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if ((e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&r->ev0)) != cudaSuccess || (e = cudaEventCreate(&r->ev1)) != cudaSuccess)
+    {
+        lg_renderer_destroy(r);
+        return set_error(LG_ERR_CUDA, "renderer init: %s", cudaGetErrorString(e));
+    }
+    *out = r;
+    return LG_OK;
+}
+
+void lg_renderer_destroy(lg_renderer* r)
+{
+    if (!r) return;
+    DeviceGuard g(r->device);
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->leaves, &r->tv, &r->mats, &r->points,
+                      &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
+        b->release();
+    if (r->ev0) cudaEventDestroy(r->ev0);
+    if (r->ev1) cudaEventDestroy(r->ev1);
+    if (r->stream) cudaStreamDestroy(r->stream);
+    delete r;
+}
+
+int lg_renderer_set_scene(lg_renderer* r, const lg_scene_desc* d)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    LG_TRY(validate_scene(d));
+    DeviceGuard g(r->device);
+    const int n = d->n_tris;
+    r->n_tris = n;
+    LG_TRY(upload_common(r, d));
+    LG_TRY(r->tris.reserve((size_t)std::max(n, 1) * sizeof(lg_triangle)));
+    LG_TRY(r->tris_in.reserve((size_t)std::max(n, 1) * sizeof(lg_triangle)));
+    LG_TRY(r->nodes.reserve((size_t)std::max(2 * n - 1, 1) * sizeof(lg_bvh_node)));
+    if (n > 0)
+        LG_TRY_CUDA(cudaMemcpyAsync(r->tris_in.p, d->tris, (size_t)n * sizeof(lg_triangle), cudaMemcpyHostToDevice,
+                                    r->stream));
+    LG_TRY(r->scratch.reserve(lbvh_scratch_bytes(n, false)));
+    int count = 0;
+    LG_TRY(lbvh_build(r->tris_in.as<lg_triangle>(), n, r->nodes.as<lg_bvh_node>(), &count, nullptr,
+                      r->tris.as<lg_triangle>(), r->scratch.p, r->scratch.bytes, r->stream));
+    r->n_nodes = count;
+    return finish_scene(r);
+}
+
+int lg_renderer_set_scene_bvh(lg_renderer* r, const lg_scene_desc* d, const lg_bvh_node* nodes, int32_t n_nodes)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    LG_TRY(validate_scene(d));
+    if (n_nodes < 0 || (n_nodes > 0 && !nodes)) return set_error(LG_ERR_INVALID, "bad node array");
+    if (d->n_tris > 0 && n_nodes == 0) return set_error(LG_ERR_INVALID, "triangles without a BVH");
+    for (int i = 0; i < n_nodes; ++i)
+    {
+        const lg_bvh_node& nd = nodes[i];
+        if (nd.triCount > 0)
+        {
+            if (nd.firstTri < 0 || (long long)nd.firstTri + nd.triCount > d->n_tris)
+                return set_error(LG_ERR_INVALID, "node %d: triangle range outside the scene", i);
+        }
+        else if (nd.triCount < 0 || nd.left <= i || nd.right <= i || nd.left >= n_nodes || nd.right >= n_nodes)
+            return set_error(LG_ERR_INVALID, "node %d: child links must point forward inside the array", i);
+    }
+    DeviceGuard g(r->device);
+    r->n_tris = d->n_tris;
+    r->n_nodes = n_nodes;
+    LG_TRY(upload_common(r, d));
+    LG_TRY(r->tris.reserve((size_t)std::max(d->n_tris, 1) * sizeof(lg_triangle)));
+    LG_TRY(r->nodes.reserve((size_t)std::max(n_nodes, 1) * sizeof(lg_bvh_node)));
+    if (d->n_tris)
+        LG_TRY_CUDA(cudaMemcpyAsync(r->tris.p, d->tris, (size_t)d->n_tris * sizeof(lg_triangle),
+                                    cudaMemcpyHostToDevice, r->stream));
+    if (n_nodes)
+        LG_TRY_CUDA(cudaMemcpyAsync(r->nodes.p, nodes, (size_t)n_nodes * sizeof(lg_bvh_node), cudaMemcpyHostToDevice,
+                                    r->stream));
+    return finish_scene(r);
+}
+
+int lg_renderer_get_bvh(lg_renderer* r, lg_bvh_node* nodes_out, int32_t* n_nodes, lg_triangle* tris_out)
+{
+    if (!r || !n_nodes) return set_error(LG_ERR_INVALID, "NULL argument");
+    DeviceGuard g(r->device);
+    *n_nodes = r->n_nodes;
+    if (nodes_out && r->n_nodes)
+        LG_TRY_CUDA(cudaMemcpyAsync(nodes_out, r->nodes.p, (size_t)r->n_nodes * sizeof(lg_bvh_node),
+                                    cudaMemcpyDeviceToHost, r->stream));
+    if (tris_out && r->n_tris)
+        LG_TRY_CUDA(cudaMemcpyAsync(tris_out, r->tris.p, (size_t)r->n_tris * sizeof(lg_triangle),
+                                    cudaMemcpyDeviceToHost, r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    return LG_OK;
+}
+
+int lg_renderer_set_counting(lg_renderer* r, int enable)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    r->counting = enable != 0;
+    return LG_OK;
+}
+
+int lg_render(lg_renderer* r, const lg_camera* cam, const lg_render_opts* o, uint8_t* rgb8, float* accum,
+              double* accum64, lg_render_stats* stats)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    DeviceGuard g(r->device);
+    if (accum64 && !(o && (o->flags & LG_RENDER_ACCUM64)))
+        return set_error(LG_ERR_INVALID, "accum64 output needs LG_RENDER_ACCUM64");
+    lg_render_stats local{};
+    LG_TRY(render_into_device(r, cam, o, stats ? stats : &local));
+    const size_t nval = (size_t)cam->width * cam->height * 3;
+    if (rgb8) LG_TRY_CUDA(cudaMemcpyAsync(rgb8, r->rgb.p, nval, cudaMemcpyDeviceToHost, r->stream));
+    if (accum) LG_TRY_CUDA(cudaMemcpyAsync(accum, r->accum.p, nval * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    if (accum64)
+        LG_TRY_CUDA(cudaMemcpyAsync(accum64, r->accum64.p, nval * sizeof(double), cudaMemcpyDeviceToHost, r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    return LG_OK;
+}
+
+int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* o, void* stream,
+                     const uint8_t** d_rgb8, const float** d_accum, const double** d_accum64)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    DeviceGuard g(r->device);
+    // Order the renderer's stream after the caller's stream.
+    if (stream)
+    {
+        cudaEvent_t ev;
+        LG_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, (cudaStream_t)stream);
+        cudaStreamWaitEvent(r->stream, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    LG_TRY(render_into_device(r, cam, o, nullptr));
+    if (stream)
+    {
+        cudaEvent_t ev;
+        LG_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, r->stream);
+        cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    else LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    if (d_rgb8) *d_rgb8 = r->rgb.as<uint8_t>();
+    if (d_accum) *d_accum = r->accum.as<float>();
+    if (d_accum64) *d_accum64 = (o->flags & LG_RENDER_ACCUM64) ? r->accum64.as<double>() : nullptr;
+    return LG_OK;
+}
+
+int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts* opts, int32_t n_jobs,
+                    uint8_t* rgb8_out, float* ms_per_job)
+{
+    if (!r || !cams || !opts || n_jobs < 0) return set_error(LG_ERR_INVALID, "bad argument");
+    DeviceGuard g(r->device);
+    size_t off = 0;
+    for (int j = 0; j < n_jobs; ++j)
+    {
+        lg_render_stats st{};
+        LG_TRY(render_into_device(r, &cams[j], &opts[j], &st));
+        const size_t nval = (size_t)cams[j].width * cams[j].height * 3;
+        if (rgb8_out)
+            LG_TRY_CUDA(cudaMemcpyAsync(rgb8_out + off, r->rgb.p, nval, cudaMemcpyDeviceToHost, r->stream));
+        off += nval;
+        if (ms_per_job) ms_per_job[j] = st.kernel_ms;
+    }
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    return LG_OK;
+}
+
+int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, float inv_spp, void* stream)
+{
+    if ((!d_accum || !d_rgb8) && n_pixels > 0) return set_error(LG_ERR_INVALID, "NULL argument");
+    LG_TRY_CUDA(launch_tonemap(d_accum, d_rgb8, (long long)n_pixels * 3, inv_spp, (cudaStream_t)stream));
+    return LG_OK;
+}
+
+int lg_write_png(const char* path, int32_t w, int32_t h, const uint8_t* rgb8)
+{
+    if (!path || !rgb8) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (!write_png(path, w, h, rgb8)) return set_error(LG_ERR_IO, "failed to write %s", path);
+    return LG_OK;
+}
+
+int lg_write_hdr(const char* path, int32_t w, int32_t h, const float* rgb32)
+{
+    if (!path || !rgb32) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (!write_hdr(path, w, h, rgb32)) return set_error(LG_ERR_IO, "failed to write %s", path);
+    return LG_OK;
+}
+
+}  // extern "C"
+
+// ---- C++ drop-ins ----
+void BuildBVH(Scene& scene, Bvh& out)
+{
+    out.nodes.clear();
+    out.rootIdx = 0;
+    const int n = (int)scene.triangles.size();
+    if (n == 0) return;
+    out.nodes.resize((size_t)(2 * n - 1));
+    int count = 0;
+    lg_triangle* tris = reinterpret_cast<lg_triangle*>(scene.triangles.data());
+    int rc = lg_build_bvh(tris, n, reinterpret_cast<lg_bvh_node*>(out.nodes.data()), &count, nullptr, tris);
+    if (rc != LG_OK)
+    {
+        std::fprintf(stderr, "BuildBVH: %s\n", lg_last_error());
+        out.nodes.clear();
+        return;
+    }
+    out.nodes.resize((size_t)count);
+}
+
+namespace
+{
+lg_camera camera_of(const Scene& s)
+{
+    lg_camera c;
+    std::memcpy(c.pos, s.camera.pos, sizeof c.pos);
+    std::memcpy(c.camera_to_world, s.camera.cameraToWorld, sizeof c.camera_to_world);
+    c.fov_y_deg = s.camera.fovYDeg;
+    c.aspect = s.camera.aspect;
+    c.near_z = s.camera.nearZ;
+    c.far_z = s.camera.farZ;
+    c.width = s.camera.imageWidth;
+    c.height = s.camera.imageHeight;
+    return c;
+}
+lg_scene_desc desc_of(const Scene& s, std::vector<float>& alb)
+{
+    lg_scene_desc d{};
+    d.camera = camera_of(s);
+    std::memcpy(&d.sun, &s.sun, sizeof d.sun);
+    d.tris = reinterpret_cast<const lg_triangle*>(s.triangles.data());
+    d.n_tris = (int32_t)s.triangles.size();
+    alb.resize(s.materials.size() * 3);
+    for (size_t i = 0; i < s.materials.size(); ++i)
+        for (int k = 0; k < 3; ++k) alb[3 * i + k] = s.materials[i].albedo[k];
+    d.mat_albedo = alb.data();
+    d.n_mats = (int32_t)s.materials.size();
+    d.points = reinterpret_cast<const lg_point_light*>(s.points.data());
+    d.n_points = (int32_t)s.points.size();
+    return d;
+}
+}  // namespace
+
+// Same signature as the reference (declared in its main.cpp:19-24).  The
+// G-buffer outputs are not produced (filled with zeros) and textures are not
+// sampled; both are reported on stderr when requested.
+void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& assetRoot, int spp, int maxBounces,
+                     std::vector<uint8_t>& outRGB, int& outW, int& outH, std::vector<uint8_t>* outAlbedo,
+                     std::vector<uint8_t>* outNormal, std::vector<uint8_t>* outWorldPos)
+{
+    (void)assetRoot;
+    outW = scene.camera.imageWidth;
+    outH = scene.camera.imageHeight;
+    outRGB.assign((size_t)outW * outH * 3, 0);
+    for (auto* v : {outAlbedo, outNormal, outWorldPos})
+        if (v) v->assign((size_t)outW * outH * 3, 0);
+    std::vector<float> alb;
+    lg_scene_desc d = desc_of(scene, alb);
+    lg_renderer* r = nullptr;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int rc = lg_renderer_create(dev, &r);
+    if (rc == LG_OK)
+        rc = lg_renderer_set_scene_bvh(r, &d, reinterpret_cast<const lg_bvh_node*>(bvh.nodes.data()),
+                                       (int32_t)bvh.nodes.size());
+    lg_render_stats st{};
+    if (rc == LG_OK)
+    {
+        lg_render_opts o{spp, maxBounces, 0, 0};
+        lg_camera cam = d.camera;
+        rc = lg_render(r, &cam, &o, outRGB.data(), nullptr, nullptr, &st);
+    }
+    if (rc != LG_OK) std::fprintf(stderr, "render failed: %s\n", lg_last_error());
+    else
+        std::printf("kernel: %.1f ms  (%d x %d, %d spp, %d bounces, %zu tris)\n", st.kernel_ms, outW, outH, spp,
+                    maxBounces, scene.triangles.size());
+    lg_renderer_destroy(r);
+}

@@ -1,0 +1,631 @@
+// trace.cu -- the path tracer: device scene conversion, trace kernel, tonemap.
+//
+// Follows the reference's device code (LuminaGI-CudaRef src/pathtracer.cu)
+// path for path: same camera model (primary_ray, :284-293), xorshift32
+// stream seeded per (pixel, chunk of 8 samples) (:193-204, :349), Moller-
+// Trumbore with |det| < 1e-6 culling (:82-107), slab test (:61-80), Lambert +
+// next-event estimation to the sun and point lights with a shadow ray even
+// at zero sun intensity (:230-272), Russian roulette from bounce 1 and
+// cosine-weighted bounces (:295-331).  Every FP32 expression keeps the
+// reference's operand order, so the compiler sees the same expressions.
+//
+// What is different (none of it changes which triangle a ray hits, except for
+// exact ties in t):
+//   * BVH records hold both children's boxes (WideNode), so one 64-byte fetch
+//     tests two boxes and traversal descends into the nearer child first and
+//     stacks the farther one; the reference pops children in fixed order and
+//     tests each box after a separate 40-byte fetch.
+//   * Triangle records for intersection are v0, e1, e2 as three float4
+//     (e1 = v1 - v0 is the same IEEE subtraction the reference does per test);
+//     normals are read from the 100-byte record only at the closest hit.
+//   * Persistent warps pull (8x4-pixel tile, chunk) work items from an atomic
+//     counter; chunk sums are added to the FP32 accumulator atomically, so the
+//     order of chunk additions (not their values) can differ from the
+//     reference's launch-per-chunk order.
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "trace.cuh"
+
+namespace lg
+{
+namespace
+{
+constexpr int kStack = 64;
+constexpr int kTraceThreads = 256;
+constexpr int kTraceMinBlocks = 4;
+
+// ---------------------------------------------------------------------------
+// Scene conversion
+// ---------------------------------------------------------------------------
+constexpr int kScanTB = 1024;
+
+__global__ void flags_kernel(const lg_bvh_node* __restrict__ nodes, int n, int* __restrict__ is_internal)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) is_internal[i] = nodes[i].triCount == 0 ? 1 : 0;
+}
+
+// In-block exclusive scan of `v` (one value per thread); returns the block total in *total.
+__device__ int block_exclusive_scan(int v, int* total)
+{
+    __shared__ int ws[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[warp] = x;
+    __syncthreads();
+    if (warp == 0)
+    {
+        int w = lane < (int)(blockDim.x >> 5) ? ws[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        ws[lane] = w;
+    }
+    __syncthreads();
+    const int excl = (warp ? ws[warp - 1] : 0) + x - v;
+    *total = ws[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return excl;
+}
+
+// Dense indices: internal nodes and leaves each numbered in BFS order.
+// Pass 1: per-block internal counts.
+__global__ void __launch_bounds__(kScanTB) count_kernel(const int* __restrict__ is_internal, int n,
+                                                        int* __restrict__ block_sums)
+{
+    const int i = blockIdx.x * kScanTB + threadIdx.x;
+    int v = i < n ? is_internal[i] : 0;
+    int total;
+    block_exclusive_scan(v, &total);
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+// Pass 2: scan of block sums (single block, loops).
+__global__ void __launch_bounds__(kScanTB) scan_sums_kernel(int* __restrict__ block_sums, int nb)
+{
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b = 0; b < nb; b += kScanTB)
+    {
+        const int i = b + threadIdx.x;
+        int v = i < nb ? block_sums[i] : 0;
+        int total;
+        int e = block_exclusive_scan(v, &total);
+        if (i < nb) block_sums[i] = carry + e;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+// Pass 3: dense index per node (internal rank or leaf rank).
+__global__ void __launch_bounds__(kScanTB) dense_kernel(const int* __restrict__ is_internal, int n,
+                                                        const int* __restrict__ block_sums, int* __restrict__ dense)
+{
+    const int i = blockIdx.x * kScanTB + threadIdx.x;
+    int v = i < n ? is_internal[i] : 0;
+    int total;
+    int e = block_exclusive_scan(v, &total) + block_sums[blockIdx.x];
+    if (i < n) dense[i] = v ? e : (i - e);  // leaves: i - (#internal before i)
+}
+
+__device__ __forceinline__ int child_link(const lg_bvh_node* nodes, const int* dense, int c)
+{
+    return nodes[c].triCount == 0 ? dense[c] : ~dense[c];
+}
+
+__global__ void wide_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ dense,
+                            WideNode* __restrict__ wide, int2* __restrict__ leaves)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const lg_bvh_node nd = nodes[i];
+    if (nd.triCount > 0)
+    {
+        leaves[dense[i]] = make_int2(nd.firstTri, nd.triCount);
+        return;
+    }
+    const lg_bvh_node a = nodes[nd.left], b = nodes[nd.right];
+    WideNode w;
+    w.xy0 = make_float4(a.bbMin[0], a.bbMax[0], a.bbMin[1], a.bbMax[1]);
+    w.xy1 = make_float4(b.bbMin[0], b.bbMax[0], b.bbMin[1], b.bbMax[1]);
+    w.z01 = make_float4(a.bbMin[2], a.bbMax[2], b.bbMin[2], b.bbMax[2]);
+    w.link = make_int4(child_link(nodes, dense, nd.left), child_link(nodes, dense, nd.right), 0, 0);
+    wide[dense[i]] = w;
+}
+
+__global__ void tri_prep_kernel(const lg_triangle* __restrict__ tris, int n, float4* __restrict__ tv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const lg_triangle t = tris[i];
+    tv[3 * i + 0] = make_float4(t.v[0][0], t.v[0][1], t.v[0][2], __int_as_float(t.material));
+    tv[3 * i + 1] = make_float4(__fsub_rn(t.v[1][0], t.v[0][0]), __fsub_rn(t.v[1][1], t.v[0][1]),
+                                __fsub_rn(t.v[1][2], t.v[0][2]), 0.0f);
+    tv[3 * i + 2] = make_float4(__fsub_rn(t.v[2][0], t.v[0][0]), __fsub_rn(t.v[2][1], t.v[0][1]),
+                                __fsub_rn(t.v[2][2], t.v[0][2]), 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Ray queries
+// ---------------------------------------------------------------------------
+// Slab test of one box (pathtracer.cu:61-80); tmin_out = max(lo, 0).
+__device__ __forceinline__ bool slab(const Ray& r, float mnx, float mxx, float mny, float mxy, float mnz, float mxz,
+                                     float tmax_in, float& tmin_out)
+{
+    float t0 = (mnx - r.o.x) * r.inv_d.x;
+    float t1 = (mxx - r.o.x) * r.inv_d.x;
+    float lo = fminf(t0, t1), hi = fmaxf(t0, t1);
+    t0 = (mny - r.o.y) * r.inv_d.y;
+    t1 = (mxy - r.o.y) * r.inv_d.y;
+    lo = fmaxf(lo, fminf(t0, t1));
+    hi = fminf(hi, fmaxf(t0, t1));
+    t0 = (mnz - r.o.z) * r.inv_d.z;
+    t1 = (mxz - r.o.z) * r.inv_d.z;
+    lo = fmaxf(lo, fminf(t0, t1));
+    hi = fminf(hi, fmaxf(t0, t1));
+    if (hi < fmaxf(lo, 0.0f) || lo > tmax_in) return false;
+    tmin_out = fmaxf(lo, 0.0f);
+    return true;
+}
+
+// Moller-Trumbore (pathtracer.cu:82-107) on a precomputed (v0, e1, e2).
+__device__ __forceinline__ bool tri_hit(const Ray& r, const float4* __restrict__ tv, int ti, float tmax, float& outT,
+                                        float& outU, float& outV)
+{
+    constexpr float kEps = 1e-6f;
+    const float4 a = __ldg(&tv[3 * ti + 0]);
+    const float4 b = __ldg(&tv[3 * ti + 1]);
+    const float4 c = __ldg(&tv[3 * ti + 2]);
+    const vec3 v0 = v3(a.x, a.y, a.z);
+    const vec3 e1 = v3(b.x, b.y, b.z);
+    const vec3 e2 = v3(c.x, c.y, c.z);
+    vec3 p = cross(r.d, e2);
+    float det = dot(e1, p);
+    if (det > -kEps && det < kEps) return false;
+    float invDet = 1.0f / det;
+    vec3 s = vsub(r.o, v0);
+    float u = dot(s, p) * invDet;
+    if (u < 0.0f || u > 1.0f) return false;
+    vec3 q = cross(s, e1);
+    float v = dot(r.d, q) * invDet;
+    if (v < 0.0f || u + v > 1.0f) return false;
+    float tt = dot(e2, q) * invDet;
+    if (tt <= kEps || tt >= tmax) return false;
+    outT = tt;
+    outU = u;
+    outV = v;
+    return true;
+}
+
+struct Counters
+{
+    unsigned long long closest, shadow, overflow, nodes, tris, leaves;
+};
+
+// Closest hit: nearer child first, farther child stacked.  Returns the
+// triangle index or -1; bestT/U/V as in traverse_closest (:109-160).
+template <bool kCount>
+__device__ int closest_hit(const DevScene& s, const Ray& r, float tmax, float& bestT, float& bestU, float& bestV,
+                           Counters& cnt)
+{
+    int stack[kStack];
+    int sp = 0;
+    int cur = s.root;
+    int bestTri = -1;
+    bestT = tmax;
+    bestU = 0.0f;
+    bestV = 0.0f;
+    if (kCount) cnt.closest++;
+    for (;;)
+    {
+        if (cur >= 0)
+        {
+            if (kCount) cnt.nodes++;
+            const float4 xy0 = __ldg(&s.nodes[cur].xy0);
+            const float4 xy1 = __ldg(&s.nodes[cur].xy1);
+            const float4 z01 = __ldg(&s.nodes[cur].z01);
+            const int4 ln = __ldg(&s.nodes[cur].link);
+            float t0, t1;
+            const bool h0 = slab(r, xy0.x, xy0.y, xy0.z, xy0.w, z01.x, z01.y, bestT, t0);
+            const bool h1 = slab(r, xy1.x, xy1.y, xy1.z, xy1.w, z01.z, z01.w, bestT, t1);
+            if (h0 && h1)
+            {
+                const bool swap = t1 < t0;
+                const int nearC = swap ? ln.y : ln.x;
+                const int farC = swap ? ln.x : ln.y;
+                if (sp < kStack) stack[sp++] = farC;
+                else if (kCount) cnt.overflow++;
+                cur = nearC;
+                continue;
+            }
+            if (h0) { cur = ln.x; continue; }
+            if (h1) { cur = ln.y; continue; }
+        }
+        else
+        {
+            const int2 lf = __ldg(&s.leaves[~cur]);
+            if (kCount) { cnt.leaves++; cnt.tris += (unsigned long long)lf.y; }
+            for (int i = 0; i < lf.y; ++i)
+            {
+                const int ti = lf.x + i;
+                float tt, uu, vv;
+                if (tri_hit(r, s.tv, ti, bestT, tt, uu, vv))
+                {
+                    bestT = tt;
+                    bestTri = ti;
+                    bestU = uu;
+                    bestV = vv;
+                }
+            }
+        }
+        if (sp == 0) break;
+        cur = stack[--sp];
+    }
+    return bestTri;
+}
+
+// Any hit within (1e-6, tmax) (traverse_occluded, :162-191).
+template <bool kCount>
+__device__ bool occluded(const DevScene& s, const Ray& r, float tmax, Counters& cnt)
+{
+    int stack[kStack];
+    int sp = 0;
+    int cur = s.root;
+    if (kCount) cnt.shadow++;
+    for (;;)
+    {
+        if (cur >= 0)
+        {
+            if (kCount) cnt.nodes++;
+            const float4 xy0 = __ldg(&s.nodes[cur].xy0);
+            const float4 xy1 = __ldg(&s.nodes[cur].xy1);
+            const float4 z01 = __ldg(&s.nodes[cur].z01);
+            const int4 ln = __ldg(&s.nodes[cur].link);
+            float t0, t1;
+            const bool h0 = slab(r, xy0.x, xy0.y, xy0.z, xy0.w, z01.x, z01.y, tmax, t0);
+            const bool h1 = slab(r, xy1.x, xy1.y, xy1.z, xy1.w, z01.z, z01.w, tmax, t1);
+            if (h0 && h1)
+            {
+                const bool swap = t1 < t0;
+                if (sp < kStack) stack[sp++] = swap ? ln.x : ln.y;
+                else if (kCount) cnt.overflow++;
+                cur = swap ? ln.y : ln.x;
+                continue;
+            }
+            if (h0) { cur = ln.x; continue; }
+            if (h1) { cur = ln.y; continue; }
+        }
+        else
+        {
+            const int2 lf = __ldg(&s.leaves[~cur]);
+            if (kCount) cnt.leaves++;
+            for (int i = 0; i < lf.y; ++i)
+            {
+                float tt, uu, vv;
+                if (kCount) cnt.tris++;
+                if (tri_hit(r, s.tv, lf.x + i, tmax, tt, uu, vv)) return true;
+            }
+        }
+        if (sp == 0) return false;
+        cur = stack[--sp];
+    }
+}
+
+// xorshift32 / randf (pathtracer.cu:193-204).
+__device__ __forceinline__ uint32_t xorshift32(uint32_t& st)
+{
+    st ^= st << 13;
+    st ^= st >> 17;
+    st ^= st << 5;
+    return st;
+}
+__device__ __forceinline__ float randf(uint32_t& st) { return (xorshift32(st) >> 8) * (1.0f / 16777216.0f); }
+
+// Frisvad frame (:206-214) and cosine-weighted direction (:216-228).
+__device__ __forceinline__ void onb(vec3 N, vec3& T, vec3& B)
+{
+    if (N.z < -0.99999f)
+    {
+        T = v3(0, -1, 0);
+        B = v3(-1, 0, 0);
+        return;
+    }
+    float a = 1.0f / (1.0f + N.z);
+    float b = -N.x * N.y * a;
+    T = v3(1.0f - N.x * N.x * a, b, -N.x);
+    B = v3(b, 1.0f - N.y * N.y * a, -N.y);
+}
+__device__ __forceinline__ vec3 sample_cos_hemi(vec3 N, uint32_t& rng)
+{
+    float u1 = randf(rng);
+    float u2 = randf(rng);
+    float r = sqrtf(u1);
+    float phi = 2.0f * 3.14159265358979f * u2;
+    float x = r * cosf(phi);
+    float y = r * sinf(phi);
+    float z = sqrtf(fmaxf(0.0f, 1.0f - u1));
+    vec3 T, B;
+    onb(N, T, B);
+    return normalize(vadd(vadd(vmul(T, x), vmul(B, y)), vmul(N, z)));
+}
+
+// Direct light at P (:230-272).
+template <bool kCount>
+__device__ vec3 shade_direct(const DevScene& s, vec3 P, vec3 N, vec3 albedo, Counters& cnt)
+{
+    constexpr float kShadowBias = 1e-3f;
+    vec3 color = v3(0, 0, 0);
+    {
+        vec3 toLight = normalize(vmul(vfrom(s.sun.dir), -1.0f));
+        float ndotl = fmaxf(0.0f, dot(N, toLight));
+        if (ndotl > 0.0f)
+        {
+            Ray shadow = make_ray(vadd(P, vmul(N, kShadowBias)), toLight);
+            if (!occluded<kCount>(s, shadow, 1e30f, cnt))
+            {
+                float I = s.sun.intensity * ndotl;
+                color = vadd(color, vhad(albedo, vmul(vfrom(s.sun.color), I)));
+            }
+        }
+    }
+    for (int i = 0; i < s.n_points; ++i)
+    {
+        const lg_point_light& L = s.points[i];
+        vec3 toLightVec = vsub(vfrom(L.pos), P);
+        float dist = len(toLightVec);
+        vec3 toLight = vmul(toLightVec, 1.0f / dist);
+        float ndotl = fmaxf(0.0f, dot(N, toLight));
+        if (ndotl <= 0.0f || dist >= L.radius * 3.0f) continue;
+        Ray shadow = make_ray(vadd(P, vmul(N, kShadowBias)), toLight);
+        if (occluded<kCount>(s, shadow, dist - kShadowBias, cnt)) continue;
+        float rr = L.radius;
+        float atten = fmaxf(0.0f, 1.0f - dist / rr);
+        atten = atten * atten;
+        float I = L.intensity * ndotl * atten;
+        color = vadd(color, vhad(albedo, vmul(vfrom(L.color), I)));
+    }
+    return color;
+}
+
+__device__ __forceinline__ Ray primary_ray(const DevCam& cam, int px, int py, float jx, float jy)
+{
+    float ndcx = (2.0f * (px + jx) / cam.width) - 1.0f;
+    float ndcy = 1.0f - (2.0f * (py + jy) / cam.height);
+    float rx = ndcx * cam.aspect * cam.tanHalfFov;
+    float ry = ndcy * cam.tanHalfFov;
+    vec3 dirCam = v3(1.0f, -rx, ry);
+    vec3 dirWorld = vadd(vadd(vmul(cam.fwd, dirCam.x), vmul(cam.left, dirCam.y)), vmul(cam.up, dirCam.z));
+    return make_ray(cam.pos, dirWorld);
+}
+
+// trace_path (:295-331).
+template <bool kCount>
+__device__ vec3 trace_path(const DevScene& s, Ray ray, int maxBounces, uint32_t& rng, Counters& cnt)
+{
+    vec3 L = v3(0, 0, 0);
+    vec3 throughput = v3(1, 1, 1);
+    for (int bounce = 0; bounce <= maxBounces; ++bounce)
+    {
+        float hitT, hitU, hitV;
+        const int tri = closest_hit<kCount>(s, ray, 1e30f, hitT, hitU, hitV, cnt);
+        if (tri < 0) break;
+        const lg_triangle& t = s.tris[tri];
+        float w = 1.0f - hitU - hitV;
+        vec3 N = normalize(v3(w * t.n[0][0] + hitU * t.n[1][0] + hitV * t.n[2][0],
+                              w * t.n[0][1] + hitU * t.n[1][1] + hitV * t.n[2][1],
+                              w * t.n[0][2] + hitU * t.n[1][2] + hitV * t.n[2][2]));
+        if (dot(N, ray.d) > 0.0f) N = vmul(N, -1.0f);
+        vec3 P = vadd(ray.o, vmul(ray.d, hitT));
+        const int mat = __float_as_int(__ldg(&s.tv[3 * tri].w));
+        const float4 alb = __ldg(&s.mats[mat]);
+        vec3 albedo = v3(alb.x, alb.y, alb.z);
+        L = vadd(L, vhad(throughput, shade_direct<kCount>(s, P, N, albedo, cnt)));
+        if (bounce == maxBounces) break;
+        if (bounce >= 1)
+        {
+            float q = fminf(0.95f, fmaxf(throughput.x, fmaxf(throughput.y, throughput.z)));
+            if (randf(rng) > q) break;
+            throughput = vmul(throughput, 1.0f / q);
+        }
+        vec3 newDir = sample_cos_hemi(N, rng);
+        ray = make_ray(vadd(P, vmul(N, 1e-3f)), newDir);
+        throughput = vhad(throughput, albedo);
+    }
+    return L;
+}
+
+// Persistent warps; work item = one 8x4 tile of one chunk of <= 8 samples.
+template <bool kCount, bool kAcc64>
+__global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned total = (unsigned)job.n_tiles * (unsigned)job.n_chunks;
+    Counters cnt{0, 0, 0, 0, 0, 0};
+    for (;;)
+    {
+        unsigned item = 0;
+        if (lane == 0) item = atomicAdd(job.work, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) break;
+        const int chunk = (int)(item / (unsigned)job.n_tiles);
+        const int tile = (int)(item % (unsigned)job.n_tiles);
+        const int px = (tile % job.tiles_x) * 8 + (lane & 7);
+        const int py = (tile / job.tiles_x) * 4 + (lane >> 3);
+        if (px >= cam.width || py >= cam.height) continue;
+        const int first = chunk * 8;
+        const int n_this = min(8, job.spp - first);
+        const int sampleBase = job.sample_base + first;
+        uint32_t rng = (uint32_t)(px * 1973 + py * 9277 + sampleBase * 26699) | 1u;
+        vec3 sum = v3(0, 0, 0);
+        for (int k = 0; k < n_this; ++k)
+        {
+            float jx = randf(rng);
+            float jy = randf(rng);
+            Ray r = primary_ray(cam, px, py, jx, jy);
+            sum = vadd(sum, trace_path<kCount>(s, r, job.max_bounces, rng, cnt));
+        }
+        const size_t i = ((size_t)py * cam.width + px) * 3;
+        if (job.n_chunks == 1)
+        {
+            job.accum[i + 0] += sum.x;
+            job.accum[i + 1] += sum.y;
+            job.accum[i + 2] += sum.z;
+        }
+        else
+        {
+            atomicAdd(&job.accum[i + 0], sum.x);
+            atomicAdd(&job.accum[i + 1], sum.y);
+            atomicAdd(&job.accum[i + 2], sum.z);
+        }
+        if (kAcc64)
+        {
+            atomicAdd(&job.accum64[i + 0], (double)sum.x);
+            atomicAdd(&job.accum64[i + 1], (double)sum.y);
+            atomicAdd(&job.accum64[i + 2], (double)sum.z);
+        }
+    }
+    if (kCount)
+    {
+        for (int o = 16; o; o >>= 1)
+        {
+            cnt.closest += __shfl_xor_sync(0xffffffffu, cnt.closest, o);
+            cnt.shadow += __shfl_xor_sync(0xffffffffu, cnt.shadow, o);
+            cnt.overflow += __shfl_xor_sync(0xffffffffu, cnt.overflow, o);
+            cnt.nodes += __shfl_xor_sync(0xffffffffu, cnt.nodes, o);
+            cnt.tris += __shfl_xor_sync(0xffffffffu, cnt.tris, o);
+            cnt.leaves += __shfl_xor_sync(0xffffffffu, cnt.leaves, o);
+        }
+        if (lane == 0 && job.counters)
+        {
+            atomicAdd(&job.counters->closest_rays, cnt.closest);
+            atomicAdd(&job.counters->shadow_rays, cnt.shadow);
+            atomicAdd(&job.counters->stack_overflows, cnt.overflow);
+            atomicAdd(&job.counters->node_fetches, cnt.nodes);
+            atomicAdd(&job.counters->tri_tests, cnt.tris);
+            atomicAdd(&job.counters->leaf_fetches, cnt.leaves);
+        }
+    }
+}
+
+// tonemap_kernel (:413-429), one value per thread.
+__global__ void tonemap_kernel(const float* __restrict__ accum, uint8_t* __restrict__ rgb, long long n, float invSpp)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v = sqrtf(fmaxf(0.0f, fminf(accum[i] * invSpp, 1.0f)));
+    rgb[i] = (uint8_t)(v * 255.0f);
+}
+
+__global__ void acc64_to_32_kernel(const double* __restrict__ a, float* __restrict__ b, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+}  // namespace
+
+DevCam make_dev_cam(const lg_camera& c)
+{
+    DevCam cam;
+    const float* m = c.camera_to_world;
+    cam.pos = v3(c.pos[0], c.pos[1], c.pos[2]);
+    cam.fwd = v3(m[0], m[1], m[2]);
+    cam.left = v3(m[4], m[5], m[6]);
+    cam.up = v3(m[8], m[9], m[10]);
+    cam.tanHalfFov = tanf(c.fov_y_deg * 0.5f * 3.14159265358979f / 180.0f);
+    cam.aspect = c.aspect;
+    cam.width = c.width;
+    cam.height = c.height;
+    return cam;
+}
+
+cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* d_wide, int2* d_leaves,
+                             int* d_scratch, int* root_host, int* n_internal_host, int* n_leaves_host,
+                             cudaStream_t stream)
+{
+    const int nb = (n_nodes + kScanTB - 1) / kScanTB;
+    int* is_internal = d_scratch;
+    int* dense = d_scratch + n_nodes;
+    int* block_sums = d_scratch + 2 * (size_t)n_nodes;
+    flags_kernel<<<nb, kScanTB, 0, stream>>>(d_nodes, n_nodes, is_internal);
+    count_kernel<<<nb, kScanTB, 0, stream>>>(is_internal, n_nodes, block_sums);
+    scan_sums_kernel<<<1, kScanTB, 0, stream>>>(block_sums, nb);
+    dense_kernel<<<nb, kScanTB, 0, stream>>>(is_internal, n_nodes, block_sums, dense);
+    wide_kernel<<<(n_nodes + 255) / 256, 256, 0, stream>>>(d_nodes, n_nodes, dense, d_wide, d_leaves);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int root_internal = 0;
+    e = cudaMemcpyAsync(&root_internal, is_internal, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    *root_host = root_internal ? 0 : ~0;
+    // n_nodes = 2L - 1 for L leaves.
+    *n_leaves_host = (n_nodes + 1) / 2;
+    *n_internal_host = n_nodes - *n_leaves_host;
+    return cudaSuccess;
+}
+
+cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cudaStream_t stream)
+{
+    if (n <= 0) return cudaSuccess;
+    tri_prep_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_tris, n, d_tv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
+                         cudaStream_t stream)
+{
+    int per_sm = 0;
+    cudaError_t e;
+    const void* fn;
+    if (count) fn = job.accum64 ? (const void*)trace_kernel<true, true> : (const void*)trace_kernel<true, false>;
+    else fn = job.accum64 ? (const void*)trace_kernel<false, true> : (const void*)trace_kernel<false, false>;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    long long want = (long long)job.n_tiles * job.n_chunks;  // warps of work
+    long long blocks = (long long)per_sm * sm_count;
+    long long max_useful = (want + (kTraceThreads / 32) - 1) / (kTraceThreads / 32);
+    if (blocks > max_useful) blocks = max_useful;
+    if (blocks < 1) blocks = 1;
+    e = cudaMemsetAsync(job.work, 0, sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    if (count)
+    {
+        if (job.accum64) trace_kernel<true, true><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
+        else trace_kernel<true, false><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
+    }
+    else
+    {
+        if (job.accum64) trace_kernel<false, true><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
+        else trace_kernel<false, false><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,
+                           cudaStream_t stream)
+{
+    if (n_values <= 0) return cudaSuccess;
+    tonemap_kernel<<<(unsigned)((n_values + 255) / 256), 256, 0, stream>>>(d_accum, d_rgb, n_values, inv_spp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_accum64_to_32(const double* d_acc64, float* d_acc32, long long n_values, cudaStream_t stream)
+{
+    if (n_values <= 0) return cudaSuccess;
+    acc64_to_32_kernel<<<(unsigned)((n_values + 255) / 256), 256, 0, stream>>>(d_acc64, d_acc32, n_values);
+    return cudaGetLastError();
+}
+}  // namespace lg

@@ -1,0 +1,82 @@
+// trace.cuh -- device scene layout and launchers of the path tracer.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "lumina.h"
+#include "vecmath.h"
+
+namespace lg
+{
+// One record per internal BVH node holding both children's boxes (64 B,
+// four 16-byte loads).  Child links: >= 0 internal record index, < 0 leaf
+// ~index into the leaf table.
+struct alignas(16) WideNode
+{
+    float4 xy0;  // child 0: min.x, max.x, min.y, max.y
+    float4 xy1;  // child 1: min.x, max.x, min.y, max.y
+    float4 z01;  // child 0 min.z, max.z, child 1 min.z, max.z
+    int4 link;   // link0, link1, unused, unused
+};
+static_assert(sizeof(WideNode) == 64, "WideNode is one 64-byte record");
+
+struct DevScene
+{
+    const WideNode* nodes;
+    const int2* leaves;        // (first triangle, count)
+    const float4* tv;          // 3 per triangle: v0 (w = material bits), e1 = v1-v0, e2 = v2-v0
+    const lg_triangle* tris;   // shading data (normals), BVH order
+    const float4* mats;        // albedo
+    const lg_point_light* points;
+    int n_points;
+    int root;                  // root link (0 = internal record 0, < 0 = leaf)
+    lg_dir_light sun;
+};
+
+struct DevCam
+{
+    vec3 pos, fwd, left, up;
+    float tanHalfFov, aspect;
+    int width, height;
+};
+
+struct RenderCounters
+{
+    unsigned long long closest_rays;
+    unsigned long long shadow_rays;
+    unsigned long long stack_overflows;
+    unsigned long long node_fetches;  // WideNode records read (64 B each)
+    unsigned long long tri_tests;     // ray/triangle tests (48 B of v0/e1/e2 each)
+    unsigned long long leaf_fetches;  // leaf-table entries read (8 B each)
+};
+
+struct TraceJob
+{
+    int spp, max_bounces, sample_base;
+    int n_chunks;          // ceil(spp / 8)
+    int tiles_x, n_tiles;  // 8 x 4 pixel tiles
+    float* accum;          // W*H*3, added to
+    double* accum64;       // optional
+    unsigned int* work;    // work counter (zeroed before launch)
+    RenderCounters* counters;  // optional
+};
+
+// Camera set-up of RenderSceneCUDA (pathtracer.cu:654-663); tanf runs on the host as there.
+DevCam make_dev_cam(const lg_camera& c);
+
+// Converts the reference node array (BFS) to WideNode records + leaf table.
+// Scratch: 2 * n_nodes ints.  Returns the root link through *root (device
+// write of one int; caller copies back) -- done inside the launcher.
+cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* d_wide, int2* d_leaves,
+                             int* d_scratch, int* root_host, int* n_internal_host, int* n_leaves_host,
+                             cudaStream_t stream);
+cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cudaStream_t stream);
+
+cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
+                         cudaStream_t stream);
+cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,
+                           cudaStream_t stream);
+cudaError_t launch_accum64_to_32(const double* d_acc64, float* d_acc32, long long n_values, cudaStream_t stream);
+}  // namespace lg

@@ -1,0 +1,132 @@
+"""ctypes binding of liblumina.so (include/lumina.h).
+
+The shared library is built in-tree (``make -C luminagi-cudaref_b200``) and is
+the only implementation: there is no Python or CPU fallback, and loading fails
+loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+import numpy as np
+
+PKG_DIR = pathlib.Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_DIR / "lib" / "liblumina.so"
+CLI_PATH = PKG_DIR / "bin" / "cuda_ref"
+
+LG_OK = 0
+LG_ERR_INVALID = -1
+LG_ERR_CUDA = -2
+LG_ERR_IO = -3
+LG_ERR_PARSE = -4
+LG_ERR_NOMEM = -5
+LG_ERR_DEVICE = -6
+LG_ERR_CAPACITY = -7
+LG_RENDER_ACCUM64 = 1
+
+# Record layouts (byte-identical to the reference's Triangle / BvhNode / lights).
+TRI_DTYPE = np.dtype([("v", "<f4", (3, 3)), ("n", "<f4", (3, 3)), ("uv", "<f4", (3, 2)), ("material", "<i4")])
+NODE_DTYPE = np.dtype([("bbMin", "<f4", (3,)), ("bbMax", "<f4", (3,)), ("left", "<i4"), ("right", "<i4"),
+                       ("firstTri", "<i4"), ("triCount", "<i4")])
+POINT_DTYPE = np.dtype([("pos", "<f4", (3,)), ("color", "<f4", (3,)), ("intensity", "<f4"), ("radius", "<f4")])
+DIR_DTYPE = np.dtype([("dir", "<f4", (3,)), ("color", "<f4", (3,)), ("intensity", "<f4")])
+assert TRI_DTYPE.itemsize == 100 and NODE_DTYPE.itemsize == 40
+assert POINT_DTYPE.itemsize == 32 and DIR_DTYPE.itemsize == 28
+
+
+class LgCamera(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("camera_to_world", C.c_float * 16), ("fov_y_deg", C.c_float),
+                ("aspect", C.c_float), ("near_z", C.c_float), ("far_z", C.c_float), ("width", C.c_int32),
+                ("height", C.c_int32)]
+
+
+class LgDirLight(C.Structure):
+    _fields_ = [("dir", C.c_float * 3), ("color", C.c_float * 3), ("intensity", C.c_float)]
+
+
+class LgSceneDesc(C.Structure):
+    _fields_ = [("camera", LgCamera), ("sun", LgDirLight), ("tris", C.c_void_p), ("n_tris", C.c_int32),
+                ("mat_albedo", C.c_void_p), ("mat_emissive", C.c_void_p), ("n_mats", C.c_int32),
+                ("points", C.c_void_p), ("n_points", C.c_int32), ("directionals", C.c_void_p),
+                ("n_directionals", C.c_int32)]
+
+
+class LgRenderOpts(C.Structure):
+    _fields_ = [("spp", C.c_int32), ("max_bounces", C.c_int32), ("sample_base", C.c_int32), ("flags", C.c_uint32)]
+
+
+class LgRenderStats(C.Structure):
+    _fields_ = [("kernel_ms", C.c_float), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("node_fetches", C.c_uint64), ("tri_tests", C.c_uint64), ("leaf_fetches", C.c_uint64)]
+
+
+class LuminaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"lumina error {code}: {msg}")
+        self.code = code
+
+
+# Every symbol include/lumina.h declares, with (restype, argtypes).
+_P = C.c_void_p
+_I = C.c_int
+SIGNATURES = {
+    "lg_last_error": (C.c_char_p, []),
+    "lg_version": (_I, []),
+    "lg_scene_load_json": (_I, [C.c_char_p, _I, _I, C.POINTER(_P)]),
+    "lg_scene_create": (_I, [C.POINTER(LgSceneDesc), C.POINTER(_P)]),
+    "lg_scene_describe": (_I, [_P, C.POINTER(LgSceneDesc)]),
+    "lg_scene_set_camera": (_I, [_P, C.POINTER(LgCamera)]),
+    "lg_scene_save_json": (_I, [_P, C.c_char_p]),
+    "lg_scene_texture": (C.c_char_p, [_P, _I]),
+    "lg_scene_destroy": (None, [_P]),
+    "lg_look_at": (None, [C.POINTER(LgCamera), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "lg_build_bvh": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P]),
+    "lg_build_bvh_device": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P, _P]),
+    "lg_renderer_create": (_I, [_I, C.POINTER(_P)]),
+    "lg_renderer_destroy": (None, [_P]),
+    "lg_renderer_set_scene": (_I, [_P, C.POINTER(LgSceneDesc)]),
+    "lg_renderer_set_scene_bvh": (_I, [_P, C.POINTER(LgSceneDesc), _P, C.c_int32]),
+    "lg_renderer_get_bvh": (_I, [_P, _P, C.POINTER(C.c_int32), _P]),
+    "lg_renderer_set_counting": (_I, [_P, _I]),
+    "lg_render": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, _P, C.POINTER(LgRenderStats)]),
+    "lg_render_device": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, C.POINTER(_P), C.POINTER(_P),
+                              C.POINTER(_P)]),
+    "lg_render_batch": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), C.c_int32, _P, _P]),
+    "lg_tonemap_device": (_I, [_P, _P, C.c_int64, C.c_float, _P]),
+    "lg_write_png": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
+    "lg_write_hdr": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads liblumina.so once; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR}` "
+                               "(the CUDA library is required; there is no fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != LG_OK:
+        raise LuminaError(rc, lib().lg_last_error().decode(errors="replace"))
+
+
+def ptr(a) -> C.c_void_p:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"], "arrays passed to liblumina must be C-contiguous"
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a)

@@ -1,0 +1,106 @@
+"""BVH build and rendering through liblumina (C ABI), for Python callers."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._ffi import (LG_RENDER_ACCUM64, NODE_DTYPE, TRI_DTYPE, LgCamera, LgRenderOpts, LgRenderStats, check, lib,
+                   ptr)
+from .scene import Camera, Scene
+
+
+def build_bvh(tris: np.ndarray):
+    """BuildBVH on the GPU (reference bvh.cpp:164-211).
+
+    Returns (nodes NODE_DTYPE[n_nodes], reordered triangles, perm) where
+    perm[i] is the input index of the triangle placed at i."""
+    tris = np.ascontiguousarray(tris, TRI_DTYPE)
+    n = len(tris)
+    nodes = np.zeros(max(2 * n - 1, 1), NODE_DTYPE)
+    perm = np.zeros(max(n, 1), np.int32)
+    out = np.zeros_like(tris)
+    count = C.c_int32(0)
+    check(lib().lg_build_bvh(ptr(tris), n, ptr(nodes), C.byref(count), ptr(perm), ptr(out)))
+    return nodes[:count.value].copy(), out, perm[:n].copy()
+
+
+class Renderer:
+    """Device-resident scene + frame buffers (one CUDA device)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        check(lib().lg_renderer_create(device, C.byref(self._h)))
+        self.scene: Scene | None = None
+
+    def close(self):
+        if self._h:
+            lib().lg_renderer_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_scene(self, scene: Scene) -> None:
+        """Uploads the scene and builds its BVH on the device."""
+        self.scene = scene
+        d = scene.desc()
+        check(lib().lg_renderer_set_scene(self._h, C.byref(d)))
+
+    def set_scene_bvh(self, scene: Scene, nodes: np.ndarray) -> None:
+        """Uploads a scene whose triangles are already in BVH order, with its nodes."""
+        self.scene = scene
+        nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+        d = scene.desc()
+        check(lib().lg_renderer_set_scene_bvh(self._h, C.byref(d), ptr(nodes), len(nodes)))
+
+    def get_bvh(self):
+        n = C.c_int32(0)
+        check(lib().lg_renderer_get_bvh(self._h, None, C.byref(n), None))
+        nodes = np.zeros(n.value, NODE_DTYPE)
+        tris = np.zeros(self.scene.n_tris if self.scene is not None else 0, TRI_DTYPE)
+        check(lib().lg_renderer_get_bvh(self._h, ptr(nodes), C.byref(n), ptr(tris)))
+        return nodes, tris
+
+    def set_counting(self, on: bool) -> None:
+        check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))
+
+    def render(self, camera: Camera | None = None, spp: int = 1, bounces: int = 0, sample_base: int = 0,
+               accum: bool = True, accum64: bool = False, rgb: bool = True):
+        """Renders one frame; returns dict(rgb (H,W,3) u8, accum (H,W,3) f32,
+        accum64, kernel_ms, closest_rays, shadow_rays)."""
+        cam = camera if camera is not None else self.scene.camera
+        c = cam.to_c()
+        W, H = int(cam.width), int(cam.height)
+        o = LgRenderOpts(spp, bounces, sample_base, LG_RENDER_ACCUM64 if accum64 else 0)
+        out_rgb = np.zeros((H, W, 3), np.uint8) if rgb else None
+        out_acc = np.zeros((H, W, 3), np.float32) if accum else None
+        out_acc64 = np.zeros((H, W, 3), np.float64) if accum64 else None
+        st = LgRenderStats()
+        check(lib().lg_render(self._h, C.byref(c), C.byref(o), ptr(out_rgb), ptr(out_acc), ptr(out_acc64),
+                              C.byref(st)))
+        return {"rgb": out_rgb, "accum": out_acc, "accum64": out_acc64, "kernel_ms": st.kernel_ms,
+                "closest_rays": int(st.closest_rays), "shadow_rays": int(st.shadow_rays),
+                "node_fetches": int(st.node_fetches), "tri_tests": int(st.tri_tests),
+                "leaf_fetches": int(st.leaf_fetches)}
+
+    def render_batch(self, cameras, spps, bounces):
+        """Renders several frames (per-job camera/spp/bounces); returns (rgb (J,H,W,3), ms per job)."""
+        J = len(cameras)
+        cams = (LgCamera * J)(*[c.to_c() for c in cameras])
+        opts = (LgRenderOpts * J)(*[LgRenderOpts(int(s), int(b), 0, 0) for s, b in zip(spps, bounces)])
+        H, W = int(cameras[0].height), int(cameras[0].width)
+        assert all(int(c.height) == H and int(c.width) == W for c in cameras), "batch frames share one size"
+        out = np.zeros((J, H, W, 3), np.uint8)
+        ms = np.zeros(J, np.float32)
+        check(lib().lg_render_batch(self._h, cams, opts, J, ptr(out), ptr(ms)))
+        return out, ms
