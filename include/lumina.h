@@ -99,6 +99,20 @@ int lg_build_bvh(const lg_triangle* tris, int32_t n_tris, lg_bvh_node* nodes_out
 int lg_build_bvh_device(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* d_nodes_out, int32_t* n_nodes_out,
                         int32_t* d_perm_out, lg_triangle* d_tris_out, void* stream);
 
+/* No counterpart in the reference.  lg_build_bvh_device for callers that may
+ * not allocate device memory (an engine's frame loop that cannot take the
+ * synchronisation of cudaMalloc/cudaFree, or a host that reserves all device
+ * memory through its own allocator).  Same arguments and results; the
+ * scratch is a fixed array in device memory that the library holds on every
+ * GPU that loads it, so at most LG_NOALLOC_MAX_TRIS triangles are accepted
+ * (larger inputs return LG_ERR_CAPACITY).  The first call on a device looks
+ * up the array's address for that device; make it before any stream capture.
+ * All calls share the one array: calls whose work overlaps on the GPU (other
+ * threads, other streams) race and must be serialised by the caller. */
+#define LG_NOALLOC_MAX_TRIS 65536
+int lg_build_bvh_device_noalloc(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* d_nodes_out,
+                                int32_t* n_nodes_out, int32_t* d_perm_out, lg_triangle* d_tris_out, void* stream);
+
 /* ---- path tracer ---- */
 typedef struct lg_renderer lg_renderer;
 

@@ -84,6 +84,7 @@ SIGNATURES = {
     "lg_look_at": (None, [C.POINTER(LgCamera), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "lg_build_bvh": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P]),
     "lg_build_bvh_device": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P, _P]),
+    "lg_build_bvh_device_noalloc": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P, _P]),
     "lg_renderer_create": (_I, [_I, C.POINTER(_P)]),
     "lg_renderer_destroy": (None, [_P]),
     "lg_renderer_set_scene": (_I, [_P, C.POINTER(LgSceneDesc)]),
