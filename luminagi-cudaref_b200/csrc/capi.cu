@@ -224,7 +224,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.n_tiles = job.tiles_x * ((cam->height + 3) / 4);
         job.accum = r->accum.as<float>();
         job.accum64 = acc64 ? r->accum64.as<double>() : nullptr;
-        job.work = r->work.as<unsigned>();
+        job.work64 = r->work.as<unsigned long long>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
         LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->stream));
     }

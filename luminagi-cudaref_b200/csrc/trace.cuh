@@ -59,7 +59,7 @@ struct TraceJob
     int tiles_x, n_tiles;  // 8 x 4 pixel tiles
     float* accum;          // W*H*3, added to
     double* accum64;       // optional
-    unsigned int* work;    // work counter (zeroed before launch)
+    unsigned long long* work64;  // work counter (zeroed by the launcher)
     RenderCounters* counters;  // optional
 };
 
