@@ -162,6 +162,36 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
 /* tonemap_kernel: rgb8 = (u8)(sqrt(clamp(accum*inv_spp, 0, 1)) * 255). */
 int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, float inv_spp, void* stream);
 
+/* ---- denoiser (reference ml/train.py:37-75 UNet, 3-channel in / 3-channel out) ----
+ * BF16 tcgen05 convolutions with FP32 accumulation; FP32 master parameters in
+ * the reference's state_dict order (d1.net.0.weight, d1.net.0.bias,
+ * d1.net.2.weight, ..., u1.net.2.bias, tail.weight, tail.bias).  Only base=32,
+ * in_ch=3 (the reference's defaults) are supported.  act_mode 0 is the
+ * reference's LeakyReLU(0.1); 1 is ReLU.  Images are FP32 NCHW in [0,1]; H and
+ * W must be multiples of 8 (tools/denoise.py pads before calling the model). */
+typedef struct lg_unet lg_unet;
+int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out);
+void lg_unet_destroy(lg_unet* u);
+int64_t lg_unet_num_params(const lg_unet* u);
+int lg_unet_set_params(lg_unet* u, const float* params, int64_t n);
+int lg_unet_get_params(lg_unet* u, float* params, int64_t n);
+/* y = clamp(x + tail(...), 0, 1); host buffers of n*3*h*w floats. */
+int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y);
+/* Same on device buffers, ordered on `stream` (a cudaStream_t; NULL = synchronous). */
+int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, float* d_y, void* stream);
+/* One 3x3 convolution layer on device buffers in the channel-blocked BF16
+ * layout ((n*C/8 + c/8)*H + y)*W + x)*8 + c%8: epilogue 0 writes act(conv+b)
+ * into channels [out_coff, out_coff+cout) of d_out (and, if d_out2, the 2x2
+ * max-pooled result into d_out2); epilogue 1 writes it 2x upsampled (nearest).
+ * Weights are FP32 [cout][cin_real][3][3]; cin >= cin_real is the blocked
+ * input's channel count (multiple of 16). */
+int lg_conv3x3_device(const void* d_in, int n, int cin, int h, int w, const float* d_w, int cin_real,
+                      const float* d_b, int cout, float slope, int epilogue, void* d_out, int out_c, int out_coff,
+                      void* d_out2, int out2_c, int out2_coff, void* stream);
+/* FP32 NCHW <-> channel-blocked BF16 (cpad channels, zero padded). */
+int lg_to_blocked_bf16(const float* d_x, int n, int c, int h, int w, void* d_out, int cpad, void* stream);
+int lg_from_blocked_bf16(const void* d_in, int n, int c, int h, int w, float* d_out, void* stream);
+
 /* ---- image output ---- */
 int lg_write_png(const char* path, int32_t w, int32_t h, const uint8_t* rgb8);
 int lg_write_hdr(const char* path, int32_t w, int32_t h, const float* rgb32);

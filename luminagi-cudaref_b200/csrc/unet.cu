@@ -1,0 +1,364 @@
+// unet.cu -- the denoiser network (reference ml/train.py:37-75) on the
+// tcgen05 convolution, and its C ABI (lg_unet_*).
+//
+// Architecture (base 32, 3-channel input): d1(3->32) d2(32->64) d3(64->128)
+// d4(128->256) at full, 1/2, 1/4, 1/8 resolution, each two 3x3 convs with an
+// activation, 2x2 max-pool between levels; u3(384->128) u2(192->64)
+// u1(96->32) on cat(up(deeper), skip) with nearest 2x upsampling; a 1x1 tail
+// to RGB; out = clamp(x + tail, 0, 1).  Activation LeakyReLU(0.1) as in the
+// reference (ReLU selectable).  Parameters are kept in FP32 in the reference's
+// state_dict order (d1.net.0.weight, d1.net.0.bias, d1.net.2.weight, ...,
+// tail.weight, tail.bias) and packed to BF16 for the kernels.
+//
+// Fusion: the concat buffers are written in place by their producers -- the
+// skip half by the encoder's second conv (which also writes the pooled tensor
+// for the next level), the upsampled half by the decoder level below (which
+// writes each pixel 2x2 times) -- and u1's second conv computes the tail,
+// residual and clamp in its epilogue.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "unet_conv.cuh"
+
+namespace lg
+{
+namespace
+{
+struct LayerDef
+{
+    int cin_real, cin, cout;
+};
+// 14 convs in state_dict order; cin is the padded channel count the kernel reads.
+constexpr LayerDef kLayers[14] = {
+    {3, 16, 32},    {32, 32, 32},   {32, 32, 64},   {64, 64, 64},   {64, 64, 128},  {128, 128, 128}, {128, 128, 256},
+    {256, 256, 256}, {384, 384, 128}, {128, 128, 128}, {192, 192, 64}, {64, 64, 64},  {96, 96, 32},   {32, 32, 32}};
+
+struct Buf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b)
+    {
+        if (b <= bytes) return LG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) return set_error(LG_ERR_NOMEM, "cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+        bytes = b;
+        return LG_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+}  // namespace
+}  // namespace lg
+
+using namespace lg;
+
+struct lg_unet
+{
+    int device = 0;
+    float slope = 0.1f;
+    cudaStream_t stream = nullptr;
+    // parameters (FP32, state_dict order) and packed BF16 weights
+    Buf params;     // all FP32 params contiguous
+    Buf packed[14];
+    size_t w_off[14], b_off[14], tail_w_off, tail_b_off, n_params;
+    bool packed_ok = false;
+    // activations, sized for (N, H, W)
+    int aN = 0, aH = 0, aW = 0;
+    Buf x0, t1, cat1, p1, t2, cat2, p2, t3, cat3, p3, t4, t5, t6, t7, u1, xin, yout, err;
+};
+
+namespace
+{
+size_t layout_params(lg_unet* u)
+{
+    size_t off = 0;
+    for (int i = 0; i < 14; ++i)
+    {
+        u->w_off[i] = off;
+        off += (size_t)kLayers[i].cout * kLayers[i].cin_real * 9;
+        u->b_off[i] = off;
+        off += (size_t)kLayers[i].cout;
+    }
+    u->tail_w_off = off;
+    off += 3 * 32;
+    u->tail_b_off = off;
+    off += 3;
+    return off;
+}
+
+int ensure_acts(lg_unet* u, int N, int H, int W)
+{
+    if (u->aN == N && u->aH == H && u->aW == W) return LG_OK;
+    const size_t px = (size_t)N * H * W, b2 = sizeof(__nv_bfloat16);
+    LG_TRY(u->x0.ensure(px * 16 * b2));
+    LG_TRY(u->t1.ensure(px * 32 * b2));
+    LG_TRY(u->cat1.ensure(px * 96 * b2));
+    LG_TRY(u->p1.ensure(px / 4 * 32 * b2));
+    LG_TRY(u->t2.ensure(px / 4 * 64 * b2));
+    LG_TRY(u->cat2.ensure(px / 4 * 192 * b2));
+    LG_TRY(u->p2.ensure(px / 16 * 64 * b2));
+    LG_TRY(u->t3.ensure(px / 16 * 128 * b2));
+    LG_TRY(u->cat3.ensure(px / 16 * 384 * b2));
+    LG_TRY(u->p3.ensure(px / 64 * 128 * b2));
+    LG_TRY(u->t4.ensure(px / 64 * 256 * b2));
+    LG_TRY(u->t5.ensure(px / 16 * 128 * b2));
+    LG_TRY(u->t6.ensure(px / 4 * 64 * b2));
+    LG_TRY(u->t7.ensure(px * 32 * b2));
+    LG_TRY(u->u1.ensure(px * 32 * b2));
+    LG_TRY(u->err.ensure(sizeof(int)));
+    u->aN = N;
+    u->aH = H;
+    u->aW = W;
+    return LG_OK;
+}
+
+int pack_all(lg_unet* u)
+{
+    if (u->packed_ok) return LG_OK;
+    for (int i = 0; i < 14; ++i)
+    {
+        const LayerDef& L = kLayers[i];
+        LG_TRY(u->packed[i].ensure(conv_packed_elems(L.cin, L.cout) * sizeof(__nv_bfloat16)));
+        LG_TRY_CUDA(conv_pack_weights((const float*)u->params.p + u->w_off[i], L.cout, L.cin_real, L.cin,
+                                      (__nv_bfloat16*)u->packed[i].p, u->stream));
+    }
+    u->packed_ok = true;
+    return LG_OK;
+}
+
+ConvArgs base_args(lg_unet* u, int layer, int N, int H, int W)
+{
+    ConvArgs a{};
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.Cin = kLayers[layer].cin;
+    a.Cout = kLayers[layer].cout;
+    a.wpack = (const __nv_bfloat16*)u->packed[layer].p;
+    a.bias = (const float*)u->params.p + u->b_off[layer];
+    a.slope = u->slope;
+    a.epilogue = kEpiStore;
+    a.err = (int*)u->err.p;
+    return a;
+}
+
+typedef __nv_bfloat16 bf;
+
+// Runs the network on a device FP32 NCHW input (N x 3 x H x W) into d_y.
+int forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
+{
+    if (N <= 0 || H <= 0 || W <= 0 || (H % 8) || (W % 8))
+        return set_error(LG_ERR_INVALID, "UNet input must be N>0 and H, W multiples of 8 (got %dx%d)", H, W);
+    LG_TRY(pack_all(u));
+    LG_TRY(ensure_acts(u, N, H, W));
+    cudaStream_t st = u->stream;
+    LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), st));
+    LG_TRY_CUDA(to_blocked_bf16(d_x, N, 3, H, W, (bf*)u->x0.p, 16, st));
+    const int H2 = H / 2, W2 = W / 2, H4 = H / 4, W4 = W / 4, H8 = H / 8, W8 = W / 8;
+    auto run = [&](int layer, const void* in, int h, int w, int epi, void* out, int out_c, int out_coff, void* out2,
+                   int out2_c, int out2_coff) -> int {
+        ConvArgs a = base_args(u, layer, N, h, w);
+        a.epilogue = epi;
+        a.out = (bf*)out;
+        a.out_C = out_c;
+        a.out_coff = out_coff;
+        a.out2 = (bf*)out2;
+        a.out2_C = out2_c;
+        a.out2_coff = out2_coff;
+        if (epi == kEpiTail)
+        {
+            a.tail_w = (const float*)u->params.p + u->tail_w_off;
+            a.tail_b = (const float*)u->params.p + u->tail_b_off;
+            a.resid = d_x;
+            a.resid_C = 3;
+            a.final_out = d_y;
+        }
+        LG_TRY_CUDA(conv3x3_forward((const bf*)in, a, st));
+        return LG_OK;
+    };
+    // encoder
+    LG_TRY(run(0, u->x0.p, H, W, kEpiStore, u->t1.p, 32, 0, nullptr, 0, 0));
+    LG_TRY(run(1, u->t1.p, H, W, kEpiStore, u->cat1.p, 96, 64, u->p1.p, 32, 0));
+    LG_TRY(run(2, u->p1.p, H2, W2, kEpiStore, u->t2.p, 64, 0, nullptr, 0, 0));
+    LG_TRY(run(3, u->t2.p, H2, W2, kEpiStore, u->cat2.p, 192, 128, u->p2.p, 64, 0));
+    LG_TRY(run(4, u->p2.p, H4, W4, kEpiStore, u->t3.p, 128, 0, nullptr, 0, 0));
+    LG_TRY(run(5, u->t3.p, H4, W4, kEpiStore, u->cat3.p, 384, 256, u->p3.p, 128, 0));
+    LG_TRY(run(6, u->p3.p, H8, W8, kEpiStore, u->t4.p, 256, 0, nullptr, 0, 0));
+    LG_TRY(run(7, u->t4.p, H8, W8, kEpiUpsample, u->cat3.p, 384, 0, nullptr, 0, 0));
+    // decoder
+    LG_TRY(run(8, u->cat3.p, H4, W4, kEpiStore, u->t5.p, 128, 0, nullptr, 0, 0));
+    LG_TRY(run(9, u->t5.p, H4, W4, kEpiUpsample, u->cat2.p, 192, 0, nullptr, 0, 0));
+    LG_TRY(run(10, u->cat2.p, H2, W2, kEpiStore, u->t6.p, 64, 0, nullptr, 0, 0));
+    LG_TRY(run(11, u->t6.p, H2, W2, kEpiUpsample, u->cat1.p, 96, 0, nullptr, 0, 0));
+    LG_TRY(run(12, u->cat1.p, H, W, kEpiStore, u->t7.p, 32, 0, nullptr, 0, 0));
+    LG_TRY(run(13, u->t7.p, H, W, kEpiTail, u->u1.p, 32, 0, nullptr, 0, 0));
+    return LG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out)
+{
+    if (!out) return set_error(LG_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    if (base != 32 || in_ch != 3)
+        return set_error(LG_ERR_INVALID, "UNet(base=%d, in_ch=%d): only base=32, in_ch=3 is supported", base, in_ch);
+    if (act_mode != 0 && act_mode != 1) return set_error(LG_ERR_INVALID, "act_mode must be 0 or 1");
+    lg_unet* u = new (std::nothrow) lg_unet();
+    if (!u) return set_error(LG_ERR_NOMEM, "out of memory");
+    cudaGetDevice(&u->device);
+    u->slope = act_mode == 0 ? 0.1f : 0.0f;
+    u->n_params = layout_params(u);
+    cudaError_t e = cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess)
+    {
+        delete u;
+        return set_error(LG_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+    }
+    int rc = u->params.ensure(u->n_params * sizeof(float));
+    if (rc != LG_OK)
+    {
+        lg_unet_destroy(u);
+        return rc;
+    }
+    cudaMemsetAsync(u->params.p, 0, u->n_params * sizeof(float), u->stream);
+    *out = u;
+    return LG_OK;
+}
+
+void lg_unet_destroy(lg_unet* u)
+{
+    if (!u) return;
+    if (u->stream) cudaStreamSynchronize(u->stream);
+    u->params.release();
+    for (auto& b : u->packed) b.release();
+    for (Buf* b : {&u->x0, &u->t1, &u->cat1, &u->p1, &u->t2, &u->cat2, &u->p2, &u->t3, &u->cat3, &u->p3, &u->t4,
+                   &u->t5, &u->t6, &u->t7, &u->u1, &u->xin, &u->yout, &u->err})
+        b->release();
+    if (u->stream) cudaStreamDestroy(u->stream);
+    delete u;
+}
+
+int64_t lg_unet_num_params(const lg_unet* u) { return u ? (int64_t)u->n_params : 0; }
+
+int lg_unet_set_params(lg_unet* u, const float* host_params, int64_t n)
+{
+    if (!u || !host_params) return set_error(LG_ERR_INVALID, "NULL argument");
+    if ((size_t)n != u->n_params)
+        return set_error(LG_ERR_INVALID, "expected %zu parameters, got %lld", u->n_params, (long long)n);
+    LG_TRY_CUDA(cudaMemcpyAsync(u->params.p, host_params, u->n_params * sizeof(float), cudaMemcpyHostToDevice,
+                                u->stream));
+    u->packed_ok = false;
+    LG_TRY(pack_all(u));
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    return LG_OK;
+}
+
+int lg_unet_get_params(lg_unet* u, float* host_params, int64_t n)
+{
+    if (!u || !host_params) return set_error(LG_ERR_INVALID, "NULL argument");
+    if ((size_t)n != u->n_params)
+        return set_error(LG_ERR_INVALID, "expected %zu parameters, got %lld", u->n_params, (long long)n);
+    LG_TRY_CUDA(cudaMemcpyAsync(host_params, u->params.p, u->n_params * sizeof(float), cudaMemcpyDeviceToHost,
+                                u->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    return LG_OK;
+}
+
+int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, float* d_y, void* stream)
+{
+    if (!u || !d_x || !d_y) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (stream)
+    {
+        cudaEvent_t ev;
+        LG_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, (cudaStream_t)stream);
+        cudaStreamWaitEvent(u->stream, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    LG_TRY(forward_device(u, d_x, n, h, w, d_y));
+    if (stream)
+    {
+        cudaEvent_t ev;
+        LG_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, u->stream);
+        cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+        cudaEventDestroy(ev);
+        return LG_OK;
+    }
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    int err = 0;
+    LG_TRY_CUDA(cudaMemcpy(&err, u->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return set_error(LG_ERR_DEVICE, "convolution kernel reported wait timeout %d", err);
+    return LG_OK;
+}
+
+int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y)
+{
+    if (!u || !x || !y) return set_error(LG_ERR_INVALID, "NULL argument");
+    const size_t bytes = (size_t)n * 3 * h * w * sizeof(float);
+    LG_TRY(u->xin.ensure(bytes));
+    LG_TRY(u->yout.ensure(bytes));
+    LG_TRY_CUDA(cudaMemcpyAsync(u->xin.p, x, bytes, cudaMemcpyHostToDevice, u->stream));
+    LG_TRY(forward_device(u, (const float*)u->xin.p, n, h, w, (float*)u->yout.p));
+    LG_TRY_CUDA(cudaMemcpyAsync(y, u->yout.p, bytes, cudaMemcpyDeviceToHost, u->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    int err = 0;
+    LG_TRY_CUDA(cudaMemcpy(&err, u->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return set_error(LG_ERR_DEVICE, "convolution kernel reported wait timeout %d", err);
+    return LG_OK;
+}
+
+// One convolution layer on device buffers (blocked BF16 in/out, FP32 PyTorch-
+// layout weights); used to test the kernel layer by layer.
+int lg_conv3x3_device(const void* d_in, int n, int cin, int h, int w, const float* d_w, int cin_real,
+                      const float* d_b, int cout, float slope, int epilogue, void* d_out, int out_c, int out_coff,
+                      void* d_out2, int out2_c, int out2_coff, void* stream)
+{
+    if (!d_in || !d_w || !d_b || !d_out) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (epilogue != kEpiStore && epilogue != kEpiUpsample)
+        return set_error(LG_ERR_INVALID, "epilogue must be 0 (store/pool) or 1 (upsample)");
+    cudaStream_t st = (cudaStream_t)stream;
+    __nv_bfloat16* packed = nullptr;
+    LG_TRY_CUDA(cudaMallocAsync((void**)&packed, conv_packed_elems(cin, cout) * sizeof(__nv_bfloat16), st));
+    cudaError_t e = conv_pack_weights(d_w, cout, cin_real, cin, packed, st);
+    ConvArgs a{};
+    a.N = n; a.H = h; a.W = w; a.Cin = cin; a.Cout = cout; a.wpack = packed; a.bias = d_b; a.slope = slope;
+    a.epilogue = epilogue; a.out = (__nv_bfloat16*)d_out; a.out_C = out_c; a.out_coff = out_coff;
+    a.out2 = (__nv_bfloat16*)d_out2; a.out2_C = out2_c; a.out2_coff = out2_coff;
+    if (e == cudaSuccess) e = conv3x3_forward((const __nv_bfloat16*)d_in, a, st);
+    cudaFreeAsync(packed, st);
+    if (e != cudaSuccess) return set_error(LG_ERR_CUDA, "conv3x3: %s", cudaGetErrorString(e));
+    LG_TRY_CUDA(cudaStreamSynchronize(st));
+    return LG_OK;
+}
+
+int lg_to_blocked_bf16(const float* d_x, int n, int c, int h, int w, void* d_out, int cpad, void* stream)
+{
+    if (cpad % 8 || cpad < c) return set_error(LG_ERR_INVALID, "cpad must be a multiple of 8 >= c");
+    LG_TRY_CUDA(to_blocked_bf16(d_x, n, c, h, w, (__nv_bfloat16*)d_out, cpad, (cudaStream_t)stream));
+    return LG_OK;
+}
+
+int lg_from_blocked_bf16(const void* d_in, int n, int c, int h, int w, float* d_out, void* stream)
+{
+    if (c % 8) return set_error(LG_ERR_INVALID, "c must be a multiple of 8");
+    LG_TRY_CUDA(from_blocked_bf16((const __nv_bfloat16*)d_in, n, c, h, w, d_out, (cudaStream_t)stream));
+    return LG_OK;
+}
+
+}  // extern "C"

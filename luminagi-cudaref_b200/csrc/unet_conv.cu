@@ -1,0 +1,467 @@
+// unet_conv.cu -- 3x3 convolution as an implicit GEMM on tcgen05 (see unet_conv.cuh).
+//
+// One CTA computes a 2-row x 128-pixel output tile for BN output channels:
+//   M = 128 pixels (one MMA per output row), N = BN, K = 9 taps x Cin.
+// Per K-block of KC input channels, thread 0
+//   * loads the input halo (4 rows x 130 pixels x KC channels) with one 5-D
+//     TMA box (out-of-range rows/columns are zero-filled: the conv padding),
+//   * bulk-copies the packed weights of the 9 taps (9 x KC x BN),
+//   * issues 9 taps x KC/16 K-steps x 2 rows tcgen05.mma (M=128, N=BN, K=16)
+//     into two TMEM accumulators; tap (dy,dx) is the same smem tile read at
+//     pixel offset (row+dy)*130 + dx, i.e. 16-byte steps of the descriptor,
+//   * commits each stage to an mbarrier that frees it for the next K-block.
+// The 4 warps then read their 32 TMEM lanes (= pixels) and apply bias and
+// activation, writing BF16 in the blocked layout, plus the fused extras:
+// 2x2 max-pool (both rows are in the tile; x pairs are adjacent lanes),
+// nearest 2x upsample into a concat buffer, or the UNet tail (1x1 conv to
+// RGB + residual + clamp).  Operands are BF16, accumulation FP32.
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "tc_ptx.cuh"
+#include "unet_conv.cuh"
+
+namespace lg
+{
+namespace
+{
+constexpr int kTileX = 128;  // output pixels per row (= MMA M)
+constexpr int kHaloX = kTileX + 2;
+constexpr int kRows = 2;     // output rows per CTA
+constexpr int kHaloY = kRows + 2;
+constexpr int kThreads = 128;
+
+struct TileCfg
+{
+    int bn, kc, stages;
+};
+
+// Tile shape per layer: BN = min(Cout, 128), KC = 32 input channels per
+// K-block (16 when Cin is not a multiple of 32), stages to fill ~100 KB (two
+// CTAs per SM) for narrow layers or ~210 KB (one CTA per SM) for wide ones.
+TileCfg pick_cfg(int Cin, int Cout)
+{
+    TileCfg c;
+    c.bn = Cout < 128 ? Cout : 128;
+    c.kc = (Cin % 32 == 0) ? 32 : 16;
+    if (c.bn == 32) c.stages = c.kc == 16 ? 4 : 2;
+    else if (c.bn == 64) c.stages = 3;
+    else c.stages = 2;
+    return c;
+}
+
+template <int BN, int KC>
+struct Smem
+{
+    static constexpr int kABytes = kHaloY * kHaloX * KC * 2;
+    static constexpr int kBBytes = 9 * KC * BN * 2;
+    static constexpr int kStage = ((kABytes + kBBytes + 1023) / 1024) * 1024;
+};
+
+__device__ __forceinline__ float act(float v, float slope) { return v > 0.0f ? v : v * slope; }
+
+__device__ __forceinline__ uint4 pack8(const float* v)
+{
+    __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]);
+    __nv_bfloat162 b = __floats2bfloat162_rn(v[2], v[3]);
+    __nv_bfloat162 c = __floats2bfloat162_rn(v[4], v[5]);
+    __nv_bfloat162 d = __floats2bfloat162_rn(v[6], v[7]);
+    uint4 u;
+    u.x = *reinterpret_cast<uint32_t*>(&a);
+    u.y = *reinterpret_cast<uint32_t*>(&b);
+    u.z = *reinterpret_cast<uint32_t*>(&c);
+    u.w = *reinterpret_cast<uint32_t*>(&d);
+    return u;
+}
+__device__ __forceinline__ float bf16r(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+// Address of pixel (n, block b, y, x) of a blocked tensor with C channels.
+__device__ __forceinline__ uint4* blk(__nv_bfloat16* base, int C, int H, int W, int n, int b, int y, int x)
+{
+    return reinterpret_cast<uint4*>(base + ((((size_t)n * (C >> 3) + b) * H + y) * W + x) * 8);
+}
+
+template <int BN, int KC, int STAGES>
+__global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
+{
+    using S = Smem<BN, KC>;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * S::kStage);
+    uint64_t* empty = full + STAGES;
+    uint64_t* done = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_fail;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n_cot = a.Cout / BN;
+    const int x0 = blockIdx.x * kTileX;
+    const int y0 = blockIdx.y * kRows;
+    const int n = blockIdx.z / n_cot;
+    const int ct = blockIdx.z % n_cot;
+    const int KB = a.Cin / KC;
+    constexpr uint32_t kCols = 2 * BN;  // two accumulators of BN FP32 columns
+    constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, BN);
+    constexpr uint32_t kLboA = kHaloY * kHaloX * 16;
+    constexpr uint32_t kLboB = BN * 16;
+
+    if (warp == 0)
+    {
+        tc::tmem_alloc(tmem_slot, kCols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+    {
+        s_fail = 0;
+        for (int s = 0; s < STAGES; ++s)
+        {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(done, 1);
+        tc::fence_mbar_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0)
+    {
+        const __nv_bfloat16* wsrc = a.wpack + (size_t)ct * KB * (9 * KC * BN);
+        auto issue_load = [&](int s, int kb) {
+            uint8_t* A = smem + s * S::kStage;
+            uint8_t* B = A + S::kABytes;
+            tc::mbar_expect_tx(&full[s], (uint32_t)(S::kABytes + S::kBBytes));
+            tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
+            tc::bulk_load(B, wsrc + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes, &full[s]);
+        };
+        const int pre = KB < STAGES ? KB : STAGES;
+        for (int s = 0; s < pre; ++s) issue_load(s, s);
+        bool ok = true;
+        for (int kb = 0; kb < KB && ok; ++kb)
+        {
+            const int s = kb % STAGES;
+            if (!tc::mbar_wait(&full[s], (uint32_t)((kb / STAGES) & 1))) { ok = false; break; }
+            tc::tc_fence_after();
+            const uint32_t abase = tc::smem_u32(smem + s * S::kStage);
+            const uint32_t bbase = abase + S::kABytes;
+#pragma unroll 1
+            for (int tap = 0; tap < 9; ++tap)
+            {
+                const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+                for (int ks = 0; ks < KC / 16; ++ks)
+                {
+                    const uint64_t bd = tc::smem_desc(bbase + (uint32_t)((tap * (KC / 8) + 2 * ks) * BN * 16), kLboB, 128);
+#pragma unroll
+                    for (int r = 0; r < kRows; ++r)
+                    {
+                        const uint32_t aoff = (uint32_t)(2 * ks) * kLboA + (uint32_t)(((r + dy) * kHaloX + dx) * 16);
+                        const uint64_t ad = tc::smem_desc(abase + aoff, kLboA, 128);
+                        tc::mma_bf16(tmem + (uint32_t)(r * BN), ad, bd, kIdesc, (kb | tap | ks) != 0 ? 1u : 0u);
+                    }
+                }
+            }
+            tc::mma_commit(&empty[s]);
+            // Refill the stage used one K-block ago (its MMAs are queued ahead of this one's).
+            if (kb >= 1)
+            {
+                const int ps = (kb - 1) % STAGES;
+                const int nk = kb - 1 + STAGES;
+                if (nk < KB)
+                {
+                    if (!tc::mbar_wait(&empty[ps], (uint32_t)(((kb - 1) / STAGES) & 1))) { ok = false; break; }
+                    issue_load(ps, nk);
+                }
+            }
+        }
+        if (!ok)
+        {
+            s_fail = 1;
+            if (a.err) atomicExch(a.err, 1);
+        }
+        tc::mma_commit(done);  // completes when every MMA issued above has finished
+    }
+    __syncwarp();
+    // Epilogue: every thread owns TMEM lane = pixel x0 + tid.
+    const bool got = tc::mbar_wait(done, 0);
+    if (!got && a.err) atomicExch(a.err, 2);
+    tc::tc_fence_after();
+    if (got && !s_fail)
+    {
+        const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
+        const int x = x0 + tid;
+        const bool xin = x < a.W;
+        if (a.epilogue == kEpiTail)
+        {
+            // BN == Cout == 32: whole pixel in this thread.
+            float o[kRows][3];
+#pragma unroll
+            for (int r = 0; r < kRows; ++r)
+            {
+                float v[32];
+                tc::tmem_ld16(lanebase + (uint32_t)(r * BN), v);
+                tc::tmem_ld16(lanebase + (uint32_t)(r * BN + 16), v + 16);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] = bf16r(act(v[c] + __ldg(&a.bias[c]), a.slope));
+                const int y = y0 + r;
+                if (a.out && xin && y < a.H)
+                {
+#pragma unroll
+                    for (int b = 0; b < 4; ++b)
+                        *blk(a.out, a.out_C, a.H, a.W, n, (a.out_coff >> 3) + b, y, x) = pack8(v + 8 * b);
+                }
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    float acc = __ldg(&a.tail_b[k]);
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&a.tail_w[k * 32 + c]), v[c], acc);
+                    o[r][k] = acc;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < kRows; ++r)
+            {
+                const int y = y0 + r;
+                if (!xin || y >= a.H) continue;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                {
+                    const size_t pi = (((size_t)n * a.resid_C + k) * a.H + y) * a.W + x;
+                    const size_t po = (((size_t)n * 3 + k) * a.H + y) * a.W + x;
+                    a.final_out[po] = fminf(fmaxf(a.resid[pi] + o[r][k], 0.0f), 1.0f);
+                }
+            }
+        }
+        else
+        {
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16)
+            {
+                float v[kRows][16];
+#pragma unroll
+                for (int r = 0; r < kRows; ++r) tc::tmem_ld16(lanebase + (uint32_t)(r * BN + c0), v[r]);
+                const int cg = ct * BN + c0;  // layer channel of v[.][0]
+#pragma unroll
+                for (int r = 0; r < kRows; ++r)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + __ldg(&a.bias[cg + j]), a.slope));
+                const int b0 = (a.out_coff + cg) >> 3;
+                if (a.epilogue == kEpiStore)
+                {
+#pragma unroll
+                    for (int r = 0; r < kRows; ++r)
+                    {
+                        const int y = y0 + r;
+                        if (xin && y < a.H)
+                        {
+                            *blk(a.out, a.out_C, a.H, a.W, n, b0, y, x) = pack8(v[r]);
+                            *blk(a.out, a.out_C, a.H, a.W, n, b0 + 1, y, x) = pack8(v[r] + 8);
+                        }
+                    }
+                    if (a.out2)
+                    {
+                        float m[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                        {
+                            float t = fmaxf(v[0][j], v[1][j]);
+                            m[j] = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, 1));
+                        }
+                        const int H2 = a.H >> 1, W2 = a.W >> 1;
+                        if (((x & 1) == 0) && (x >> 1) < W2 && (y0 >> 1) < H2)
+                        {
+                            const int pb = (a.out2_coff + cg) >> 3;
+                            *blk(a.out2, a.out2_C, H2, W2, n, pb, y0 >> 1, x >> 1) = pack8(m);
+                            *blk(a.out2, a.out2_C, H2, W2, n, pb + 1, y0 >> 1, x >> 1) = pack8(m + 8);
+                        }
+                    }
+                }
+                else  // kEpiUpsample: nearest 2x into a 2H x 2W buffer
+                {
+                    const int H2 = a.H * 2, W2 = a.W * 2;
+#pragma unroll
+                    for (int r = 0; r < kRows; ++r)
+                    {
+                        const int y = y0 + r;
+                        if (!xin || y >= a.H) continue;
+                        const uint4 lo = pack8(v[r]), hi = pack8(v[r] + 8);
+#pragma unroll
+                        for (int i = 0; i < 2; ++i)
+#pragma unroll
+                            for (int jx = 0; jx < 2; ++jx)
+                            {
+                                *blk(a.out, a.out_C, H2, W2, n, b0, 2 * y + i, 2 * x + jx) = lo;
+                                *blk(a.out, a.out_C, H2, W2, n, b0 + 1, 2 * y + i, 2 * x + jx) = hi;
+                            }
+                    }
+                }
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, kCols);
+    }
+}
+
+// ---- host side ----
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+// 5-D map over a blocked BF16 tensor: (8 channels, W, H, C/8, N), box
+// (8, 130, 4, KC/8, 1).
+cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int KC)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)(C / 8), (cuuint64_t)N};
+    cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)(C / 8) * H * W * 16};
+    cuuint32_t box[5] = {8, (cuuint32_t)kHaloX, (cuuint32_t)kHaloY, (cuuint32_t)(KC / 8), 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int BN, int KC, int STAGES>
+cudaError_t launch(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
+{
+    CUtensorMap m;
+    cudaError_t e = make_map(&m, in, a.N, a.Cin, a.H, a.W, KC);
+    if (e != cudaSuccess) return e;
+    const int smem = STAGES * Smem<BN, KC>::kStage + 1024 + 256;
+    static bool attr_done = false;
+    if (!attr_done)
+    {
+        e = cudaFuncSetAttribute(conv3x3_tc_kernel<BN, KC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_done = true;
+    }
+    dim3 grid((a.W + kTileX - 1) / kTileX, (a.H + kRows - 1) / kRows, a.N * (a.Cout / BN));
+    conv3x3_tc_kernel<BN, KC, STAGES><<<grid, kThreads, smem, stream>>>(m, a);
+    return cudaGetLastError();
+}
+
+__global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real, int Cin, int BN, int KC,
+                            __nv_bfloat16* __restrict__ out, size_t total)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    // i -> (ct, kb, tap, kc8, j, e), innermost last
+    size_t r = i;
+    const int e = (int)(r % 8); r /= 8;
+    const int j = (int)(r % BN); r /= BN;
+    const int kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
+    const int tap = (int)(r % 9); r /= 9;
+    const int KB = Cin / KC;
+    const int kb = (int)(r % KB); r /= KB;
+    const int ct = (int)r;
+    const int co = ct * BN + j;
+    const int ci = kb * KC + kc8 * 8 + e;
+    float v = 0.0f;
+    if (ci < Cin_real) v = w[(((size_t)co * Cin_real + ci) * 3 + tap / 3) * 3 + tap % 3];
+    out[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void to_blocked_kernel(const float* __restrict__ x, int N, int C, int H, int W,
+                                  __nv_bfloat16* __restrict__ out, int Cpad)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over N * Cpad * H * W
+    const size_t total = (size_t)N * Cpad * H * W;
+    if (i >= total) return;
+    size_t r = i;
+    const int e = (int)(r % 8); r /= 8;
+    const int xx = (int)(r % W); r /= W;
+    const int y = (int)(r % H); r /= H;
+    const int b = (int)(r % (Cpad / 8)); r /= (Cpad / 8);
+    const int n = (int)r;
+    const int c = b * 8 + e;
+    float v = c < C ? x[(((size_t)n * C + c) * H + y) * W + xx] : 0.0f;
+    out[i] = __float2bfloat16_rn(v);
+}
+
+__global__ void from_blocked_kernel(const __nv_bfloat16* __restrict__ in, int N, int C, int H, int W,
+                                    float* __restrict__ out)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over N*C*H*W (NCHW)
+    const size_t total = (size_t)N * C * H * W;
+    if (i >= total) return;
+    size_t r = i;
+    const int xx = (int)(r % W); r /= W;
+    const int y = (int)(r % H); r /= H;
+    const int c = (int)(r % C); r /= C;
+    const int n = (int)r;
+    out[i] = __bfloat162float(in[((((size_t)n * (C / 8) + c / 8) * H + y) * W + xx) * 8 + c % 8]);
+}
+}  // namespace
+
+size_t conv_packed_elems(int Cin, int Cout) { return (size_t)9 * Cin * Cout; }
+
+cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
+                              cudaStream_t stream)
+{
+    const TileCfg c = pick_cfg(Cin, Cout);
+    const size_t total = conv_packed_elems(Cin, Cout);
+    pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, Cin, c.bn, c.kc, d_packed,
+                                                                     total);
+    return cudaGetLastError();
+}
+
+cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
+{
+    if (a.Cin % 16 != 0 || (a.Cout != 32 && a.Cout != 64 && a.Cout != 128 && a.Cout != 256)) return cudaErrorInvalidValue;
+    if (a.epilogue == kEpiTail && a.Cout != 32) return cudaErrorInvalidValue;
+    if (a.epilogue == kEpiStore && a.out2 && ((a.H & 1) || (a.W & 1))) return cudaErrorInvalidValue;
+    const TileCfg c = pick_cfg(a.Cin, a.Cout);
+    if (c.bn == 32 && c.kc == 16) return launch<32, 16, 4>(in, a, stream);
+    if (c.bn == 32 && c.kc == 32) return launch<32, 32, 2>(in, a, stream);
+    if (c.bn == 64 && c.kc == 32) return launch<64, 32, 3>(in, a, stream);
+    if (c.bn == 128 && c.kc == 32) return launch<128, 32, 2>(in, a, stream);
+    if (c.bn == 64 && c.kc == 16) return launch<64, 16, 4>(in, a, stream);
+    if (c.bn == 128 && c.kc == 16) return launch<128, 16, 3>(in, a, stream);
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,
+                            cudaStream_t stream)
+{
+    const size_t total = (size_t)N * Cpad * H * W;
+    to_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(x, N, C, H, W, out, Cpad);
+    return cudaGetLastError();
+}
+
+cudaError_t from_blocked_bf16(const __nv_bfloat16* in, int N, int C, int H, int W, float* out, cudaStream_t stream)
+{
+    const size_t total = (size_t)N * C * H * W;
+    from_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(in, N, C, H, W, out);
+    return cudaGetLastError();
+}
+}  // namespace lg

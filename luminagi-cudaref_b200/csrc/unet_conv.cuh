@@ -1,0 +1,63 @@
+// unet_conv.cuh -- 3x3 "same" convolution on tcgen05 tensor cores.
+//
+// Activations live in device memory as BF16 in a channel-blocked layout:
+// element (n, c, y, x) of a C-channel H x W tensor is at
+//     (((n * C/8 + c/8) * H + y) * W + x) * 8 + c % 8
+// i.e. planes of 8 channels, 16 bytes per pixel.  A 5-D TMA box of that
+// tensor lands in shared memory exactly in the MMA's no-swizzle K-major
+// layout, and a one-pixel shift of a 3x3 tap is a 16-byte shift of the MMA
+// descriptor, so each input tile is loaded once for all nine taps.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace lg
+{
+enum ConvEpilogue : int
+{
+    kEpiStore = 0,     // act(acc + bias) -> out (and, if out2, 2x2 max-pooled -> out2)
+    kEpiUpsample = 1,  // act(acc + bias) -> out at 2x resolution (nearest, 4 copies)
+    kEpiTail = 2,      // act(acc + bias) -> out (optional); 1x1 conv to 3 + residual + clamp -> final (FP32 NCHW)
+};
+
+struct ConvArgs
+{
+    int N, H, W;         // spatial size of input and output
+    int Cin;             // input channels (the tensor map's channel count; multiple of 16)
+    int Cout;            // output channels of the layer
+    const __nv_bfloat16* wpack;  // packed weights (conv_pack_weights)
+    const float* bias;           // [Cout]
+    float slope;                 // activation: x > 0 ? x : slope * x (0.1 LeakyReLU, 0 ReLU)
+    int epilogue;                // ConvEpilogue
+    __nv_bfloat16* out;          // blocked output (may be null for kEpiTail)
+    int out_C, out_coff;         // channel count of `out` and first channel written
+    __nv_bfloat16* out2;         // pooled output (kEpiStore, may be null)
+    int out2_C, out2_coff;
+    const float* tail_w;         // [3][Cout] (kEpiTail, Cout == 32)
+    const float* tail_b;         // [3]
+    const float* resid;          // FP32 NCHW input image (kEpiTail), channels 0..2 used, resid_C channels
+    int resid_C;
+    float* final_out;            // FP32 NCHW [N][3][H][W]
+    int* err;                    // set non-zero by a kernel that hit a wait limit
+};
+
+// Bytes of packed weights for a layer (BF16).
+size_t conv_packed_elems(int Cin, int Cout);
+// Packs PyTorch-layout FP32 weights w[Cout][Cin_real][3][3] into the layout
+// the kernel streams (input channels beyond Cin_real are zero).
+cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
+                              cudaStream_t stream);
+
+// Launches the convolution reading `in` (blocked BF16, N x Cin x H x W).
+cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream);
+
+// FP32 NCHW (C channels) -> blocked BF16 with Cpad channels (zero padded).
+cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,
+                            cudaStream_t stream);
+// Blocked BF16 (C channels) -> FP32 NCHW.
+cudaError_t from_blocked_bf16(const __nv_bfloat16* in, int N, int C, int H, int W, float* out, cudaStream_t stream);
+}  // namespace lg

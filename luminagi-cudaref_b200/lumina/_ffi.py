@@ -96,6 +96,16 @@ SIGNATURES = {
                               C.POINTER(_P)]),
     "lg_render_batch": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), C.c_int32, _P, _P]),
     "lg_tonemap_device": (_I, [_P, _P, C.c_int64, C.c_float, _P]),
+    "lg_unet_create": (_I, [_I, _I, _I, C.POINTER(_P)]),
+    "lg_unet_destroy": (None, [_P]),
+    "lg_unet_num_params": (C.c_int64, [_P]),
+    "lg_unet_set_params": (_I, [_P, _P, C.c_int64]),
+    "lg_unet_get_params": (_I, [_P, _P, C.c_int64]),
+    "lg_unet_forward": (_I, [_P, _P, _I, _I, _I, _P]),
+    "lg_unet_forward_device": (_I, [_P, _P, _I, _I, _I, _P, _P]),
+    "lg_conv3x3_device": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, C.c_float, _I, _P, _I, _I, _P, _I, _I, _P]),
+    "lg_to_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _I, _P]),
+    "lg_from_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "lg_write_png": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
     "lg_write_hdr": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
 }

@@ -1,0 +1,104 @@
+"""The denoiser (reference ml/train.py UNet) on liblumina's tensor-core kernels.
+
+`UNet` holds FP32 master parameters in the reference's state_dict order and
+runs the BF16 tcgen05 forward pass.  `denoise_rgb8` follows tools/denoise.py:
+u8/255, replicate-pad to multiples of 8, run, crop, clip*255+0.5.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._ffi import check, lib, ptr
+
+# state_dict keys and shapes of the reference UNet(base=32, in_ch=3).
+_BLOCKS = [("d1", 3, 32), ("d2", 32, 64), ("d3", 64, 128), ("d4", 128, 256), ("u3", 384, 128), ("u2", 192, 64),
+           ("u1", 96, 32)]
+PARAM_SHAPES = []
+for _name, _cin, _cout in _BLOCKS:
+    PARAM_SHAPES += [(f"{_name}.net.0.weight", (_cout, _cin, 3, 3)), (f"{_name}.net.0.bias", (_cout,)),
+                     (f"{_name}.net.2.weight", (_cout, _cout, 3, 3)), (f"{_name}.net.2.bias", (_cout,))]
+PARAM_SHAPES += [("tail.weight", (3, 32, 1, 1)), ("tail.bias", (3,))]
+N_PARAMS = int(sum(np.prod(s) for _, s in PARAM_SHAPES))
+
+
+def flatten_state_dict(sd) -> np.ndarray:
+    """Reference state_dict (tensors or arrays) -> flat FP32 in key order."""
+    out = []
+    for k, shp in PARAM_SHAPES:
+        v = sd[k]
+        v = v.detach().cpu().float().numpy() if hasattr(v, "detach") else np.asarray(v, np.float32)
+        assert tuple(v.shape) == shp, (k, v.shape, shp)
+        out.append(v.ravel())
+    return np.concatenate(out).astype(np.float32)
+
+
+def unflatten(flat: np.ndarray) -> dict:
+    out, off = {}, 0
+    for k, shp in PARAM_SHAPES:
+        n = int(np.prod(shp))
+        out[k] = flat[off:off + n].reshape(shp)
+        off += n
+    return out
+
+
+class UNet:
+    def __init__(self, base: int = 32, in_ch: int = 3, act: str = "leaky"):
+        self._h = C.c_void_p()
+        check(lib().lg_unet_create(base, in_ch, 0 if act == "leaky" else 1, C.byref(self._h)))
+        self.n_params = int(lib().lg_unet_num_params(self._h))
+        assert self.n_params == N_PARAMS
+
+    def close(self):
+        if self._h:
+            lib().lg_unet_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, flat: np.ndarray) -> None:
+        flat = np.ascontiguousarray(flat, np.float32)
+        check(lib().lg_unet_set_params(self._h, ptr(flat), len(flat)))
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, np.float32)
+        check(lib().lg_unet_get_params(self._h, ptr(out), len(out)))
+        return out
+
+    def load_state_dict(self, sd) -> None:
+        self.set_params(flatten_state_dict(sd))
+
+    def load_checkpoint(self, path: str) -> None:
+        """Loads a reference checkpoint dict {"model": state_dict, "base", "in_ch"} (ml/train.py:216)."""
+        import torch
+        ck = torch.load(path, map_location="cpu", weights_only=True)
+        if ck.get("base", 32) != 32 or ck.get("in_ch", 3) != 3:
+            raise ValueError("only base=32, in_ch=3 checkpoints are supported")
+        self.load_state_dict(ck["model"])
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        """x: (N,3,H,W) FP32 in [0,1], H and W multiples of 8."""
+        x = np.ascontiguousarray(x, np.float32)
+        n, c, h, w = x.shape
+        assert c == 3
+        y = np.empty_like(x)
+        check(lib().lg_unet_forward(self._h, ptr(x), n, h, w, ptr(y)))
+        return y
+
+    def forward_device(self, d_x: int, n: int, h: int, w: int, d_y: int, stream: int = 0) -> None:
+        check(lib().lg_unet_forward_device(self._h, C.c_void_p(d_x), n, h, w, C.c_void_p(d_y),
+                                           C.c_void_p(stream) if stream else None))
+
+    def denoise_rgb8(self, img: np.ndarray) -> np.ndarray:
+        """tools/denoise.py:34-52: (H,W,3) u8 -> (H,W,3) u8."""
+        x = img.astype(np.float32) / 255.0
+        H, W = x.shape[:2]
+        ph, pw = (8 - H % 8) % 8, (8 - W % 8) % 8
+        x = np.pad(x, ((0, ph), (0, pw), (0, 0)), mode="edge")
+        y = self.forward(x.transpose(2, 0, 1)[None])[0].transpose(1, 2, 0)[:H, :W]
+        return (np.clip(y, 0.0, 1.0) * 255.0 + 0.5).astype(np.uint8)

@@ -1,0 +1,39 @@
+"""The PyTorch restatement of the reference UNet (oracle/unet_ref.py) pinned to
+the reference module's own output (tests/golden/unet_golden.npz, made by
+tests/golden/make_unet_golden.py from ml/train.py)."""
+import pathlib
+
+import numpy as np
+import torch
+
+import unet_ref
+from lumina import unet as lunet
+
+GOLD = pathlib.Path(__file__).resolve().parent / "golden" / "unet_golden.npz"
+
+
+def test_restatement_matches_reference_module():
+    g = np.load(GOLD)
+    m = unet_ref.UNetRef().eval()
+    flat = unet_ref.make_params(int(g["seed"]), m)
+    assert len(flat) == int(g["n_params"]) == 1946947
+    assert abs(float(flat.astype(np.float64).sum()) - float(g["param_sum"])) < 1e-9
+    unet_ref.load_flat(m, flat)
+    with torch.no_grad():
+        y = m(torch.from_numpy(g["x"])).numpy()
+    assert np.abs(y - g["y"]).max() < 1e-6
+
+
+def test_param_layout_matches_reference_keys():
+    m = unet_ref.UNetRef()
+    assert [(k, s) for k, s in unet_ref.param_shapes(m)] == lunet.PARAM_SHAPES
+    assert lunet.N_PARAMS == 1946947
+
+
+def test_bf16_emulation_is_close_to_fp32():
+    g = np.load(GOLD)
+    m = unet_ref.load_flat(unet_ref.UNetRef().eval(), unet_ref.make_params(int(g["seed"])))
+    with torch.no_grad():
+        a = m(torch.from_numpy(g["x"]))
+        b = unet_ref.forward_bf16(m, torch.from_numpy(g["x"]))
+    assert float((a - b).abs().max()) < 0.1

@@ -1,0 +1,131 @@
+"""Tensor-core 3x3 convolution and the full denoiser on the GPU, checked
+against PyTorch FP32 references (oracle/unet_ref.py):
+
+* one layer: the kernel's BF16 output vs conv2d in FP32 on the same BF16-
+  rounded inputs/weights, rounded to BF16 -- differences come only from FP32
+  summation order, so >= 99.9% of values must agree within 1 BF16 ulp;
+* the whole UNet: vs the same network with BF16 rounding at the kernels'
+  rounding points (tight), and vs the plain FP32 network (the precision cost
+  of BF16, reported and bounded)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import lumina
+from lumina import _ffi
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+F = torch.nn.functional
+
+import unet_ref  # noqa: E402
+
+
+def q(t):
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def blocked(x, cpad):
+    n, c, h, w = x.shape
+    out = torch.zeros(n * cpad * h * w, dtype=torch.bfloat16, device="cuda")
+    _ffi.check(_ffi.lib().lg_to_blocked_bf16(C.c_void_p(x.data_ptr()), n, c, h, w, C.c_void_p(out.data_ptr()),
+                                            cpad, None))
+    return out
+
+
+def unblock(buf, n, c, h, w):
+    out = torch.empty((n, c, h, w), dtype=torch.float32, device="cuda")
+    _ffi.check(_ffi.lib().lg_from_blocked_bf16(C.c_void_p(buf.data_ptr()), n, c, h, w, C.c_void_p(out.data_ptr()),
+                                              None))
+    torch.cuda.synchronize()
+    return out
+
+
+def close_frac(got, ref):
+    ulp = 2.0 ** -7  # BF16 has 8 significant bits
+    ok = (got - ref).abs() <= ulp * ref.abs() + 1e-6
+    return float(ok.float().mean())
+
+
+@pytest.mark.parametrize("cin_real,cin,cout,n,h,w", [
+    (3, 16, 32, 1, 16, 40),
+    (32, 32, 32, 2, 10, 130),
+    (32, 32, 64, 1, 8, 24),
+    (64, 64, 128, 1, 6, 200),
+    (128, 128, 256, 1, 4, 16),
+    (384, 384, 128, 1, 4, 24),
+    (192, 192, 64, 2, 8, 8),
+    (96, 96, 32, 1, 9, 33),
+])
+def test_conv_layer_matches_torch(cin_real, cin, cout, n, h, w):
+    g = torch.Generator(device="cpu").manual_seed(cin * 7 + cout)
+    x = torch.rand((n, cin_real, h, w), generator=g).cuda()
+    wt = (torch.randn((cout, cin_real, 3, 3), generator=g) * (2.0 / (cin_real * 9)) ** 0.5).cuda()
+    b = (torch.rand((cout,), generator=g) * 0.1 - 0.05).cuda()
+    xin = blocked(x, cin)
+    out_c, coff = cout + 32, 16  # write into a wider buffer at an offset (concat by addressing)
+    out = torch.zeros(n * out_c * h * w, dtype=torch.bfloat16, device="cuda")
+    pool = (h % 2 == 0) and (w % 2 == 0)
+    out2 = torch.zeros(n * cout * (h // 2) * (w // 2), dtype=torch.bfloat16, device="cuda") if pool else None
+    _ffi.check(_ffi.lib().lg_conv3x3_device(
+        C.c_void_p(xin.data_ptr()), n, cin, h, w, C.c_void_p(wt.data_ptr()), cin_real, C.c_void_p(b.data_ptr()), cout,
+        0.1, 0, C.c_void_p(out.data_ptr()), out_c, coff, C.c_void_p(out2.data_ptr()) if pool else None, cout, 0, None))
+    got = unblock(out, n, out_c, h, w)[:, coff:coff + cout]
+    ref = q(F.leaky_relu(F.conv2d(q(x), q(wt), b, padding=1), 0.1))
+    assert close_frac(got, ref) >= 0.999
+    assert float((got - ref).abs().max()) < 0.05
+    untouched = unblock(out, n, out_c, h, w)[:, :coff]
+    assert float(untouched.abs().max()) == 0.0
+    if pool:
+        gp = unblock(out2, n, cout, h // 2, w // 2)
+        assert close_frac(gp, F.max_pool2d(ref, 2)) >= 0.999
+
+
+def test_conv_upsample_epilogue():
+    n, cin, cout, h, w = 1, 64, 64, 6, 20
+    g = torch.Generator(device="cpu").manual_seed(5)
+    x = torch.rand((n, cin, h, w), generator=g).cuda()
+    wt = (torch.randn((cout, cin, 3, 3), generator=g) * 0.05).cuda()
+    b = torch.zeros(cout).cuda()
+    xin = blocked(x, cin)
+    out_c = 192
+    out = torch.zeros(n * out_c * 2 * h * 2 * w, dtype=torch.bfloat16, device="cuda")
+    _ffi.check(_ffi.lib().lg_conv3x3_device(
+        C.c_void_p(xin.data_ptr()), n, cin, h, w, C.c_void_p(wt.data_ptr()), cin, C.c_void_p(b.data_ptr()), cout, 0.1,
+        1, C.c_void_p(out.data_ptr()), out_c, 64, None, 0, 0, None))
+    got = unblock(out, n, out_c, 2 * h, 2 * w)[:, 64:128]
+    ref = F.interpolate(q(F.leaky_relu(F.conv2d(q(x), q(wt), b, padding=1), 0.1)), scale_factor=2, mode="nearest")
+    assert close_frac(got, ref) >= 0.999
+
+
+@pytest.mark.parametrize("n,h,w", [(2, 32, 48), (1, 64, 136)])
+def test_unet_forward_matches_torch(n, h, w):
+    flat = unet_ref.make_params(77)
+    net = lumina.UNet()
+    net.set_params(flat)
+    assert np.array_equal(net.get_params(), flat)
+    x = np.random.default_rng(3).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
+    y = net.forward(x)
+    m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
+    with torch.no_grad():
+        ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x)).numpy()
+        ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64).numpy()
+        ref_f = m(torch.from_numpy(x)).numpy()
+    err_q = np.abs(y - ref_q)
+    err_f = np.abs(y - ref_f)
+    # Noise floor: the same BF16-rounded network summed in FP32 vs FP64 already
+    # differs this much (a different summation order flips BF16 roundings).
+    floor = np.abs(ref_q - ref_q64)
+    print(f"UNet {n}x{h}x{w}: vs BF16-emulated max {err_q.max():.2e} mean {err_q.mean():.2e} "
+          f"(floor max {floor.max():.2e} mean {floor.mean():.2e}); vs FP32 max {err_f.max():.2e} "
+          f"mean {err_f.mean():.2e}")
+    assert err_q.mean() <= 2.0 * floor.mean() + 1e-4
+    assert err_q.max() <= 2.0 * floor.max() + 2e-3
+    assert err_f.mean() < 5e-3 and err_f.max() < 0.1
+
+
+def test_unet_rejects_bad_size():
+    net = lumina.UNet()
+    with pytest.raises(lumina.LuminaError):
+        net.forward(np.zeros((1, 3, 12, 16), np.float32))
