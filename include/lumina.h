@@ -179,6 +179,21 @@ int lg_unet_get_params(lg_unet* u, float* params, int64_t n);
 int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y);
 /* Same on device buffers, ordered on `stream` (a cudaStream_t; NULL = synchronous). */
 int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, float* d_y, void* stream);
+/* Training (reference ml/train.py:184-201): mean L1 loss of the network output
+ * against target, backward pass on the tensor cores, and one Adam step
+ * (betas 0.9/0.999, eps 1e-8, bias correction, as torch.optim.Adam) on the
+ * FP32 master parameters.  d_x, d_target: device FP32 NCHW n x 3 x h x w.
+ * *loss_out (may be NULL) receives the loss before the update. */
+int lg_unet_train_step(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float lr,
+                       float* loss_out);
+/* The loss and the gradient of every parameter (host, state_dict order)
+ * without updating them. */
+int lg_unet_loss_grad(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float* grads,
+                      float* loss_out);
+/* One Adam step with the gradients of the last lg_unet_loss_grad call. */
+int lg_unet_adam_apply(lg_unet* u, float lr);
+/* Clears the Adam moments and step count. */
+int lg_unet_adam_reset(lg_unet* u);
 /* One 3x3 convolution layer on device buffers in the channel-blocked BF16
  * layout ((n*C/8 + c/8)*H + y)*W + x)*8 + c%8: epilogue 0 writes act(conv+b)
  * into channels [out_coff, out_coff+cout) of d_out (and, if d_out2, the 2x2

@@ -25,60 +25,9 @@
 #include "common.h"
 #include "unet_conv.cuh"
 
-namespace lg
-{
-namespace
-{
-struct LayerDef
-{
-    int cin_real, cin, cout;
-};
-// 14 convs in state_dict order; cin is the padded channel count the kernel reads.
-constexpr LayerDef kLayers[14] = {
-    {3, 16, 32},    {32, 32, 32},   {32, 32, 64},   {64, 64, 64},   {64, 64, 128},  {128, 128, 128}, {128, 128, 256},
-    {256, 256, 256}, {384, 384, 128}, {128, 128, 128}, {192, 192, 64}, {64, 64, 64},  {96, 96, 32},   {32, 32, 32}};
-
-struct Buf
-{
-    void* p = nullptr;
-    size_t bytes = 0;
-    int ensure(size_t b)
-    {
-        if (b <= bytes) return LG_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) return set_error(LG_ERR_NOMEM, "cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
-        bytes = b;
-        return LG_OK;
-    }
-    void release()
-    {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-};
-}  // namespace
-}  // namespace lg
+#include "unet_internal.cuh"
 
 using namespace lg;
-
-struct lg_unet
-{
-    int device = 0;
-    float slope = 0.1f;
-    cudaStream_t stream = nullptr;
-    // parameters (FP32, state_dict order) and packed BF16 weights
-    Buf params;     // all FP32 params contiguous
-    Buf packed[14];
-    size_t w_off[14], b_off[14], tail_w_off, tail_b_off, n_params;
-    bool packed_ok = false;
-    // activations, sized for (N, H, W)
-    int aN = 0, aH = 0, aW = 0;
-    Buf x0, t1, cat1, p1, t2, cat2, p2, t3, cat3, p3, t4, t5, t6, t7, u1, xin, yout, err;
-};
 
 namespace
 {
@@ -125,7 +74,7 @@ int ensure_acts(lg_unet* u, int N, int H, int W)
     return LG_OK;
 }
 
-int pack_all(lg_unet* u)
+int pack_all_impl(lg_unet* u)
 {
     if (u->packed_ok) return LG_OK;
     for (int i = 0; i < 14; ++i)
@@ -158,11 +107,11 @@ ConvArgs base_args(lg_unet* u, int layer, int N, int H, int W)
 typedef __nv_bfloat16 bf;
 
 // Runs the network on a device FP32 NCHW input (N x 3 x H x W) into d_y.
-int forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
+int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
 {
     if (N <= 0 || H <= 0 || W <= 0 || (H % 8) || (W % 8))
         return set_error(LG_ERR_INVALID, "UNet input must be N>0 and H, W multiples of 8 (got %dx%d)", H, W);
-    LG_TRY(pack_all(u));
+    LG_TRY(pack_all_impl(u));
     LG_TRY(ensure_acts(u, N, H, W));
     cudaStream_t st = u->stream;
     LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), st));
@@ -209,6 +158,15 @@ int forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y
 }
 }  // namespace
 
+namespace lg
+{
+int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
+{
+    return forward_device_impl(u, d_x, N, H, W, d_y);
+}
+int unet_pack_all(lg_unet* u) { return pack_all_impl(u); }
+}  // namespace lg
+
 extern "C" {
 
 int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out)
@@ -221,6 +179,7 @@ int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out)
     lg_unet* u = new (std::nothrow) lg_unet();
     if (!u) return set_error(LG_ERR_NOMEM, "out of memory");
     cudaGetDevice(&u->device);
+    cudaDeviceGetAttribute(&u->sm_count, cudaDevAttrMultiProcessorCount, u->device);
     u->slope = act_mode == 0 ? 0.1f : 0.0f;
     u->n_params = layout_params(u);
     cudaError_t e = cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking);
@@ -247,8 +206,11 @@ void lg_unet_destroy(lg_unet* u)
     u->params.release();
     for (auto& b : u->packed) b.release();
     for (Buf* b : {&u->x0, &u->t1, &u->cat1, &u->p1, &u->t2, &u->cat2, &u->p2, &u->t3, &u->cat3, &u->p3, &u->t4,
-                   &u->t5, &u->t6, &u->t7, &u->u1, &u->xin, &u->yout, &u->err})
+                   &u->t5, &u->t6, &u->t7, &u->u1, &u->xin, &u->yout, &u->err, &u->grads, &u->adam_m, &u->adam_v,
+                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt})
         b->release();
+    for (auto& b : u->packed_dg) b.release();
+    for (auto& b : u->dz) b.release();
     if (u->stream) cudaStreamDestroy(u->stream);
     delete u;
 }
@@ -263,7 +225,8 @@ int lg_unet_set_params(lg_unet* u, const float* host_params, int64_t n)
     LG_TRY_CUDA(cudaMemcpyAsync(u->params.p, host_params, u->n_params * sizeof(float), cudaMemcpyHostToDevice,
                                 u->stream));
     u->packed_ok = false;
-    LG_TRY(pack_all(u));
+    u->packed_dg_ok = false;
+    LG_TRY(pack_all_impl(u));
     LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
     return LG_OK;
 }
@@ -290,7 +253,7 @@ int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, fl
         cudaStreamWaitEvent(u->stream, ev, 0);
         cudaEventDestroy(ev);
     }
-    LG_TRY(forward_device(u, d_x, n, h, w, d_y));
+    LG_TRY(forward_device_impl(u, d_x, n, h, w, d_y));
     if (stream)
     {
         cudaEvent_t ev;
@@ -314,7 +277,7 @@ int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y)
     LG_TRY(u->xin.ensure(bytes));
     LG_TRY(u->yout.ensure(bytes));
     LG_TRY_CUDA(cudaMemcpyAsync(u->xin.p, x, bytes, cudaMemcpyHostToDevice, u->stream));
-    LG_TRY(forward_device(u, (const float*)u->xin.p, n, h, w, (float*)u->yout.p));
+    LG_TRY(forward_device_impl(u, (const float*)u->xin.p, n, h, w, (float*)u->yout.p));
     LG_TRY_CUDA(cudaMemcpyAsync(y, u->yout.p, bytes, cudaMemcpyDeviceToHost, u->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
     int err = 0;

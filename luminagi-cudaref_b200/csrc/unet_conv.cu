@@ -87,6 +87,123 @@ __device__ __forceinline__ uint4* blk(__nv_bfloat16* base, int C, int H, int W, 
     return reinterpret_cast<uint4*>(base + ((((size_t)n * (C >> 3) + b) * H + y) * W + x) * 8);
 }
 
+__device__ __forceinline__ void unpack8(uint4 u, float* v)
+{
+    const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const float2 f = __bfloat1622float2(h[i]);
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+    }
+}
+// 16 channels (two blocks starting at block b) of pixel (n, y, x).
+__device__ __forceinline__ void load16(const __nv_bfloat16* base, int C, int H, int W, int n, int b, int y, int x,
+                                       float* v)
+{
+    unpack8(__ldg(reinterpret_cast<const uint4*>(base + ((((size_t)n * (C >> 3) + b) * H + y) * W + x) * 8)), v);
+    unpack8(__ldg(reinterpret_cast<const uint4*>(base + ((((size_t)n * (C >> 3) + b + 1) * H + y) * W + x) * 8)),
+            v + 8);
+}
+__device__ __forceinline__ float dact(float y, float slope) { return y > 0.0f ? 1.0f : slope; }
+
+// Input-gradient epilogues (see ConvEpilogue).  v[r][j]: gradient of conv
+// input channel cg+j at (y0+r, x) of this (backward) convolution.
+__device__ __forceinline__ void bwd_epilogue(const ConvArgs& a, float (&v)[kRows][16], int n, int y0, int x, int cg,
+                                             int b0)
+{
+    const bool xin = x < a.W;
+    const int rb = (a.ref_coff + cg) >> 3;
+    if (a.epilogue == kEpiBwdMask || a.epilogue == kEpiBwdStore)
+    {
+#pragma unroll
+        for (int r = 0; r < kRows; ++r)
+        {
+            const int y = y0 + r;
+            if (!xin || y >= a.H) continue;
+            float o[16];
+            if (a.epilogue == kEpiBwdMask)
+            {
+                float ref[16];
+                load16(a.ref, a.ref_C, a.H, a.W, n, rb, y, x, ref);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) o[j] = v[r][j] * dact(ref[j], a.slope);
+            }
+            else
+            {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) o[j] = v[r][j];
+            }
+            *blk(a.out, a.out_C, a.H, a.W, n, b0, y, x) = pack8(o);
+            *blk(a.out, a.out_C, a.H, a.W, n, b0 + 1, y, x) = pack8(o + 8);
+        }
+    }
+    else if (a.epilogue == kEpiBwdSumPool)
+    {
+        // Gradient of a nearest 2x upsample: sum of the 2x2 children.
+        float s[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+        {
+            const float t = v[0][j] + v[1][j];
+            s[j] = t + __shfl_xor_sync(0xffffffffu, t, 1);
+        }
+        const int H2 = a.H >> 1, W2 = a.W >> 1;
+        if (((x & 1) == 0) && (x >> 1) < W2 && (y0 >> 1) < H2)
+        {
+            // act' of the upsampled tensor is read at the even child (ref is 2x too).
+            float ref[16];
+            load16(a.ref, a.ref_C, a.H, a.W, n, rb, y0, x, ref);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) s[j] *= dact(ref[j], a.slope);
+            *blk(a.out, a.out_C, H2, W2, n, b0, y0 >> 1, x >> 1) = pack8(s);
+            *blk(a.out, a.out_C, H2, W2, n, b0 + 1, y0 >> 1, x >> 1) = pack8(s + 8);
+        }
+    }
+    else  // kEpiBwdUnpool: this conv ran at the pooled resolution; ref/skip/out are 2H x 2W
+    {
+        const int H2 = a.H * 2, W2 = a.W * 2;
+        const int sb = (a.skip_coff + cg) >> 3;
+#pragma unroll 1
+        for (int r = 0; r < kRows; ++r)
+        {
+            const int y = y0 + r;
+            if (!xin || y >= a.H) continue;
+            float win[4][16];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) load16(a.ref, a.ref_C, H2, W2, n, rb, 2 * y + (q >> 1), 2 * x + (q & 1), win[q]);
+            // First maximum in raster order wins, as max_pool2d's backward routes it.
+            int arg[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+            {
+                int best = 0;
+                float bv = win[0][j];
+#pragma unroll
+                for (int q = 1; q < 4; ++q)
+                    if (win[q][j] > bv) { bv = win[q][j]; best = q; }
+                arg[j] = best;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+            {
+                const int yy = 2 * y + (q >> 1), xx = 2 * x + (q & 1);
+                float g[16];
+                load16(a.skip, a.skip_C, H2, W2, n, sb, yy, xx, g);
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                    const float t = g[j] + (arg[j] == q ? v[r][j] : 0.0f);
+                    g[j] = t * dact(win[q][j], a.slope);
+                }
+                *blk(a.out, a.out_C, H2, W2, n, b0, yy, xx) = pack8(g);
+                *blk(a.out, a.out_C, H2, W2, n, b0 + 1, yy, xx) = pack8(g + 8);
+            }
+        }
+    }
+}
+
 template <int BN, int KC, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
 {
@@ -250,12 +367,19 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 #pragma unroll
                 for (int r = 0; r < kRows; ++r) tc::tmem_ld16(lanebase + (uint32_t)(r * BN + c0), v[r]);
                 const int cg = ct * BN + c0;  // layer channel of v[.][0]
+                if (a.epilogue <= kEpiUpsample)
+                {
 #pragma unroll
-                for (int r = 0; r < kRows; ++r)
+                    for (int r = 0; r < kRows; ++r)
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + __ldg(&a.bias[cg + j]), a.slope));
+                        for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + __ldg(&a.bias[cg + j]), a.slope));
+                }
                 const int b0 = (a.out_coff + cg) >> 3;
-                if (a.epilogue == kEpiStore)
+                if (a.epilogue >= kEpiBwdMask)
+                {
+                    bwd_epilogue(a, v, n, y0, x, cg, b0);
+                }
+                else if (a.epilogue == kEpiStore)
                 {
 #pragma unroll
                     for (int r = 0; r < kRows; ++r)
@@ -391,6 +515,30 @@ __global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real,
     out[i] = __float2bfloat16_rn(v);
 }
 
+// Input-gradient weights: output (ct, kb, tap, kc8, j, e) of a conv with
+// Cin' = Cout (forward) and Cout' = ci_cnt reads w[co = ci'][ci_lo + co'][2-ky][2-kx].
+__global__ void pack_dgrad_kernel(const float* __restrict__ w, int Cout, int Cin_real, int ci_lo, int ci_cnt, int BN,
+                                  int KC, __nv_bfloat16* __restrict__ out, size_t total)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    size_t r = i;
+    const int e = (int)(r % 8); r /= 8;
+    const int j = (int)(r % BN); r /= BN;
+    const int kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
+    const int tap = (int)(r % 9); r /= 9;
+    const int KB = Cout / KC;
+    const int kb = (int)(r % KB); r /= KB;
+    const int ct = (int)r;
+    const int cop = ct * BN + j;             // output channel of the backward conv
+    const int cip = kb * KC + kc8 * 8 + e;   // its input channel = forward output channel
+    const int ky = 2 - tap / 3, kx = 2 - tap % 3;
+    const int ci = ci_lo + cop;
+    float v = 0.0f;
+    if (cop < ci_cnt && ci < Cin_real) v = w[(((size_t)cip * Cin_real + ci) * 3 + ky) * 3 + kx];
+    out[i] = __float2bfloat16_rn(v);
+}
+
 __global__ void to_blocked_kernel(const float* __restrict__ x, int N, int C, int H, int W,
                                   __nv_bfloat16* __restrict__ out, int Cpad)
 {
@@ -435,11 +583,25 @@ cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin,
     return cudaGetLastError();
 }
 
+cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
+                                    __nv_bfloat16* d_packed, cudaStream_t stream)
+{
+    const TileCfg c = pick_cfg(Cout, ci_cnt);
+    const size_t total = conv_packed_elems(Cout, ci_cnt);
+    pack_dgrad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, ci_lo, ci_cnt, c.bn,
+                                                                           c.kc, d_packed, total);
+    return cudaGetLastError();
+}
+
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
 {
     if (a.Cin % 16 != 0 || (a.Cout != 32 && a.Cout != 64 && a.Cout != 128 && a.Cout != 256)) return cudaErrorInvalidValue;
     if (a.epilogue == kEpiTail && a.Cout != 32) return cudaErrorInvalidValue;
     if (a.epilogue == kEpiStore && a.out2 && ((a.H & 1) || (a.W & 1))) return cudaErrorInvalidValue;
+    if (a.epilogue == kEpiBwdSumPool && ((a.H & 1) || (a.W & 1))) return cudaErrorInvalidValue;
+    if ((a.epilogue == kEpiBwdMask || a.epilogue == kEpiBwdSumPool || a.epilogue == kEpiBwdUnpool) && !a.ref)
+        return cudaErrorInvalidValue;
+    if (a.epilogue == kEpiBwdUnpool && !a.skip) return cudaErrorInvalidValue;
     const TileCfg c = pick_cfg(a.Cin, a.Cout);
     if (c.bn == 32 && c.kc == 16) return launch<32, 16, 4>(in, a, stream);
     if (c.bn == 32 && c.kc == 32) return launch<32, 32, 2>(in, a, stream);

@@ -22,6 +22,11 @@ enum ConvEpilogue : int
     kEpiStore = 0,     // act(acc + bias) -> out (and, if out2, 2x2 max-pooled -> out2)
     kEpiUpsample = 1,  // act(acc + bias) -> out at 2x resolution (nearest, 4 copies)
     kEpiTail = 2,      // act(acc + bias) -> out (optional); 1x1 conv to 3 + residual + clamp -> final (FP32 NCHW)
+    // Backward (input-gradient) epilogues; no bias is added.
+    kEpiBwdMask = 3,     // out = acc * act'(ref) at the same position
+    kEpiBwdSumPool = 4,  // acc at 2x resolution -> 2x2 sum -> * act'(ref at 1x) -> out (1x)
+    kEpiBwdStore = 5,    // out = acc
+    kEpiBwdUnpool = 6,   // acc = d(pooled); route to the max of ref's 2x2 window, add skip, * act'(ref) -> out (2x)
 };
 
 struct ConvArgs
@@ -43,6 +48,11 @@ struct ConvArgs
     int resid_C;
     float* final_out;            // FP32 NCHW [N][3][H][W]
     int* err;                    // set non-zero by a kernel that hit a wait limit
+    // backward epilogues
+    const __nv_bfloat16* ref;    // forward activation whose act' masks the gradient
+    int ref_C, ref_coff;
+    const __nv_bfloat16* skip;   // kEpiBwdUnpool: gradient arriving through the skip connection (2x res)
+    int skip_C, skip_coff;
 };
 
 // Bytes of packed weights for a layer (BF16).
@@ -51,6 +61,12 @@ size_t conv_packed_elems(int Cin, int Cout);
 // the kernel streams (input channels beyond Cin_real are zero).
 cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
                               cudaStream_t stream);
+
+// Packs the input-gradient weights of a forward conv w[Cout][Cin_real][3][3]:
+// w'[ci][co][ky][kx] = w[co][ci][2-ky][2-kx] for ci in [ci_lo, ci_lo+ci_cnt),
+// as a convolution with Cin' = Cout input and ci_cnt output channels.
+cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
+                                    __nv_bfloat16* d_packed, cudaStream_t stream);
 
 // Launches the convolution reading `in` (blocked BF16, N x Cin x H x W).
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream);

@@ -1,0 +1,78 @@
+// unet_internal.cuh -- the denoiser object shared by unet.cu (forward, C ABI)
+// and unet_train.cu (backward, Adam).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "unet_conv.cuh"
+
+namespace lg
+{
+struct LayerDef
+{
+    int cin_real, cin, cout;
+};
+// 14 convs in state_dict order; cin is the padded channel count the kernel reads.
+constexpr LayerDef kLayers[14] = {
+    {3, 16, 32},    {32, 32, 32},   {32, 32, 64},   {64, 64, 64},   {64, 64, 128},  {128, 128, 128}, {128, 128, 256},
+    {256, 256, 256}, {384, 384, 128}, {128, 128, 128}, {192, 192, 64}, {64, 64, 64},  {96, 96, 32},   {32, 32, 32}};
+
+struct Buf
+{
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b)
+    {
+        if (b <= bytes) return LG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) return set_error(LG_ERR_NOMEM, "cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+        bytes = b;
+        return LG_OK;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+}  // namespace lg
+
+
+struct lg_unet
+{
+    using Buf = lg::Buf;
+    int device = 0;
+    float slope = 0.1f;
+    cudaStream_t stream = nullptr;
+    // parameters (FP32, state_dict order) and packed BF16 weights
+    Buf params;     // all FP32 params contiguous
+    Buf packed[14];
+    size_t w_off[14], b_off[14], tail_w_off, tail_b_off, n_params;
+    bool packed_ok = false;
+    // activations, sized for (N, H, W)
+    int aN = 0, aH = 0, aW = 0;
+    Buf x0, t1, cat1, p1, t2, cat2, p2, t3, cat3, p3, t4, t5, t6, t7, u1, xin, yout, err;
+    // training state
+    int sm_count = 148;
+    Buf grads, adam_m, adam_v, loss;
+    Buf packed_dg[17];   // input-gradient weights (see unet_train.cu)
+    bool packed_dg_ok = false;
+    long long adam_t = 0;
+    int gN = 0, gH = 0, gW = 0;
+    Buf dz[14], gs1, gs2, gs3, tgt;
+};
+
+namespace lg
+{
+int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y);
+int unet_pack_all(lg_unet* u);
+}  // namespace lg
+

@@ -1,0 +1,381 @@
+// unet_train.cu -- backward pass and Adam for the denoiser (reference
+// ml/train.py:184-201: L1 loss, loss.backward(), Adam step).
+//
+// Gradients flow as BF16 tensors in the channel-blocked layout; every GEMM
+// accumulates in FP32 and parameters and their gradients stay FP32.
+//   * L1 + clamp + tail: one per-pixel kernel (mean |pred - target|, clamp
+//     passes the gradient where 0 <= x + tail <= 1, 1x1 tail weight/bias
+//     gradients, and the gradient into u1's second conv times act').
+//   * Input gradients: the forward tcgen05 convolution with flipped,
+//     transposed weights; its epilogue applies act' of the producer's output
+//     (kEpiBwdMask), sums the 2x2 children of an upsampled tensor
+//     (kEpiBwdSumPool), keeps the skip-connection part (kEpiBwdStore), or routes
+//     a pooled gradient to the window maximum and adds the skip part
+//     (kEpiBwdUnpool).  Concat inputs are split into their two sources.
+//   * Weight gradients: unet_wgrad.cu; bias gradients: a channel reduction.
+//   * Adam (betas 0.9/0.999, eps 1e-8, no weight decay, bias-corrected, as
+//     torch.optim.Adam) on the FP32 master parameters, then re-packing to BF16.
+#include <cmath>
+#include <cstdint>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "unet_internal.cuh"
+#include "unet_wgrad.cuh"
+
+using namespace lg;
+
+namespace
+{
+typedef __nv_bfloat16 bf;
+
+// Input-gradient convolutions: (forward layer, input-channel slice, epilogue).
+struct DgradDef
+{
+    int layer, ci_lo, ci_cnt, epi;
+};
+constexpr DgradDef kDgrad[16] = {
+    {13, 0, 32, kEpiBwdMask},     {12, 0, 64, kEpiBwdSumPool}, {12, 64, 32, kEpiBwdStore}, {11, 0, 64, kEpiBwdMask},
+    {10, 0, 128, kEpiBwdSumPool}, {10, 128, 64, kEpiBwdStore}, {9, 0, 128, kEpiBwdMask},   {8, 0, 256, kEpiBwdSumPool},
+    {8, 256, 128, kEpiBwdStore},  {7, 0, 256, kEpiBwdMask},    {6, 0, 128, kEpiBwdUnpool}, {5, 0, 128, kEpiBwdMask},
+    {4, 0, 64, kEpiBwdUnpool},    {3, 0, 64, kEpiBwdMask},     {2, 0, 32, kEpiBwdUnpool},  {1, 0, 32, kEpiBwdMask}};
+
+__device__ __forceinline__ float dact(float y, float slope) { return y > 0.0f ? 1.0f : slope; }
+
+// One thread per pixel.  u1: blocked BF16 (32 ch); x, target, pred: FP32 NCHW.
+__global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __restrict__ x,
+                                     const float* __restrict__ target, const float* __restrict__ tw,
+                                     const float* __restrict__ tb, int N, int H, int W, float slope, float inv_numel,
+                                     bf* __restrict__ dz, float* __restrict__ dtw, float* __restrict__ dtb,
+                                     float* __restrict__ loss)
+{
+    __shared__ float red[8][100];
+    const int HW = H * W;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float gtw[96], gtb[3], l = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 96; ++i) gtw[i] = 0.0f;
+    gtb[0] = gtb[1] = gtb[2] = 0.0f;
+    if (p < (long long)N * HW)
+    {
+        const int n = (int)(p / HW), q = (int)(p % HW);
+        float v[32];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+        {
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(u1 + (((size_t)n * 4 + b) * HW + q) * 8));
+            const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+                const float2 f = __bfloat1622float2(h[i]);
+                v[8 * b + 2 * i] = f.x;
+                v[8 * b + 2 * i + 1] = f.y;
+            }
+        }
+        float gpre[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            float acc = __ldg(&tb[k]);  // same order as the forward epilogue
+#pragma unroll
+            for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&tw[k * 32 + c]), v[c], acc);
+            const size_t pi = ((size_t)n * 3 + k) * HW + q;
+            const float pre = x[pi] + acc;
+            const float pred = fminf(fmaxf(pre, 0.0f), 1.0f);
+            const float diff = pred - target[pi];
+            l += fabsf(diff);
+            const float g = (diff > 0.0f ? 1.0f : (diff < 0.0f ? -1.0f : 0.0f)) * inv_numel;
+            gpre[k] = (pre >= 0.0f && pre <= 1.0f) ? g : 0.0f;
+            gtb[k] = gpre[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int c = 0; c < 32; ++c) gtw[k * 32 + c] = gpre[k] * v[c];
+        float d[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+            d[c] = (__ldg(&tw[c]) * gpre[0] + __ldg(&tw[32 + c]) * gpre[1] + __ldg(&tw[64 + c]) * gpre[2]) *
+                   dact(v[c], slope);
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+        {
+            __nv_bfloat162 h[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(d[8 * b + 2 * i], d[8 * b + 2 * i + 1]);
+            *reinterpret_cast<uint4*>(dz + (((size_t)n * 4 + b) * HW + q) * 8) = *reinterpret_cast<uint4*>(h);
+        }
+    }
+    // block reduction of the 96 + 3 + 1 partial sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto wsum = [](float t) {
+        for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        return t;
+    };
+#pragma unroll 4
+    for (int i = 0; i < 96; ++i)
+    {
+        const float t = wsum(gtw[i]);
+        if (lane == 0) red[warp][i] = t;
+    }
+    for (int k = 0; k < 3; ++k)
+    {
+        const float t = wsum(gtb[k]);
+        if (lane == 0) red[warp][96 + k] = t;
+    }
+    const float lt = wsum(l);
+    if (lane == 0) red[warp][99] = lt;
+    __syncthreads();
+    if (threadIdx.x < 100)
+    {
+        float t = 0.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
+        if (threadIdx.x < 96) atomicAdd(&dtw[threadIdx.x], t);
+        else if (threadIdx.x < 99) atomicAdd(&dtb[threadIdx.x - 96], t);
+        else atomicAdd(loss, t);
+    }
+}
+
+// torch.optim.Adam: m <- b1 m + (1-b1) g; v <- b2 v + (1-b2) g^2;
+// p <- p - (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps).
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, size_t n, float lr, float b1, float b2, float eps, float bc1,
+                            float bc2_sqrt)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = m[i] + (1.0f - b1) * (gi - m[i]);
+    const float vi = v[i] * b2 + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float denom = sqrtf(vi) / bc2_sqrt + eps;
+    p[i] -= (lr / bc1) * mi / denom;
+}
+
+int ensure_train(lg_unet* u, int N, int H, int W)
+{
+    const size_t np = u->n_params;
+    LG_TRY(u->grads.ensure(np * sizeof(float)));
+    if (!u->adam_m.p)
+    {
+        LG_TRY(u->adam_m.ensure(np * sizeof(float)));
+        LG_TRY(u->adam_v.ensure(np * sizeof(float)));
+        LG_TRY_CUDA(cudaMemsetAsync(u->adam_m.p, 0, np * sizeof(float), u->stream));
+        LG_TRY_CUDA(cudaMemsetAsync(u->adam_v.p, 0, np * sizeof(float), u->stream));
+    }
+    LG_TRY(u->loss.ensure(sizeof(float)));
+    if (u->gN == N && u->gH == H && u->gW == W) return LG_OK;
+    const size_t px = (size_t)N * H * W, b2 = sizeof(bf);
+    const size_t lvl[4] = {px, px / 4, px / 16, px / 64};
+    const int lv[14] = {0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0};  // output level of each layer
+    for (int i = 0; i < 14; ++i) LG_TRY(u->dz[i].ensure(lvl[lv[i]] * kLayers[i].cout * b2));
+    LG_TRY(u->gs1.ensure(px * 32 * b2));
+    LG_TRY(u->gs2.ensure(px / 4 * 64 * b2));
+    LG_TRY(u->gs3.ensure(px / 16 * 128 * b2));
+    u->gN = N;
+    u->gH = H;
+    u->gW = W;
+    return LG_OK;
+}
+
+int pack_dgrad(lg_unet* u)
+{
+    if (u->packed_dg_ok) return LG_OK;
+    for (int k = 0; k < 16; ++k)
+    {
+        const DgradDef& d = kDgrad[k];
+        const LayerDef& L = kLayers[d.layer];
+        LG_TRY(u->packed_dg[k].ensure(conv_packed_elems(L.cout, d.ci_cnt) * sizeof(bf)));
+        LG_TRY_CUDA(conv_pack_weights_dgrad((const float*)u->params.p + u->w_off[d.layer], L.cout, L.cin_real, d.ci_lo,
+                                            d.ci_cnt, (bf*)u->packed_dg[k].p, u->stream));
+    }
+    u->packed_dg_ok = true;
+    return LG_OK;
+}
+
+// Forward (activations kept), L1 loss and every parameter gradient into u->grads.
+int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H, int W, float* loss_host)
+{
+    LG_TRY(ensure_train(u, N, H, W));
+    LG_TRY(u->yout.ensure((size_t)N * 3 * H * W * sizeof(float)));
+    LG_TRY(unet_forward_device(u, d_x, N, H, W, (float*)u->yout.p));
+    LG_TRY(pack_dgrad(u));
+    cudaStream_t st = u->stream;
+    float* G = (float*)u->grads.p;
+    const float* P = (const float*)u->params.p;
+    LG_TRY_CUDA(cudaMemsetAsync(G, 0, u->n_params * sizeof(float), st));
+    LG_TRY_CUDA(cudaMemsetAsync(u->loss.p, 0, sizeof(float), st));
+    const long long npx = (long long)N * H * W;
+    const float inv_numel = 1.0f / (float)(npx * 3);
+    tail_backward_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(
+        (const bf*)u->u1.p, d_x, d_t, P + u->tail_w_off, P + u->tail_b_off, N, H, W, u->slope, inv_numel,
+        (bf*)u->dz[13].p, G + u->tail_w_off, G + u->tail_b_off, (float*)u->loss.p);
+    LG_TRY_CUDA(cudaGetLastError());
+
+    const int hs[4] = {H, H / 2, H / 4, H / 8}, ws[4] = {W, W / 2, W / 4, W / 8};
+    const int lv_out[14] = {0, 0, 1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 0, 0};
+    // forward inputs of each layer (blocked BF16)
+    const void* in_of[14] = {u->x0.p, u->t1.p, u->p1.p, u->t2.p, u->p2.p, u->t3.p, u->p3.p,
+                             u->t4.p, u->cat3.p, u->t5.p, u->cat2.p, u->t6.p, u->cat1.p, u->t7.p};
+    auto wgrad = [&](int L) -> int {
+        const int lv = lv_out[L];
+        WgradArgs a{};
+        a.N = N;
+        a.H = hs[lv];
+        a.W = ws[lv];
+        a.Cout = kLayers[L].cout;
+        a.Cin = kLayers[L].cin;
+        a.Cin_real = kLayers[L].cin_real;
+        a.dw = G + u->w_off[L];
+        a.err = (int*)u->err.p;
+        LG_TRY_CUDA(conv3x3_wgrad((const bf*)u->dz[L].p, (const bf*)in_of[L], a, u->sm_count, st));
+        LG_TRY_CUDA(conv_bias_grad((const bf*)u->dz[L].p, N, kLayers[L].cout, hs[lv], ws[lv], G + u->b_off[L], st));
+        return LG_OK;
+    };
+    auto dgrad = [&](int k, void* out, int out_c, const void* ref, int ref_c, int ref_coff, const void* skip,
+                     int skip_c) -> int {
+        const DgradDef& d = kDgrad[k];
+        const int lv = lv_out[d.layer];  // the backward conv runs at the forward layer's resolution
+        ConvArgs a{};
+        a.N = N;
+        a.H = hs[lv];
+        a.W = ws[lv];
+        a.Cin = kLayers[d.layer].cout;
+        a.Cout = d.ci_cnt;
+        a.wpack = (const bf*)u->packed_dg[k].p;
+        a.slope = u->slope;
+        a.epilogue = d.epi;
+        a.out = (bf*)out;
+        a.out_C = out_c;
+        a.out_coff = 0;
+        a.ref = (const bf*)ref;
+        a.ref_C = ref_c;
+        a.ref_coff = ref_coff;
+        a.skip = (const bf*)skip;
+        a.skip_C = skip_c;
+        a.skip_coff = 0;
+        a.err = (int*)u->err.p;
+        LG_TRY_CUDA(conv3x3_forward((const bf*)u->dz[d.layer].p, a, st));
+        return LG_OK;
+    };
+    // decoder, from the output back
+    LG_TRY(wgrad(13));
+    LG_TRY(dgrad(0, u->dz[12].p, 32, u->t7.p, 32, 0, nullptr, 0));
+    LG_TRY(wgrad(12));
+    LG_TRY(dgrad(1, u->dz[11].p, 64, u->cat1.p, 96, 0, nullptr, 0));
+    LG_TRY(dgrad(2, u->gs1.p, 32, nullptr, 0, 0, nullptr, 0));
+    LG_TRY(wgrad(11));
+    LG_TRY(dgrad(3, u->dz[10].p, 64, u->t6.p, 64, 0, nullptr, 0));
+    LG_TRY(wgrad(10));
+    LG_TRY(dgrad(4, u->dz[9].p, 128, u->cat2.p, 192, 0, nullptr, 0));
+    LG_TRY(dgrad(5, u->gs2.p, 64, nullptr, 0, 0, nullptr, 0));
+    LG_TRY(wgrad(9));
+    LG_TRY(dgrad(6, u->dz[8].p, 128, u->t5.p, 128, 0, nullptr, 0));
+    LG_TRY(wgrad(8));
+    LG_TRY(dgrad(7, u->dz[7].p, 256, u->cat3.p, 384, 0, nullptr, 0));
+    LG_TRY(dgrad(8, u->gs3.p, 128, nullptr, 0, 0, nullptr, 0));
+    // encoder
+    LG_TRY(wgrad(7));
+    LG_TRY(dgrad(9, u->dz[6].p, 256, u->t4.p, 256, 0, nullptr, 0));
+    LG_TRY(wgrad(6));
+    LG_TRY(dgrad(10, u->dz[5].p, 128, u->cat3.p, 384, 256, u->gs3.p, 128));
+    LG_TRY(wgrad(5));
+    LG_TRY(dgrad(11, u->dz[4].p, 128, u->t3.p, 128, 0, nullptr, 0));
+    LG_TRY(wgrad(4));
+    LG_TRY(dgrad(12, u->dz[3].p, 64, u->cat2.p, 192, 128, u->gs2.p, 64));
+    LG_TRY(wgrad(3));
+    LG_TRY(dgrad(13, u->dz[2].p, 64, u->t2.p, 64, 0, nullptr, 0));
+    LG_TRY(wgrad(2));
+    LG_TRY(dgrad(14, u->dz[1].p, 32, u->cat1.p, 96, 64, u->gs1.p, 32));
+    LG_TRY(wgrad(1));
+    LG_TRY(dgrad(15, u->dz[0].p, 32, u->t1.p, 32, 0, nullptr, 0));
+    LG_TRY(wgrad(0));
+    if (loss_host)
+    {
+        float s = 0.0f;
+        LG_TRY_CUDA(cudaMemcpyAsync(&s, u->loss.p, sizeof(float), cudaMemcpyDeviceToHost, st));
+        LG_TRY_CUDA(cudaStreamSynchronize(st));
+        *loss_host = s * inv_numel;
+    }
+    return LG_OK;
+}
+
+int adam_step(lg_unet* u, float lr)
+{
+    u->adam_t += 1;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float bc1 = 1.0f - (float)std::pow(0.9, (double)u->adam_t);
+    const float bc2 = 1.0f - (float)std::pow(0.999, (double)u->adam_t);
+    const size_t n = u->n_params;
+    adam_kernel<<<(unsigned)((n + 255) / 256), 256, 0, u->stream>>>((float*)u->params.p, (const float*)u->grads.p,
+                                                                    (float*)u->adam_m.p, (float*)u->adam_v.p, n, lr, b1,
+                                                                    b2, eps, bc1, sqrtf(bc2));
+    LG_TRY_CUDA(cudaGetLastError());
+    u->packed_ok = false;
+    u->packed_dg_ok = false;
+    LG_TRY(unet_pack_all(u));
+    return LG_OK;
+}
+
+int check_err(lg_unet* u)
+{
+    int err = 0;
+    LG_TRY_CUDA(cudaMemcpyAsync(&err, u->err.p, sizeof(int), cudaMemcpyDeviceToHost, u->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    if (err) return set_error(LG_ERR_DEVICE, "a tensor-core kernel reported wait timeout %d", err);
+    return LG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int lg_unet_train_step(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float lr,
+                       float* loss_out)
+{
+    if (!u || !d_x || !d_target) return set_error(LG_ERR_INVALID, "NULL argument");
+    float loss = 0.0f;
+    LG_TRY(loss_and_grads(u, d_x, d_target, n, h, w, loss_out ? &loss : nullptr));
+    LG_TRY(adam_step(u, lr));
+    LG_TRY(check_err(u));
+    if (loss_out) *loss_out = loss;
+    return LG_OK;
+}
+
+int lg_unet_loss_grad(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float* grads_host,
+                      float* loss_out)
+{
+    if (!u || !d_x || !d_target) return set_error(LG_ERR_INVALID, "NULL argument");
+    float loss = 0.0f;
+    LG_TRY(loss_and_grads(u, d_x, d_target, n, h, w, &loss));
+    if (grads_host)
+        LG_TRY_CUDA(cudaMemcpyAsync(grads_host, u->grads.p, u->n_params * sizeof(float), cudaMemcpyDeviceToHost,
+                                    u->stream));
+    LG_TRY(check_err(u));
+    if (loss_out) *loss_out = loss;
+    return LG_OK;
+}
+
+int lg_unet_adam_apply(lg_unet* u, float lr)
+{
+    if (!u) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (!u->grads.p || !u->adam_m.p) return set_error(LG_ERR_INVALID, "no gradients yet: call lg_unet_loss_grad first");
+    LG_TRY(adam_step(u, lr));
+    return check_err(u);
+}
+
+int lg_unet_adam_reset(lg_unet* u)
+{
+    if (!u) return set_error(LG_ERR_INVALID, "NULL argument");
+    u->adam_t = 0;
+    if (u->adam_m.p)
+    {
+        LG_TRY_CUDA(cudaMemsetAsync(u->adam_m.p, 0, u->n_params * sizeof(float), u->stream));
+        LG_TRY_CUDA(cudaMemsetAsync(u->adam_v.p, 0, u->n_params * sizeof(float), u->stream));
+    }
+    return LG_OK;
+}
+
+}  // extern "C"

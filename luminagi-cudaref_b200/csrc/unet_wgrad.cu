@@ -1,0 +1,295 @@
+// unet_wgrad.cu -- weight gradient of a 3x3 convolution on tcgen05.
+//
+//   dW[co][ci][ky][kx] += sum over (n, y, x) of dZ[n][co][y][x] * X[n][ci][y+ky-1][x+kx-1]
+//
+// A GEMM with M = output channels (128 per CTA), N = input channels (BNW per
+// CTA), K = pixels.  Both operands come straight from the channel-blocked
+// BF16 activations: a TMA box of 8 channels x 128 pixels per channel block
+// is, in shared memory, a stack of 8-pixel x 8-channel core matrices -- the
+// MMA's MN-major no-swizzle layout with K = pixels.  One CTA owns one kernel
+// row ky and all three kx taps: the X box is 130 pixels wide and tap kx reads
+// it 16*kx bytes further on, accumulating into three TMEM tiles.  Each CTA
+// sums a chunk of image rows and adds its partial dW to global memory with
+// FP32 atomics.
+#include <cstdint>
+#include <mutex>
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "tc_ptx.cuh"
+#include "unet_wgrad.cuh"
+
+namespace lg
+{
+namespace
+{
+constexpr int kPix = 128;         // pixels per K-chunk (one row segment)
+constexpr int kXHalo = kPix + 2;
+constexpr int kThreads = 128;
+constexpr int kStages = 3;
+
+template <int BNW>
+struct WSmem
+{
+    static constexpr int kABytes = 16 * kPix * 16;          // 16 channel blocks (M = 128) x 128 px
+    static constexpr int kBBytes = (BNW / 8) * kXHalo * 16;
+    static constexpr int kStage = ((kABytes + kBBytes + 1023) / 1024) * 1024;
+};
+
+template <int BNW>
+__global__ void __launch_bounds__(kThreads, 1)
+    wgrad_kernel(const __grid_constant__ CUtensorMap map_dz, const __grid_constant__ CUtensorMap map_x, WgradArgs a)
+{
+    using S = WSmem<BNW>;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * S::kStage);
+    uint64_t* empty = full + kStages;
+    uint64_t* done = empty + kStages;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_fail;
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int n_cit = a.Cin / BNW;
+    const int ky = blockIdx.y / n_cit;
+    const int ci0 = (blockIdx.y % n_cit) * BNW;
+    const int co0 = blockIdx.z * 128;
+    const int rows = a.N * a.H;
+    const int r0 = blockIdx.x * a.rows_per_cta;
+    const int r1 = min(rows, r0 + a.rows_per_cta);
+    const int xsegs = (a.W + kPix - 1) / kPix;
+    const int steps = (r1 - r0) * xsegs;
+    const int co_blocks = min(16, (a.Cout - co0) / 8);  // channel blocks loaded; the rest stay zero
+    constexpr uint32_t kCols = (3 * BNW <= 32) ? 32 : (3 * BNW <= 64) ? 64 : (3 * BNW <= 128) ? 128 : (3 * BNW <= 256) ? 256 : 512;
+    // M = 128, N = BNW, both operands MN-major.
+    constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, BNW) | (1u << 15) | (1u << 16);
+    const uint32_t a_bytes = (uint32_t)(co_blocks * kPix * 16);
+
+    // Zero the A buffers once: channel blocks beyond Cout are never written by TMA.
+    for (int i = tid; i < kStages * S::kStage / 16; i += kThreads)
+        reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
+    tc::fence_proxy_async();
+    if (warp == 0)
+    {
+        tc::tmem_alloc(tmem_slot, kCols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+    {
+        s_fail = 0;
+        for (int s = 0; s < kStages; ++s)
+        {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(done, 1);
+        tc::fence_mbar_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0 && steps > 0)
+    {
+        auto issue = [&](int s, int step) {
+            const int r = r0 + step / xsegs;
+            const int x0 = (step % xsegs) * kPix;
+            const int n = r / a.H, y = r % a.H;
+            uint8_t* A = smem + s * S::kStage;
+            uint8_t* B = A + S::kABytes;
+            tc::mbar_expect_tx(&full[s], a_bytes + (uint32_t)S::kBBytes);
+            tc::tma_load_5d(A, &map_dz, &full[s], 0, x0, y, co0 / 8, n);
+            tc::tma_load_5d(B, &map_x, &full[s], 0, x0 - 1, y + ky - 1, ci0 / 8, n);
+        };
+        const int pre = steps < kStages ? steps : kStages;
+        for (int s = 0; s < pre; ++s) issue(s, s);
+        bool ok = true;
+        for (int step = 0; step < steps; ++step)
+        {
+            const int s = step % kStages;
+            if (!tc::mbar_wait(&full[s], (uint32_t)((step / kStages) & 1))) { ok = false; break; }
+            tc::tc_fence_after();
+            const uint32_t abase = tc::smem_u32(smem + s * S::kStage);
+            const uint32_t bbase = abase + S::kABytes;
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                for (int ks = 0; ks < kPix / 16; ++ks)
+                {
+                    const uint64_t ad = tc::smem_desc(abase + (uint32_t)(ks * 16 * 16), 128, kPix * 16);
+                    const uint64_t bd = tc::smem_desc(bbase + (uint32_t)((ks * 16 + dx) * 16), 128, kXHalo * 16);
+                    tc::mma_bf16(tmem + (uint32_t)(dx * BNW), ad, bd, kIdesc, (step | ks) != 0 ? 1u : 0u);
+                }
+            tc::mma_commit(&empty[s]);
+            if (step >= 1)
+            {
+                const int ps = (step - 1) % kStages;
+                const int nk = step - 1 + kStages;
+                if (nk < steps)
+                {
+                    if (!tc::mbar_wait(&empty[ps], (uint32_t)(((step - 1) / kStages) & 1))) { ok = false; break; }
+                    issue(ps, nk);
+                }
+            }
+        }
+        if (!ok)
+        {
+            s_fail = 1;
+            if (a.err) atomicExch(a.err, 3);
+        }
+        tc::mma_commit(done);
+    }
+    __syncwarp();
+    if (steps > 0)
+    {
+        const bool got = tc::mbar_wait(done, 0);
+        if (!got && a.err) atomicExch(a.err, 4);
+        tc::tc_fence_after();
+        const int co = co0 + tid;  // TMEM lane = output channel
+        if (got && !s_fail)
+        {
+            const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+            for (int dx = 0; dx < 3; ++dx)
+#pragma unroll 1
+                for (int c0 = 0; c0 < BNW; c0 += 16)
+                {
+                    float v[16];
+                    tc::tmem_ld16(lanebase + (uint32_t)(dx * BNW + c0), v);
+                    if (co < a.Cout)
+                    {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                        {
+                            const int ci = ci0 + c0 + j;
+                            if (ci < a.Cin_real)
+                                atomicAdd(&a.dw[(((size_t)co * a.Cin_real + ci) * 3 + ky) * 3 + dx], v[j]);
+                        }
+                    }
+                }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+    {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, kCols);
+    }
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int box_x, int box_cb)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)(C / 8), (cuuint64_t)N};
+    cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)(C / 8) * H * W * 16};
+    cuuint32_t box[5] = {8, (cuuint32_t)box_x, 1, (cuuint32_t)box_cb, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int BNW>
+cudaError_t launch_w(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
+                     cudaStream_t stream)
+{
+    CUtensorMap mdz, mx;
+    cudaError_t e = make_map(&mdz, dz, a.N, a.Cout, a.H, a.W, kPix, a.Cout / 8 < 16 ? a.Cout / 8 : 16);
+    if (e != cudaSuccess) return e;
+    e = make_map(&mx, x, a.N, a.Cin, a.H, a.W, kXHalo, BNW / 8);
+    if (e != cudaSuccess) return e;
+    const int smem = kStages * WSmem<BNW>::kStage + 1024 + 256;
+    static bool attr = false;
+    if (!attr)
+    {
+        e = cudaFuncSetAttribute(wgrad_kernel<BNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    WgradArgs b = a;
+    const int cot = (a.Cout + 127) / 128, cit = a.Cin / BNW;
+    const int rows = a.N * a.H;
+    int chunks = (2 * sm_count) / (3 * cit * cot);
+    if (chunks < 1) chunks = 1;
+    if (chunks > rows) chunks = rows;
+    b.rows_per_cta = (rows + chunks - 1) / chunks;
+    chunks = (rows + b.rows_per_cta - 1) / b.rows_per_cta;
+    dim3 grid(chunks, 3 * cit, cot);
+    wgrad_kernel<BNW><<<grid, kThreads, smem, stream>>>(mdz, mx, b);
+    return cudaGetLastError();
+}
+
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW, float* __restrict__ db)
+{
+    // block (c-block, chunk): 8 channels of a range of pixels
+    const int cb = blockIdx.y;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const size_t pixels = (size_t)N * HW;
+    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += (size_t)gridDim.x * blockDim.x)
+    {
+        const size_t n = p / HW, q = p % HW;
+        const uint4 u = __ldg(reinterpret_cast<const uint4*>(dz + ((n * (C / 8) + cb) * HW + q) * 8));
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            const float2 f = __bfloat1622float2(h[i]);
+            acc[2 * i] += f.x;
+            acc[2 * i + 1] += f.y;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+    {
+        float v = acc[i];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&db[cb * 8 + i], v);
+    }
+}
+}  // namespace
+
+cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
+                          cudaStream_t stream)
+{
+    if (a.Cout % 32 || a.Cin % 16) return cudaErrorInvalidValue;
+    const int bnw = a.Cin % 128 == 0 ? 128 : a.Cin % 64 == 0 ? 64 : a.Cin % 32 == 0 ? 32 : 16;
+    switch (bnw)
+    {
+    case 128: return launch_w<128>(dz, x, a, sm_count, stream);
+    case 64: return launch_w<64>(dz, x, a, sm_count, stream);
+    case 32: return launch_w<32>(dz, x, a, sm_count, stream);
+    default: return launch_w<16>(dz, x, a, sm_count, stream);
+    }
+}
+
+cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, cudaStream_t stream)
+{
+    dim3 grid(64, C / 8);
+    bias_grad_kernel<<<grid, 256, 0, stream>>>(dz, N, C, H * W, db);
+    return cudaGetLastError();
+}
+}  // namespace lg

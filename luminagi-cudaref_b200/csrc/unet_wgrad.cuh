@@ -1,0 +1,24 @@
+// unet_wgrad.cuh -- weight and bias gradients of the 3x3 convolution.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace lg
+{
+struct WgradArgs
+{
+    int N, H, W;
+    int Cout;       // channels of dZ (multiple of 32)
+    int Cin;        // channels of the blocked input X (multiple of 16)
+    int Cin_real;   // channels that have weights (<= Cin)
+    int rows_per_cta;  // set by the launcher
+    float* dw;      // [Cout][Cin_real][3][3], added to
+    int* err;
+};
+
+// dW += sum over pixels of dZ (x) shifted X; both blocked BF16 at N x C x H x W.
+cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
+                          cudaStream_t stream);
+// db += sum over pixels of dZ.
+cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, cudaStream_t stream);
+}  // namespace lg

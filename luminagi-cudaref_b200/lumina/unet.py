@@ -94,6 +94,26 @@ class UNet:
         check(lib().lg_unet_forward_device(self._h, C.c_void_p(d_x), n, h, w, C.c_void_p(d_y),
                                            C.c_void_p(stream) if stream else None))
 
+    def train_step(self, d_x: int, d_target: int, n: int, h: int, w: int, lr: float) -> float:
+        """One L1 + Adam step on device FP32 NCHW batches; returns the loss before the update."""
+        loss = C.c_float(0)
+        check(lib().lg_unet_train_step(self._h, C.c_void_p(d_x), C.c_void_p(d_target), n, h, w, lr, C.byref(loss)))
+        return float(loss.value)
+
+    def loss_grad(self, d_x: int, d_target: int, n: int, h: int, w: int):
+        """(loss, flat FP32 gradient) without updating the parameters."""
+        g = np.zeros(self.n_params, np.float32)
+        loss = C.c_float(0)
+        check(lib().lg_unet_loss_grad(self._h, C.c_void_p(d_x), C.c_void_p(d_target), n, h, w, ptr(g), C.byref(loss)))
+        return float(loss.value), g
+
+    def adam_apply(self, lr: float) -> None:
+        """Adam step with the gradients of the last loss_grad call."""
+        check(lib().lg_unet_adam_apply(self._h, lr))
+
+    def adam_reset(self) -> None:
+        check(lib().lg_unet_adam_reset(self._h))
+
     def denoise_rgb8(self, img: np.ndarray) -> np.ndarray:
         """tools/denoise.py:34-52: (H,W,3) u8 -> (H,W,3) u8."""
         x = img.astype(np.float32) / 255.0
