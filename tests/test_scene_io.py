@@ -1,0 +1,159 @@
+"""scene.json loader/writer, PNG/HDR writers and the C ABI surface, on the CPU.
+
+The loader is checked float-bit for float-bit against what the reference's
+own LoadSceneJSON produced for the committed fixtures
+(tests/golden/*_ref.json, made by tests/golden/make_scene_golden.py), and
+against the reference loader itself when oracle/_ref is built."""
+import json
+import pathlib
+import re
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+import lumina
+import oracle as O
+from lumina import _ffi
+
+GOLD = pathlib.Path(__file__).resolve().parent / "golden"
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+
+
+def bits(a):
+    return [struct.unpack("<I", struct.pack("<f", float(x)))[0] for x in np.asarray(a, np.float32).ravel()]
+
+
+@pytest.mark.parametrize("name", ["mock_scene", "tricky_scene"])
+def test_loader_matches_reference_fixture(name):
+    ref = json.loads((GOLD / f"{name}_ref.json").read_text())
+    s = lumina.Scene.load_json(GOLD / f"{name}.json")
+    c = s.camera
+    assert bits(c.pos) == ref["camera"]["pos"]
+    assert bits(c.camera_to_world) == ref["camera"]["m"]
+    assert bits([c.fov_y_deg]) == ref["camera"]["fov"] and bits([c.aspect]) == ref["camera"]["aspect"]
+    assert bits([c.near_z]) == ref["camera"]["near"] and bits([c.far_z]) == ref["camera"]["far"]
+    assert (c.width, c.height) == (ref["camera"]["w"], ref["camera"]["h"])
+    assert bits(list(s.sun["dir"]) + list(s.sun["color"]) + [s.sun["intensity"]]) == ref["sun"]
+    assert bits(s.tris.view(np.float32).reshape(len(s.tris), 25)[:, :24]) == ref["tris"]
+    assert [int(m) for m in s.tris["material"]] == ref["mats"]
+    assert bits(s.mat_albedo) == ref["albedo"] and bits(s.mat_emissive) == ref["emissive"]
+    assert len(s.points) == ref["n_points"] and bits(s.points.view(np.float32)) == ref["points"]
+    assert len(s.directionals) == ref["n_directionals"]
+    assert bits(s.directionals.view(np.float32)) == ref["directionals"]
+
+
+def test_mock_scene_bvh_pins():
+    # The reference's test_bvh on scenes/mock_scene.json: 1 node, root bounds (-2,-2,0)..(2,2,5).
+    ref = json.loads((GOLD / "mock_scene_ref.json").read_text())
+    s = lumina.Scene.load_json(GOLD / "mock_scene.json")
+    nodes, _, _, _ = O.oracle_build_bvh(s.tris)
+    assert len(nodes) == ref["n_nodes"] == 1
+    assert nodes.view(np.uint32).ravel().tolist() == ref["bvh_nodes"]
+    assert list(nodes[0]["bbMin"]) == [-2, -2, 0] and list(nodes[0]["bbMax"]) == [2, 2, 5]
+
+
+def test_texture_path_and_escapes():
+    h = _ffi.C.c_void_p() if hasattr(_ffi, "C") else None
+    import ctypes as C
+    h = C.c_void_p()
+    _ffi.check(_ffi.lib().lg_scene_load_json(str(GOLD / "tricky_scene.json").encode(), 0, 1, C.byref(h)))
+    try:
+        assert _ffi.lib().lg_scene_texture(h, 0) == b""
+        assert _ffi.lib().lg_scene_texture(h, 1) == 'tex\\stone "a".png'.encode()
+    finally:
+        _ffi.lib().lg_scene_destroy(h)
+
+
+def test_round_trip_and_reference_reads_our_json(tmp_path, box_scene):
+    p = tmp_path / "box.json"
+    box_scene.save_json(p)
+    back = lumina.Scene.load_json(p, threads=4)
+    assert back.tris.tobytes() == box_scene.tris.tobytes()
+    assert back.mat_albedo.tobytes() == box_scene.mat_albedo.tobytes()
+    assert back.points.tobytes() == box_scene.points.tobytes()
+    assert np.array_equal(back.camera.camera_to_world, box_scene.camera.camera_to_world)
+    if O.ref_available():
+        r = O.ref_load_scene(str(p))
+        assert r["tris"].tobytes() == box_scene.tris.tobytes()
+
+
+def test_parallel_parse_equals_serial(tmp_path, small_engine_scene):
+    p = tmp_path / "eng.json"
+    small_engine_scene.save_json(p)
+    a = lumina.Scene.load_json(p, threads=1)
+    b = lumina.Scene.load_json(p, threads=8)
+    assert a.tris.tobytes() == b.tris.tobytes() == small_engine_scene.tris.tobytes()
+
+
+@pytest.mark.parametrize("text,code,needle", [
+    (None, _ffi.LG_ERR_IO, "failed to open"),
+    ('{"version": 1, "camera": {', _ffi.LG_ERR_PARSE, "JSON parse error"),
+    ('{"version": 2}', _ffi.LG_ERR_PARSE, "unsupported version 2"),
+    ('{"camera": {}}', _ffi.LG_ERR_PARSE, "unsupported version 0"),
+    ('{"version": 1, "sun": {}}', _ffi.LG_ERR_PARSE, "missing key"),
+    ('{"version": 1} trailing', _ffi.LG_ERR_PARSE, "JSON parse error"),
+])
+def test_loader_errors(tmp_path, text, code, needle):
+    p = tmp_path / "bad.json"
+    if text is not None:
+        p.write_text(text)
+    with pytest.raises(lumina.LuminaError) as e:
+        lumina.Scene.load_json(p)
+    assert e.value.code == code
+    assert needle in str(e.value)
+
+
+def test_png_and_hdr_writers(tmp_path):
+    from PIL import Image
+    rng = np.random.default_rng(0)
+    img = rng.integers(0, 256, (37, 53, 3), dtype=np.uint8)
+    p = tmp_path / "x.png"
+    _ffi.check(_ffi.lib().lg_write_png(str(p).encode(), 53, 37, _ffi.ptr(img)))
+    assert np.array_equal(np.asarray(Image.open(p).convert("RGB")), img)
+    lin = rng.uniform(0, 4, (5, 7, 3)).astype(np.float32)
+    q = tmp_path / "x.hdr"
+    _ffi.check(_ffi.lib().lg_write_hdr(str(q).encode(), 7, 5, _ffi.ptr(lin)))
+    data = q.read_bytes()
+    hdr_end = data.index(b"-Y 5 +X 7\n") + len(b"-Y 5 +X 7\n")
+    rgbe = np.frombuffer(data[hdr_end:], np.uint8).reshape(5, 7, 4).astype(np.float64)
+    dec = rgbe[..., :3] * np.ldexp(1.0, (rgbe[..., 3:4] - 136).astype(int))
+    # RGBE keeps 8 mantissa bits relative to the pixel's largest component.
+    assert (np.abs(dec - lin) <= lin.max(axis=2, keepdims=True) / 128.0).all()
+
+
+def test_look_at_matches_reference_formula():
+    cam = lumina.look_at_camera([1.0, 2.0, 3.0], [4.0, -2.0, 3.5], 64, 32)
+    f = np.array([3.0, -4.0, 0.5], np.float32)
+    f /= np.float32(np.sqrt(np.float32(f @ f)))
+    l = np.array([-f[1], f[0], 0.0], np.float32)
+    l /= np.float32(np.sqrt(np.float32(l @ l)))
+    m = cam.camera_to_world
+    assert np.allclose(m[0:3], f, atol=1e-7) and np.allclose(m[4:7], l, atol=1e-7)
+    assert np.allclose(m[8:11], np.cross(f, l), atol=1e-6) and np.allclose(m[12:15], [1, 2, 3])
+
+
+def test_abi_exports_every_declared_symbol():
+    header = (ROOT / "include" / "lumina.h").read_text()
+    declared = set(re.findall(r"\b(lg_[a-z0-9_]+)\s*\(", header))
+    assert len(declared) > 30
+    exported = subprocess.run(["nm", "-D", "--defined-only", str(_ffi.LIB_PATH)], capture_output=True,
+                              text=True).stdout
+    names = set(re.findall(r" T (lg_[a-z0-9_]+)", exported))
+    assert declared <= names, declared - names
+    assert declared <= set(_ffi.SIGNATURES), declared - set(_ffi.SIGNATURES)
+    lib = _ffi.lib()
+    assert lib.lg_version() >= 100
+
+
+def test_cli_usage_and_load_errors(tmp_path):
+    cli = str(_ffi.CLI_PATH)
+    r = subprocess.run([cli], capture_output=True, text=True)
+    assert r.returncode == 1 and "usage:" in r.stderr
+    r = subprocess.run([cli, str(tmp_path / "missing.json")], capture_output=True, text=True)
+    assert r.returncode == 2 and "[scene] failed to open" in r.stderr
+    bad = tmp_path / "v2.json"
+    bad.write_text('{"version": 2}')
+    r = subprocess.run([cli, str(bad)], capture_output=True, text=True)
+    assert r.returncode == 2 and "unsupported version 2" in r.stderr
