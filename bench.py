@@ -61,6 +61,7 @@ def parse_args():
     ap.add_argument("--bounces", type=int, default=2)
     ap.add_argument("--scene", default="engine", choices=["engine", "box"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-denoise", action="store_true", help="skip the 8spp+UNet vs 256spp timing")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
     return ap.parse_args()
 
@@ -150,6 +151,21 @@ def cpu_baseline(scene, nodes, tris, spp, bounces, target_s, impl_kind="referenc
             "ms_per_frame_scaled": dt * 1e3 * H / n_rows}
 
 
+def max_over_ranks(v: float, dist, device="cpu") -> float:
+    """The slowest rank's time (every rank takes the same collective steps)."""
+    if not dist:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(rays_per_frame: int, steps: int, world: int, ms_total_max: float) -> float:
+    """Whole-job Mrays/s of `world` replicas each rendering `steps` frames, timed by the slowest rank."""
+    return rays_per_frame * steps * world / (ms_total_max / 1e3) / 1e6
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -237,13 +253,9 @@ def main():
             step_device()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ms_total = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms_total], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist, f"cuda:{dev}")
     ms_step = ms_total / args.steps
-    value = rays * args.steps * world / (ms_total / 1e3) / 1e6
+    value = replica_throughput(rays, args.steps, world, ms_total)
 
     # kernel-only duration (events around trace + tonemap on the renderer's stream)
     kms = []
@@ -273,13 +285,46 @@ def main():
     for _ in range(args.steps):
         step_e2e()
     torch.cuda.synchronize(dev)
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, dist, f"cuda:{dev}")
     h2d = scene.tris.nbytes + scene.mat_albedo.nbytes + scene.points.nbytes
     d2h = W * H * 3
+
+    # Headline comparison on the same frame: 8 spp + UNet denoise vs the plain 256-spp render (device time).
+    denoise = None
+    if not args.no_denoise and args.scene == "engine":
+        net = lumina.UNet()
+        rng = np.random.default_rng(0)
+        net.set_params(rng.normal(0, 0.02, net.n_params).astype(np.float32))  # cost does not depend on the values
+        x = torch.empty((1, 3, H, W), device=f"cuda:{dev}")
+        y = torch.empty_like(x)
+        o8 = _ffi.LgRenderOpts(8, args.bounces, 0, 0)
+        o256 = _ffi.LgRenderOpts(256, args.bounces, 0, 0)
+        rgbp = C.c_void_p()
+
+        def step_denoised():
+            _ffi.check(_ffi.lib().lg_render_device(r._h, C.byref(cam), C.byref(o8), C.c_void_p(stream.cuda_stream),
+                                                   C.byref(rgbp), None, None))
+            _ffi.check(_ffi.lib().lg_rgb8_to_f32(rgbp, 1, H, W, C.c_void_p(x.data_ptr()),
+                                                C.c_void_p(stream.cuda_stream)))
+            net.forward_device(x.data_ptr(), 1, H, W, y.data_ptr(), stream.cuda_stream)
+
+        def timed(fn, reps):
+            fn()
+            torch.cuda.synchronize(dev)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(reps):
+                fn()
+            a1.record(stream)
+            torch.cuda.synchronize(dev)
+            return a0.elapsed_time(a1) / reps
+
+        ms_d = timed(step_denoised, 5)
+        ms_p = timed(lambda: _ffi.check(_ffi.lib().lg_render_device(
+            r._h, C.byref(cam), C.byref(o256), C.c_void_p(stream.cuda_stream), None, None, None)), 1)
+        denoise = {"ms_8spp_plus_unet": ms_d, "ms_256spp": ms_p, "speedup": ms_p / ms_d,
+                   "quality": "PSNR/SSIM vs a 1024-spp FP64 judge: profiles/surrogate_engine_1728x864.md"}
+        net.close()
 
     line = {"metric": "Mrays/s (plain render; ms/frame alongside)", "value": value, "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -294,6 +339,8 @@ def main():
                          "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
             "gpu_launches": args.steps * 2,
             "clocks": clk.summary()}
+    if denoise:
+        line["denoise"] = denoise
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(scene, nodes_dev, tris_dev, args.spp, args.bounces, args.cpu_seconds)

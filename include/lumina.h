@@ -207,6 +207,17 @@ int lg_conv3x3_device(const void* d_in, int n, int cin, int h, int w, const floa
 int lg_to_blocked_bf16(const float* d_x, int n, int c, int h, int w, void* d_out, int cpad, void* stream);
 int lg_from_blocked_bf16(const void* d_in, int n, int c, int h, int w, float* d_out, void* stream);
 
+/* ---- image plumbing between renderer and denoiser (device buffers) ---- */
+/* n frames of h*w*3 bytes (HWC) -> FP32 NCHW u8/255 (ml/train.py:102-103). */
+int lg_rgb8_to_f32(const uint8_t* d_rgb, int n, int h, int w, float* d_out, void* stream);
+/* FP32 NCHW -> h*w*3 bytes per frame: (u8)(clip(v,0,1)*255 + 0.5) (tools/denoise.py:51). */
+int lg_f32_to_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream);
+/* n_crops square crops (crop x crop, all 3 channels) of FP32 NCHW images
+ * (n_images x 3 x h x w) at host-given (img_idx, ys, xs) into d_out
+ * (n_crops x 3 x crop x crop). */
+int lg_gather_crops(const float* d_images, int n_images, int h, int w, const int32_t* img_idx, const int32_t* ys,
+                    const int32_t* xs, int n_crops, int crop, float* d_out, void* stream);
+
 /* ---- image output ---- */
 int lg_write_png(const char* path, int32_t w, int32_t h, const uint8_t* rgb8);
 int lg_write_hdr(const char* path, int32_t w, int32_t h, const float* rgb32);

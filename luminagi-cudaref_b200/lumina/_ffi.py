@@ -110,6 +110,9 @@ SIGNATURES = {
     "lg_conv3x3_device": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, C.c_float, _I, _P, _I, _I, _P, _I, _I, _P]),
     "lg_to_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _I, _P]),
     "lg_from_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _P]),
+    "lg_rgb8_to_f32": (_I, [_P, _I, _I, _I, _P, _P]),
+    "lg_f32_to_rgb8": (_I, [_P, _I, _I, _I, _P, _P]),
+    "lg_gather_crops": (_I, [_P, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P]),
     "lg_write_png": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
     "lg_write_hdr": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
 }
