@@ -145,6 +145,9 @@ int lg_renderer_set_scene_bvh(lg_renderer* r, const lg_scene_desc* scene, const 
 /* Copy back the device BVH (nodes_out may be NULL to query the count). */
 int lg_renderer_get_bvh(lg_renderer* r, lg_bvh_node* nodes_out, int32_t* n_nodes, lg_triangle* tris_out);
 int lg_renderer_set_counting(lg_renderer* r, int enable);
+/* Traversal records: 4 (default; two binary levels per 128-byte record) or 2
+ * (one binary node per 64-byte record).  Both traverse the same BVH. */
+int lg_renderer_set_bvh_width(lg_renderer* r, int width);
 /* Render one frame.  rgb8 (W*H*3 bytes) and accum (W*H*3 floats, sum over
  * samples as RenderSceneCUDA's accumulator) are host buffers; either may be
  * NULL.  accum64 (W*H*3 doubles) requires LG_RENDER_ACCUM64. */

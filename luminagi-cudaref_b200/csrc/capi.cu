@@ -101,9 +101,10 @@ struct lg_renderer
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool counting = false;
     // scene
-    int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0;
+    int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0, root4 = 0;
+    int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
     lg_dir_light sun{};
-    DevBuf tris, tris_in, nodes, wide, leaves, tv, mats, points, scratch;
+    DevBuf tris, tris_in, nodes, wide, wide4, leaves, tv, mats, points, scratch;
     // frame
     DevBuf accum, accum64, rgb, work, counters;
     int fw = 0, fh = 0;
@@ -167,11 +168,16 @@ int finish_scene(lg_renderer* r)
     LG_TRY(r->wide.reserve((size_t)r->n_nodes * sizeof(WideNode)));
     LG_TRY(r->leaves.reserve((size_t)r->n_nodes * sizeof(int2)));
     LG_TRY(r->tv.reserve((size_t)r->n_tris * 3 * sizeof(float4)));
-    size_t need = ((size_t)r->n_nodes * 2 + (size_t)r->n_nodes / 1024 + 8) * sizeof(int);
+    const size_t nb = (size_t)r->n_nodes / 1024 + 1;
+    size_t need = ((size_t)r->n_nodes * 6 + 2 * nb + 16) * sizeof(int);
     LG_TRY(r->scratch.reserve(need));
-    int root = 0, ni = 0, nl = 0;
+    LG_TRY(r->wide4.reserve(((size_t)r->n_nodes / 2 + 1) * sizeof(Wide4Node)));
+    int root = 0, ni = 0, nl = 0, root4 = 0, n4 = 0;
     LG_TRY_CUDA(build_wide_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide.as<WideNode>(),
                                  r->leaves.as<int2>(), r->scratch.as<int>(), &root, &ni, &nl, r->stream));
+    LG_TRY_CUDA(build_wide4_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide4.as<Wide4Node>(),
+                                  r->scratch.as<int>(), &root4, &n4, r->stream));
+    r->root4 = root4;
     LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
     r->root = root;
@@ -214,6 +220,8 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         s.points = r->points.as<lg_point_light>();
         s.n_points = r->n_points;
         s.root = r->root;
+        s.nodes4 = r->wide4.as<Wide4Node>();
+        s.root4 = r->root4;
         s.sun = r->sun;
         TraceJob job;
         job.spp = o->spp;
@@ -226,7 +234,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.accum64 = acc64 ? r->accum64.as<double>() : nullptr;
         job.work64 = r->work.as<unsigned long long>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
-        LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->stream));
+        LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->stream));
     }
     const float inv = 1.0f / (float)o->spp;
     LG_TRY_CUDA(launch_tonemap(r->accum.as<float>(), r->rgb.as<uint8_t>(), nval, inv, r->stream));
@@ -495,7 +503,7 @@ void lg_renderer_destroy(lg_renderer* r)
     if (!r) return;
     DeviceGuard g(r->device);
     if (r->stream) cudaStreamSynchronize(r->stream);
-    for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->leaves, &r->tv, &r->mats, &r->points,
+    for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
         b->release();
     if (r->ev0) cudaEventDestroy(r->ev0);
@@ -570,6 +578,14 @@ int lg_renderer_get_bvh(lg_renderer* r, lg_bvh_node* nodes_out, int32_t* n_nodes
         LG_TRY_CUDA(cudaMemcpyAsync(tris_out, r->tris.p, (size_t)r->n_tris * sizeof(lg_triangle),
                                     cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    return LG_OK;
+}
+
+int lg_renderer_set_bvh_width(lg_renderer* r, int width)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (width != 2 && width != 4) return set_error(LG_ERR_INVALID, "BVH width must be 2 or 4");
+    r->bvh_width = width;
     return LG_OK;
 }
 

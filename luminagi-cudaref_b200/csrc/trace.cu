@@ -146,6 +146,82 @@ __global__ void wide_kernel(const lg_bvh_node* __restrict__ nodes, int n, const 
     wide[dense[i]] = w;
 }
 
+// ---- 4-wide collapse ----
+__global__ void parent_kernel(const lg_bvh_node* __restrict__ nodes, int n, int* __restrict__ parent)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (i == 0) parent[0] = -1;
+    const lg_bvh_node nd = nodes[i];
+    if (nd.triCount == 0)
+    {
+        parent[nd.left] = i;
+        parent[nd.right] = i;
+    }
+}
+// is4[i] = internal node at even depth (depth by walking up; tree depth <= ~32).
+__global__ void even_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ parent,
+                            int* __restrict__ is4)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int d = 0;
+    for (int a = i; a != 0; a = parent[a]) ++d;
+    is4[i] = (nodes[i].triCount == 0 && (d & 1) == 0) ? 1 : 0;
+}
+// Per-block totals, scan and dense numbering are shared with build_wide_nodes
+// (count_kernel / scan_sums_kernel / dense_kernel).
+__device__ __forceinline__ void put_child(float (&lo)[3][4], float (&hi)[3][4], int (&ln)[4], int& k,
+                                          const lg_bvh_node& c, int link)
+{
+    for (int a = 0; a < 3; ++a)
+    {
+        lo[a][k] = c.bbMin[a];
+        hi[a][k] = c.bbMax[a];
+    }
+    ln[k] = link;
+    ++k;
+}
+__global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ is4,
+                             const int* __restrict__ dense4, const int* __restrict__ dense2,
+                             Wide4Node* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !is4[i]) return;
+    const lg_bvh_node nd = nodes[i];
+    float lo[3][4], hi[3][4];
+    int ln[4];
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < 4; ++k) { lo[a][k] = 1.0f; hi[a][k] = 0.0f; }
+    for (int k = 0; k < 4; ++k) ln[k] = kEmptyLink;
+    int k = 0;
+    const int cs[2] = {nd.left, nd.right};
+    for (int j = 0; j < 2; ++j)
+    {
+        const lg_bvh_node c = nodes[cs[j]];
+        if (c.triCount > 0) put_child(lo, hi, ln, k, c, ~dense2[cs[j]]);
+        else
+        {
+            const int gs[2] = {c.left, c.right};
+            for (int g = 0; g < 2; ++g)
+            {
+                const lg_bvh_node gc = nodes[gs[g]];
+                put_child(lo, hi, ln, k, gc, gc.triCount > 0 ? ~dense2[gs[g]] : dense4[gs[g]]);
+            }
+        }
+    }
+    Wide4Node w;
+    w.lox = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    w.hix = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    w.loy = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    w.hiy = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    w.loz = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    w.hiz = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    w.link = make_int4(ln[0], ln[1], ln[2], ln[3]);
+    w.pad = make_int4(0, 0, 0, 0);
+    out[dense4[i]] = w;
+}
+
 __global__ void tri_prep_kernel(const lg_triangle* __restrict__ tris, int n, float4* __restrict__ tv)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -214,6 +290,90 @@ struct Counters
 {
     unsigned long long closest, shadow, overflow, nodes, tris, leaves;
 };
+
+__device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
+{
+    if (tb < ta)
+    {
+        const float t = ta; ta = tb; tb = t;
+        const int l = la; la = lb; lb = l;
+    }
+}
+
+// The 4-wide form of the traversal below: one 128-byte record tests up to
+// four child boxes (same slab arithmetic); hit children are ordered by entry
+// distance, the nearest is entered and the rest stacked nearest-on-top.
+template <bool kCount>
+__device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
+                                         float& bestU, float& bestV, Counters& cnt)
+{
+    int stack[kStack];
+    int sp = 0;
+    int cur = s.root4;
+    int bestTri = -1;
+    bestT = tmax;
+    bestU = 0.0f;
+    bestV = 0.0f;
+    if (kCount) { if (anyhit) cnt.shadow++; else cnt.closest++; }
+    for (;;)
+    {
+        if (cur >= 0)
+        {
+            if (kCount) cnt.nodes++;
+            const Wide4Node* nd = &s.nodes4[cur];
+            const float4 lx = __ldg(&nd->lox), hx = __ldg(&nd->hix);
+            const float4 ly = __ldg(&nd->loy), hy = __ldg(&nd->hiy);
+            const float4 lz = __ldg(&nd->loz), hz = __ldg(&nd->hiz);
+            const int4 ln = __ldg(&nd->link);
+            const float inf = __int_as_float(0x7f800000);
+            float t0 = inf, t1 = inf, t2 = inf, t3 = inf;
+            float te;
+            if (ln.x != kEmptyLink && slab(r, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, bestT, te)) t0 = te;
+            if (ln.y != kEmptyLink && slab(r, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, bestT, te)) t1 = te;
+            if (ln.z != kEmptyLink && slab(r, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, bestT, te)) t2 = te;
+            if (ln.w != kEmptyLink && slab(r, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, bestT, te)) t3 = te;
+            int l0 = ln.x, l1 = ln.y, l2 = ln.z, l3 = ln.w;
+            cswap(t0, l0, t1, l1);
+            cswap(t2, l2, t3, l3);
+            cswap(t0, l0, t2, l2);
+            cswap(t1, l1, t3, l3);
+            cswap(t1, l1, t2, l2);
+            if (t0 != inf)
+            {
+                // push farthest first so the nearest remaining is on top
+                if (t3 != inf) { if (sp < kStack) stack[sp++] = l3; else if (kCount) cnt.overflow++; }
+                if (t2 != inf) { if (sp < kStack) stack[sp++] = l2; else if (kCount) cnt.overflow++; }
+                if (t1 != inf) { if (sp < kStack) stack[sp++] = l1; else if (kCount) cnt.overflow++; }
+                cur = l0;
+                continue;
+            }
+        }
+        else
+        {
+            const int2 lf = __ldg(&s.leaves[~cur]);
+            if (kCount) { cnt.leaves++; }
+            bool done = false;
+            for (int i = 0; i < lf.y; ++i)
+            {
+                const int ti = lf.x + i;
+                float tt, uu, vv;
+                if (kCount) cnt.tris++;
+                if (tri_hit(r, s.tv, ti, bestT, tt, uu, vv))
+                {
+                    bestT = tt;
+                    bestTri = ti;
+                    bestU = uu;
+                    bestV = vv;
+                    if (anyhit) { done = true; break; }
+                }
+            }
+            if (done) break;
+        }
+        if (sp == 0) break;
+        cur = stack[--sp];
+    }
+    return bestTri;
+}
 
 // One traversal loop serves closest-hit rays (traverse_closest, :109-160)
 // and shadow rays (traverse_occluded, :162-191): the nearer child is taken
@@ -465,8 +625,8 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
 // the loop is one warp-wide traversal (camera, bounce or shadow ray per lane)
 // followed by a short state update.  Items are numbered chunk-major, then by
 // 8x4 pixel tile, so neighbouring lanes start on neighbouring pixels.
-template <bool kCount, bool kAcc64, int kMinBlocks = kTraceMinBlocks>
-__global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
+template <bool kCount, bool kAcc64, int kWidth>
+__global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -515,7 +675,8 @@ __global__ void __launch_bounds__(kTraceThreads, kMinBlocks) trace_kernel(DevSce
         if (active)
         {
             float hitT, hitU, hitV;
-            const int tri = traverse<kCount>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
+            const int tri = kWidth == 4 ? traverse4<kCount>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt)
+                                        : traverse<kCount>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
             if (!advance(st, s, cam, job.max_bounces, tri, hitT, hitU, hitV))
             {
                 active = false;
@@ -622,6 +783,36 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
     return cudaSuccess;
 }
 
+cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node* d_wide4, int* d_scratch,
+                              int* root4_host, int* n4_host, cudaStream_t stream)
+{
+    // scratch: [is_internal | dense2 | block_sums] from build_wide_nodes, then [parent | is4 | dense4 | sums4]
+    const int nb = (n_nodes + kScanTB - 1) / kScanTB;
+    const int* dense2 = d_scratch + n_nodes;
+    int* parent = d_scratch + 2 * (size_t)n_nodes + nb + 8;
+    int* is4 = parent + n_nodes;
+    int* dense4 = is4 + n_nodes;
+    int* sums4 = dense4 + n_nodes;
+    const int tb = 256, g = (n_nodes + tb - 1) / tb;
+    parent_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, parent);
+    even_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, parent, is4);
+    count_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4);
+    scan_sums_kernel<<<1, kScanTB, 0, stream>>>(sums4, nb);
+    dense_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4, dense4);
+    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, d_wide4);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    int root_is4 = 0, last_d = 0, last_v = 0;
+    e = cudaMemcpyAsync(&root_is4, is4, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_d, dense4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_v, is4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    *root4_host = root_is4 ? 0 : ~0;
+    *n4_host = last_v ? last_d + 1 : -1;  // count is only needed for sizing checks
+    return cudaSuccess;
+}
+
 cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cudaStream_t stream)
 {
     if (n <= 0) return cudaSuccess;
@@ -629,12 +820,12 @@ cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cu
     return cudaGetLastError();
 }
 
-template <int MB>
-static cudaError_t launch_trace_mb(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
-                                  cudaStream_t stream)
+template <int W>
+static cudaError_t launch_trace_w(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
+                                 cudaStream_t stream)
 {
-    const void* fn = count ? (job.accum64 ? (const void*)trace_kernel<true, true, MB> : (const void*)trace_kernel<true, false, MB>)
-                           : (job.accum64 ? (const void*)trace_kernel<false, true, MB> : (const void*)trace_kernel<false, false, MB>);
+    const void* fn = count ? (job.accum64 ? (const void*)trace_kernel<true, true, W> : (const void*)trace_kernel<true, false, W>)
+                           : (job.accum64 ? (const void*)trace_kernel<false, true, W> : (const void*)trace_kernel<false, false, W>);
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, 0);
     if (e != cudaSuccess) return e;
@@ -648,23 +839,25 @@ static cudaError_t launch_trace_mb(const DevScene& s, const DevCam& cam, const T
     const int g = (int)blocks;
     if (count)
     {
-        if (job.accum64) trace_kernel<true, true, MB><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
-        else trace_kernel<true, false, MB><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
+        if (job.accum64) trace_kernel<true, true, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
+        else trace_kernel<true, false, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
     }
     else
     {
-        if (job.accum64) trace_kernel<false, true, MB><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
-        else trace_kernel<false, false, MB><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
+        if (job.accum64) trace_kernel<false, true, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
+        else trace_kernel<false, false, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
     }
     return cudaGetLastError();
 }
 
 // Four 256-thread blocks per SM (64 registers) measured fastest on B200:
-// 653 ms per 64-spp engine-scale frame vs 745 ms at three and 1007 ms at two.
+// 653 ms per 64-spp engine-scale frame (binary nodes) vs 745 ms at three
+// and 1007 ms at two.
 cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
-                         cudaStream_t stream)
+                         int width, cudaStream_t stream)
 {
-    return launch_trace_mb<kTraceMinBlocks>(s, cam, job, count, sm_count, stream);
+    if (width == 4) return launch_trace_w<4>(s, cam, job, count, sm_count, stream);
+    return launch_trace_w<2>(s, cam, job, count, sm_count, stream);
 }
 
 cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,

@@ -22,8 +22,22 @@ struct alignas(16) WideNode
 };
 static_assert(sizeof(WideNode) == 64, "WideNode is one 64-byte record");
 
+// A 4-wide node collapsed from two levels of the binary BVH: the boxes of up
+// to four children, struct-of-arrays in one 128-byte line (eight 16-byte
+// loads).  Links as in WideNode; kEmptyLink marks an absent child.
+struct alignas(16) Wide4Node
+{
+    float4 lox, hix, loy, hiy, loz, hiz;  // child i in component i
+    int4 link;
+    int4 pad;
+};
+static_assert(sizeof(Wide4Node) == 128, "Wide4Node is one 128-byte line");
+constexpr int kEmptyLink = 0x7fffffff;
+
 struct DevScene
 {
+    const Wide4Node* nodes4;   // 4-wide records (used when width == 4)
+    int root4;
     const WideNode* nodes;
     const int2* leaves;        // (first triangle, count)
     const float4* tv;          // 3 per triangle: v0 (w = material bits), e1 = v1-v0, e2 = v2-v0
@@ -72,10 +86,16 @@ DevCam make_dev_cam(const lg_camera& c);
 cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* d_wide, int2* d_leaves,
                              int* d_scratch, int* root_host, int* n_internal_host, int* n_leaves_host,
                              cudaStream_t stream);
+// Collapses the binary BVH (BFS order) into 4-wide records: every internal
+// node at even depth becomes a record whose children are its grandchildren
+// (or its children, when those are leaves).  Must follow build_wide_nodes on
+// the same scratch (it reuses the leaf numbering).  Scratch: 5 * n_nodes ints.
+cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node* d_wide4, int* d_scratch,
+                              int* root4_host, int* n4_host, cudaStream_t stream);
 cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cudaStream_t stream);
 
 cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
-                         cudaStream_t stream);
+                         int width, cudaStream_t stream);
 cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,
                            cudaStream_t stream);
 cudaError_t launch_accum64_to_32(const double* d_acc64, float* d_acc32, long long n_values, cudaStream_t stream);

@@ -91,6 +91,7 @@ SIGNATURES = {
     "lg_renderer_set_scene_bvh": (_I, [_P, C.POINTER(LgSceneDesc), _P, C.c_int32]),
     "lg_renderer_get_bvh": (_I, [_P, _P, C.POINTER(C.c_int32), _P]),
     "lg_renderer_set_counting": (_I, [_P, _I]),
+    "lg_renderer_set_bvh_width": (_I, [_P, _I]),
     "lg_render": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, _P, C.POINTER(LgRenderStats)]),
     "lg_render_device": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, C.POINTER(_P), C.POINTER(_P),
                               C.POINTER(_P)]),

@@ -1,0 +1,93 @@
+"""Device-timed micro-benchmarks of the library's kernels.
+
+    python -m lumina.perf unet  [--n 1] [--h 864] [--w 1728] [--reps 10]
+    python -m lumina.perf trace [--spp 8] [--bounces 2] [--width 4] [--reps 2]
+    python -m lumina.perf bvh   [--reps 5]
+
+Prints one JSON line.  Used for the profiles (run under ncu) and for quick
+A/B measurements; bench.py is the benchmark of record.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+
+def _events(torch):
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def unet(a):
+    import torch
+
+    from .unet import UNet
+    net = UNet()
+    net.set_params(np.random.default_rng(5).normal(0, 0.02, net.n_params).astype(np.float32))
+    x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
+    y = torch.empty_like(x)
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        net.forward_device(x.data_ptr(), a.n, a.h, a.w, y.data_ptr(), st.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = _events(torch)
+    e0.record(st)
+    for _ in range(a.reps):
+        net.forward_device(x.data_ptr(), a.n, a.h, a.w, y.data_ptr(), st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.reps
+    flops = 2 * 162240 * a.n * a.h * a.w
+    return {"kernel": "unet_forward", "n": a.n, "h": a.h, "w": a.w, "ms": ms, "tflops": flops / ms / 1e9}
+
+
+def trace(a):
+    from .render import Renderer
+    from .scene import engine_scene
+    sc = engine_scene(seed=7)
+    r = Renderer(0)
+    r.set_scene(sc)
+    r.set_bvh_width(a.width)
+    r.set_counting(True)
+    c = r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)
+    r.set_counting(False)
+    rays = c["closest_rays"] + c["shadow_rays"]
+    ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for _ in range(a.reps)]
+    return {"kernel": "trace", "spp": a.spp, "width": a.width, "ms": ms, "rays": rays,
+            "mrays_per_s": rays / min(ms) / 1e3, "nodes_per_ray": c["node_fetches"] / rays,
+            "tris_per_ray": c["tri_tests"] / rays}
+
+
+def bvh(a):
+    import time
+
+    from .render import build_bvh
+    from .scene import engine_scene
+    sc = engine_scene(seed=7)
+    build_bvh(sc.tris)
+    t = []
+    for _ in range(a.reps):
+        t0 = time.perf_counter()
+        build_bvh(sc.tris)
+        t.append((time.perf_counter() - t0) * 1e3)
+    return {"kernel": "lbvh (host in/out, incl. 105 MB upload and download)", "triangles": sc.n_tris,
+            "ms": t}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["unet", "trace", "bvh"])
+    ap.add_argument("--n", type=int, default=1)
+    ap.add_argument("--h", type=int, default=864)
+    ap.add_argument("--w", type=int, default=1728)
+    ap.add_argument("--spp", type=int, default=8)
+    ap.add_argument("--bounces", type=int, default=2)
+    ap.add_argument("--width", type=int, default=4)
+    ap.add_argument("--reps", type=int, default=10)
+    a = ap.parse_args(argv)
+    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh}[a.what](a)))
+
+
+if __name__ == "__main__":
+    main()

@@ -71,6 +71,10 @@ class Renderer:
         check(lib().lg_renderer_get_bvh(self._h, ptr(nodes), C.byref(n), ptr(tris)))
         return nodes, tris
 
+    def set_bvh_width(self, width: int) -> None:
+        """Traversal records: 4-wide (default) or 2-wide; same BVH, same hits."""
+        check(lib().lg_renderer_set_bvh_width(self._h, int(width)))
+
     def set_counting(self, on: bool) -> None:
         check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))
 

@@ -41,3 +41,24 @@ def test_tonemap_matches_oracle():
     import oracle as O
     acc = np.random.default_rng(2).uniform(-0.5, 3.0, (8, 9, 3)).astype(np.float32)
     assert np.array_equal(M.tonemap_u8(acc), O.oracle_tonemap(acc, 1))
+
+
+def test_diff_report_cli(tmp_path):
+    import subprocess
+    import sys
+    from PIL import Image
+    rng = np.random.default_rng(4)
+    a = rng.integers(0, 256, (24, 40, 3), dtype=np.uint8)
+    b = np.clip(a.astype(int) + rng.integers(-3, 4, a.shape), 0, 255).astype(np.uint8)
+    pa, pb = tmp_path / "a.png", tmp_path / "b.png"
+    Image.fromarray(a).save(pa)
+    Image.fromarray(b).save(pb)
+    out = tmp_path / "r.html"
+    pkg = pathlib.Path(__file__).resolve().parent.parent / "luminagi-cudaref_b200"
+    r = subprocess.run([sys.executable, "-m", "lumina.diff", str(pa), str(pb), "--out", str(out)], cwd=pkg,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert f"PSNR {M.psnr(a, b):.2f} dB | SSIM {M.ssim(a, b):.4f} | MAD {M.mad(a, b):.2f}" in r.stdout
+    assert out.exists() and out.with_suffix(".heatmap.png").exists()
+    heat = np.asarray(Image.open(out.with_suffix(".heatmap.png")))
+    assert heat.shape == (24, 40, 3)

@@ -18,31 +18,34 @@ def match_fraction(a, b):
     return float(close.all(axis=2).mean())
 
 
-def render_ours(scene, nodes, tris, spp, bounces, camera=None, **kw):
+def render_ours(scene, nodes, tris, spp, bounces, camera=None, width=4, **kw):
     sc = lumina.Scene(scene.camera, scene.sun, tris, scene.mat_albedo, scene.mat_emissive, scene.points)
     with lumina.Renderer(0) as r:
         r.set_scene_bvh(sc, nodes)
+        r.set_bvh_width(width)
         return r.render(camera=camera, spp=spp, bounces=bounces, **kw)
 
 
+@pytest.mark.parametrize("width", [2, 4])
 @pytest.mark.parametrize("spp,bounces", [(1, 0), (8, 2), (20, 2)])
-def test_box_scene_vs_reference_gpu(box_scene, spp, bounces):
+def test_box_scene_vs_reference_gpu(box_scene, spp, bounces, width):
     if not O.ref_available():
         pytest.skip("reference oracle not built")
     nodes, tris, _, _ = O.oracle_build_bvh(box_scene.tris)
-    ours = render_ours(box_scene, nodes, tris, spp, bounces)
+    ours = render_ours(box_scene, nodes, tris, spp, bounces, width=width)
     ref_acc, ref_rgb, _ = O.ref_render_gpu(box_scene, nodes, tris, spp, bounces)
     f = match_fraction(ours["accum"], ref_acc)
     assert f >= 0.999, f
     assert float((ours["rgb"] == ref_rgb).all(axis=2).mean()) >= 0.999
 
 
-def test_engine_small_vs_reference_gpu(small_engine_scene):
+@pytest.mark.parametrize("width", [2, 4])
+def test_engine_small_vs_reference_gpu(small_engine_scene, width):
     if not O.ref_available():
         pytest.skip("reference oracle not built")
     sc = small_engine_scene
     nodes, tris, _, _ = O.oracle_build_bvh(sc.tris)
-    ours = render_ours(sc, nodes, tris, 64, 2)
+    ours = render_ours(sc, nodes, tris, 64, 2, width=width)
     ref_acc, ref_rgb, _ = O.ref_render_gpu(sc, nodes, tris, 64, 2)
     assert match_fraction(ours["accum"], ref_acc) >= 0.999
 
