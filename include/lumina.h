@@ -162,6 +162,12 @@ int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
 int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts* opts, int32_t n_jobs,
                     uint8_t* rgb8_out, float* ms_per_job);
 
+/* gbuffer_kernel (src/pathtracer.cu:366-411): primary hit through each pixel
+ * centre; albedo, normal*0.5+0.5 and world position normalised by the BVH root
+ * box, each W*H*3 bytes (host buffers, any may be NULL).  Misses give albedo 0,
+ * normal (128,128,255), position 0. */
+int lg_render_gbuffer(lg_renderer* r, const lg_camera* cam, uint8_t* albedo, uint8_t* normal, uint8_t* worldpos);
+
 /* tonemap_kernel: rgb8 = (u8)(sqrt(clamp(accum*inv_spp, 0, 1)) * 255). */
 int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, float inv_spp, void* stream);
 

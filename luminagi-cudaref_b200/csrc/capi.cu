@@ -103,6 +103,8 @@ struct lg_renderer
     // scene
     int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0, root4 = 0;
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
+    lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
+    DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     lg_dir_light sun{};
     DevBuf tris, tris_in, nodes, wide, wide4, leaves, tv, mats, points, scratch;
     // frame
@@ -178,6 +180,7 @@ int finish_scene(lg_renderer* r)
     LG_TRY_CUDA(build_wide4_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide4.as<Wide4Node>(),
                                   r->scratch.as<int>(), &root4, &n4, r->stream));
     r->root4 = root4;
+    LG_TRY_CUDA(cudaMemcpyAsync(&r->root_node, r->nodes.p, sizeof(lg_bvh_node), cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
     r->root = root;
@@ -197,6 +200,23 @@ int ensure_frame(lg_renderer* r, int w, int h, bool acc64)
     return LG_OK;
 }
 
+DevScene dev_scene(const lg_renderer* r)
+{
+    DevScene s;
+    s.nodes = r->wide.as<WideNode>();
+    s.leaves = r->leaves.as<int2>();
+    s.tv = r->tv.as<float4>();
+    s.tris = r->tris.as<lg_triangle>();
+    s.mats = r->mats.as<float4>();
+    s.points = r->points.as<lg_point_light>();
+    s.n_points = r->n_points;
+    s.root = r->root;
+    s.nodes4 = r->wide4.as<Wide4Node>();
+    s.root4 = r->root4;
+    s.sun = r->sun;
+    return s;
+}
+
 int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* o, lg_render_stats* stats)
 {
     if (!r || !cam || !o) return set_error(LG_ERR_INVALID, "NULL argument");
@@ -211,18 +231,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
     LG_TRY_CUDA(cudaEventRecord(r->ev0, r->stream));
     if (o->spp > 0 && r->n_nodes > 0)
     {
-        DevScene s;
-        s.nodes = r->wide.as<WideNode>();
-        s.leaves = r->leaves.as<int2>();
-        s.tv = r->tv.as<float4>();
-        s.tris = r->tris.as<lg_triangle>();
-        s.mats = r->mats.as<float4>();
-        s.points = r->points.as<lg_point_light>();
-        s.n_points = r->n_points;
-        s.root = r->root;
-        s.nodes4 = r->wide4.as<Wide4Node>();
-        s.root4 = r->root4;
-        s.sun = r->sun;
+        const DevScene s = dev_scene(r);
         TraceJob job;
         job.spp = o->spp;
         job.max_bounces = o->max_bounces;
@@ -503,6 +512,7 @@ void lg_renderer_destroy(lg_renderer* r)
     if (!r) return;
     DeviceGuard g(r->device);
     if (r->stream) cudaStreamSynchronize(r->stream);
+    r->gbuf.release();
     for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
         b->release();
@@ -664,6 +674,39 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
     return LG_OK;
 }
 
+int lg_render_gbuffer(lg_renderer* r, const lg_camera* cam, uint8_t* albedo, uint8_t* normal, uint8_t* worldpos)
+{
+    if (!r || !cam) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (cam->width <= 0 || cam->height <= 0) return set_error(LG_ERR_INVALID, "image size %dx%d", cam->width, cam->height);
+    DeviceGuard g(r->device);
+    const size_t n = (size_t)cam->width * cam->height * 3;
+    LG_TRY(r->gbuf.reserve(3 * n));
+    uint8_t* base = r->gbuf.as<uint8_t>();
+    if (r->n_nodes == 0)
+    {
+        // nothing to hit: every pixel is a miss
+        LG_TRY_CUDA(cudaMemsetAsync(base, 0, 3 * n, r->stream));
+        std::vector<uint8_t> miss(n);
+        for (size_t i = 0; i < n; i += 3) { miss[i] = 128; miss[i + 1] = 128; miss[i + 2] = 255; }
+        LG_TRY_CUDA(cudaMemcpyAsync(base + n, miss.data(), n, cudaMemcpyHostToDevice, r->stream));
+    }
+    else
+    {
+        // Scene box from the BVH root, inverse extent clamped at 1e-6 (pathtracer.cu:728-734).
+        const lg_bvh_node& root = r->root_node;
+        const vec3 bbMin = v3(root.bbMin[0], root.bbMin[1], root.bbMin[2]);
+        const vec3 ext = vsub(v3(root.bbMax[0], root.bbMax[1], root.bbMax[2]), bbMin);
+        const vec3 inv = v3(1.0f / std::max(ext.x, 1e-6f), 1.0f / std::max(ext.y, 1e-6f), 1.0f / std::max(ext.z, 1e-6f));
+        LG_TRY_CUDA(launch_gbuffer(dev_scene(r), make_dev_cam(*cam), bbMin, inv, base, base + n, base + 2 * n,
+                                   r->bvh_width, r->stream));
+    }
+    if (albedo) LG_TRY_CUDA(cudaMemcpyAsync(albedo, base, n, cudaMemcpyDeviceToHost, r->stream));
+    if (normal) LG_TRY_CUDA(cudaMemcpyAsync(normal, base + n, n, cudaMemcpyDeviceToHost, r->stream));
+    if (worldpos) LG_TRY_CUDA(cudaMemcpyAsync(worldpos, base + 2 * n, n, cudaMemcpyDeviceToHost, r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    return LG_OK;
+}
+
 int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, float inv_spp, void* stream)
 {
     if ((!d_accum || !d_rgb8) && n_pixels > 0) return set_error(LG_ERR_INVALID, "NULL argument");
@@ -741,8 +784,8 @@ lg_scene_desc desc_of(const Scene& s, std::vector<float>& alb)
 }  // namespace
 
 // Same signature as the reference (declared in its main.cpp:19-24).  The
-// G-buffer outputs are not produced (filled with zeros) and textures are not
-// sampled; both are reported on stderr when requested.
+// G-buffer images are produced when all three outputs are given (as the
+// reference does, pathtracer.cu:726-747).
 void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& assetRoot, int spp, int maxBounces,
                      std::vector<uint8_t>& outRGB, int& outW, int& outH, std::vector<uint8_t>* outAlbedo,
                      std::vector<uint8_t>* outNormal, std::vector<uint8_t>* outWorldPos)
@@ -773,5 +816,11 @@ void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& asse
     else
         std::printf("kernel: %.1f ms  (%d x %d, %d spp, %d bounces, %zu tris)\n", st.kernel_ms, outW, outH, spp,
                     maxBounces, scene.triangles.size());
+    if (rc == LG_OK && outAlbedo && outNormal && outWorldPos)
+    {
+        lg_camera cam = d.camera;
+        rc = lg_render_gbuffer(r, &cam, outAlbedo->data(), outNormal->data(), outWorldPos->data());
+        if (rc != LG_OK) std::fprintf(stderr, "gbuffer failed: %s\n", lg_last_error());
+    }
     lg_renderer_destroy(r);
 }

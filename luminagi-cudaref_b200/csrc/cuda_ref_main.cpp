@@ -11,8 +11,9 @@
 // (1 usage, 2 scene load, 3 PNG write) follow main.cpp:93-229.  The scene is
 // uploaded and its BVH built on the device once; batch jobs only change the
 // camera.  --sort is accepted and ignored (one trace path serves both).
-// --gbuffer is accepted but no auxiliary images are written (reported on
-// stderr).  --hdr additionally writes the linear radiance (accum / spp).
+// --gbuffer also writes <stem>.albedo.png, <stem>.normal.png and
+// <stem>.worldpos.png (main.cpp:177-184, 220-227).  --hdr additionally writes
+// the linear radiance (accum / spp).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -61,6 +62,23 @@ std::vector<BatchJob> read_batch_file(const std::string& path)
 double ms_since(std::chrono::steady_clock::time_point t0)
 {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// <dir>/<stem>.albedo.png etc. next to the colour image.
+void write_gbuffer(lg_renderer* r, const lg_camera& cam, const std::string& png)
+{
+    const size_t n = (size_t)cam.width * cam.height * 3;
+    std::vector<uint8_t> alb(n), nrm(n), wp(n);
+    if (lg_render_gbuffer(r, &cam, alb.data(), nrm.data(), wp.data()) != LG_OK)
+    {
+        std::fprintf(stderr, "gbuffer: %s\n", lg_last_error());
+        return;
+    }
+    std::filesystem::path p(png);
+    const std::string stem = (p.parent_path() / p.stem()).string();
+    lg_write_png((stem + ".albedo.png").c_str(), cam.width, cam.height, alb.data());
+    lg_write_png((stem + ".normal.png").c_str(), cam.width, cam.height, nrm.data());
+    lg_write_png((stem + ".worldpos.png").c_str(), cam.width, cam.height, wp.data());
 }
 
 void make_parent_dirs(const std::string& p)
@@ -113,7 +131,6 @@ int main(int argc, char** argv)
                      argv[0]);
         return 1;
     }
-    if (gbuffer) std::fprintf(stderr, "note: --gbuffer auxiliary images are not produced by this build\n");
 
     lg_scene* scene = nullptr;
     if (lg_scene_load_json(jsonPath, 1, 0, &scene) != LG_OK) return 2;
@@ -178,6 +195,7 @@ int main(int argc, char** argv)
             const double ms = ms_since(t0);
             make_parent_dirs(j.out_png);
             lg_write_png(j.out_png.c_str(), W, H, rgb.data());
+            if (gbuffer) write_gbuffer(r, cam, j.out_png);
             std::printf("[%zu/%zu] %s  spp=%d  render=%.1f ms\n", k + 1, jobs.size(), j.out_png.c_str(), j.spp, ms);
         }
         lg_renderer_destroy(r);
@@ -200,6 +218,11 @@ int main(int argc, char** argv)
     std::printf("kernel: %.1f ms  (%d x %d, %d spp, %d bounces, %d tris)\n", st.kernel_ms, W, H, spp, bounces,
                 desc.n_tris);
     std::printf("render: %.1f ms (%d x %d)\n", ms_since(t2), W, H);
+    if (gbuffer)
+    {
+        make_parent_dirs(pngPath);
+        write_gbuffer(r, desc.camera, pngPath);
+    }
     lg_renderer_destroy(r);
     if (lg_write_png(pngPath.c_str(), W, H, rgb.data()) != LG_OK)
     {

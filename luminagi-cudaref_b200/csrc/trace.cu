@@ -725,6 +725,53 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
     }
 }
 
+// gbuffer_kernel (:366-411): primary hit through the pixel centre; albedo,
+// encoded normal and box-normalised world position as 8-bit RGB.
+__device__ __forceinline__ uint8_t enc8(float v) { return (uint8_t)(fminf(1.0f, fmaxf(0.0f, v)) * 255.0f); }
+
+template <int kWidth>
+__global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* __restrict__ albedo_out,
+                               uint8_t* __restrict__ normal_out, uint8_t* __restrict__ worldpos_out)
+{
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= cam.width || py >= cam.height) return;
+    Ray r = primary_ray(cam, px, py, 0.5f, 0.5f);
+    float hitT, hitU, hitV;
+    Counters cnt{0, 0, 0, 0, 0, 0};
+    const int tri = kWidth == 4 ? traverse4<false>(s, r, 1e30f, false, hitT, hitU, hitV, cnt)
+                                : traverse<false>(s, r, 1e30f, false, hitT, hitU, hitV, cnt);
+    const size_t i = ((size_t)py * cam.width + px) * 3;
+    if (tri < 0)
+    {
+        albedo_out[i + 0] = albedo_out[i + 1] = albedo_out[i + 2] = 0;
+        normal_out[i + 0] = 128;
+        normal_out[i + 1] = 128;
+        normal_out[i + 2] = 255;
+        worldpos_out[i + 0] = worldpos_out[i + 1] = worldpos_out[i + 2] = 0;
+        return;
+    }
+    const lg_triangle& t = s.tris[tri];
+    float w = 1.0f - hitU - hitV;
+    vec3 N = normalize(v3(w * t.n[0][0] + hitU * t.n[1][0] + hitV * t.n[2][0],
+                          w * t.n[0][1] + hitU * t.n[1][1] + hitV * t.n[2][1],
+                          w * t.n[0][2] + hitU * t.n[1][2] + hitV * t.n[2][2]));
+    if (dot(N, r.d) > 0.0f) N = vmul(N, -1.0f);
+    const int mat = __float_as_int(__ldg(&s.tv[3 * tri].w));
+    const float4 a = __ldg(&s.mats[mat]);
+    albedo_out[i + 0] = enc8(a.x);
+    albedo_out[i + 1] = enc8(a.y);
+    albedo_out[i + 2] = enc8(a.z);
+    normal_out[i + 0] = enc8(N.x * 0.5f + 0.5f);
+    normal_out[i + 1] = enc8(N.y * 0.5f + 0.5f);
+    normal_out[i + 2] = enc8(N.z * 0.5f + 0.5f);
+    vec3 P = vadd(r.o, vmul(r.d, hitT));
+    vec3 Pn = vhad(vsub(P, bbMin), bbInvExtent);
+    worldpos_out[i + 0] = enc8(Pn.x);
+    worldpos_out[i + 1] = enc8(Pn.y);
+    worldpos_out[i + 2] = enc8(Pn.z);
+}
+
 // tonemap_kernel (:413-429), one value per thread.
 __global__ void tonemap_kernel(const float* __restrict__ accum, uint8_t* __restrict__ rgb, long long n, float invSpp)
 {
@@ -858,6 +905,16 @@ cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& j
 {
     if (width == 4) return launch_trace_w<4>(s, cam, job, count, sm_count, stream);
     return launch_trace_w<2>(s, cam, job, count, sm_count, stream);
+}
+
+cudaError_t launch_gbuffer(const DevScene& s, const DevCam& cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* d_albedo,
+                           uint8_t* d_normal, uint8_t* d_worldpos, int width, cudaStream_t stream)
+{
+    dim3 block(16, 16);
+    dim3 grid((cam.width + 15) / 16, (cam.height + 15) / 16);
+    if (width == 4) gbuffer_kernel<4><<<grid, block, 0, stream>>>(s, cam, bbMin, bbInvExtent, d_albedo, d_normal, d_worldpos);
+    else gbuffer_kernel<2><<<grid, block, 0, stream>>>(s, cam, bbMin, bbInvExtent, d_albedo, d_normal, d_worldpos);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,

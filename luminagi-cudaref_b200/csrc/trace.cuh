@@ -96,6 +96,9 @@ cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cu
 
 cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
                          int width, cudaStream_t stream);
+// Primary-hit G-buffer (albedo, encoded normal, box-normalised position), W*H*3 bytes each.
+cudaError_t launch_gbuffer(const DevScene& s, const DevCam& cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* d_albedo,
+                           uint8_t* d_normal, uint8_t* d_worldpos, int width, cudaStream_t stream);
 cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,
                            cudaStream_t stream);
 cudaError_t launch_accum64_to_32(const double* d_acc64, float* d_acc32, long long n_values, cudaStream_t stream);

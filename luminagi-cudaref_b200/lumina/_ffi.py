@@ -97,6 +97,7 @@ SIGNATURES = {
                               C.POINTER(_P)]),
     "lg_render_batch": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), C.c_int32, _P, _P]),
     "lg_tonemap_device": (_I, [_P, _P, C.c_int64, C.c_float, _P]),
+    "lg_render_gbuffer": (_I, [_P, C.POINTER(LgCamera), _P, _P, _P]),
     "lg_unet_create": (_I, [_I, _I, _I, C.POINTER(_P)]),
     "lg_unet_destroy": (None, [_P]),
     "lg_unet_num_params": (C.c_int64, [_P]),

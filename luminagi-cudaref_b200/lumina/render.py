@@ -97,6 +97,15 @@ class Renderer:
                 "node_fetches": int(st.node_fetches), "tri_tests": int(st.tri_tests),
                 "leaf_fetches": int(st.leaf_fetches)}
 
+    def gbuffer(self, camera: Camera | None = None):
+        """Primary-hit (albedo, normal, worldpos) 8-bit images (reference gbuffer_kernel)."""
+        cam = camera if camera is not None else self.scene.camera
+        c = cam.to_c()
+        H, W = int(cam.height), int(cam.width)
+        out = [np.zeros((H, W, 3), np.uint8) for _ in range(3)]
+        check(lib().lg_render_gbuffer(self._h, C.byref(c), ptr(out[0]), ptr(out[1]), ptr(out[2])))
+        return tuple(out)
+
     def render_batch(self, cameras, spps, bounces):
         """Renders several frames (per-job camera/spp/bounces); returns (rgb (J,H,W,3), ms per job)."""
         J = len(cameras)

@@ -209,3 +209,22 @@ def ref_render_gpu(scene, nodes, tris, spp, bounces, camera=None):
 
 def ref_omp_threads() -> int:
     return rlib().ref_omp_max_threads()
+
+
+def ref_gbuffer_gpu(scene, nodes, tris, camera=None):
+    """The reference gbuffer_kernel on the GPU; returns (albedo, normal, worldpos) (H,W,3) u8."""
+    cam = camera if camera is not None else scene.camera
+    H, W = int(cam.height), int(cam.width)
+    out = [np.zeros((H, W, 3), np.uint8) for _ in range(3)]
+    c = cam_desc(cam)
+    sun = _sun(scene)
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    tris = np.ascontiguousarray(tris, TRI_DTYPE)
+    alb = np.ascontiguousarray(scene.mat_albedo, np.float32)
+    emi = np.ascontiguousarray(scene.mat_emissive, np.float32)
+    pts = np.ascontiguousarray(scene.points, POINT_DTYPE)
+    rc = rlib().ref_gbuffer_gpu(_p(nodes), len(nodes), _p(tris), len(tris), _p(alb), _p(emi), len(alb), _p(pts),
+                                len(pts), _p(sun), C.byref(c), _p(out[0]), _p(out[1]), _p(out[2]))
+    if rc != 0:
+        raise RuntimeError(f"reference G-buffer failed with CUDA error {rc}")
+    return tuple(out)

@@ -265,4 +265,70 @@ done:
 #undef RCHK
 }
 
+// ---- G-buffer with the reference gbuffer_kernel, box from the root node as
+// RenderSceneCUDA computes it (pathtracer.cu:726-747).  Node buffer padded as above.
+int ref_gbuffer_gpu(const BvhNode* nodes, int nNodes, const Triangle* tris, int nTris, const float* matAlbedo,
+                    const float* matEmissive, int nMats, const PointLight* points, int nPoints,
+                    const DirectionalLight* sun, const CameraDesc* camDesc, uint8_t* albHost, uint8_t* nrmHost,
+                    uint8_t* wpHost)
+{
+#define RCHK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { rc = (int)e_; goto done; } } while (0)
+    int rc = 0;
+    std::vector<DeviceMaterial> mats = make_mats(matAlbedo, matEmissive, nMats);
+    const CameraGPU cam = make_cam(*camDesc);
+    const int W = cam.width, H = cam.height;
+    const size_t imgBytes = (size_t)W * H * 3;
+    const int nPad = nNodes < kShmemBvhNodes ? kShmemBvhNodes : nNodes;
+    BvhNode* d_nodes = nullptr;
+    Triangle* d_tris = nullptr;
+    DeviceMaterial* d_mats = nullptr;
+    PointLight* d_points = nullptr;
+    uint8_t *d_alb = nullptr, *d_nrm = nullptr, *d_wp = nullptr;
+    DeviceScene s{};
+    dim3 block(16, 16);
+    dim3 grid((W + 15) / 16, (H + 15) / 16);
+    const BvhNode& root = nodes[0];
+    vec3 bbMin = v3(root.bbMin[0], root.bbMin[1], root.bbMin[2]);
+    vec3 bbMax = v3(root.bbMax[0], root.bbMax[1], root.bbMax[2]);
+    vec3 ext = vsub(bbMax, bbMin);
+    vec3 invExt = v3(1.0f / fmaxf(ext.x, 1e-6f), 1.0f / fmaxf(ext.y, 1e-6f), 1.0f / fmaxf(ext.z, 1e-6f));
+    RCHK(cudaMalloc(&d_nodes, (size_t)nPad * sizeof(BvhNode)));
+    RCHK(cudaMemset(d_nodes, 0, (size_t)nPad * sizeof(BvhNode)));
+    RCHK(cudaMemcpy(d_nodes, nodes, (size_t)nNodes * sizeof(BvhNode), cudaMemcpyHostToDevice));
+    RCHK(cudaMalloc(&d_tris, (size_t)(nTris > 0 ? nTris : 1) * sizeof(Triangle)));
+    if (nTris) RCHK(cudaMemcpy(d_tris, tris, (size_t)nTris * sizeof(Triangle), cudaMemcpyHostToDevice));
+    RCHK(cudaMalloc(&d_mats, (size_t)(nMats > 0 ? nMats : 1) * sizeof(DeviceMaterial)));
+    if (nMats) RCHK(cudaMemcpy(d_mats, mats.data(), (size_t)nMats * sizeof(DeviceMaterial), cudaMemcpyHostToDevice));
+    if (nPoints)
+    {
+        RCHK(cudaMalloc(&d_points, (size_t)nPoints * sizeof(PointLight)));
+        RCHK(cudaMemcpy(d_points, points, (size_t)nPoints * sizeof(PointLight), cudaMemcpyHostToDevice));
+    }
+    RCHK(cudaMalloc(&d_alb, imgBytes));
+    RCHK(cudaMalloc(&d_nrm, imgBytes));
+    RCHK(cudaMalloc(&d_wp, imgBytes));
+    s.nodes = d_nodes;
+    s.tris = d_tris;
+    s.mats = d_mats;
+    s.points = d_points;
+    s.numPoints = nPoints;
+    s.sun = *sun;
+    gbuffer_kernel<<<grid, block>>>(s, cam, bbMin, invExt, d_alb, d_nrm, d_wp);
+    RCHK(cudaGetLastError());
+    RCHK(cudaDeviceSynchronize());
+    RCHK(cudaMemcpy(albHost, d_alb, imgBytes, cudaMemcpyDeviceToHost));
+    RCHK(cudaMemcpy(nrmHost, d_nrm, imgBytes, cudaMemcpyDeviceToHost));
+    RCHK(cudaMemcpy(wpHost, d_wp, imgBytes, cudaMemcpyDeviceToHost));
+done:
+    cudaFree(d_nodes);
+    cudaFree(d_tris);
+    cudaFree(d_mats);
+    cudaFree(d_points);
+    cudaFree(d_alb);
+    cudaFree(d_nrm);
+    cudaFree(d_wp);
+    return rc;
+#undef RCHK
+}
+
 }  // extern "C"

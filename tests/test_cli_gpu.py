@@ -91,3 +91,19 @@ def test_denoise_rgb8_contract():
     # BF16 summation-order noise is ~0.4 of an 8-bit step (see test_unet_forward_matches_torch).
     diff = np.abs(got.astype(int) - ref.astype(int))
     assert diff.max() <= 6 and np.mean(diff <= 1) > 0.95
+
+
+def test_gbuffer_outputs(small_box):
+    """--gbuffer writes <stem>.albedo/.normal/.worldpos.png beside the colour image (main.cpp:177-184)."""
+    sc, p, d = small_box
+    out = d / "g" / "frame.png"
+    r = subprocess.run([str(_ffi.CLI_PATH), str(p), str(out), "--spp", "1", "--bounces", "0", "--gbuffer"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    with lumina.Renderer(0) as rr:
+        rr.set_scene(sc)
+        ref = rr.gbuffer()
+    for name, img in zip(("albedo", "normal", "worldpos"), ref):
+        f = d / "g" / f"frame.{name}.png"
+        assert f.exists()
+        assert np.array_equal(_png(f), img)
