@@ -79,7 +79,17 @@ int lg_scene_set_camera(lg_scene* s, const lg_camera* cam);
 int lg_scene_save_json(const lg_scene* s, const char* path);
 /* Material texture path (may be ""), owned by s. */
 const char* lg_scene_texture(const lg_scene* s, int material);
+/* Sets a material's texture path (the JSON "diffuse_tex" value). */
+int lg_scene_set_texture(lg_scene* s, int material, const char* path);
 void lg_scene_destroy(lg_scene* s);
+
+/* ---- images ----
+ * lg_image_load: stbi_load(path, &w, &h, &n, 4) as load_texture_to_device
+ * uses it (src/pathtracer.cu:553-560), for PNG files (every colour type, bit
+ * depth and interlace mode): 8-bit RGBA, top row first.  *rgba8 is released
+ * with lg_image_free. */
+int lg_image_load(const char* path, int32_t* w, int32_t* h, uint8_t** rgba8);
+void lg_image_free(uint8_t* rgba8);
 
 /* overwrite_camera (src/main.cpp:29-59): forward = normalize(target-pos),
  * left = normalize(-fy, fx, 0) (fallback +Y), up = forward x left.
@@ -148,6 +158,16 @@ int lg_renderer_set_counting(lg_renderer* r, int enable);
 /* Traversal records: 4 (default; two binary levels per 128-byte record) or 2
  * (one binary node per 64-byte record).  Both traverse the same BVH. */
 int lg_renderer_set_bvh_width(lg_renderer* r, int width);
+/* Diffuse texture of one material (load_texture_to_device + sample_albedo,
+ * src/pathtracer.cu:553-579, 274-282): w x h RGBA8 host pixels, sampled as
+ * sRGB with bilinear filtering and wrapping at uv (u, 1 - v).  rgba8 = NULL
+ * removes it.  Setting a scene clears every texture. */
+int lg_renderer_set_texture(lg_renderer* r, int material, const uint8_t* rgba8, int32_t w, int32_t h);
+/* Loads each material's "diffuse_tex" from asset_root + "/" + path
+ * (RenderSceneCUDA, src/pathtracer.cu:597-613); files that cannot be read
+ * count as missing.  s must be the scene the renderer holds. */
+int lg_renderer_load_textures(lg_renderer* r, const lg_scene* s, const char* asset_root, int32_t* loaded,
+                              int32_t* missing);
 /* Render one frame.  rgb8 (W*H*3 bytes) and accum (W*H*3 floats, sum over
  * samples as RenderSceneCUDA's accumulator) are host buffers; either may be
  * NULL.  accum64 (W*H*3 doubles) requires LG_RENDER_ACCUM64. */

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -23,6 +24,7 @@ bool load_scene_file(const std::string& path, Scene& out, bool verbose, int thre
 bool save_scene_file(const Scene& sc, const std::string& path, int threads);
 bool write_png(const char* path, int w, int h, const uint8_t* rgb);
 bool write_hdr(const char* path, int w, int h, const float* rgb);
+bool decode_png(const char* path, int& w, int& h, std::vector<uint8_t>& rgba, std::string& err);
 
 namespace
 {
@@ -105,6 +107,11 @@ struct lg_renderer
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
+    // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
+    std::vector<cudaArray_t> tex_arrays;
+    std::vector<unsigned long long> tex_objs;  // cudaTextureObject_t, 0 = untextured
+    DevBuf texs;                               // device copy of tex_objs
+    int n_textured = 0;
     lg_dir_light sun{};
     DevBuf tris, tris_in, nodes, wide, wide4, leaves, tv, mats, points, scratch;
     // frame
@@ -146,9 +153,22 @@ int validate_scene(const lg_scene_desc* d)
     return LG_OK;
 }
 
+void clear_textures(lg_renderer* r)
+{
+    for (unsigned long long t : r->tex_objs)
+        if (t) cudaDestroyTextureObject((cudaTextureObject_t)t);
+    for (cudaArray_t a : r->tex_arrays)
+        if (a) cudaFreeArray(a);
+    r->tex_objs.assign((size_t)r->n_mats, 0ull);
+    r->tex_arrays.assign((size_t)r->n_mats, nullptr);
+    r->n_textured = 0;
+}
+
 int upload_common(lg_renderer* r, const lg_scene_desc* d)
 {
+    if (r->stream) cudaStreamSynchronize(r->stream);
     r->n_mats = d->n_mats;
+    clear_textures(r);  // a new scene starts untextured
     r->n_points = d->n_points;
     r->sun = d->sun;
     std::vector<float4> m((size_t)std::max(d->n_mats, 1));
@@ -208,6 +228,7 @@ DevScene dev_scene(const lg_renderer* r)
     s.tv = r->tv.as<float4>();
     s.tris = r->tris.as<lg_triangle>();
     s.mats = r->mats.as<float4>();
+    s.texs = r->n_textured ? r->texs.as<unsigned long long>() : nullptr;
     s.points = r->points.as<lg_point_light>();
     s.n_points = r->n_points;
     s.root = r->root;
@@ -393,7 +414,37 @@ const char* lg_scene_texture(const lg_scene* s, int material)
     return s->s.materials[(size_t)material].diffuseTex.c_str();
 }
 
+int lg_scene_set_texture(lg_scene* s, int material, const char* path)
+{
+    if (!s || !path) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (material < 0 || material >= (int)s->s.materials.size())
+        return set_error(LG_ERR_INVALID, "material %d out of range", material);
+    s->s.materials[(size_t)material].diffuseTex = path;
+    return LG_OK;
+}
+
 void lg_scene_destroy(lg_scene* s) { delete s; }
+
+// ---- images ----
+int lg_image_load(const char* path, int32_t* w, int32_t* h, uint8_t** rgba8)
+{
+    if (!path || !w || !h || !rgba8) return set_error(LG_ERR_INVALID, "NULL argument");
+    *rgba8 = nullptr;
+    std::vector<uint8_t> px;
+    std::string err;
+    int iw = 0, ih = 0;
+    if (!decode_png(path, iw, ih, px, err))
+        return set_error(err == "cannot open" ? LG_ERR_IO : LG_ERR_PARSE, "%s: %s", path, err.c_str());
+    uint8_t* out = (uint8_t*)std::malloc(px.size());
+    if (!out) return set_error(LG_ERR_NOMEM, "out of memory");
+    std::memcpy(out, px.data(), px.size());
+    *w = iw;
+    *h = ih;
+    *rgba8 = out;
+    return LG_OK;
+}
+
+void lg_image_free(uint8_t* rgba8) { std::free(rgba8); }
 
 // overwrite_camera (reference main.cpp:29-59).
 void lg_look_at(lg_camera* cam, const float pos[3], const float tgt[3])
@@ -512,6 +563,9 @@ void lg_renderer_destroy(lg_renderer* r)
     if (!r) return;
     DeviceGuard g(r->device);
     if (r->stream) cudaStreamSynchronize(r->stream);
+    r->n_mats = 0;
+    clear_textures(r);
+    r->texs.release();
     r->gbuf.release();
     for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
@@ -596,6 +650,86 @@ int lg_renderer_set_bvh_width(lg_renderer* r, int width)
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
     if (width != 2 && width != 4) return set_error(LG_ERR_INVALID, "BVH width must be 2 or 4");
     r->bvh_width = width;
+    return LG_OK;
+}
+
+int lg_renderer_set_texture(lg_renderer* r, int material, const uint8_t* rgba8, int32_t w, int32_t h)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (material < 0 || material >= r->n_mats) return set_error(LG_ERR_INVALID, "material %d out of range", material);
+    if (rgba8 && (w <= 0 || h <= 0)) return set_error(LG_ERR_INVALID, "texture size %dx%d", w, h);
+    DeviceGuard g(r->device);
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    const size_t m = (size_t)material;
+    if (r->tex_objs[m])
+    {
+        cudaDestroyTextureObject((cudaTextureObject_t)r->tex_objs[m]);
+        cudaFreeArray(r->tex_arrays[m]);
+        r->tex_objs[m] = 0;
+        r->tex_arrays[m] = nullptr;
+        --r->n_textured;
+    }
+    if (rgba8)
+    {
+        // uchar4 array read as sRGB, normalised float, bilinear, wrapping (pathtracer.cu:562-576).
+        cudaChannelFormatDesc fmt = cudaCreateChannelDesc<uchar4>();
+        cudaArray_t arr = nullptr;
+        LG_TRY_CUDA(cudaMallocArray(&arr, &fmt, (size_t)w, (size_t)h));
+        cudaError_t e = cudaMemcpy2DToArray(arr, 0, 0, rgba8, (size_t)w * 4, (size_t)w * 4, (size_t)h,
+                                            cudaMemcpyHostToDevice);
+        cudaResourceDesc res{};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = cudaAddressModeWrap;
+        td.addressMode[1] = cudaAddressModeWrap;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = cudaReadModeNormalizedFloat;
+        td.normalizedCoords = 1;
+        td.sRGB = 1;
+        cudaTextureObject_t obj = 0;
+        if (e == cudaSuccess) e = cudaCreateTextureObject(&obj, &res, &td, nullptr);
+        if (e != cudaSuccess)
+        {
+            cudaFreeArray(arr);
+            return set_error(LG_ERR_CUDA, "texture upload: %s", cudaGetErrorString(e));
+        }
+        r->tex_arrays[m] = arr;
+        r->tex_objs[m] = (unsigned long long)obj;
+        ++r->n_textured;
+    }
+    LG_TRY(r->texs.reserve((size_t)std::max(r->n_mats, 1) * sizeof(unsigned long long)));
+    LG_TRY_CUDA(cudaMemcpy(r->texs.p, r->tex_objs.data(), (size_t)r->n_mats * sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice));
+    return LG_OK;
+}
+
+int lg_renderer_load_textures(lg_renderer* r, const lg_scene* s, const char* asset_root, int32_t* loaded,
+                              int32_t* missing)
+{
+    if (!r || !s || !asset_root) return set_error(LG_ERR_INVALID, "NULL argument");
+    if ((int)s->s.materials.size() != r->n_mats)
+        return set_error(LG_ERR_INVALID, "scene has %zu materials, renderer %d", s->s.materials.size(), r->n_mats);
+    int nl = 0, nm = 0;
+    for (int m = 0; m < r->n_mats; ++m)
+    {
+        const std::string& rel = s->s.materials[(size_t)m].diffuseTex;
+        if (rel.empty()) continue;
+        const std::string full = std::string(asset_root) + "/" + rel;
+        int32_t w = 0, h = 0;
+        uint8_t* px = nullptr;
+        if (lg_image_load(full.c_str(), &w, &h, &px) != LG_OK)
+        {
+            ++nm;
+            continue;
+        }
+        const int rc = lg_renderer_set_texture(r, m, px, w, h);
+        lg_image_free(px);
+        LG_TRY(rc);
+        ++nl;
+    }
+    if (loaded) *loaded = nl;
+    if (missing) *missing = nm;
     return LG_OK;
 }
 
@@ -790,7 +924,6 @@ void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& asse
                      std::vector<uint8_t>& outRGB, int& outW, int& outH, std::vector<uint8_t>* outAlbedo,
                      std::vector<uint8_t>* outNormal, std::vector<uint8_t>* outWorldPos)
 {
-    (void)assetRoot;
     outW = scene.camera.imageWidth;
     outH = scene.camera.imageHeight;
     outRGB.assign((size_t)outW * outH * 3, 0);
@@ -805,6 +938,29 @@ void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& asse
     if (rc == LG_OK)
         rc = lg_renderer_set_scene_bvh(r, &d, reinterpret_cast<const lg_bvh_node*>(bvh.nodes.data()),
                                        (int32_t)bvh.nodes.size());
+    if (rc == LG_OK)
+    {
+        // Textures resolved against assetRoot and reported as the reference does (pathtracer.cu:597-613).
+        int loaded = 0, missing = 0;
+        for (size_t m = 0; m < scene.materials.size() && rc == LG_OK; ++m)
+        {
+            const std::string& rel = scene.materials[m].diffuseTex;
+            if (rel.empty()) continue;
+            const std::string full = assetRoot + "/" + rel;
+            int32_t w = 0, h = 0;
+            uint8_t* px = nullptr;
+            if (lg_image_load(full.c_str(), &w, &h, &px) != LG_OK)
+            {
+                std::fprintf(stderr, "  texture not found: %s\n", full.c_str());
+                ++missing;
+                continue;
+            }
+            rc = lg_renderer_set_texture(r, (int)m, px, w, h);
+            lg_image_free(px);
+            ++loaded;
+        }
+        std::printf("textures: %d loaded, %d missing (of %zu materials)\n", loaded, missing, scene.materials.size());
+    }
     lg_render_stats st{};
     if (rc == LG_OK)
     {

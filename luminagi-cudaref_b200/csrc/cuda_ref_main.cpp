@@ -11,7 +11,8 @@
 // (1 usage, 2 scene load, 3 PNG write) follow main.cpp:93-229.  The scene is
 // uploaded and its BVH built on the device once; batch jobs only change the
 // camera.  --sort is accepted and ignored (one trace path serves both).
-// --gbuffer also writes <stem>.albedo.png, <stem>.normal.png and
+// Diffuse textures resolve against --asset-root (default: the scene file's
+// grandparent directory, main.cpp:140-141).  --gbuffer also writes <stem>.albedo.png, <stem>.normal.png and
 // <stem>.worldpos.png (main.cpp:177-184, 220-227).  --hdr additionally writes
 // the linear radiance (accum / spp).
 #include <chrono>
@@ -81,6 +82,31 @@ void write_gbuffer(lg_renderer* r, const lg_camera& cam, const std::string& png)
     lg_write_png((stem + ".worldpos.png").c_str(), cam.width, cam.height, wp.data());
 }
 
+// Diffuse textures from <assetRoot>/<diffuse_tex>, reported as RenderSceneCUDA
+// does (pathtracer.cu:597-613); unreadable files leave the material untextured.
+void load_textures(lg_renderer* r, lg_scene* scene, int n_mats, const std::string& assetRoot)
+{
+    int loaded = 0, missing = 0;
+    for (int m = 0; m < n_mats; ++m)
+    {
+        const std::string rel = lg_scene_texture(scene, m);
+        if (rel.empty()) continue;
+        const std::string full = assetRoot + "/" + rel;
+        int32_t w = 0, h = 0;
+        uint8_t* px = nullptr;
+        if (lg_image_load(full.c_str(), &w, &h, &px) != LG_OK)
+        {
+            std::fprintf(stderr, "  texture not found: %s\n", full.c_str());
+            ++missing;
+            continue;
+        }
+        if (lg_renderer_set_texture(r, m, px, w, h) != LG_OK) std::fprintf(stderr, "%s\n", lg_last_error());
+        else ++loaded;
+        lg_image_free(px);
+    }
+    std::printf("textures: %d loaded, %d missing (of %d materials)\n", loaded, missing, n_mats);
+}
+
 void make_parent_dirs(const std::string& p)
 {
     std::error_code ec;
@@ -136,12 +162,7 @@ int main(int argc, char** argv)
     if (lg_scene_load_json(jsonPath, 1, 0, &scene) != LG_OK) return 2;
     lg_scene_desc desc;
     lg_scene_describe(scene, &desc);
-    for (int m = 0; m < desc.n_mats; ++m)
-        if (lg_scene_texture(scene, m)[0])
-        {
-            std::fprintf(stderr, "note: diffuse textures are not sampled by this build (material %d)\n", m);
-            break;
-        }
+    if (assetRoot.empty()) assetRoot = std::filesystem::path(jsonPath).parent_path().parent_path().string();
 
     if (haveCamPos && haveCamTgt)
     {
@@ -166,6 +187,7 @@ int main(int argc, char** argv)
         return 4;
     }
     const double bvh_ms = ms_since(t_bvh0);
+    load_textures(r, scene, desc.n_mats, assetRoot);
     int32_t n_nodes = 0;
     lg_renderer_get_bvh(r, nullptr, &n_nodes, nullptr);
     const int W = desc.camera.width, H = desc.camera.height;

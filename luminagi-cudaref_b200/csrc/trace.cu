@@ -531,6 +531,29 @@ __device__ __forceinline__ bool light_query(const DevScene& s, int li, vec3 P, v
     return true;
 }
 
+// sample_albedo (:274-282) at a hit: the material's diffuse texture at the
+// interpolated uv (traverse_closest's expressions, :156-157) with v flipped,
+// else the material's constant albedo.  The texture objects are created
+// as the reference creates them (uchar4 array, sRGB, bilinear, wrap,
+// normalised coordinates), so the texture unit filters identically.
+__device__ __forceinline__ vec3 hit_albedo(const DevScene& s, const lg_triangle& t, int mat, float w, float hitU,
+                                           float hitV)
+{
+    if (s.texs)
+    {
+        const unsigned long long tx = __ldg(&s.texs[mat]);
+        if (tx)
+        {
+            const float u = w * t.uv[0][0] + hitU * t.uv[1][0] + hitV * t.uv[2][0];
+            const float v = w * t.uv[0][1] + hitU * t.uv[1][1] + hitV * t.uv[2][1];
+            const float4 c = tex2D<float4>((cudaTextureObject_t)tx, u, 1.0f - v);
+            return v3(c.x, c.y, c.z);
+        }
+    }
+    const float4 alb = __ldg(&s.mats[mat]);
+    return v3(alb.x, alb.y, alb.z);
+}
+
 // Per-lane path state of the chunk being traced (accumulate_kernel's sample
 // loop, :352-358, and trace_path, :295-331, unrolled into a state machine).
 struct PathState
@@ -575,8 +598,7 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
             st.N = N;
             st.P = vadd(st.ray.o, vmul(st.ray.d, hitT));
             const int mat = __float_as_int(__ldg(&s.tv[3 * tri].w));
-            const float4 alb = __ldg(&s.mats[mat]);
-            st.albedo = v3(alb.x, alb.y, alb.z);
+            st.albedo = hit_albedo(s, t, mat, w, hitU, hitV);
             st.color = v3(0, 0, 0);
         }
     }
@@ -758,7 +780,7 @@ __global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExt
                           w * t.n[0][2] + hitU * t.n[1][2] + hitV * t.n[2][2]));
     if (dot(N, r.d) > 0.0f) N = vmul(N, -1.0f);
     const int mat = __float_as_int(__ldg(&s.tv[3 * tri].w));
-    const float4 a = __ldg(&s.mats[mat]);
+    const vec3 a = hit_albedo(s, t, mat, w, hitU, hitV);
     albedo_out[i + 0] = enc8(a.x);
     albedo_out[i + 1] = enc8(a.y);
     albedo_out[i + 2] = enc8(a.z);

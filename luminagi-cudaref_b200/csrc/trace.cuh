@@ -43,6 +43,7 @@ struct DevScene
     const float4* tv;          // 3 per triangle: v0 (w = material bits), e1 = v1-v0, e2 = v2-v0
     const lg_triangle* tris;   // shading data (normals), BVH order
     const float4* mats;        // albedo
+    const unsigned long long* texs;  // per material: diffuse texture object or 0; nullptr when none is set
     const lg_point_light* points;
     int n_points;
     int root;                  // root link (0 = internal record 0, < 0 = leaf)

@@ -80,7 +80,10 @@ SIGNATURES = {
     "lg_scene_set_camera": (_I, [_P, C.POINTER(LgCamera)]),
     "lg_scene_save_json": (_I, [_P, C.c_char_p]),
     "lg_scene_texture": (C.c_char_p, [_P, _I]),
+    "lg_scene_set_texture": (_I, [_P, _I, C.c_char_p]),
     "lg_scene_destroy": (None, [_P]),
+    "lg_image_load": (_I, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.POINTER(C.c_uint8))]),
+    "lg_image_free": (None, [C.POINTER(C.c_uint8)]),
     "lg_look_at": (None, [C.POINTER(LgCamera), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "lg_build_bvh": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P]),
     "lg_build_bvh_device": (_I, [_P, C.c_int32, _P, C.POINTER(C.c_int32), _P, _P, _P]),
@@ -92,6 +95,8 @@ SIGNATURES = {
     "lg_renderer_get_bvh": (_I, [_P, _P, C.POINTER(C.c_int32), _P]),
     "lg_renderer_set_counting": (_I, [_P, _I]),
     "lg_renderer_set_bvh_width": (_I, [_P, _I]),
+    "lg_renderer_set_texture": (_I, [_P, _I, _P, C.c_int32, C.c_int32]),
+    "lg_renderer_load_textures": (_I, [_P, _P, C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "lg_render": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, _P, C.POINTER(LgRenderStats)]),
     "lg_render_device": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, C.POINTER(_P), C.POINTER(_P),
                               C.POINTER(_P)]),

@@ -75,6 +75,29 @@ class Renderer:
         """Traversal records: 4-wide (default) or 2-wide; same BVH, same hits."""
         check(lib().lg_renderer_set_bvh_width(self._h, int(width)))
 
+    def set_texture(self, material: int, rgba) -> None:
+        """Diffuse texture of one material: (H,W,4) u8 RGBA, or None to remove it."""
+        if rgba is None:
+            check(lib().lg_renderer_set_texture(self._h, int(material), None, 0, 0))
+            return
+        rgba = np.ascontiguousarray(rgba, np.uint8)
+        assert rgba.ndim == 3 and rgba.shape[2] == 4, "texture must be (H, W, 4) uint8"
+        check(lib().lg_renderer_set_texture(self._h, int(material), ptr(rgba), rgba.shape[1], rgba.shape[0]))
+
+    def load_textures(self, asset_root: str):
+        """Loads the scene's textures from asset_root/<diffuse_tex>; returns (loaded, missing)."""
+        from .image import load_image
+        loaded = missing = 0
+        for m, rel in enumerate(self.scene.textures if self.scene is not None else []):
+            if not rel:
+                continue
+            try:
+                self.set_texture(m, load_image(f"{asset_root}/{rel}"))
+                loaded += 1
+            except OSError:
+                missing += 1
+        return loaded, missing
+
     def set_counting(self, on: bool) -> None:
         check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))
 

@@ -64,6 +64,7 @@ class Scene:
     mat_emissive: np.ndarray  # (M, 3) f32
     points: np.ndarray  # POINT_DTYPE (P,)
     directionals: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0, DIR_DTYPE))
+    textures: list = dataclasses.field(default_factory=list)  # per material "diffuse_tex" ('' = none)
 
     def __post_init__(self):
         self.tris = np.ascontiguousarray(self.tris, TRI_DTYPE)
@@ -96,6 +97,9 @@ class Scene:
         d = self.desc()
         check(lib().lg_scene_create(C.byref(d), C.byref(h)))
         try:
+            for m, t in enumerate(self.textures):
+                if t:
+                    check(lib().lg_scene_set_texture(h, m, str(t).encode()))
             check(lib().lg_scene_save_json(h, str(path).encode()))
         finally:
             lib().lg_scene_destroy(h)
@@ -108,7 +112,9 @@ class Scene:
         try:
             d = LgSceneDesc()
             check(lib().lg_scene_describe(h, C.byref(d)))
-            return Scene._from_desc(d)
+            sc = Scene._from_desc(d)
+            sc.textures = [lib().lg_scene_texture(h, m).decode() for m in range(d.n_mats)]
+            return sc
         finally:
             lib().lg_scene_destroy(h)
 

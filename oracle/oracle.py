@@ -228,3 +228,22 @@ def ref_gbuffer_gpu(scene, nodes, tris, camera=None):
     if rc != 0:
         raise RuntimeError(f"reference G-buffer failed with CUDA error {rc}")
     return tuple(out)
+
+
+def ref_set_textures(paths):
+    """Per-material texture files for ref_render_gpu / ref_gbuffer_gpu ('' or None: untextured)."""
+    arr = (C.c_char_p * max(len(paths), 1))(*[(p or "").encode() for p in paths])
+    rlib().ref_set_textures(len(paths), arr)
+
+
+def ref_image_load(path):
+    """stbi_load(path, 4 channels) as the reference uses it; returns (H,W,4) u8 or None."""
+    L = rlib()
+    w, h = C.c_int(), C.c_int()
+    out = C.POINTER(C.c_uint8)()
+    if L.ref_image_load(str(path).encode(), C.byref(w), C.byref(h), C.byref(out)) != 0:
+        return None
+    try:
+        return np.ctypeslib.as_array(out, shape=(h.value, w.value, 4)).copy()
+    finally:
+        L.ref_image_free(out)

@@ -189,6 +189,27 @@ int ref_trace_cpu(const BvhNode* nodes, const Triangle* tris, const float* matAl
 
 int ref_omp_max_threads(void) { return omp_get_max_threads(); }
 
+// ---- textures: per-material file paths used by the GPU entry points below
+// (load_texture_to_device, pathtracer.cu:553-579, on each non-empty path).
+static std::vector<std::string> g_texPaths;
+
+void ref_set_textures(int nMats, const char* const* paths)
+{
+    g_texPaths.assign((size_t)(nMats > 0 ? nMats : 0), std::string());
+    for (int i = 0; i < nMats && paths; ++i)
+        if (paths[i]) g_texPaths[(size_t)i] = paths[i];
+}
+
+// stbi_load(path, &w, &h, &n, 4) as the reference calls it; *out is freed with ref_image_free.
+int ref_image_load(const char* path, int* w, int* h, unsigned char** out)
+{
+    int n = 0;
+    *out = stbi_load(path, w, h, &n, 4);
+    return *out ? 0 : 1;
+}
+
+void ref_image_free(unsigned char* p) { stbi_image_free(p); }
+
 // ---- GPU render with the reference kernels, launched as RenderSceneCUDA
 // launches them.  The node buffer is padded to at least 255 nodes because
 // accumulate_kernel stages nodes[0..254] into shared memory unconditionally
@@ -202,6 +223,10 @@ int ref_render_gpu(const BvhNode* nodes, int nNodes, const Triangle* tris, int n
 #define RCHK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { rc = (int)e_; goto done; } } while (0)
     int rc = 0;
     std::vector<DeviceMaterial> mats = make_mats(matAlbedo, matEmissive, nMats);
+    std::vector<cudaArray_t> texArrays((size_t)(nMats > 0 ? nMats : 0), nullptr);
+    for (int i = 0; i < nMats && i < (int)g_texPaths.size(); ++i)
+        if (!g_texPaths[(size_t)i].empty() && !load_texture_to_device(g_texPaths[(size_t)i], texArrays[(size_t)i], mats[(size_t)i].tex))
+            mats[(size_t)i].tex = 0;
     const CameraGPU cam = make_cam(*camDesc);
     const int W = cam.width, H = cam.height;
     const int nPad = nNodes < kShmemBvhNodes ? kShmemBvhNodes : nNodes;
@@ -261,6 +286,8 @@ done:
     cudaFree(d_points);
     cudaFree(d_accum);
     cudaFree(d_image);
+    for (size_t i = 0; i < texArrays.size(); ++i)
+        if (texArrays[i]) { cudaDestroyTextureObject(mats[i].tex); cudaFreeArray(texArrays[i]); }
     return rc;
 #undef RCHK
 }
@@ -275,6 +302,10 @@ int ref_gbuffer_gpu(const BvhNode* nodes, int nNodes, const Triangle* tris, int 
 #define RCHK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { rc = (int)e_; goto done; } } while (0)
     int rc = 0;
     std::vector<DeviceMaterial> mats = make_mats(matAlbedo, matEmissive, nMats);
+    std::vector<cudaArray_t> texArrays((size_t)(nMats > 0 ? nMats : 0), nullptr);
+    for (int i = 0; i < nMats && i < (int)g_texPaths.size(); ++i)
+        if (!g_texPaths[(size_t)i].empty() && !load_texture_to_device(g_texPaths[(size_t)i], texArrays[(size_t)i], mats[(size_t)i].tex))
+            mats[(size_t)i].tex = 0;
     const CameraGPU cam = make_cam(*camDesc);
     const int W = cam.width, H = cam.height;
     const size_t imgBytes = (size_t)W * H * 3;
@@ -327,6 +358,8 @@ done:
     cudaFree(d_alb);
     cudaFree(d_nrm);
     cudaFree(d_wp);
+    for (size_t i = 0; i < texArrays.size(); ++i)
+        if (texArrays[i]) { cudaDestroyTextureObject(mats[i].tex); cudaFreeArray(texArrays[i]); }
     return rc;
 #undef RCHK
 }
