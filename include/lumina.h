@@ -191,11 +191,13 @@ int lg_render_gbuffer(lg_renderer* r, const lg_camera* cam, uint8_t* albedo, uin
 /* tonemap_kernel: rgb8 = (u8)(sqrt(clamp(accum*inv_spp, 0, 1)) * 255). */
 int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, float inv_spp, void* stream);
 
-/* ---- denoiser (reference ml/train.py:37-75 UNet, 3-channel in / 3-channel out) ----
+/* ---- denoiser (reference ml/train.py:37-75 UNet, 3- or 12-channel in / 3-channel out) ----
  * BF16 tcgen05 convolutions with FP32 accumulation; FP32 master parameters in
  * the reference's state_dict order (d1.net.0.weight, d1.net.0.bias,
- * d1.net.2.weight, ..., u1.net.2.bias, tail.weight, tail.bias).  Only base=32,
- * in_ch=3 (the reference's defaults) are supported.  act_mode 0 is the
+ * d1.net.2.weight, ..., u1.net.2.bias, tail.weight, tail.bias).  base must be
+ * 32; in_ch is 3 (the reference's default) or up to 16 -- 12 is train.py's
+ * --gbuffer variant, colour + albedo + normal + position stacked as channels
+ * (train.py:112-119); the residual uses x[:, :3].  act_mode 0 is the
  * reference's LeakyReLU(0.1); 1 is ReLU.  Images are FP32 NCHW in [0,1]; H and
  * W must be multiples of 8 (tools/denoise.py pads before calling the model). */
 typedef struct lg_unet lg_unet;
@@ -204,14 +206,15 @@ void lg_unet_destroy(lg_unet* u);
 int64_t lg_unet_num_params(const lg_unet* u);
 int lg_unet_set_params(lg_unet* u, const float* params, int64_t n);
 int lg_unet_get_params(lg_unet* u, float* params, int64_t n);
-/* y = clamp(x + tail(...), 0, 1); host buffers of n*3*h*w floats. */
+/* y = clamp(x[:, :3] + tail(...), 0, 1); host buffers, x n*in_ch*h*w and y n*3*h*w floats. */
 int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y);
 /* Same on device buffers, ordered on `stream` (a cudaStream_t; NULL = synchronous). */
 int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, float* d_y, void* stream);
 /* Training (reference ml/train.py:184-201): mean L1 loss of the network output
  * against target, backward pass on the tensor cores, and one Adam step
  * (betas 0.9/0.999, eps 1e-8, bias correction, as torch.optim.Adam) on the
- * FP32 master parameters.  d_x, d_target: device FP32 NCHW n x 3 x h x w.
+ * FP32 master parameters.  d_x: device FP32 NCHW n x in_ch x h x w;
+ * d_target: n x 3 x h x w.
  * *loss_out (may be NULL) receives the loss before the update. */
 int lg_unet_train_step(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float lr,
                        float* loss_out);

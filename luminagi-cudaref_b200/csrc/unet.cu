@@ -1,11 +1,12 @@
 // unet.cu -- the denoiser network (reference ml/train.py:37-75) on the
 // tcgen05 convolution, and its C ABI (lg_unet_*).
 //
-// Architecture (base 32, 3-channel input): d1(3->32) d2(32->64) d3(64->128)
+// Architecture (base 32, 3- or 12-channel input): d1(in->32) d2(32->64) d3(64->128)
 // d4(128->256) at full, 1/2, 1/4, 1/8 resolution, each two 3x3 convs with an
 // activation, 2x2 max-pool between levels; u3(384->128) u2(192->64)
 // u1(96->32) on cat(up(deeper), skip) with nearest 2x upsampling; a 1x1 tail
-// to RGB; out = clamp(x + tail, 0, 1).  Activation LeakyReLU(0.1) as in the
+// to RGB; out = clamp(x[:, :3] + tail, 0, 1).  The 12-channel variant
+// (train.py --gbuffer) stacks colour, albedo, normal and position images.  Activation LeakyReLU(0.1) as in the
 // reference (ReLU selectable).  Parameters are kept in FP32 in the reference's
 // state_dict order (d1.net.0.weight, d1.net.0.bias, d1.net.2.weight, ...,
 // tail.weight, tail.bias) and packed to BF16 for the kernels.
@@ -37,7 +38,7 @@ size_t layout_params(lg_unet* u)
     for (int i = 0; i < 14; ++i)
     {
         u->w_off[i] = off;
-        off += (size_t)kLayers[i].cout * kLayers[i].cin_real * 9;
+        off += (size_t)kLayers[i].cout * layer_cin_real(u, i) * 9;
         u->b_off[i] = off;
         off += (size_t)kLayers[i].cout;
     }
@@ -81,7 +82,7 @@ int pack_all_impl(lg_unet* u)
     {
         const LayerDef& L = kLayers[i];
         LG_TRY(u->packed[i].ensure(conv_packed_elems(L.cin, L.cout) * sizeof(__nv_bfloat16)));
-        LG_TRY_CUDA(conv_pack_weights((const float*)u->params.p + u->w_off[i], L.cout, L.cin_real, L.cin,
+        LG_TRY_CUDA(conv_pack_weights((const float*)u->params.p + u->w_off[i], L.cout, layer_cin_real(u, i), L.cin,
                                       (__nv_bfloat16*)u->packed[i].p, u->stream));
     }
     u->packed_ok = true;
@@ -106,7 +107,7 @@ ConvArgs base_args(lg_unet* u, int layer, int N, int H, int W)
 
 typedef __nv_bfloat16 bf;
 
-// Runs the network on a device FP32 NCHW input (N x 3 x H x W) into d_y.
+// Runs the network on a device FP32 NCHW input (N x in_ch x H x W) into d_y (N x 3 x H x W).
 int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
 {
     if (N <= 0 || H <= 0 || W <= 0 || (H % 8) || (W % 8))
@@ -115,7 +116,7 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     LG_TRY(ensure_acts(u, N, H, W));
     cudaStream_t st = u->stream;
     LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), st));
-    LG_TRY_CUDA(to_blocked_bf16(d_x, N, 3, H, W, (bf*)u->x0.p, 16, st));
+    LG_TRY_CUDA(to_blocked_bf16(d_x, N, u->in_ch, H, W, (bf*)u->x0.p, 16, st));
     const int H2 = H / 2, W2 = W / 2, H4 = H / 4, W4 = W / 4, H8 = H / 8, W8 = W / 8;
     auto run = [&](int layer, const void* in, int h, int w, int epi, void* out, int out_c, int out_coff, void* out2,
                    int out2_c, int out2_coff) -> int {
@@ -132,7 +133,7 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
             a.tail_w = (const float*)u->params.p + u->tail_w_off;
             a.tail_b = (const float*)u->params.p + u->tail_b_off;
             a.resid = d_x;
-            a.resid_C = 3;
+            a.resid_C = u->in_ch;  // residual on x[:, :3]
             a.final_out = d_y;
         }
         LG_TRY_CUDA(conv3x3_forward((const bf*)in, a, st));
@@ -173,14 +174,16 @@ int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out)
 {
     if (!out) return set_error(LG_ERR_INVALID, "NULL argument");
     *out = nullptr;
-    if (base != 32 || in_ch != 3)
-        return set_error(LG_ERR_INVALID, "UNet(base=%d, in_ch=%d): only base=32, in_ch=3 is supported", base, in_ch);
+    if (base != 32 || in_ch < 3 || in_ch > kLayers[0].cin)
+        return set_error(LG_ERR_INVALID, "UNet(base=%d, in_ch=%d): base must be 32 and in_ch in [3, %d]", base, in_ch,
+                         kLayers[0].cin);
     if (act_mode != 0 && act_mode != 1) return set_error(LG_ERR_INVALID, "act_mode must be 0 or 1");
     lg_unet* u = new (std::nothrow) lg_unet();
     if (!u) return set_error(LG_ERR_NOMEM, "out of memory");
     cudaGetDevice(&u->device);
     cudaDeviceGetAttribute(&u->sm_count, cudaDevAttrMultiProcessorCount, u->device);
     u->slope = act_mode == 0 ? 0.1f : 0.0f;
+    u->in_ch = in_ch;
     u->n_params = layout_params(u);
     cudaError_t e = cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess)
@@ -274,9 +277,10 @@ int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y)
 {
     if (!u || !x || !y) return set_error(LG_ERR_INVALID, "NULL argument");
     const size_t bytes = (size_t)n * 3 * h * w * sizeof(float);
-    LG_TRY(u->xin.ensure(bytes));
+    const size_t in_bytes = (size_t)n * u->in_ch * h * w * sizeof(float);
+    LG_TRY(u->xin.ensure(in_bytes));
     LG_TRY(u->yout.ensure(bytes));
-    LG_TRY_CUDA(cudaMemcpyAsync(u->xin.p, x, bytes, cudaMemcpyHostToDevice, u->stream));
+    LG_TRY_CUDA(cudaMemcpyAsync(u->xin.p, x, in_bytes, cudaMemcpyHostToDevice, u->stream));
     LG_TRY(forward_device_impl(u, (const float*)u->xin.p, n, h, w, (float*)u->yout.p));
     LG_TRY_CUDA(cudaMemcpyAsync(y, u->yout.p, bytes, cudaMemcpyDeviceToHost, u->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(u->stream));

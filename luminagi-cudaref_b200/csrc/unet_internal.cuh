@@ -50,6 +50,7 @@ struct lg_unet
 {
     using Buf = lg::Buf;
     int device = 0;
+    int in_ch = 3;  // input channels: 3 (colour) or 12 (colour + albedo, normal, position)
     float slope = 0.1f;
     cudaStream_t stream = nullptr;
     // parameters (FP32, state_dict order) and packed BF16 weights
@@ -72,6 +73,9 @@ struct lg_unet
 
 namespace lg
 {
+// Real input channels of conv `i`: the first takes the network input (padded
+// to kLayers[0].cin = 16 channels in the blocked layout), the rest are fixed.
+inline int layer_cin_real(const lg_unet* u, int i) { return i == 0 ? u->in_ch : kLayers[i].cin_real; }
 int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y);
 int unet_pack_all(lg_unet* u);
 }  // namespace lg

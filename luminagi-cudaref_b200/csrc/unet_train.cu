@@ -44,7 +44,7 @@ constexpr DgradDef kDgrad[16] = {
 __device__ __forceinline__ float dact(float y, float slope) { return y > 0.0f ? 1.0f : slope; }
 
 // One thread per pixel.  u1: blocked BF16 (32 ch); x, target, pred: FP32 NCHW.
-__global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __restrict__ x,
+__global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __restrict__ x, int xC,
                                      const float* __restrict__ target, const float* __restrict__ tw,
                                      const float* __restrict__ tb, int N, int H, int W, float slope, float inv_numel,
                                      bf* __restrict__ dz, float* __restrict__ dtw, float* __restrict__ dtb,
@@ -82,7 +82,7 @@ __global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __r
 #pragma unroll
             for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&tw[k * 32 + c]), v[c], acc);
             const size_t pi = ((size_t)n * 3 + k) * HW + q;
-            const float pre = x[pi] + acc;
+            const float pre = x[((size_t)n * xC + k) * HW + q] + acc;
             const float pred = fminf(fmaxf(pre, 0.0f), 1.0f);
             const float diff = pred - target[pi];
             l += fabsf(diff);
@@ -189,7 +189,7 @@ int pack_dgrad(lg_unet* u)
         const DgradDef& d = kDgrad[k];
         const LayerDef& L = kLayers[d.layer];
         LG_TRY(u->packed_dg[k].ensure(conv_packed_elems(L.cout, d.ci_cnt) * sizeof(bf)));
-        LG_TRY_CUDA(conv_pack_weights_dgrad((const float*)u->params.p + u->w_off[d.layer], L.cout, L.cin_real, d.ci_lo,
+        LG_TRY_CUDA(conv_pack_weights_dgrad((const float*)u->params.p + u->w_off[d.layer], L.cout, layer_cin_real(u, d.layer), d.ci_lo,
                                             d.ci_cnt, (bf*)u->packed_dg[k].p, u->stream));
     }
     u->packed_dg_ok = true;
@@ -211,7 +211,7 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
     const long long npx = (long long)N * H * W;
     const float inv_numel = 1.0f / (float)(npx * 3);
     tail_backward_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(
-        (const bf*)u->u1.p, d_x, d_t, P + u->tail_w_off, P + u->tail_b_off, N, H, W, u->slope, inv_numel,
+        (const bf*)u->u1.p, d_x, u->in_ch, d_t, P + u->tail_w_off, P + u->tail_b_off, N, H, W, u->slope, inv_numel,
         (bf*)u->dz[13].p, G + u->tail_w_off, G + u->tail_b_off, (float*)u->loss.p);
     LG_TRY_CUDA(cudaGetLastError());
 
@@ -228,7 +228,7 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
         a.W = ws[lv];
         a.Cout = kLayers[L].cout;
         a.Cin = kLayers[L].cin;
-        a.Cin_real = kLayers[L].cin_real;
+        a.Cin_real = layer_cin_real(u, L);
         a.dw = G + u->w_off[L];
         a.err = (int*)u->err.p;
         LG_TRY_CUDA(conv3x3_wgrad((const bf*)u->dz[L].p, (const bf*)in_of[L], a, u->sm_count, st));

@@ -10,6 +10,9 @@
      (the last one partial); L1 loss; Adam; validation L1 on crops of the
      held-out poses; the best-validation parameters are kept and saved in the
      reference checkpoint format {"model", "base", "in_ch"}.
+     With --gbuffer the network is train.py's 12-channel variant: the input
+     stacks the noisy colour with the albedo, normal and position images of
+     the G-buffer pass (train.py:112-119); the residual stays on colour.
   3. Evaluation on held-out poses against a judge rendered with FP64
      per-pixel accumulators: PSNR / SSIM of the 8-bit sqrt-tonemapped images
      (tools/diff.py) for the noisy render, the denoised render and the plain
@@ -54,13 +57,30 @@ def judge_u8(r: Renderer, cam, spp: int, bounces: int) -> np.ndarray:
     return metrics.tonemap_u8(lin)
 
 
-def make_dataset(r: Renderer, cams, noisy_spp: int, clean_spp: int, bounces: int):
+def gbuffer_to_f32(r: Renderer, cam, out_ptr: int) -> None:
+    """G-buffer pass (albedo, normal, position; u8/255) into 9 FP32 planes at out_ptr."""
+    torch = _torch()
+    H, W = int(cam.height), int(cam.width)
+    planes = torch.from_numpy(np.stack(r.gbuffer(cam))).cuda()  # (3, H, W, 3) u8
+    _ffi.check(_ffi.lib().lg_rgb8_to_f32(C.c_void_p(planes.data_ptr()), 3, H, W, C.c_void_p(out_ptr), None))
+    torch.cuda.synchronize()
+
+
+def make_input(r: Renderer, cam, spp: int, bounces: int, out, sample_base: int = 0) -> None:
+    """Network input of one frame into out (C x H x W, C = 3 or 12): the
+    render, then for 12 channels the G-buffer images after it."""
+    render_to_f32(r, cam, spp, bounces, out.data_ptr(), sample_base)
+    if out.shape[0] == 12:
+        gbuffer_to_f32(r, cam, out[3].data_ptr())
+
+
+def make_dataset(r: Renderer, cams, noisy_spp: int, clean_spp: int, bounces: int, in_ch: int = 3):
     torch = _torch()
     H, W = int(cams[0].height), int(cams[0].width)
-    noisy = torch.empty((len(cams), 3, H, W), device="cuda")
-    clean = torch.empty_like(noisy)
+    noisy = torch.empty((len(cams), in_ch, H, W), device="cuda")
+    clean = torch.empty((len(cams), 3, H, W), device="cuda")
     for i, cam in enumerate(cams):
-        render_to_f32(r, cam, noisy_spp, bounces, noisy[i].data_ptr())
+        make_input(r, cam, noisy_spp, bounces, noisy[i])
         # a disjoint sample range keeps the clean target independent of the noisy input
         render_to_f32(r, cam, clean_spp, bounces, clean[i].data_ptr(), sample_base=100000)
     torch.cuda.synchronize()
@@ -68,14 +88,18 @@ def make_dataset(r: Renderer, cams, noisy_spp: int, clean_spp: int, bounces: int
 
 
 def gather(images, idx, ys, xs, crop):
+    """Crops (all channels) of FP32 NCHW images; C a multiple of 3: a C-channel
+    image is gathered as C/3 consecutive 3-channel images."""
     torch = _torch()
     n = len(idx)
-    out = torch.empty((n, 3, crop, crop), device="cuda")
-    I, Hh, Ww = images.shape[0], images.shape[2], images.shape[3]
+    I, Cc, Hh, Ww = images.shape
+    g = Cc // 3
+    out = torch.empty((n, Cc, crop, crop), device="cuda")
     a = lambda v: np.ascontiguousarray(v, np.int32)
-    ii, yy, xx = a(idx), a(ys), a(xs)
-    _ffi.check(_ffi.lib().lg_gather_crops(C.c_void_p(images.data_ptr()), I, Hh, Ww, _ffi.ptr(ii), _ffi.ptr(yy),
-                                          _ffi.ptr(xx), n, crop, C.c_void_p(out.data_ptr()), None))
+    ii = a((np.asarray(idx, np.int64)[:, None] * g + np.arange(g)[None, :]).reshape(-1))
+    yy, xx = a(np.repeat(ys, g)), a(np.repeat(xs, g))
+    _ffi.check(_ffi.lib().lg_gather_crops(C.c_void_p(images.data_ptr()), I * g, Hh, Ww, _ffi.ptr(ii), _ffi.ptr(yy),
+                                          _ffi.ptr(xx), n * g, crop, C.c_void_p(out.data_ptr()), None))
     return out
 
 
@@ -112,14 +136,14 @@ def train(net: UNet, noisy, clean, train_idx, val_idx, epochs=120, batch=16, cro
     return best, best_val, hist
 
 
-def save_checkpoint(params: np.ndarray, path: str) -> None:
+def save_checkpoint(params: np.ndarray, path: str, in_ch: int = 3) -> None:
     """Reference checkpoint format (ml/train.py:216), loadable by tools/denoise.py."""
     torch = _torch()
-    sd = {k: torch.from_numpy(np.ascontiguousarray(v)) for k, v in unflatten(params).items()}
-    torch.save({"model": sd, "base": 32, "in_ch": 3}, path)
+    sd = {k: torch.from_numpy(np.ascontiguousarray(v)) for k, v in unflatten(params, in_ch).items()}
+    torch.save({"model": sd, "base": 32, "in_ch": in_ch}, path)
 
 
-def eval_frames(r: Renderer, cams, noisy_spp, clean_spp, judge_spp, bounces):
+def eval_frames(r: Renderer, cams, noisy_spp, clean_spp, judge_spp, bounces, in_ch: int = 3):
     """Held-out frames: judge (FP64 accumulators), noisy and clean renders with their device times."""
     torch = _torch()
     H, W = int(cams[0].height), int(cams[0].width)
@@ -129,8 +153,8 @@ def eval_frames(r: Renderer, cams, noisy_spp, clean_spp, judge_spp, bounces):
         judge = judge_u8(r, cam, judge_spp, bounces)
         noisy = r.render(camera=cam, spp=noisy_spp, bounces=bounces, accum=False)
         clean = r.render(camera=cam, spp=clean_spp, bounces=bounces, accum=False, sample_base=100000)
-        x = torch.empty((1, 3, H, W), device="cuda")
-        render_to_f32(r, cam, noisy_spp, bounces, x.data_ptr())
+        x = torch.empty((1, in_ch, H, W), device="cuda")
+        make_input(r, cam, noisy_spp, bounces, x[0])
         out.append({"judge": judge, "noisy": noisy["rgb"], "clean": clean["rgb"], "x": x,
                     "noisy_ms": noisy["kernel_ms"], "clean_ms": clean["kernel_ms"]})
     return out
@@ -143,7 +167,7 @@ def evaluate(net: UNet, frames):
     for f in frames:
         x = f["x"]
         _, _, H, W = x.shape
-        y = torch.empty_like(x)
+        y = torch.empty((1, 3, H, W), device="cuda")
         u8 = torch.empty((H * W * 3,), dtype=torch.uint8, device="cuda")
         st = torch.cuda.current_stream()
         net.forward_device(x.data_ptr(), 1, H, W, y.data_ptr(), st.cuda_stream)  # warm
@@ -166,12 +190,12 @@ def evaluate(net: UNet, frames):
     return agg, rows
 
 
-def he_init(seed: int) -> np.ndarray:
+def he_init(seed: int, in_ch: int = 3) -> np.ndarray:
     """Seeded He-normal conv weights, zero biases, state_dict order."""
-    from .unet import PARAM_SHAPES
+    from .unet import param_shapes
     rng = np.random.default_rng(seed)
     out = []
-    for k, shp in PARAM_SHAPES:
+    for k, shp in param_shapes(in_ch):
         if k.endswith("weight"):
             fan_in = int(np.prod(shp[1:]))
             out.append(rng.normal(0, math.sqrt(2.0 / fan_in), shp).astype(np.float32).ravel())
@@ -196,34 +220,36 @@ def main(argv=None):
     ap.add_argument("--height", type=int, default=864)
     ap.add_argument("--checkpoint", default="")
     ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--gbuffer", action="store_true", help="12-channel network on colour + G-buffer (train.py --gbuffer)")
     a = ap.parse_args(argv)
+    in_ch = 12 if a.gbuffer else 3
     torch = _torch()
     t0 = time.time()
     sc = engine_scene(seed=7, width=a.width, height=a.height)
     r = Renderer(0)
     r.set_scene(sc)
     cams = [sc.camera.look_at(p, t) for p, t in orbit_poses(a.poses, seed=11, center=ENGINE_CENTER)]
-    noisy, clean = make_dataset(r, cams, a.noisy_spp, a.clean_spp, a.bounces)
+    noisy, clean = make_dataset(r, cams, a.noisy_spp, a.clean_spp, a.bounces, in_ch)
     t_data = time.time() - t0
     perm = np.random.RandomState(a.seed).permutation(a.poses)
     val_idx, train_idx = perm[:a.val].tolist(), perm[a.val:].tolist()
     t1 = time.time()
-    frames = eval_frames(r, [cams[i] for i in val_idx], a.noisy_spp, a.clean_spp, a.judge_spp, a.bounces)
+    frames = eval_frames(r, [cams[i] for i in val_idx], a.noisy_spp, a.clean_spp, a.judge_spp, a.bounces, in_ch)
     t_judge = time.time() - t1
     recipes = a.recipe or ["config:120:16:128:1e-4:1"]
     res = {"config": vars(a), "triangles": sc.n_tris, "train_poses": len(train_idx), "val_poses": len(val_idx),
            "data_seconds": t_data, "eval_render_seconds": t_judge, "recipes": {}}
     for spec in recipes:
         name, ep, bs, cr, lr, cpi = spec.split(":")
-        net = UNet()
-        net.set_params(he_init(a.seed))
+        net = UNet(in_ch=in_ch)
+        net.set_params(he_init(a.seed, in_ch))
         t2 = time.time()
         best, best_val, hist = train(net, noisy, clean, train_idx, val_idx, int(ep), int(bs), int(cr), float(lr),
                                      int(cpi), a.seed, log=lambda m: print(f"[{name}] {m}", flush=True))
         t_train = time.time() - t2
         net.set_params(best)
         if a.checkpoint:
-            save_checkpoint(best, f"{a.checkpoint}.{name}.pt")
+            save_checkpoint(best, f"{a.checkpoint}.{name}.pt", in_ch)
         agg, rows = evaluate(net, frames)
         res["recipes"][name] = {"spec": spec, "train_seconds": t_train, "best_val_l1": best_val,
                                 "history_tail": hist[-3:], "eval": agg, "per_pose": rows}

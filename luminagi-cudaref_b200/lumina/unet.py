@@ -12,21 +12,28 @@ import numpy as np
 
 from ._ffi import check, lib, ptr
 
-# state_dict keys and shapes of the reference UNet(base=32, in_ch=3).
-_BLOCKS = [("d1", 3, 32), ("d2", 32, 64), ("d3", 64, 128), ("d4", 128, 256), ("u3", 384, 128), ("u2", 192, 64),
+# state_dict keys and shapes of the reference UNet(base=32, in_ch).
+_BLOCKS = [("d1", None, 32), ("d2", 32, 64), ("d3", 64, 128), ("d4", 128, 256), ("u3", 384, 128), ("u2", 192, 64),
            ("u1", 96, 32)]
-PARAM_SHAPES = []
-for _name, _cin, _cout in _BLOCKS:
-    PARAM_SHAPES += [(f"{_name}.net.0.weight", (_cout, _cin, 3, 3)), (f"{_name}.net.0.bias", (_cout,)),
-                     (f"{_name}.net.2.weight", (_cout, _cout, 3, 3)), (f"{_name}.net.2.bias", (_cout,))]
-PARAM_SHAPES += [("tail.weight", (3, 32, 1, 1)), ("tail.bias", (3,))]
+
+
+def param_shapes(in_ch: int = 3):
+    out = []
+    for name, cin, cout in _BLOCKS:
+        cin = in_ch if cin is None else cin
+        out += [(f"{name}.net.0.weight", (cout, cin, 3, 3)), (f"{name}.net.0.bias", (cout,)),
+                (f"{name}.net.2.weight", (cout, cout, 3, 3)), (f"{name}.net.2.bias", (cout,))]
+    return out + [("tail.weight", (3, 32, 1, 1)), ("tail.bias", (3,))]
+
+
+PARAM_SHAPES = param_shapes(3)
 N_PARAMS = int(sum(np.prod(s) for _, s in PARAM_SHAPES))
 
 
-def flatten_state_dict(sd) -> np.ndarray:
+def flatten_state_dict(sd, in_ch: int = 3) -> np.ndarray:
     """Reference state_dict (tensors or arrays) -> flat FP32 in key order."""
     out = []
-    for k, shp in PARAM_SHAPES:
+    for k, shp in param_shapes(in_ch):
         v = sd[k]
         v = v.detach().cpu().float().numpy() if hasattr(v, "detach") else np.asarray(v, np.float32)
         assert tuple(v.shape) == shp, (k, v.shape, shp)
@@ -34,9 +41,9 @@ def flatten_state_dict(sd) -> np.ndarray:
     return np.concatenate(out).astype(np.float32)
 
 
-def unflatten(flat: np.ndarray) -> dict:
+def unflatten(flat: np.ndarray, in_ch: int = 3) -> dict:
     out, off = {}, 0
-    for k, shp in PARAM_SHAPES:
+    for k, shp in param_shapes(in_ch):
         n = int(np.prod(shp))
         out[k] = flat[off:off + n].reshape(shp)
         off += n
@@ -47,8 +54,9 @@ class UNet:
     def __init__(self, base: int = 32, in_ch: int = 3, act: str = "leaky"):
         self._h = C.c_void_p()
         check(lib().lg_unet_create(base, in_ch, 0 if act == "leaky" else 1, C.byref(self._h)))
+        self.in_ch = in_ch
         self.n_params = int(lib().lg_unet_num_params(self._h))
-        assert self.n_params == N_PARAMS
+        assert self.n_params == int(sum(np.prod(s) for _, s in param_shapes(in_ch)))
 
     def close(self):
         if self._h:
@@ -71,22 +79,23 @@ class UNet:
         return out
 
     def load_state_dict(self, sd) -> None:
-        self.set_params(flatten_state_dict(sd))
+        self.set_params(flatten_state_dict(sd, self.in_ch))
 
     def load_checkpoint(self, path: str) -> None:
         """Loads a reference checkpoint dict {"model": state_dict, "base", "in_ch"} (ml/train.py:216)."""
         import torch
         ck = torch.load(path, map_location="cpu", weights_only=True)
-        if ck.get("base", 32) != 32 or ck.get("in_ch", 3) != 3:
-            raise ValueError("only base=32, in_ch=3 checkpoints are supported")
+        if ck.get("base", 32) != 32 or ck.get("in_ch", 3) != self.in_ch:
+            raise ValueError(f"checkpoint is base={ck.get('base', 32)}, in_ch={ck.get('in_ch', 3)}; "
+                             f"this UNet is base=32, in_ch={self.in_ch}")
         self.load_state_dict(ck["model"])
 
     def forward(self, x: np.ndarray) -> np.ndarray:
-        """x: (N,3,H,W) FP32 in [0,1], H and W multiples of 8."""
+        """x: (N,in_ch,H,W) FP32 in [0,1], H and W multiples of 8; returns (N,3,H,W)."""
         x = np.ascontiguousarray(x, np.float32)
         n, c, h, w = x.shape
-        assert c == 3
-        y = np.empty_like(x)
+        assert c == self.in_ch
+        y = np.empty((n, 3, h, w), np.float32)
         check(lib().lg_unet_forward(self._h, ptr(x), n, h, w, ptr(y)))
         return y
 
@@ -114,9 +123,13 @@ class UNet:
     def adam_reset(self) -> None:
         check(lib().lg_unet_adam_reset(self._h))
 
-    def denoise_rgb8(self, img: np.ndarray) -> np.ndarray:
-        """tools/denoise.py:34-52: (H,W,3) u8 -> (H,W,3) u8."""
-        x = img.astype(np.float32) / 255.0
+    def denoise_rgb8(self, img: np.ndarray, albedo=None, normal=None, worldpos=None) -> np.ndarray:
+        """tools/denoise.py:34-52: (H,W,3) u8 -> (H,W,3) u8.  A 12-channel
+        network also takes the G-buffer images (H,W,3) u8, stacked after the
+        colour as the reference's --gbuffer dataset stacks them (train.py:112-119)."""
+        planes = [img] + ([albedo, normal, worldpos] if self.in_ch == 12 else [])
+        assert all(p is not None for p in planes), "a 12-channel network needs albedo, normal and worldpos"
+        x = np.concatenate([p.astype(np.float32) / 255.0 for p in planes], axis=2)
         H, W = x.shape[:2]
         ph, pw = (8 - H % 8) % 8, (8 - W % 8) % 8
         x = np.pad(x, ((0, ph), (0, pw), (0, 0)), mode="edge")

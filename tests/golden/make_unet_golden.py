@@ -1,4 +1,4 @@
-"""Writes tests/golden/unet_golden.npz from the reference's own UNet module.
+"""Writes tests/golden/unet_golden.npz and unet12_golden.npz from the reference's own UNet module.
 
 Run in a checkout that has the reference at REF (default /root/reference):
     python tests/golden/make_unet_golden.py
@@ -36,3 +36,14 @@ with torch.no_grad():
 np.savez_compressed(HERE / "unet_golden.npz", seed=SEED, x=x, y=y, n_params=len(flat),
                     param_sum=np.float64(flat.astype(np.float64).sum()))
 print("wrote", HERE / "unet_golden.npz", "params", len(flat), "out mean", float(y.mean()))
+
+# The 12-channel variant (train.py --gbuffer: colour + albedo + normal + position).
+ref12 = UNet(base=32, in_ch=12).eval()
+flat12 = unet_ref.make_params(SEED + 12, ref12)
+unet_ref.load_flat(ref12, flat12)
+x12 = np.random.default_rng(SEED + 13).uniform(0.0, 1.0, (2, 12, 16, 24)).astype(np.float32)
+with torch.no_grad():
+    y12 = ref12(torch.from_numpy(x12)).numpy()
+np.savez_compressed(HERE / "unet12_golden.npz", seed=SEED + 12, x=x12, y=y12, n_params=len(flat12),
+                    param_sum=np.float64(flat12.astype(np.float64).sum()))
+print("wrote", HERE / "unet12_golden.npz", "params", len(flat12), "out mean", float(y12.mean()))

@@ -107,3 +107,27 @@ def test_gbuffer_outputs(small_box):
         f = d / "g" / f"frame.{name}.png"
         assert f.exists()
         assert np.array_equal(_png(f), img)
+
+
+@pytest.mark.parametrize("in_ch", [3, 12])
+def test_denoise_cli(tmp_path, in_ch):
+    """python -m lumina.denoise (tools/denoise.py drop-in) on a reference-format checkpoint."""
+    import sys
+    from lumina import surrogate
+    params = surrogate.he_init(5, in_ch)
+    ck = tmp_path / "ck.pt"
+    surrogate.save_checkpoint(params, str(ck), in_ch)
+    rng = np.random.default_rng(in_ch)
+    imgs = [rng.integers(0, 256, (21, 30, 3), dtype=np.uint8) for _ in range(4)]
+    names = ["frame.png", "frame.albedo.png", "frame.normal.png", "frame.worldpos.png"]
+    for n, im in zip(names, imgs):
+        lumina.lib().lg_write_png(str(tmp_path / n).encode(), 30, 21, np.ascontiguousarray(im).ctypes.data)
+    out = tmp_path / "den.png"
+    r = subprocess.run([sys.executable, "-m", "lumina.denoise", str(ck), str(tmp_path / "frame.png"), str(out)],
+                       capture_output=True, text=True, cwd=str(_ffi.PKG_DIR))
+    assert r.returncode == 0, r.stderr
+    assert "inference:" in r.stdout and "(30x21, base=32)" in r.stdout
+    net = lumina.UNet(in_ch=in_ch)
+    net.set_params(params)
+    want = net.denoise_rgb8(*imgs[:1 if in_ch == 3 else 4])
+    assert np.array_equal(_png(out), want)

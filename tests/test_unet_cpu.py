@@ -28,6 +28,21 @@ def test_param_layout_matches_reference_keys():
     m = unet_ref.UNetRef()
     assert [(k, s) for k, s in unet_ref.param_shapes(m)] == lunet.PARAM_SHAPES
     assert lunet.N_PARAMS == 1946947
+    m12 = unet_ref.UNetRef(in_ch=12)
+    assert [(k, s) for k, s in unet_ref.param_shapes(m12)] == lunet.param_shapes(12)
+
+
+def test_restatement_matches_reference_module_12ch():
+    """The 12-channel (--gbuffer) variant: residual on the first 3 channels."""
+    g = np.load(GOLD.parent / "unet12_golden.npz")
+    m = unet_ref.UNetRef(in_ch=12).eval()
+    flat = unet_ref.make_params(int(g["seed"]), m)
+    assert len(flat) == int(g["n_params"]) == 1949539
+    assert abs(float(flat.astype(np.float64).sum()) - float(g["param_sum"])) < 1e-9
+    unet_ref.load_flat(m, flat)
+    with torch.no_grad():
+        y = m(torch.from_numpy(g["x"])).numpy()
+    assert np.abs(y - g["y"]).max() < 1e-6
 
 
 def test_bf16_emulation_is_close_to_fp32():

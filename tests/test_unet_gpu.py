@@ -99,15 +99,16 @@ def test_conv_upsample_epilogue():
     assert close_frac(got, ref) >= 0.999
 
 
-@pytest.mark.parametrize("n,h,w", [(2, 32, 48), (1, 64, 136)])
-def test_unet_forward_matches_torch(n, h, w):
-    flat = unet_ref.make_params(77)
-    net = lumina.UNet()
+@pytest.mark.parametrize("n,h,w,in_ch", [(2, 32, 48, 3), (1, 64, 136, 3), (2, 32, 48, 12)])
+def test_unet_forward_matches_torch(n, h, w, in_ch):
+    flat = unet_ref.make_params(77, unet_ref.UNetRef(in_ch=in_ch))
+    net = lumina.UNet(in_ch=in_ch)
     net.set_params(flat)
     assert np.array_equal(net.get_params(), flat)
-    x = np.random.default_rng(3).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
+    x = np.random.default_rng(3).uniform(0, 1, (n, in_ch, h, w)).astype(np.float32)
     y = net.forward(x)
-    m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
+    assert y.shape == (n, 3, h, w)
+    m = unet_ref.load_flat(unet_ref.UNetRef(in_ch=in_ch).eval(), flat)
     with torch.no_grad():
         ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x)).numpy()
         ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64).numpy()
@@ -131,24 +132,28 @@ def test_unet_rejects_bad_size():
         net.forward(np.zeros((1, 3, 12, 16), np.float32))
 
 
-def _batch(n, h, w, seed):
+def _batch(n, h, w, seed, in_ch=3):
     rng = np.random.default_rng(seed)
     clean = rng.uniform(0.1, 0.9, (n, 3, h, w)).astype(np.float32)
     noisy = np.clip(clean + rng.normal(0, 0.1, clean.shape), 0, 1).astype(np.float32)
+    if in_ch > 3:  # auxiliary planes (G-buffer stand-ins) after the colour
+        aux = rng.uniform(0, 1, (n, in_ch - 3, h, w)).astype(np.float32)
+        noisy = np.concatenate([noisy, aux], axis=1)
     return noisy, clean
 
 
-def test_unet_gradients_match_torch_autograd():
+@pytest.mark.parametrize("in_ch", [3, 12])
+def test_unet_gradients_match_torch_autograd(in_ch):
     """Gradients of the mean L1 loss from the project's backward kernels vs
     torch autograd through the FP32 network, per parameter tensor."""
-    flat = unet_ref.make_params(21)
-    net = lumina.UNet()
+    flat = unet_ref.make_params(21, unet_ref.UNetRef(in_ch=in_ch))
+    net = lumina.UNet(in_ch=in_ch)
     net.set_params(flat)
     n, h, w = 2, 32, 48
-    noisy, clean = _batch(n, h, w, 4)
+    noisy, clean = _batch(n, h, w, 4, in_ch)
     dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
     loss, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
-    m = unet_ref.load_flat(unet_ref.UNetRef(), flat)
+    m = unet_ref.load_flat(unet_ref.UNetRef(in_ch=in_ch), flat)
     out = m(torch.from_numpy(noisy))
     ref_loss = F.l1_loss(out, torch.from_numpy(clean))
     ref_loss.backward()
@@ -187,3 +192,23 @@ def test_unet_adam_step_and_training_reduces_loss():
     losses = [l0] + [net.train_step(dx.data_ptr(), dt.data_ptr(), n, h, w, lr) for _ in range(30)]
     print("training losses:", [round(x, 4) for x in losses[::5]])
     assert losses[-1] < 0.7 * losses[0]
+
+
+def test_denoise_rgb8_gbuffer_variant():
+    """12-channel network through denoise_rgb8: colour + albedo + normal + position u8 planes."""
+    flat = unet_ref.make_params(31, unet_ref.UNetRef(in_ch=12))
+    net = lumina.UNet(in_ch=12)
+    net.set_params(flat)
+    rng = np.random.default_rng(2)
+    imgs = [rng.integers(0, 256, (20, 27, 3), dtype=np.uint8) for _ in range(4)]
+    got = net.denoise_rgb8(*imgs)
+    x = np.concatenate([i.astype(np.float32) / 255.0 for i in imgs], axis=2).transpose(2, 0, 1)[None]
+    x = F.pad(torch.from_numpy(x), (0, 5, 0, 4), mode="replicate")
+    m = unet_ref.load_flat(unet_ref.UNetRef(in_ch=12).eval(), flat)
+    with torch.no_grad():
+        y = unet_ref.forward_bf16(m, x)[0, :, :20, :27].numpy().transpose(1, 2, 0)
+    ref = (np.clip(y, 0, 1) * 255.0 + 0.5).astype(np.uint8)
+    diff = np.abs(got.astype(int) - ref.astype(int))
+    assert diff.max() <= 6 and np.mean(diff <= 1) > 0.95
+    with pytest.raises(AssertionError):
+        net.denoise_rgb8(imgs[0])
