@@ -71,12 +71,17 @@ int lg_version(void);
 /* ---- scene.json (drop-in for LoadSceneJSON) ---- */
 typedef struct lg_scene lg_scene;
 /* flags: bit0 = print the reference's "[scene] loaded ..." summary to stdout.
- * threads: host threads for parsing the triangle array (<= 0: all cores). */
+ * threads: host threads for parsing the triangle array (<= 0: all cores).
+ * A binary scene file (lg_scene_save_bin; first bytes "LGSCENE1") is
+ * recognised by its magic and loaded without text parsing. */
 int lg_scene_load_json(const char* path, int flags, int threads, lg_scene** out);
 int lg_scene_create(const lg_scene_desc* desc, lg_scene** out); /* deep copy */
 int lg_scene_describe(const lg_scene* s, lg_scene_desc* out);   /* pointers stay owned by s */
 int lg_scene_set_camera(lg_scene* s, const lg_camera* cam);
 int lg_scene_save_json(const lg_scene* s, const char* path);
+/* Binary scene file: the scene.json content with every record in its memory
+ * layout (Triangle records verbatim), for fast ingest. */
+int lg_scene_save_bin(const lg_scene* s, const char* path);
 /* Material texture path (may be ""), owned by s. */
 const char* lg_scene_texture(const lg_scene* s, int material);
 /* Sets a material's texture path (the JSON "diffuse_tex" value). */

@@ -22,6 +22,7 @@ namespace lg
 {
 bool load_scene_file(const std::string& path, Scene& out, bool verbose, int threads, std::string& err);
 bool save_scene_file(const Scene& sc, const std::string& path, int threads);
+bool save_scene_bin(const Scene& sc, const std::string& path);
 bool write_png(const char* path, int w, int h, const uint8_t* rgb);
 bool write_hdr(const char* path, int w, int h, const float* rgb);
 bool decode_png(const char* path, int& w, int& h, std::vector<uint8_t>& rgba, std::string& err);
@@ -405,6 +406,13 @@ int lg_scene_save_json(const lg_scene* s, const char* path)
 {
     if (!s || !path) return set_error(LG_ERR_INVALID, "NULL argument");
     if (!save_scene_file(s->s, path, 0)) return set_error(LG_ERR_IO, "cannot write %s", path);
+    return LG_OK;
+}
+
+int lg_scene_save_bin(const lg_scene* s, const char* path)
+{
+    if (!s || !path) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (!save_scene_bin(s->s, path)) return set_error(LG_ERR_IO, "cannot write %s", path);
     return LG_OK;
 }
 

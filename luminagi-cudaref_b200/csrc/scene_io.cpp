@@ -1,15 +1,21 @@
-// scene_io.cpp -- scene.json loader and writer, PNG and Radiance HDR output.
+// scene_io.cpp -- scene.json loader and writer, the binary scene file, PNG and
+// Radiance HDR output.
 //
 // Loader: drop-in for LoadSceneJSON (reference src/scene_loader.cpp:26-138)
 // with the same schema (version 1; camera, sun, lights[], materials[],
 // triangles[]), the same number conversion (a JSON integer converts to float
 // directly, a JSON real is read as double then narrowed to float, as
 // nlohmann::json's get<float>() does) and the same messages.  It is a
-// schema-driven parser over the file bytes instead of a DOM: the top level is
-// scanned once, the triangle array's element offsets are recorded during that
-// scan, and the elements are parsed by several host threads.  Where the
+// schema-driven parser over the file bytes instead of a DOM.  The triangle
+// array is parsed by several host threads at once, each from a guessed
+// element boundary in its share of the bytes, the guesses checked to chain
+// (parse_triangles_speculative); when they do not, the top level is scanned
+// once recording each element's offset and the elements are then parsed in
+// parallel from those offsets.  Where the
 // reference lets nlohmann throw out of LoadSceneJSON on a missing key (the
 // process terminates), this loader prints "[scene] ..." and returns false.
+// A file that begins with the binary scene magic ("LGSCENE1", layout below)
+// is read as a binary scene instead: same content, no text parsing.
 #include <algorithm>
 #include <charconv>
 #include <cmath>
@@ -21,6 +27,10 @@
 #include <thread>
 #include <vector>
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 #include <zlib.h>
 
 #include "bvh.h"
@@ -365,6 +375,102 @@ void parse_triangle(Cursor& c, Triangle& t)
     if (!hm) missing("mat");
 }
 
+// The triangle array parsed by several threads without a serial pre-scan.
+// The bytes from the array's '[' to the end of the file are cut into equal
+// shares; share 0 starts at the array, every other share at the first '{'
+// at or after its cut (a guessed element start), and each parses whole
+// elements until the next element would start in the following share or the
+// array closes.  The guesses are accepted only if every share begins exactly
+// where the previous one stopped, so by induction from share 0 each share
+// parsed the true elements and the result equals a serial parse.  Returns
+// false, leaving `c` and `out` untouched, when a guess does not chain or a
+// share meets a parse error; the caller then takes the serial path (which
+// also produces the reference's error message).
+bool parse_triangles_speculative(Cursor& c, std::vector<Triangle>& out, int nt)
+{
+    struct Share
+    {
+        const char* first = nullptr;  // first element start parsed (or guessed)
+        const char* next = nullptr;   // element start where the share stopped
+        const char* close = nullptr;  // just past ']' when the array ended here
+        std::vector<Triangle> tris;
+        bool bad = false;
+    };
+    const char* b = c.p;
+    const size_t bytes = (size_t)(c.end - b);
+    std::vector<const char*> cut((size_t)nt + 1);
+    for (int k = 0; k <= nt; ++k) cut[(size_t)k] = b + bytes * (size_t)k / (size_t)nt;
+    std::vector<Share> sh((size_t)nt);
+    auto work = [&](int k) {
+        Share& s = sh[(size_t)k];
+        const char* hi = cut[(size_t)k + 1];
+        Cursor q{c.beg, cut[(size_t)k], c.end};
+        try
+        {
+            if (k == 0)
+            {
+                q.expect('[');
+                if (q.peek() == ']') { s.first = q.p; s.close = q.p + 1; return; }
+            }
+            else
+            {
+                const void* f = std::memchr(q.p, '{', (size_t)(c.end - q.p));
+                if (!f) { s.bad = true; return; }
+                q.p = static_cast<const char*>(f);
+                if (q.p >= hi) { s.first = s.next = q.p; return; }
+            }
+            s.first = q.p;
+            s.tris.reserve((size_t)(hi - q.p) / 200 + 16);
+            for (;;)
+            {
+                if (q.peek() != '{') { s.bad = true; return; }
+                Triangle t;
+                parse_triangle(q, t);
+                s.tris.push_back(t);
+                const char d = q.peek();
+                ++q.p;
+                if (d == ']') { s.close = q.p; return; }
+                if (d != ',') { s.bad = true; return; }
+                q.ws();
+                if (q.p >= hi) { s.next = q.p; return; }
+            }
+        }
+        catch (const ParseError&) { s.bad = true; }
+    };
+    {
+        std::vector<std::thread> pool;
+        for (int k = 1; k < nt; ++k) pool.emplace_back(work, k);
+        work(0);
+        for (auto& t : pool) t.join();
+    }
+    size_t total = 0;
+    int used = 0;
+    const char* close = nullptr;
+    for (int k = 0; k < nt; ++k)
+    {
+        const Share& s = sh[(size_t)k];
+        if (s.bad || (k > 0 && s.first != sh[(size_t)k - 1].next)) return false;
+        total += s.tris.size();
+        used = k + 1;
+        if (s.close) { close = s.close; break; }
+    }
+    if (!close) return false;
+    out.resize(total);
+    std::vector<size_t> off((size_t)used + 1, 0);
+    for (int k = 0; k < used; ++k) off[(size_t)k + 1] = off[(size_t)k] + sh[(size_t)k].tris.size();
+    {
+        std::vector<std::thread> pool;
+        for (int k = 0; k < used; ++k)
+            pool.emplace_back([&, k] {
+                const auto& v = sh[(size_t)k].tris;
+                if (!v.empty()) std::memcpy(&out[off[(size_t)k]], v.data(), v.size() * sizeof(Triangle));
+            });
+        for (auto& t : pool) t.join();
+    }
+    c.p = close;
+    return true;
+}
+
 }  // namespace
 
 // Parses a whole scene file held in memory.  Returns an empty string on
@@ -376,6 +482,9 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
     {
         Span sv, sc, ss, sl, sm, st;
         std::vector<const char*> tri_starts;
+        bool tris_parsed = false;  // the speculative parallel parse succeeded
+        unsigned hw = std::thread::hardware_concurrency();
+        const int nt_all = threads > 0 ? threads : (int)(hw ? hw : 1);
         for_members(c, [&](const std::string& k, Cursor& v) {
             Span* s = nullptr;
             if (k == "version") s = &sv;
@@ -386,6 +495,13 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
             else if (k == "triangles") { s = &st; tri_starts.clear(); }
             v.ws();
             const char* b = v.p;
+            if (s == &st)
+            {
+                // Shares of at least 1 MB; small arrays take the serial scan.
+                const int nt = (int)std::min<size_t>((size_t)nt_all, (size_t)(v.end - v.p) >> 20);
+                tris_parsed = nt > 1 && v.peek() == '[' && parse_triangles_speculative(v, out.triangles, nt);
+                if (tris_parsed) { st.p = b; st.end = v.p; return; }
+            }
             v.skip(s == &st ? &tri_starts : nullptr);
             if (s) { s->p = b; s->end = v.p; }
         });
@@ -511,13 +627,13 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
             });
         }
         if (!st.present()) missing("triangles");
+        if (!tris_parsed)
         {
             Cursor v{data, st.p, st.end};
             if (v.peek() != '[') v.fail("triangles must be an array");
             const size_t n = tri_starts.size();
             out.triangles.assign(n, Triangle{});
-            unsigned hw = std::thread::hardware_concurrency();
-            int nt = threads > 0 ? threads : (int)(hw ? hw : 1);
+            int nt = nt_all;
             const size_t min_per_thread = 16384;
             if ((size_t)nt > n / min_per_thread + 1) nt = (int)(n / min_per_thread + 1);
             std::vector<std::string> errs((size_t)nt);
@@ -551,36 +667,58 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
     return std::string();
 }
 
+bool is_scene_bin(const char* data, size_t size);
+std::string parse_scene_bin(const char* data, size_t size, Scene& out);
+
 bool load_scene_file(const std::string& path, Scene& out, bool verbose, int threads, std::string& err)
 {
-    FILE* f = std::fopen(path.c_str(), "rb");
-    if (!f)
+    // The file is mapped read-only (pages prefaulted from the page cache) and
+    // parsed in place; files that cannot be mapped are read into memory.
+    const int fd = ::open(path.c_str(), O_RDONLY);
+    struct stat stt;
+    if (fd < 0 || ::fstat(fd, &stt) != 0)
     {
+        if (fd >= 0) ::close(fd);
         err = "failed to open " + path;
         std::fprintf(stderr, "[scene] %s\n", err.c_str());
         set_error(LG_ERR_IO, "[scene] %s", err.c_str());
         return false;
     }
-    std::fseek(f, 0, SEEK_END);
-    long sz = std::ftell(f);
-    std::fseek(f, 0, SEEK_SET);
-    std::unique_ptr<char[]> buf(new (std::nothrow) char[sz > 0 ? (size_t)sz : 1]);
-    if (!buf)
+    const size_t sz = (size_t)stt.st_size;
+    void* map = sz > 0 && S_ISREG(stt.st_mode) ? ::mmap(nullptr, sz, PROT_READ, MAP_PRIVATE | MAP_POPULATE, fd, 0)
+                                               : MAP_FAILED;
+    std::vector<char> copy;
+    const char* data = nullptr;
+    size_t got = 0;
+    if (map != MAP_FAILED)
     {
-        std::fclose(f);
-        set_error(LG_ERR_NOMEM, "[scene] out of memory reading %s", path.c_str());
-        return false;
+        data = static_cast<const char*>(map);
+        got = sz;
     }
-    size_t got = sz > 0 ? std::fread(buf.get(), 1, (size_t)sz, f) : 0;
-    std::fclose(f);
-    if ((long)got != sz)
+    else
     {
-        set_error(LG_ERR_IO, "[scene] short read on %s", path.c_str());
-        std::fprintf(stderr, "[scene] short read on %s\n", path.c_str());
-        return false;
+        char chunk[1 << 16];
+        ssize_t r;
+        while ((r = ::read(fd, chunk, sizeof chunk)) > 0) copy.insert(copy.end(), chunk, chunk + r);
+        if (r < 0)
+        {
+            ::close(fd);
+            set_error(LG_ERR_IO, "[scene] read error on %s", path.c_str());
+            std::fprintf(stderr, "[scene] read error on %s\n", path.c_str());
+            return false;
+        }
+        data = copy.data();
+        got = copy.size();
     }
+    ::close(fd);
+    struct Unmap
+    {
+        void* m;
+        size_t n;
+        ~Unmap() { if (m != MAP_FAILED) ::munmap(m, n); }
+    } unmap{map, sz};
     Scene s;
-    std::string msg = parse_scene(buf.get(), got, s, threads);
+    std::string msg = is_scene_bin(data, got) ? parse_scene_bin(data, got, s) : parse_scene(data, got, s, threads);
     if (!msg.empty())
     {
         if (msg[0] == '!')
@@ -822,6 +960,157 @@ bool write_hdr(const char* path, int w, int h, const float* rgb)
         ok = std::fwrite(line.data(), 1, line.size(), f) == line.size();
     }
     return (std::fclose(f) == 0) && ok;
+}
+
+// ---------------------------------------------------------------------------
+// Binary scene file: the same content as scene.json with every record stored
+// in its in-memory layout, so loading is one sequential read per array.
+//
+//   0   char[8]  "LGSCENE1"
+//   8   u32      version (1), u32 flags (0)
+//   16  i32      n_tris, n_mats, n_points, n_directionals
+//   32  camera   pos[3], camera_to_world[16], fov_y_deg, aspect, near, far (f32),
+//                image_width, image_height (i32)                      (100 B)
+//   132 sun      direction[3], color[3], intensity (f32)               (28 B)
+//   160 materials n_mats x {albedo[3], emissive[3] f32, u32 tex_len}, then the
+//                texture paths (tex_len bytes each, no terminator)
+//       points   n_points x 32 B, directionals n_directionals x 28 B
+//       zero padding to a multiple of 64 bytes
+//       triangles n_tris x 100 B (Triangle records)
+// All values little-endian.
+// ---------------------------------------------------------------------------
+namespace
+{
+constexpr char kBinMagic[8] = {'L', 'G', 'S', 'C', 'E', 'N', 'E', '1'};
+
+struct BinWriter
+{
+    std::vector<unsigned char> b;
+    template <class T>
+    void put(const T& v)
+    {
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+        b.insert(b.end(), p, p + sizeof(T));
+    }
+    void raw(const void* p, size_t n)
+    {
+        const unsigned char* q = static_cast<const unsigned char*>(p);
+        b.insert(b.end(), q, q + n);
+    }
+};
+
+struct BinReader
+{
+    const unsigned char* p;
+    const unsigned char* end;
+    bool ok = true;
+    void raw(void* dst, size_t n)
+    {
+        if ((size_t)(end - p) < n) { ok = false; return; }
+        std::memcpy(dst, p, n);
+        p += n;
+    }
+    template <class T>
+    T get()
+    {
+        T v{};
+        raw(&v, sizeof v);
+        return v;
+    }
+};
+}  // namespace
+
+bool is_scene_bin(const char* data, size_t size) { return size >= 8 && std::memcmp(data, kBinMagic, 8) == 0; }
+
+bool save_scene_bin(const Scene& sc, const std::string& path)
+{
+    BinWriter w;
+    w.raw(kBinMagic, 8);
+    w.put<uint32_t>(1);
+    w.put<uint32_t>(0);
+    w.put<int32_t>((int32_t)sc.triangles.size());
+    w.put<int32_t>((int32_t)sc.materials.size());
+    w.put<int32_t>((int32_t)sc.points.size());
+    w.put<int32_t>((int32_t)sc.directionals.size());
+    w.raw(sc.camera.pos, 12);
+    w.raw(sc.camera.cameraToWorld, 64);
+    w.put(sc.camera.fovYDeg);
+    w.put(sc.camera.aspect);
+    w.put(sc.camera.nearZ);
+    w.put(sc.camera.farZ);
+    w.put<int32_t>(sc.camera.imageWidth);
+    w.put<int32_t>(sc.camera.imageHeight);
+    w.raw(sc.sun.dir, 12);
+    w.raw(sc.sun.color, 12);
+    w.put(sc.sun.intensity);
+    for (const Material& m : sc.materials)
+    {
+        w.raw(m.albedo, 12);
+        w.raw(m.emissive, 12);
+        w.put<uint32_t>((uint32_t)m.diffuseTex.size());
+    }
+    for (const Material& m : sc.materials) w.raw(m.diffuseTex.data(), m.diffuseTex.size());
+    if (!sc.points.empty()) w.raw(sc.points.data(), sc.points.size() * sizeof(PointLight));
+    if (!sc.directionals.empty()) w.raw(sc.directionals.data(), sc.directionals.size() * sizeof(DirectionalLight));
+    while (w.b.size() % 64) w.b.push_back(0);
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return false;
+    bool ok = std::fwrite(w.b.data(), 1, w.b.size(), f) == w.b.size();
+    const size_t tb = sc.triangles.size() * sizeof(Triangle);
+    ok = ok && (tb == 0 || std::fwrite(sc.triangles.data(), 1, tb, f) == tb);
+    return (std::fclose(f) == 0) && ok;
+}
+
+// Parses a whole binary scene held in memory; returns "" or an error message.
+std::string parse_scene_bin(const char* data, size_t size, Scene& out)
+{
+    BinReader r{reinterpret_cast<const unsigned char*>(data), reinterpret_cast<const unsigned char*>(data) + size};
+    char magic[8];
+    r.raw(magic, 8);
+    const uint32_t version = r.get<uint32_t>();
+    r.get<uint32_t>();
+    if (!r.ok || version != 1) return "!unsupported binary scene version";
+    const int32_t nt = r.get<int32_t>(), nm = r.get<int32_t>(), np = r.get<int32_t>(), nd = r.get<int32_t>();
+    if (!r.ok || nt < 0 || nm < 0 || np < 0 || nd < 0) return "!corrupt binary scene header";
+    r.raw(out.camera.pos, 12);
+    r.raw(out.camera.cameraToWorld, 64);
+    out.camera.fovYDeg = r.get<float>();
+    out.camera.aspect = r.get<float>();
+    out.camera.nearZ = r.get<float>();
+    out.camera.farZ = r.get<float>();
+    out.camera.imageWidth = r.get<int32_t>();
+    out.camera.imageHeight = r.get<int32_t>();
+    r.raw(out.sun.dir, 12);
+    r.raw(out.sun.color, 12);
+    out.sun.intensity = r.get<float>();
+    if ((size_t)(r.end - r.p) < (size_t)nm * 28) return "!truncated binary scene";
+    out.materials.resize((size_t)nm);
+    std::vector<uint32_t> tl((size_t)nm);
+    for (int32_t i = 0; i < nm; ++i)
+    {
+        r.raw(out.materials[(size_t)i].albedo, 12);
+        r.raw(out.materials[(size_t)i].emissive, 12);
+        tl[(size_t)i] = r.get<uint32_t>();
+    }
+    for (int32_t i = 0; i < nm && r.ok; ++i)
+    {
+        if ((size_t)(r.end - r.p) < tl[(size_t)i]) { r.ok = false; break; }
+        out.materials[(size_t)i].diffuseTex.assign(reinterpret_cast<const char*>(r.p), tl[(size_t)i]);
+        r.p += tl[(size_t)i];
+    }
+    if (!r.ok || (size_t)(r.end - r.p) < (size_t)np * sizeof(PointLight) + (size_t)nd * sizeof(DirectionalLight))
+        return "!truncated binary scene";
+    out.points.resize((size_t)np);
+    if (np) r.raw(out.points.data(), (size_t)np * sizeof(PointLight));
+    out.directionals.resize((size_t)nd);
+    if (nd) r.raw(out.directionals.data(), (size_t)nd * sizeof(DirectionalLight));
+    const size_t at = (size_t)(r.p - reinterpret_cast<const unsigned char*>(data));
+    r.p += (64 - at % 64) % 64;
+    const size_t tb = (size_t)nt * sizeof(Triangle);
+    if (r.p > r.end || (size_t)(r.end - r.p) != tb) return "!truncated binary scene";
+    out.triangles.resize((size_t)nt);
+    if (nt) r.raw(out.triangles.data(), tb);
+    return r.ok ? std::string() : std::string("!truncated binary scene");
 }
 
 }  // namespace lg

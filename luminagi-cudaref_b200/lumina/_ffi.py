@@ -79,6 +79,7 @@ SIGNATURES = {
     "lg_scene_describe": (_I, [_P, C.POINTER(LgSceneDesc)]),
     "lg_scene_set_camera": (_I, [_P, C.POINTER(LgCamera)]),
     "lg_scene_save_json": (_I, [_P, C.c_char_p]),
+    "lg_scene_save_bin": (_I, [_P, C.c_char_p]),
     "lg_scene_texture": (C.c_char_p, [_P, _I]),
     "lg_scene_set_texture": (_I, [_P, _I, C.c_char_p]),
     "lg_scene_destroy": (None, [_P]),

@@ -92,7 +92,7 @@ class Scene:
         d.directionals, d.n_directionals = ptr(self.directionals), len(self.directionals)
         return d
 
-    def save_json(self, path: str) -> None:
+    def _save(self, path: str, fn: str) -> None:
         h = C.c_void_p()
         d = self.desc()
         check(lib().lg_scene_create(C.byref(d), C.byref(h)))
@@ -100,13 +100,22 @@ class Scene:
             for m, t in enumerate(self.textures):
                 if t:
                     check(lib().lg_scene_set_texture(h, m, str(t).encode()))
-            check(lib().lg_scene_save_json(h, str(path).encode()))
+            check(getattr(lib(), fn)(h, str(path).encode()))
         finally:
             lib().lg_scene_destroy(h)
 
+    def save_json(self, path: str) -> None:
+        """scene.json in the reference schema (scene_loader.cpp:26-138)."""
+        self._save(path, "lg_scene_save_json")
+
+    def save_bin(self, path: str) -> None:
+        """Binary scene file (same content; loads without text parsing)."""
+        self._save(path, "lg_scene_save_bin")
+
     @staticmethod
     def load_json(path: str, verbose: bool = False, threads: int = 0) -> "Scene":
-        """LoadSceneJSON (reference scene_loader.cpp:26-138) through the C library."""
+        """LoadSceneJSON (reference scene_loader.cpp:26-138) through the C library;
+        binary scene files are recognised and loaded too."""
         h = C.c_void_p()
         check(lib().lg_scene_load_json(str(path).encode(), 1 if verbose else 0, threads, C.byref(h)))
         try:

@@ -157,3 +157,77 @@ def test_cli_usage_and_load_errors(tmp_path):
     bad.write_text('{"version": 2}')
     r = subprocess.run([cli, str(bad)], capture_output=True, text=True)
     assert r.returncode == 2 and "unsupported version 2" in r.stderr
+
+
+def _big_json(n, extra="", bad_at=-1, seed=0):
+    """A scene.json with n triangles (a few MB, so the loader splits the array
+    across threads); `extra` is spliced into every triangle object."""
+    rng = np.random.default_rng(seed)
+    vals = rng.uniform(-5, 5, (n, 24)).round(4)
+    head = ('{"version": 1, "camera": {"pos": [0,0,1], "camera_to_world": [1,0,0,0,0,1,0,0,0,0,1,0,0,0,1,1],'
+            ' "fov_y_deg": 60, "aspect": 2, "near": 0.1, "far": 100, "image_width": 64, "image_height": 32},'
+            ' "sun": {"direction": [0,0,-1], "color": [1,1,1], "intensity": 1}, "lights": [],'
+            ' "materials": [{"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]}], "triangles": [\n')
+    parts = []
+    for i in range(n):
+        v = vals[i]
+        mat = "" if i == bad_at else ', "mat": 0'
+        parts.append('{"v": [[%s,%s,%s],[%s,%s,%s],[%s,%s,%s]], "n": [[%s,%s,%s],[%s,%s,%s],[%s,%s,%s]], '
+                     '"uv": [[%s,%s],[%s,%s],[%s,%s]]%s%s}' % (*v, extra, mat))
+    return head + ",\n".join(parts) + "\n]}\n"
+
+
+@pytest.mark.parametrize("extra", ["", ', "x": {"a": "{{{", "b": [1, {"c": "}"}]}', ', "s": "{\\"v\\": [1]}"'])
+def test_split_parse_matches_serial_and_reference(tmp_path, extra):
+    """The array is parsed in byte shares from guessed element starts; objects
+    and braces inside elements make guesses fail, and the loader must then fall
+    back to the serial scan with the same result."""
+    p = tmp_path / "big.json"
+    p.write_text(_big_json(24000, extra))
+    assert p.stat().st_size > 4 << 20
+    a = lumina.Scene.load_json(p, threads=1)
+    for t in (2, 5, 8):
+        b = lumina.Scene.load_json(p, threads=t)
+        assert b.tris.tobytes() == a.tris.tobytes()
+    assert a.n_tris == 24000
+    if O.ref_available():
+        assert O.ref_load_scene(str(p))["tris"].tobytes() == a.tris.tobytes()
+
+
+def test_split_parse_error_message_matches_serial(tmp_path):
+    p = tmp_path / "bad_big.json"
+    p.write_text(_big_json(24000, bad_at=17000))
+    msgs = []
+    for t in (1, 8):
+        with pytest.raises(lumina.LuminaError) as e:
+            lumina.Scene.load_json(p, threads=t)
+        msgs.append(str(e.value))
+    assert msgs[0] == msgs[1] and 'missing key "mat"' in msgs[0]
+
+
+def test_binary_scene_round_trip(tmp_path, small_engine_scene):
+    sc = small_engine_scene
+    sc2 = lumina.Scene(sc.camera, sc.sun, sc.tris, sc.mat_albedo, sc.mat_emissive, sc.points,
+                       textures=["tex/a.png"] + [""] * (len(sc.mat_albedo) - 1))
+    p = tmp_path / "eng.lgscene"
+    sc2.save_bin(p)
+    assert p.read_bytes()[:8] == b"LGSCENE1"
+    back = lumina.Scene.load_json(p)
+    assert back.tris.tobytes() == sc.tris.tobytes()
+    assert back.mat_albedo.tobytes() == sc.mat_albedo.tobytes()
+    assert back.mat_emissive.tobytes() == sc.mat_emissive.tobytes()
+    assert back.points.tobytes() == sc.points.tobytes()
+    assert back.sun.tobytes() == np.asarray(sc.sun).tobytes()
+    assert np.array_equal(back.camera.camera_to_world, sc.camera.camera_to_world)
+    assert back.camera.width == sc.camera.width and back.camera.height == sc.camera.height
+    assert back.textures == sc2.textures
+    # JSON and binary files of one scene load to the same arrays
+    q = tmp_path / "eng.json"
+    sc2.save_json(q)
+    assert lumina.Scene.load_json(q).tris.tobytes() == back.tris.tobytes()
+    # truncation is an error, not a short scene
+    t = tmp_path / "trunc.lgscene"
+    t.write_bytes(p.read_bytes()[:-100])
+    with pytest.raises(lumina.LuminaError) as e:
+        lumina.Scene.load_json(t)
+    assert "truncated binary scene" in str(e.value)
