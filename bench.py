@@ -19,6 +19,9 @@ counting pass) with ms/frame alongside.
   cpu_baseline  the reference's own trace code (oracle/_ref, compiled from its
             sources for the host) with OpenMP on all host cores, on a bounded
             sample of rows; rays counted by the oracle on the same rows.
+  ingest    scene-file load times: this library on scene.json and on the
+            binary scene file, and the reference's LoadSceneJSON on the same
+            JSON (host only).
 
 --impl reference times only that CPU path (the reference renderer has no
 other CPU path) and prints its line.  Multi-GPU: replicas (each rank renders
@@ -63,6 +66,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-denoise", action="store_true", help="skip the 8spp+UNet vs 256spp timing")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--no-ingest", action="store_true", help="skip the scene-file load timing")
     return ap.parse_args()
 
 
@@ -149,6 +153,55 @@ def cpu_baseline(scene, nodes, tris, spp, bounces, target_s, impl_kind="referenc
             "sample": f"every {step}th row ({n_rows} of {H} rows) of the same frame, {spp} spp, {bounces} bounces; "
                       f"{rays} rays in {dt:.2f} s",
             "ms_per_frame_scaled": dt * 1e3 * H / n_rows}
+
+
+def ingest_timing(scene, with_reference: bool):
+    """Scene-file load times (host): this library's loader on the scene written
+    as scene.json and as the binary scene file, best of 3 each, and the
+    reference's LoadSceneJSON (oracle/_ref) on the same JSON once.  Files go to
+    a temporary directory and are removed afterwards."""
+    import ctypes as C
+    import tempfile
+    from lumina import _ffi
+    out = {"triangles": scene.n_tris, "threads": os.cpu_count()}
+    with tempfile.TemporaryDirectory() as d:
+        pj, pb = os.path.join(d, "scene.json"), os.path.join(d, "scene.lgscene")
+        scene.save_json(pj)
+        scene.save_bin(pb)
+        out["json_bytes"], out["bin_bytes"] = os.path.getsize(pj), os.path.getsize(pb)
+        L = _ffi.lib()
+        for key, path in (("json_s", pj), ("bin_s", pb)):
+            best = float("inf")
+            for _ in range(3):
+                h = C.c_void_p()
+                t0 = time.perf_counter()
+                _ffi.check(L.lg_scene_load_json(path.encode(), 0, 0, C.byref(h)))
+                best = min(best, time.perf_counter() - t0)
+                L.lg_scene_destroy(h)
+            out[key] = best
+        if with_reference:
+            try:
+                sys.path.insert(0, str(ROOT / "oracle"))
+                import oracle as O
+                # the reference loader prints its summary with printf: keep fd 1 clean
+                sys.stdout.flush()
+                saved = os.dup(1)
+                devnull = os.open(os.devnull, os.O_WRONLY)
+                os.dup2(devnull, 1)
+                try:
+                    t0 = time.perf_counter()
+                    ok = O.ref_load_scene(pj) is not None
+                    dt = time.perf_counter() - t0
+                finally:
+                    os.dup2(saved, 1)
+                    os.close(saved)
+                    os.close(devnull)
+                out["reference_json_s"] = dt if ok else None
+                out["speedup_json"] = out["reference_json_s"] / out["json_s"] if ok else None
+            except Exception as e:  # the reference build is test infrastructure; report, don't fail
+                out["reference_json_s"] = None
+                out["reference_error"] = str(e)
+    return out
 
 
 def max_over_ranks(v: float, dist, device="cpu") -> float:
@@ -341,6 +394,8 @@ def main():
             "clocks": clk.summary()}
     if denoise:
         line["denoise"] = denoise
+    if rank == 0 and world == 1 and not args.no_ingest:
+        line["ingest"] = ingest_timing(scene, with_reference=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(scene, nodes_dev, tris_dev, args.spp, args.bounces, args.cpu_seconds)

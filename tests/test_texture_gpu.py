@@ -89,7 +89,7 @@ def test_textured_gbuffer_vs_reference_gpu(textured):
 
 def test_cli_textures(textured):
     sc, root = textured
-    out = root / "out" / "t.png"
+    out = root / "t.png"  # as in the reference, a single render does not create directories
     scene = root / "scenes" / "scene.json"
     r = subprocess.run([str(_ffi.CLI_PATH), str(scene), str(out), "--spp", "2", "--bounces", "1"],
                        capture_output=True, text=True)
