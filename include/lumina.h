@@ -163,6 +163,14 @@ int lg_renderer_set_counting(lg_renderer* r, int enable);
 /* Traversal records: 4 (default; two binary levels per 128-byte record) or 2
  * (one binary node per 64-byte record).  Both traverse the same BVH. */
 int lg_renderer_set_bvh_width(lg_renderer* r, int width);
+/* Ray/triangle test.  LG_ISECT_MOLLER_TRUMBORE (default) is the reference's
+ * ray_tri (src/pathtracer.cu:82-107) and the parity mode.
+ * LG_ISECT_WATERTIGHT is the watertight test of Woop, Benthin and Wald (JCGT
+ * 2013): no ray passes between triangles that share an edge or a vertex;
+ * results differ from the reference on the pixels whose rays graze edges. */
+#define LG_ISECT_MOLLER_TRUMBORE 0
+#define LG_ISECT_WATERTIGHT 1
+int lg_renderer_set_intersection(lg_renderer* r, int mode);
 /* Diffuse texture of one material (load_texture_to_device + sample_albedo,
  * src/pathtracer.cu:553-579, 274-282): w x h RGBA8 host pixels, sampled as
  * sRGB with bilinear filtering and wrapping at uv (u, 1 - v).  rgba8 = NULL

@@ -106,6 +106,7 @@ struct lg_renderer
     // scene
     int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0, root4 = 0;
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
+    bool watertight = false;  // ray/triangle test: Moller-Trumbore (the reference's) or watertight
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
@@ -202,7 +203,7 @@ int finish_scene(lg_renderer* r)
                                   r->scratch.as<int>(), &root4, &n4, r->stream));
     r->root4 = root4;
     LG_TRY_CUDA(cudaMemcpyAsync(&r->root_node, r->nodes.p, sizeof(lg_bvh_node), cudaMemcpyDeviceToHost, r->stream));
-    LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->stream));
+    LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->watertight, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
     r->root = root;
     return LG_OK;
@@ -265,7 +266,8 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.accum64 = acc64 ? r->accum64.as<double>() : nullptr;
         job.work64 = r->work.as<unsigned long long>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
-        LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->stream));
+        LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->watertight,
+                                 r->stream));
     }
     const float inv = 1.0f / (float)o->spp;
     LG_TRY_CUDA(launch_tonemap(r->accum.as<float>(), r->rgb.as<uint8_t>(), nval, inv, r->stream));
@@ -741,6 +743,23 @@ int lg_renderer_load_textures(lg_renderer* r, const lg_scene* s, const char* ass
     return LG_OK;
 }
 
+int lg_renderer_set_intersection(lg_renderer* r, int mode)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (mode != LG_ISECT_MOLLER_TRUMBORE && mode != LG_ISECT_WATERTIGHT)
+        return set_error(LG_ERR_INVALID, "intersection mode must be 0 (Moller-Trumbore) or 1 (watertight)");
+    const bool wt = mode == LG_ISECT_WATERTIGHT;
+    if (wt == r->watertight) return LG_OK;
+    DeviceGuard g(r->device);
+    r->watertight = wt;
+    if (r->n_tris > 0)
+    {
+        LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), wt, r->stream));
+        LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    }
+    return LG_OK;
+}
+
 int lg_renderer_set_counting(lg_renderer* r, int enable)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
@@ -840,7 +859,7 @@ int lg_render_gbuffer(lg_renderer* r, const lg_camera* cam, uint8_t* albedo, uin
         const vec3 ext = vsub(v3(root.bbMax[0], root.bbMax[1], root.bbMax[2]), bbMin);
         const vec3 inv = v3(1.0f / std::max(ext.x, 1e-6f), 1.0f / std::max(ext.y, 1e-6f), 1.0f / std::max(ext.z, 1e-6f));
         LG_TRY_CUDA(launch_gbuffer(dev_scene(r), make_dev_cam(*cam), bbMin, inv, base, base + n, base + 2 * n,
-                                   r->bvh_width, r->stream));
+                                   r->bvh_width, r->watertight, r->stream));
     }
     if (albedo) LG_TRY_CUDA(cudaMemcpyAsync(albedo, base, n, cudaMemcpyDeviceToHost, r->stream));
     if (normal) LG_TRY_CUDA(cudaMemcpyAsync(normal, base + n, n, cudaMemcpyDeviceToHost, r->stream));

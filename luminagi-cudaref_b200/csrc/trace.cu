@@ -222,12 +222,19 @@ __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const
     out[dense4[i]] = w;
 }
 
-__global__ void tri_prep_kernel(const lg_triangle* __restrict__ tris, int n, float4* __restrict__ tv)
+__global__ void tri_prep_kernel(const lg_triangle* __restrict__ tris, int n, float4* __restrict__ tv, int watertight)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const lg_triangle t = tris[i];
     tv[3 * i + 0] = make_float4(t.v[0][0], t.v[0][1], t.v[0][2], __int_as_float(t.material));
+    if (watertight)
+    {
+        // the watertight test needs the shared vertices themselves, not edges
+        tv[3 * i + 1] = make_float4(t.v[1][0], t.v[1][1], t.v[1][2], 0.0f);
+        tv[3 * i + 2] = make_float4(t.v[2][0], t.v[2][1], t.v[2][2], 0.0f);
+        return;
+    }
     tv[3 * i + 1] = make_float4(__fsub_rn(t.v[1][0], t.v[0][0]), __fsub_rn(t.v[1][1], t.v[0][1]),
                                 __fsub_rn(t.v[1][2], t.v[0][2]), 0.0f);
     tv[3 * i + 2] = make_float4(__fsub_rn(t.v[2][0], t.v[0][0]), __fsub_rn(t.v[2][1], t.v[0][1]),
@@ -286,6 +293,68 @@ __device__ __forceinline__ bool tri_hit(const Ray& r, const float4* __restrict__
     return true;
 }
 
+// Watertight ray/triangle test (Woop, Benthin, Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2013) on (v0, v1, v2): vertices are
+// translated to the ray origin and sheared so the ray runs along +z; the
+// three 2-D edge functions are products and differences rounded once each
+// (no contraction), so an edge shared by two triangles gives opposite-signed
+// values in both and a ray through the edge or a shared vertex cannot pass
+// between them; exact zeros are re-evaluated in double.  Same outputs as
+// tri_hit: u, v are the weights of v1 and v2, and the hit must satisfy
+// 1e-6 < t < tmax.  No determinant epsilon: only det == 0 is rejected.
+__device__ __forceinline__ float comp(vec3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ bool tri_hit_wt(const Ray& r, const float4* __restrict__ tv, int ti, float tmax,
+                                           float& outT, float& outU, float& outV)
+{
+    constexpr float kEps = 1e-6f;
+    const float ax = fabsf(r.d.x), ay = fabsf(r.d.y), az = fabsf(r.d.z);
+    const int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const float dz = comp(r.d, kz);
+    if (dz < 0.0f) { const int t = kx; kx = ky; ky = t; }
+    const float Sz = __frcp_rn(dz);
+    const float Sx = __fmul_rn(comp(r.d, kx), Sz), Sy = __fmul_rn(comp(r.d, ky), Sz);
+    const float4 a4 = __ldg(&tv[3 * ti + 0]);
+    const float4 b4 = __ldg(&tv[3 * ti + 1]);
+    const float4 c4 = __ldg(&tv[3 * ti + 2]);
+    const vec3 A = v3(__fsub_rn(a4.x, r.o.x), __fsub_rn(a4.y, r.o.y), __fsub_rn(a4.z, r.o.z));
+    const vec3 B = v3(__fsub_rn(b4.x, r.o.x), __fsub_rn(b4.y, r.o.y), __fsub_rn(b4.z, r.o.z));
+    const vec3 C = v3(__fsub_rn(c4.x, r.o.x), __fsub_rn(c4.y, r.o.y), __fsub_rn(c4.z, r.o.z));
+    const float Az = comp(A, kz), Bz = comp(B, kz), Cz = comp(C, kz);
+    const float Ax = __fsub_rn(comp(A, kx), __fmul_rn(Sx, Az)), Ay = __fsub_rn(comp(A, ky), __fmul_rn(Sy, Az));
+    const float Bx = __fsub_rn(comp(B, kx), __fmul_rn(Sx, Bz)), By = __fsub_rn(comp(B, ky), __fmul_rn(Sy, Bz));
+    const float Cx = __fsub_rn(comp(C, kx), __fmul_rn(Sx, Cz)), Cy = __fsub_rn(comp(C, ky), __fmul_rn(Sy, Cz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f)
+    {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float T = U * __fmul_rn(Sz, Az) + V * __fmul_rn(Sz, Bz) + W * __fmul_rn(Sz, Cz);
+    const float invDet = 1.0f / det;
+    const float tt = T * invDet;
+    if (tt <= kEps || tt >= tmax) return false;
+    outT = tt;
+    outU = V * invDet;
+    outV = W * invDet;
+    return true;
+}
+
+template <bool kWT>
+__device__ __forceinline__ bool tri_test(const Ray& r, const float4* __restrict__ tv, int ti, float tmax, float& outT,
+                                         float& outU, float& outV)
+{
+    return kWT ? tri_hit_wt(r, tv, ti, tmax, outT, outU, outV) : tri_hit(r, tv, ti, tmax, outT, outU, outV);
+}
+
 struct Counters
 {
     unsigned long long closest, shadow, overflow, nodes, tris, leaves;
@@ -303,7 +372,7 @@ __device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
 // The 4-wide form of the traversal below: one 128-byte record tests up to
 // four child boxes (same slab arithmetic); hit children are ordered by entry
 // distance, the nearest is entered and the rest stacked nearest-on-top.
-template <bool kCount>
+template <bool kCount, bool kWT>
 __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
                                          float& bestU, float& bestV, Counters& cnt)
 {
@@ -358,7 +427,7 @@ __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float 
                 const int ti = lf.x + i;
                 float tt, uu, vv;
                 if (kCount) cnt.tris++;
-                if (tri_hit(r, s.tv, ti, bestT, tt, uu, vv))
+                if (tri_test<kWT>(r, s.tv, ti, bestT, tt, uu, vv))
                 {
                     bestT = tt;
                     bestTri = ti;
@@ -381,7 +450,7 @@ __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float 
 // Keeping a single copy of this loop in the kernel lets lanes tracing
 // different kinds of rays execute it together and keeps the code small.
 // Returns the hit triangle or -1; bestT/U/V as in traverse_closest.
-template <bool kCount>
+template <bool kCount, bool kWT>
 __device__ __forceinline__ int traverse(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
                                         float& bestU, float& bestV, Counters& cnt)
 {
@@ -429,7 +498,7 @@ __device__ __forceinline__ int traverse(const DevScene& s, const Ray& r, float t
                 const int ti = lf.x + i;
                 float tt, uu, vv;
                 if (kCount) cnt.tris++;
-                if (tri_hit(r, s.tv, ti, bestT, tt, uu, vv))
+                if (tri_test<kWT>(r, s.tv, ti, bestT, tt, uu, vv))
                 {
                     bestT = tt;
                     bestTri = ti;
@@ -647,7 +716,7 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
 // the loop is one warp-wide traversal (camera, bounce or shadow ray per lane)
 // followed by a short state update.  Items are numbered chunk-major, then by
 // 8x4 pixel tile, so neighbouring lanes start on neighbouring pixels.
-template <bool kCount, bool kAcc64, int kWidth>
+template <bool kCount, bool kAcc64, int kWidth, bool kWT>
 __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
 {
     const int lane = threadIdx.x & 31;
@@ -697,8 +766,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         if (active)
         {
             float hitT, hitU, hitV;
-            const int tri = kWidth == 4 ? traverse4<kCount>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt)
-                                        : traverse<kCount>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
+            const int tri = kWidth == 4 ? traverse4<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt)
+                                        : traverse<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
             if (!advance(st, s, cam, job.max_bounces, tri, hitT, hitU, hitV))
             {
                 active = false;
@@ -751,7 +820,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
 // encoded normal and box-normalised world position as 8-bit RGB.
 __device__ __forceinline__ uint8_t enc8(float v) { return (uint8_t)(fminf(1.0f, fmaxf(0.0f, v)) * 255.0f); }
 
-template <int kWidth>
+template <int kWidth, bool kWT>
 __global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* __restrict__ albedo_out,
                                uint8_t* __restrict__ normal_out, uint8_t* __restrict__ worldpos_out)
 {
@@ -761,8 +830,8 @@ __global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExt
     Ray r = primary_ray(cam, px, py, 0.5f, 0.5f);
     float hitT, hitU, hitV;
     Counters cnt{0, 0, 0, 0, 0, 0};
-    const int tri = kWidth == 4 ? traverse4<false>(s, r, 1e30f, false, hitT, hitU, hitV, cnt)
-                                : traverse<false>(s, r, 1e30f, false, hitT, hitU, hitV, cnt);
+    const int tri = kWidth == 4 ? traverse4<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt)
+                                : traverse<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt);
     const size_t i = ((size_t)py * cam.width + px) * 3;
     if (tri < 0)
     {
@@ -882,19 +951,18 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node
     return cudaSuccess;
 }
 
-cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cudaStream_t stream)
+cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bool watertight, cudaStream_t stream)
 {
     if (n <= 0) return cudaSuccess;
-    tri_prep_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_tris, n, d_tv);
+    tri_prep_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_tris, n, d_tv, watertight ? 1 : 0);
     return cudaGetLastError();
 }
 
-template <int W>
-static cudaError_t launch_trace_w(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
-                                 cudaStream_t stream)
+template <bool kCount, bool kAcc64, int W, bool kWT>
+static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const TraceJob& job, int sm_count,
+                                  cudaStream_t stream)
 {
-    const void* fn = count ? (job.accum64 ? (const void*)trace_kernel<true, true, W> : (const void*)trace_kernel<true, false, W>)
-                           : (job.accum64 ? (const void*)trace_kernel<false, true, W> : (const void*)trace_kernel<false, false, W>);
+    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT>;
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, 0);
     if (e != cudaSuccess) return e;
@@ -905,37 +973,42 @@ static cudaError_t launch_trace_w(const DevScene& s, const DevCam& cam, const Tr
     if (blocks < 1) blocks = 1;
     e = cudaMemsetAsync(job.work64, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    const int g = (int)blocks;
-    if (count)
-    {
-        if (job.accum64) trace_kernel<true, true, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
-        else trace_kernel<true, false, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
-    }
-    else
-    {
-        if (job.accum64) trace_kernel<false, true, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
-        else trace_kernel<false, false, W><<<g, kTraceThreads, 0, stream>>>(s, cam, job);
-    }
+    trace_kernel<kCount, kAcc64, W, kWT><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
     return cudaGetLastError();
+}
+
+template <int W, bool kWT>
+static cudaError_t launch_trace_w(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
+                                 cudaStream_t stream)
+{
+    if (count)
+        return job.accum64 ? launch_trace_t<true, true, W, kWT>(s, cam, job, sm_count, stream)
+                           : launch_trace_t<true, false, W, kWT>(s, cam, job, sm_count, stream);
+    return job.accum64 ? launch_trace_t<false, true, W, kWT>(s, cam, job, sm_count, stream)
+                       : launch_trace_t<false, false, W, kWT>(s, cam, job, sm_count, stream);
 }
 
 // Four 256-thread blocks per SM (64 registers) measured fastest on B200:
 // 653 ms per 64-spp engine-scale frame (binary nodes) vs 745 ms at three
 // and 1007 ms at two.
 cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
-                         int width, cudaStream_t stream)
+                         int width, bool watertight, cudaStream_t stream)
 {
-    if (width == 4) return launch_trace_w<4>(s, cam, job, count, sm_count, stream);
-    return launch_trace_w<2>(s, cam, job, count, sm_count, stream);
+    if (watertight)
+        return width == 4 ? launch_trace_w<4, true>(s, cam, job, count, sm_count, stream)
+                          : launch_trace_w<2, true>(s, cam, job, count, sm_count, stream);
+    return width == 4 ? launch_trace_w<4, false>(s, cam, job, count, sm_count, stream)
+                      : launch_trace_w<2, false>(s, cam, job, count, sm_count, stream);
 }
 
 cudaError_t launch_gbuffer(const DevScene& s, const DevCam& cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* d_albedo,
-                           uint8_t* d_normal, uint8_t* d_worldpos, int width, cudaStream_t stream)
+                           uint8_t* d_normal, uint8_t* d_worldpos, int width, bool watertight, cudaStream_t stream)
 {
     dim3 block(16, 16);
     dim3 grid((cam.width + 15) / 16, (cam.height + 15) / 16);
-    if (width == 4) gbuffer_kernel<4><<<grid, block, 0, stream>>>(s, cam, bbMin, bbInvExtent, d_albedo, d_normal, d_worldpos);
-    else gbuffer_kernel<2><<<grid, block, 0, stream>>>(s, cam, bbMin, bbInvExtent, d_albedo, d_normal, d_worldpos);
+    auto k = width == 4 ? (watertight ? gbuffer_kernel<4, true> : gbuffer_kernel<4, false>)
+                        : (watertight ? gbuffer_kernel<2, true> : gbuffer_kernel<2, false>);
+    k<<<grid, block, 0, stream>>>(s, cam, bbMin, bbInvExtent, d_albedo, d_normal, d_worldpos);
     return cudaGetLastError();
 }
 

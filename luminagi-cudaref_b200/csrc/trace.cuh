@@ -93,13 +93,15 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
 // the same scratch (it reuses the leaf numbering).  Scratch: 5 * n_nodes ints.
 cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node* d_wide4, int* d_scratch,
                               int* root4_host, int* n4_host, cudaStream_t stream);
-cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, cudaStream_t stream);
+// Intersection records, 3 float4 per triangle (w of the first = material):
+// (v0, v1-v0, v2-v0) for Moller-Trumbore, (v0, v1, v2) for the watertight test.
+cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bool watertight, cudaStream_t stream);
 
 cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
-                         int width, cudaStream_t stream);
+                         int width, bool watertight, cudaStream_t stream);
 // Primary-hit G-buffer (albedo, encoded normal, box-normalised position), W*H*3 bytes each.
 cudaError_t launch_gbuffer(const DevScene& s, const DevCam& cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* d_albedo,
-                           uint8_t* d_normal, uint8_t* d_worldpos, int width, cudaStream_t stream);
+                           uint8_t* d_normal, uint8_t* d_worldpos, int width, bool watertight, cudaStream_t stream);
 cudaError_t launch_tonemap(const float* d_accum, uint8_t* d_rgb, long long n_values, float inv_spp,
                            cudaStream_t stream);
 cudaError_t launch_accum64_to_32(const double* d_acc64, float* d_acc32, long long n_values, cudaStream_t stream);

@@ -25,6 +25,8 @@ LG_ERR_NOMEM = -5
 LG_ERR_DEVICE = -6
 LG_ERR_CAPACITY = -7
 LG_RENDER_ACCUM64 = 1
+LG_ISECT_MOLLER_TRUMBORE = 0
+LG_ISECT_WATERTIGHT = 1
 
 # Record layouts (byte-identical to the reference's Triangle / BvhNode / lights).
 TRI_DTYPE = np.dtype([("v", "<f4", (3, 3)), ("n", "<f4", (3, 3)), ("uv", "<f4", (3, 2)), ("material", "<i4")])
@@ -96,6 +98,7 @@ SIGNATURES = {
     "lg_renderer_get_bvh": (_I, [_P, _P, C.POINTER(C.c_int32), _P]),
     "lg_renderer_set_counting": (_I, [_P, _I]),
     "lg_renderer_set_bvh_width": (_I, [_P, _I]),
+    "lg_renderer_set_intersection": (_I, [_P, _I]),
     "lg_renderer_set_texture": (_I, [_P, _I, _P, C.c_int32, C.c_int32]),
     "lg_renderer_load_textures": (_I, [_P, _P, C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "lg_render": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, _P, C.POINTER(LgRenderStats)]),

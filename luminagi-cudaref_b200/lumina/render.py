@@ -98,6 +98,11 @@ class Renderer:
                 missing += 1
         return loaded, missing
 
+    def set_intersection(self, mode: str) -> None:
+        """'mt' (Moller-Trumbore, the reference's test; default) or 'watertight'."""
+        modes = {"mt": 0, "watertight": 1}
+        check(lib().lg_renderer_set_intersection(self._h, modes[mode]))
+
     def set_counting(self, on: bool) -> None:
         check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))
 
