@@ -210,16 +210,28 @@ int lg_tonemap_device(const float* d_accum, uint8_t* d_rgb8, int64_t n_pixels, f
  * d1.net.2.weight, ..., u1.net.2.bias, tail.weight, tail.bias).  base must be
  * 32; in_ch is 3 (the reference's default) or up to 16 -- 12 is train.py's
  * --gbuffer variant, colour + albedo + normal + position stacked as channels
- * (train.py:112-119); the residual uses x[:, :3].  act_mode 0 is the
- * reference's LeakyReLU(0.1); 1 is ReLU.  Images are FP32 NCHW in [0,1]; H and
- * W must be multiples of 8 (tools/denoise.py pads before calling the model). */
+ * (train.py:112-119); the residual uses x[:, :3].  Images are FP32 NCHW; H
+ * and W must be multiples of 8 (tools/denoise.py pads before calling the model).
+ * mode 0 is the reference network: LeakyReLU(0.1), nearest upsampling, input
+ * in [0,1], out = clamp(x[:, :3] + tail, 0, 1).  Mode bits select the
+ * configuration-4 variant the reference does not ship:
+ *   LG_UNET_RELU      ReLU activations;
+ *   LG_UNET_BILINEAR  bilinear 2x upsampling (align_corners=False);
+ *   LG_UNET_LOG_HDR   HDR radiance in and out: the network sees log1p(x), the
+ *                     residual is taken in log space, out = expm1(max(y, 0));
+ *                     its training loss is L1 between max(y, 0) and log1p(target).
+ * LG_UNET_HDR_VARIANT = all three. */
+#define LG_UNET_RELU 1
+#define LG_UNET_BILINEAR 2
+#define LG_UNET_LOG_HDR 4
+#define LG_UNET_HDR_VARIANT 7
 typedef struct lg_unet lg_unet;
-int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out);
+int lg_unet_create(int base, int in_ch, int mode, lg_unet** out);
 void lg_unet_destroy(lg_unet* u);
 int64_t lg_unet_num_params(const lg_unet* u);
 int lg_unet_set_params(lg_unet* u, const float* params, int64_t n);
 int lg_unet_get_params(lg_unet* u, float* params, int64_t n);
-/* y = clamp(x[:, :3] + tail(...), 0, 1); host buffers, x n*in_ch*h*w and y n*3*h*w floats. */
+/* y = clamp(x[:, :3] + tail(...), 0, 1) (mode 0); host buffers, x n*in_ch*h*w and y n*3*h*w floats. */
 int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y);
 /* Same on device buffers, ordered on `stream` (a cudaStream_t; NULL = synchronous). */
 int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, float* d_y, void* stream);
@@ -257,6 +269,12 @@ int lg_from_blocked_bf16(const void* d_in, int n, int c, int h, int w, float* d_
 int lg_rgb8_to_f32(const uint8_t* d_rgb, int n, int h, int w, float* d_out, void* stream);
 /* FP32 NCHW -> h*w*3 bytes per frame: (u8)(clip(v,0,1)*255 + 0.5) (tools/denoise.py:51). */
 int lg_f32_to_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream);
+/* n accumulators (h*w*3 sums over samples, HWC) * inv_spp -> FP32 NCHW linear
+ * radiance (the HDR denoiser's input). */
+int lg_accum_to_f32(const float* d_accum, int n, int h, int w, float inv_spp, float* d_out, void* stream);
+/* FP32 NCHW linear radiance -> h*w*3 bytes (HWC) with tonemap_kernel's formula
+ * (u8)(sqrt(clamp(v, 0, 1)) * 255). */
+int lg_f32_tonemap_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream);
 /* n_crops square crops (crop x crop, all 3 channels) of FP32 NCHW images
  * (n_images x 3 x h x w) at host-given (img_idx, ys, xs) into d_out
  * (n_crops x 3 x crop x crop). */

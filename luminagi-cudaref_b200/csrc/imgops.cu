@@ -5,6 +5,8 @@
 //                    ml/train.py:102-103, tools/denoise.py:34)
 //   lg_f32_to_rgb8:  FP32 NCHW -> 8-bit HWC with clip(v,0,1)*255 + 0.5 truncated
 //                    (tools/denoise.py:51)
+//   lg_accum_to_f32 / lg_f32_tonemap_rgb8: the HDR denoiser's linear input from
+//                    the accumulator, and its output tonemapped as tonemap_kernel does
 //   lg_gather_crops: square crops of several FP32 NCHW images into one batch
 //                    (ml/train.py:104-110 random crops)
 #include <cstdint>
@@ -38,6 +40,32 @@ __global__ void f32_to_rgb8_kernel(const float* __restrict__ in, long long n, in
     const long long img = px / HW, p = px % HW;
     const float v = fminf(fmaxf(in[(img * 3 + c) * HW + p], 0.0f), 1.0f);
     out[i] = (uint8_t)(v * 255.0f + 0.5f);
+}
+
+// accum (HWC sums over spp) * inv_spp -> FP32 NCHW linear radiance.
+__global__ void accum_to_f32_kernel(const float* __restrict__ acc, long long n, int H, int W, float inv_spp,
+                                    float* __restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over n*3*H*W (NCHW)
+    const long long HW = (long long)H * W;
+    if (i >= n * 3 * HW) return;
+    const long long img = i / (3 * HW), r = i % (3 * HW);
+    const int c = (int)(r / HW);
+    const long long p = r % HW;
+    out[i] = acc[(img * HW + p) * 3 + c] * inv_spp;
+}
+
+// FP32 NCHW linear radiance -> HWC u8 with tonemap_kernel's formula.
+__global__ void f32_tonemap_kernel(const float* __restrict__ in, long long n, int H, int W, uint8_t* __restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over n*H*W*3 (HWC)
+    const long long HW = (long long)H * W;
+    if (i >= n * HW * 3) return;
+    const int c = (int)(i % 3);
+    const long long px = i / 3;
+    const long long img = px / HW, p = px % HW;
+    const float v = sqrtf(fmaxf(0.0f, fminf(in[(img * 3 + c) * HW + p], 1.0f)));
+    out[i] = (uint8_t)(v * 255.0f);
 }
 
 struct Crop
@@ -78,6 +106,27 @@ int lg_f32_to_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void*
     const long long total = (long long)n * 3 * h * w;
     if (total == 0) return LG_OK;
     f32_to_rgb8_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_in, n, h, w, d_rgb);
+    LG_TRY_CUDA(cudaGetLastError());
+    return LG_OK;
+}
+
+int lg_accum_to_f32(const float* d_accum, int n, int h, int w, float inv_spp, float* d_out, void* stream)
+{
+    if (!d_accum || !d_out || n < 0 || h <= 0 || w <= 0) return lg::set_error(LG_ERR_INVALID, "bad argument");
+    const long long total = (long long)n * 3 * h * w;
+    if (total == 0) return LG_OK;
+    accum_to_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_accum, n, h, w, inv_spp,
+                                                                                           d_out);
+    LG_TRY_CUDA(cudaGetLastError());
+    return LG_OK;
+}
+
+int lg_f32_tonemap_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream)
+{
+    if (!d_rgb || !d_in || n < 0 || h <= 0 || w <= 0) return lg::set_error(LG_ERR_INVALID, "bad argument");
+    const long long total = (long long)n * 3 * h * w;
+    if (total == 0) return LG_OK;
+    f32_tonemap_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_in, n, h, w, d_rgb);
     LG_TRY_CUDA(cudaGetLastError());
     return LG_OK;
 }

@@ -68,6 +68,12 @@ int ensure_acts(lg_unet* u, int N, int H, int W)
     LG_TRY(u->t6.ensure(px / 4 * 64 * b2));
     LG_TRY(u->t7.ensure(px * 32 * b2));
     LG_TRY(u->u1.ensure(px * 32 * b2));
+    if (u->bilinear)
+    {
+        LG_TRY(u->lo7.ensure(px / 64 * 256 * b2));
+        LG_TRY(u->lo9.ensure(px / 16 * 128 * b2));
+        LG_TRY(u->lo11.ensure(px / 4 * 64 * b2));
+    }
     LG_TRY(u->err.ensure(sizeof(int)));
     u->aN = N;
     u->aH = H;
@@ -116,7 +122,7 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     LG_TRY(ensure_acts(u, N, H, W));
     cudaStream_t st = u->stream;
     LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), st));
-    LG_TRY_CUDA(to_blocked_bf16(d_x, N, u->in_ch, H, W, (bf*)u->x0.p, 16, st));
+    LG_TRY_CUDA(to_blocked_bf16(d_x, N, u->in_ch, H, W, (bf*)u->x0.p, 16, st, u->log_hdr));
     const int H2 = H / 2, W2 = W / 2, H4 = H / 4, W4 = W / 4, H8 = H / 8, W8 = W / 8;
     auto run = [&](int layer, const void* in, int h, int w, int epi, void* out, int out_c, int out_coff, void* out2,
                    int out2_c, int out2_coff) -> int {
@@ -134,6 +140,7 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
             a.tail_b = (const float*)u->params.p + u->tail_b_off;
             a.resid = d_x;
             a.resid_C = u->in_ch;  // residual on x[:, :3]
+            a.log_hdr = u->log_hdr ? 1 : 0;
             a.final_out = d_y;
         }
         LG_TRY_CUDA(conv3x3_forward((const bf*)in, a, st));
@@ -147,12 +154,21 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     LG_TRY(run(4, u->p2.p, H4, W4, kEpiStore, u->t3.p, 128, 0, nullptr, 0, 0));
     LG_TRY(run(5, u->t3.p, H4, W4, kEpiStore, u->cat3.p, 384, 256, u->p3.p, 128, 0));
     LG_TRY(run(6, u->p3.p, H8, W8, kEpiStore, u->t4.p, 256, 0, nullptr, 0, 0));
-    LG_TRY(run(7, u->t4.p, H8, W8, kEpiUpsample, u->cat3.p, 384, 0, nullptr, 0, 0));
+    // The conv before each upsampling writes its output 2x upsampled into the
+    // first channels of the next level's concat buffer: nearest copies in its
+    // epilogue, or (bilinear) a stored low-resolution result and a resampling pass.
+    auto up = [&](int layer, const void* in, int h, int w, Buf& lo, int c, void* cat, int cat_c) -> int {
+        if (!u->bilinear) return run(layer, in, h, w, kEpiUpsample, cat, cat_c, 0, nullptr, 0, 0);
+        LG_TRY(run(layer, in, h, w, kEpiStore, lo.p, c, 0, nullptr, 0, 0));
+        LG_TRY_CUDA(bilinear_up2((const bf*)lo.p, N, c, h, w, (bf*)cat, cat_c, 0, st));
+        return LG_OK;
+    };
+    LG_TRY(up(7, u->t4.p, H8, W8, u->lo7, 256, u->cat3.p, 384));
     // decoder
     LG_TRY(run(8, u->cat3.p, H4, W4, kEpiStore, u->t5.p, 128, 0, nullptr, 0, 0));
-    LG_TRY(run(9, u->t5.p, H4, W4, kEpiUpsample, u->cat2.p, 192, 0, nullptr, 0, 0));
+    LG_TRY(up(9, u->t5.p, H4, W4, u->lo9, 128, u->cat2.p, 192));
     LG_TRY(run(10, u->cat2.p, H2, W2, kEpiStore, u->t6.p, 64, 0, nullptr, 0, 0));
-    LG_TRY(run(11, u->t6.p, H2, W2, kEpiUpsample, u->cat1.p, 96, 0, nullptr, 0, 0));
+    LG_TRY(up(11, u->t6.p, H2, W2, u->lo11, 64, u->cat1.p, 96));
     LG_TRY(run(12, u->cat1.p, H, W, kEpiStore, u->t7.p, 32, 0, nullptr, 0, 0));
     LG_TRY(run(13, u->t7.p, H, W, kEpiTail, u->u1.p, 32, 0, nullptr, 0, 0));
     return LG_OK;
@@ -177,12 +193,15 @@ int lg_unet_create(int base, int in_ch, int act_mode, lg_unet** out)
     if (base != 32 || in_ch < 3 || in_ch > kLayers[0].cin)
         return set_error(LG_ERR_INVALID, "UNet(base=%d, in_ch=%d): base must be 32 and in_ch in [3, %d]", base, in_ch,
                          kLayers[0].cin);
-    if (act_mode != 0 && act_mode != 1) return set_error(LG_ERR_INVALID, "act_mode must be 0 or 1");
+    if (act_mode & ~(LG_UNET_RELU | LG_UNET_BILINEAR | LG_UNET_LOG_HDR))
+        return set_error(LG_ERR_INVALID, "unknown UNet mode bits 0x%x", act_mode);
     lg_unet* u = new (std::nothrow) lg_unet();
     if (!u) return set_error(LG_ERR_NOMEM, "out of memory");
     cudaGetDevice(&u->device);
     cudaDeviceGetAttribute(&u->sm_count, cudaDevAttrMultiProcessorCount, u->device);
-    u->slope = act_mode == 0 ? 0.1f : 0.0f;
+    u->slope = (act_mode & LG_UNET_RELU) ? 0.0f : 0.1f;
+    u->bilinear = (act_mode & LG_UNET_BILINEAR) != 0;
+    u->log_hdr = (act_mode & LG_UNET_LOG_HDR) != 0;
     u->in_ch = in_ch;
     u->n_params = layout_params(u);
     cudaError_t e = cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking);
@@ -210,7 +229,7 @@ void lg_unet_destroy(lg_unet* u)
     for (auto& b : u->packed) b.release();
     for (Buf* b : {&u->x0, &u->t1, &u->cat1, &u->p1, &u->t2, &u->cat2, &u->p2, &u->t3, &u->cat3, &u->p3, &u->t4,
                    &u->t5, &u->t6, &u->t7, &u->u1, &u->xin, &u->yout, &u->err, &u->grads, &u->adam_m, &u->adam_v,
-                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt})
+                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt, &u->lo7, &u->lo9, &u->lo11, &u->gup})
         b->release();
     for (auto& b : u->packed_dg) b.release();
     for (auto& b : u->dz) b.release();

@@ -354,7 +354,8 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
                 {
                     const size_t pi = (((size_t)n * a.resid_C + k) * a.H + y) * a.W + x;
                     const size_t po = (((size_t)n * 3 + k) * a.H + y) * a.W + x;
-                    a.final_out[po] = fminf(fmaxf(a.resid[pi] + o[r][k], 0.0f), 1.0f);
+                    if (a.log_hdr) a.final_out[po] = expm1f(fmaxf(log1pf(a.resid[pi]) + o[r][k], 0.0f));
+                    else a.final_out[po] = fminf(fmaxf(a.resid[pi] + o[r][k], 0.0f), 1.0f);
                 }
             }
         }
@@ -540,7 +541,7 @@ __global__ void pack_dgrad_kernel(const float* __restrict__ w, int Cout, int Cin
 }
 
 __global__ void to_blocked_kernel(const float* __restrict__ x, int N, int C, int H, int W,
-                                  __nv_bfloat16* __restrict__ out, int Cpad)
+                                  __nv_bfloat16* __restrict__ out, int Cpad, int log1p_in)
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over N * Cpad * H * W
     const size_t total = (size_t)N * Cpad * H * W;
@@ -553,6 +554,7 @@ __global__ void to_blocked_kernel(const float* __restrict__ x, int N, int C, int
     const int n = (int)r;
     const int c = b * 8 + e;
     float v = c < C ? x[(((size_t)n * C + c) * H + y) * W + xx] : 0.0f;
+    if (log1p_in) v = log1pf(v);
     out[i] = __float2bfloat16_rn(v);
 }
 
@@ -613,10 +615,10 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
 }
 
 cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,
-                            cudaStream_t stream)
+                            cudaStream_t stream, bool log1p_in)
 {
     const size_t total = (size_t)N * Cpad * H * W;
-    to_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(x, N, C, H, W, out, Cpad);
+    to_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(x, N, C, H, W, out, Cpad, log1p_in ? 1 : 0);
     return cudaGetLastError();
 }
 

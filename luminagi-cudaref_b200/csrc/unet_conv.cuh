@@ -22,6 +22,7 @@ enum ConvEpilogue : int
     kEpiStore = 0,     // act(acc + bias) -> out (and, if out2, 2x2 max-pooled -> out2)
     kEpiUpsample = 1,  // act(acc + bias) -> out at 2x resolution (nearest, 4 copies)
     kEpiTail = 2,      // act(acc + bias) -> out (optional); 1x1 conv to 3 + residual + clamp -> final (FP32 NCHW)
+                       // (log_hdr: residual on log1p(input), out = expm1(max(y, 0)))
     // Backward (input-gradient) epilogues; no bias is added.
     kEpiBwdMask = 3,     // out = acc * act'(ref) at the same position
     kEpiBwdSumPool = 4,  // acc at 2x resolution -> 2x2 sum -> * act'(ref at 1x) -> out (1x)
@@ -46,6 +47,7 @@ struct ConvArgs
     const float* tail_b;         // [3]
     const float* resid;          // FP32 NCHW input image (kEpiTail), channels 0..2 used, resid_C channels
     int resid_C;
+    int log_hdr;                 // kEpiTail: the HDR variant's log-space residual and expm1 output
     float* final_out;            // FP32 NCHW [N][3][H][W]
     int* err;                    // set non-zero by a kernel that hit a wait limit
     // backward epilogues
@@ -71,9 +73,21 @@ cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, in
 // Launches the convolution reading `in` (blocked BF16, N x Cin x H x W).
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream);
 
-// FP32 NCHW (C channels) -> blocked BF16 with Cpad channels (zero padded).
+// FP32 NCHW (C channels) -> blocked BF16 with Cpad channels (zero padded);
+// log1p_in applies log1p to every value first (the HDR variant's input).
 cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,
-                            cudaStream_t stream);
+                            cudaStream_t stream, bool log1p_in = false);
+
+// Bilinear 2x upsampling (F.interpolate(scale_factor=2, mode="bilinear",
+// align_corners=False)) of a blocked BF16 tensor N x C x h x w into channels
+// [coff, coff + C) of a blocked tensor N x out_C x 2h x 2w.
+cudaError_t bilinear_up2(const __nv_bfloat16* in, int N, int C, int h, int w, __nv_bfloat16* out, int out_C,
+                         int coff, cudaStream_t stream);
+// Its adjoint, masked by the activation derivative: g_lo = up2^T(g_hi) *
+// act'(ref), where g_hi is N x C x 2h x 2w and ref, g_lo are N x C x h x w
+// (all blocked BF16).
+cudaError_t bilinear_up2_adjoint(const __nv_bfloat16* g_hi, int N, int C, int h, int w, const __nv_bfloat16* ref,
+                                 float slope, __nv_bfloat16* g_lo, cudaStream_t stream);
 // Blocked BF16 (C channels) -> FP32 NCHW.
 cudaError_t from_blocked_bf16(const __nv_bfloat16* in, int N, int C, int H, int W, float* out, cudaStream_t stream);
 }  // namespace lg

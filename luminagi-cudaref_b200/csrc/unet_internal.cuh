@@ -52,6 +52,8 @@ struct lg_unet
     int device = 0;
     int in_ch = 3;  // input channels: 3 (colour) or 12 (colour + albedo, normal, position)
     float slope = 0.1f;
+    bool bilinear = false;  // decoder upsampling: nearest (reference) or bilinear
+    bool log_hdr = false;   // log1p input, log-space residual, expm1 output (HDR variant)
     cudaStream_t stream = nullptr;
     // parameters (FP32, state_dict order) and packed BF16 weights
     Buf params;     // all FP32 params contiguous
@@ -61,6 +63,7 @@ struct lg_unet
     // activations, sized for (N, H, W)
     int aN = 0, aH = 0, aW = 0;
     Buf x0, t1, cat1, p1, t2, cat2, p2, t3, cat3, p3, t4, t5, t6, t7, u1, xin, yout, err;
+    Buf lo7, lo9, lo11;  // bilinear mode: low-resolution outputs of the convs before each upsampling
     // training state
     int sm_count = 148;
     Buf grads, adam_m, adam_v, loss;
@@ -69,6 +72,7 @@ struct lg_unet
     long long adam_t = 0;
     int gN = 0, gH = 0, gW = 0;
     Buf dz[14], gs1, gs2, gs3, tgt;
+    Buf gup;  // bilinear mode: full-resolution gradient of an upsampled concat half
 };
 
 namespace lg

@@ -44,7 +44,7 @@ constexpr DgradDef kDgrad[16] = {
 __device__ __forceinline__ float dact(float y, float slope) { return y > 0.0f ? 1.0f : slope; }
 
 // One thread per pixel.  u1: blocked BF16 (32 ch); x, target, pred: FP32 NCHW.
-__global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __restrict__ x, int xC,
+__global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __restrict__ x, int xC, int log_hdr,
                                      const float* __restrict__ target, const float* __restrict__ tw,
                                      const float* __restrict__ tb, int N, int H, int W, float slope, float inv_numel,
                                      bf* __restrict__ dz, float* __restrict__ dtw, float* __restrict__ dtb,
@@ -82,12 +82,14 @@ __global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __r
 #pragma unroll
             for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&tw[k * 32 + c]), v[c], acc);
             const size_t pi = ((size_t)n * 3 + k) * HW + q;
-            const float pre = x[((size_t)n * xC + k) * HW + q] + acc;
-            const float pred = fminf(fmaxf(pre, 0.0f), 1.0f);
-            const float diff = pred - target[pi];
+            const float xv = x[((size_t)n * xC + k) * HW + q];
+            // reference: L1(clamp(x + t, 0, 1), target); HDR variant: L1(max(log1p(x) + t, 0), log1p(target))
+            const float pre = (log_hdr ? log1pf(xv) : xv) + acc;
+            const float pred = log_hdr ? fmaxf(pre, 0.0f) : fminf(fmaxf(pre, 0.0f), 1.0f);
+            const float diff = pred - (log_hdr ? log1pf(target[pi]) : target[pi]);
             l += fabsf(diff);
             const float g = (diff > 0.0f ? 1.0f : (diff < 0.0f ? -1.0f : 0.0f)) * inv_numel;
-            gpre[k] = (pre >= 0.0f && pre <= 1.0f) ? g : 0.0f;
+            gpre[k] = (pre >= 0.0f && (log_hdr || pre <= 1.0f)) ? g : 0.0f;
             gtb[k] = gpre[k];
         }
 #pragma unroll
@@ -175,6 +177,7 @@ int ensure_train(lg_unet* u, int N, int H, int W)
     LG_TRY(u->gs1.ensure(px * 32 * b2));
     LG_TRY(u->gs2.ensure(px / 4 * 64 * b2));
     LG_TRY(u->gs3.ensure(px / 16 * 128 * b2));
+    if (u->bilinear) LG_TRY(u->gup.ensure(px * 64 * b2));  // largest upsampled half: 64 ch at full size
     u->gN = N;
     u->gH = H;
     u->gW = W;
@@ -211,7 +214,7 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
     const long long npx = (long long)N * H * W;
     const float inv_numel = 1.0f / (float)(npx * 3);
     tail_backward_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(
-        (const bf*)u->u1.p, d_x, u->in_ch, d_t, P + u->tail_w_off, P + u->tail_b_off, N, H, W, u->slope, inv_numel,
+        (const bf*)u->u1.p, d_x, u->in_ch, u->log_hdr ? 1 : 0, d_t, P + u->tail_w_off, P + u->tail_b_off, N, H, W, u->slope, inv_numel,
         (bf*)u->dz[13].p, G + u->tail_w_off, G + u->tail_b_off, (float*)u->loss.p);
     LG_TRY_CUDA(cudaGetLastError());
 
@@ -236,7 +239,7 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
         return LG_OK;
     };
     auto dgrad = [&](int k, void* out, int out_c, const void* ref, int ref_c, int ref_coff, const void* skip,
-                     int skip_c) -> int {
+                     int skip_c, int epi = -1) -> int {
         const DgradDef& d = kDgrad[k];
         const int lv = lv_out[d.layer];  // the backward conv runs at the forward layer's resolution
         ConvArgs a{};
@@ -247,7 +250,7 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
         a.Cout = d.ci_cnt;
         a.wpack = (const bf*)u->packed_dg[k].p;
         a.slope = u->slope;
-        a.epilogue = d.epi;
+        a.epilogue = epi >= 0 ? epi : d.epi;
         a.out = (bf*)out;
         a.out_C = out_c;
         a.out_coff = 0;
@@ -265,17 +268,28 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
     LG_TRY(wgrad(13));
     LG_TRY(dgrad(0, u->dz[12].p, 32, u->t7.p, 32, 0, nullptr, 0));
     LG_TRY(wgrad(12));
-    LG_TRY(dgrad(1, u->dz[11].p, 64, u->cat1.p, 96, 0, nullptr, 0));
+    // Gradient of an upsampled concat half back to the low-resolution conv
+    // output: the 2x2 sum of nearest upsampling fused in the epilogue, or
+    // (bilinear) the full-resolution gradient stored and passed through the
+    // upsampling's adjoint, each times act' of the stored output.
+    auto up_grad = [&](int k, int layer, void* cat, int cat_c, const Buf& lo, int c, int h, int w) -> int {
+        if (!u->bilinear) return dgrad(k, u->dz[layer].p, c, cat, cat_c, 0, nullptr, 0);
+        LG_TRY(dgrad(k, u->gup.p, c, nullptr, 0, 0, nullptr, 0, kEpiBwdStore));
+        LG_TRY_CUDA(bilinear_up2_adjoint((const bf*)u->gup.p, N, c, h, w, (const bf*)lo.p, u->slope,
+                                         (bf*)u->dz[layer].p, st));
+        return LG_OK;
+    };
+    LG_TRY(up_grad(1, 11, u->cat1.p, 96, u->lo11, 64, H / 2, W / 2));
     LG_TRY(dgrad(2, u->gs1.p, 32, nullptr, 0, 0, nullptr, 0));
     LG_TRY(wgrad(11));
     LG_TRY(dgrad(3, u->dz[10].p, 64, u->t6.p, 64, 0, nullptr, 0));
     LG_TRY(wgrad(10));
-    LG_TRY(dgrad(4, u->dz[9].p, 128, u->cat2.p, 192, 0, nullptr, 0));
+    LG_TRY(up_grad(4, 9, u->cat2.p, 192, u->lo9, 128, H / 4, W / 4));
     LG_TRY(dgrad(5, u->gs2.p, 64, nullptr, 0, 0, nullptr, 0));
     LG_TRY(wgrad(9));
     LG_TRY(dgrad(6, u->dz[8].p, 128, u->t5.p, 128, 0, nullptr, 0));
     LG_TRY(wgrad(8));
-    LG_TRY(dgrad(7, u->dz[7].p, 256, u->cat3.p, 384, 0, nullptr, 0));
+    LG_TRY(up_grad(7, 7, u->cat3.p, 384, u->lo7, 256, H / 8, W / 8));
     LG_TRY(dgrad(8, u->gs3.p, 128, nullptr, 0, 0, nullptr, 0));
     // encoder
     LG_TRY(wgrad(7));

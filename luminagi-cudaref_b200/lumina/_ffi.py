@@ -27,6 +27,7 @@ LG_ERR_CAPACITY = -7
 LG_RENDER_ACCUM64 = 1
 LG_ISECT_MOLLER_TRUMBORE = 0
 LG_ISECT_WATERTIGHT = 1
+LG_UNET_RELU, LG_UNET_BILINEAR, LG_UNET_LOG_HDR, LG_UNET_HDR_VARIANT = 1, 2, 4, 7
 
 # Record layouts (byte-identical to the reference's Triangle / BvhNode / lights).
 TRI_DTYPE = np.dtype([("v", "<f4", (3, 3)), ("n", "<f4", (3, 3)), ("uv", "<f4", (3, 2)), ("material", "<i4")])
@@ -123,6 +124,8 @@ SIGNATURES = {
     "lg_from_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "lg_rgb8_to_f32": (_I, [_P, _I, _I, _I, _P, _P]),
     "lg_f32_to_rgb8": (_I, [_P, _I, _I, _I, _P, _P]),
+    "lg_accum_to_f32": (_I, [_P, _I, _I, _I, C.c_float, _P, _P]),
+    "lg_f32_tonemap_rgb8": (_I, [_P, _I, _I, _I, _P, _P]),
     "lg_gather_crops": (_I, [_P, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P]),
     "lg_write_png": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),
     "lg_write_hdr": (_I, [C.c_char_p, C.c_int32, C.c_int32, _P]),

@@ -41,6 +41,8 @@ def main(argv=None) -> int:
     base, in_ch = ck.get("base", 32), ck.get("in_ch", 3)
     if in_ch not in (3, 12):
         sys.exit(f"checkpoint expects {in_ch}-ch input; not supported by this script")
+    if ck.get("variant", "ref") != "ref":
+        sys.exit("checkpoint is the HDR variant (radiance in/out); this script denoises 8-bit PNGs")
     net = UNet(base=base, in_ch=in_ch)
     net.load_state_dict(ck["model"])
 

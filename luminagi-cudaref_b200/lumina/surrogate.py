@@ -10,6 +10,8 @@
      (the last one partial); L1 loss; Adam; validation L1 on crops of the
      held-out poses; the best-validation parameters are kept and saved in the
      reference checkpoint format {"model", "base", "in_ch"}.
+     With --variant hdr the network is the configuration-4 one (ReLU,
+     bilinear upsampling, log1p HDR radiance in/out) trained on accum/spp.
      With --gbuffer the network is train.py's 12-channel variant: the input
      stacks the noisy colour with the albedo, normal and position images of
      the G-buffer pass (train.py:112-119); the residual stays on colour.
@@ -41,13 +43,18 @@ def _torch():
     return torch
 
 
-def render_to_f32(r: Renderer, cam, spp: int, bounces: int, out_ptr: int, sample_base: int = 0):
-    """Renders one frame and writes its tonemapped u8/255 image (3 x H x W FP32) at out_ptr."""
+def render_to_f32(r: Renderer, cam, spp: int, bounces: int, out_ptr: int, sample_base: int = 0, hdr: bool = False):
+    """Renders one frame into 3 x H x W FP32 at out_ptr: its tonemapped u8/255
+    image (reference variant) or its linear radiance accum/spp (hdr)."""
     c = cam.to_c()
     o = _ffi.LgRenderOpts(spp, bounces, sample_base, 0)
-    rgb = C.c_void_p()
-    _ffi.check(_ffi.lib().lg_render_device(r._h, C.byref(c), C.byref(o), None, C.byref(rgb), None, None))
-    _ffi.check(_ffi.lib().lg_rgb8_to_f32(rgb, 1, int(cam.height), int(cam.width), C.c_void_p(out_ptr), None))
+    rgb, acc = C.c_void_p(), C.c_void_p()
+    _ffi.check(_ffi.lib().lg_render_device(r._h, C.byref(c), C.byref(o), None, C.byref(rgb), C.byref(acc), None))
+    H, W = int(cam.height), int(cam.width)
+    if hdr:
+        _ffi.check(_ffi.lib().lg_accum_to_f32(acc, 1, H, W, 1.0 / spp, C.c_void_p(out_ptr), None))
+    else:
+        _ffi.check(_ffi.lib().lg_rgb8_to_f32(rgb, 1, H, W, C.c_void_p(out_ptr), None))
 
 
 def judge_u8(r: Renderer, cam, spp: int, bounces: int) -> np.ndarray:
@@ -66,23 +73,24 @@ def gbuffer_to_f32(r: Renderer, cam, out_ptr: int) -> None:
     torch.cuda.synchronize()
 
 
-def make_input(r: Renderer, cam, spp: int, bounces: int, out, sample_base: int = 0) -> None:
+def make_input(r: Renderer, cam, spp: int, bounces: int, out, sample_base: int = 0, hdr: bool = False) -> None:
     """Network input of one frame into out (C x H x W, C = 3 or 12): the
     render, then for 12 channels the G-buffer images after it."""
-    render_to_f32(r, cam, spp, bounces, out.data_ptr(), sample_base)
+    render_to_f32(r, cam, spp, bounces, out.data_ptr(), sample_base, hdr)
     if out.shape[0] == 12:
         gbuffer_to_f32(r, cam, out[3].data_ptr())
 
 
-def make_dataset(r: Renderer, cams, noisy_spp: int, clean_spp: int, bounces: int, in_ch: int = 3):
+def make_dataset(r: Renderer, cams, noisy_spp: int, clean_spp: int, bounces: int, in_ch: int = 3,
+                 hdr: bool = False):
     torch = _torch()
     H, W = int(cams[0].height), int(cams[0].width)
     noisy = torch.empty((len(cams), in_ch, H, W), device="cuda")
     clean = torch.empty((len(cams), 3, H, W), device="cuda")
     for i, cam in enumerate(cams):
-        make_input(r, cam, noisy_spp, bounces, noisy[i])
+        make_input(r, cam, noisy_spp, bounces, noisy[i], hdr=hdr)
         # a disjoint sample range keeps the clean target independent of the noisy input
-        render_to_f32(r, cam, clean_spp, bounces, clean[i].data_ptr(), sample_base=100000)
+        render_to_f32(r, cam, clean_spp, bounces, clean[i].data_ptr(), sample_base=100000, hdr=hdr)
     torch.cuda.synchronize()
     return noisy, clean
 
@@ -136,14 +144,18 @@ def train(net: UNet, noisy, clean, train_idx, val_idx, epochs=120, batch=16, cro
     return best, best_val, hist
 
 
-def save_checkpoint(params: np.ndarray, path: str, in_ch: int = 3) -> None:
-    """Reference checkpoint format (ml/train.py:216), loadable by tools/denoise.py."""
+def save_checkpoint(params: np.ndarray, path: str, in_ch: int = 3, variant: str = "ref") -> None:
+    """Reference checkpoint format (ml/train.py:216), loadable by tools/denoise.py;
+    the hdr variant adds "variant": "hdr"."""
     torch = _torch()
     sd = {k: torch.from_numpy(np.ascontiguousarray(v)) for k, v in unflatten(params, in_ch).items()}
-    torch.save({"model": sd, "base": 32, "in_ch": in_ch}, path)
+    ck = {"model": sd, "base": 32, "in_ch": in_ch}
+    if variant != "ref":
+        ck["variant"] = variant
+    torch.save(ck, path)
 
 
-def eval_frames(r: Renderer, cams, noisy_spp, clean_spp, judge_spp, bounces, in_ch: int = 3):
+def eval_frames(r: Renderer, cams, noisy_spp, clean_spp, judge_spp, bounces, in_ch: int = 3, hdr: bool = False):
     """Held-out frames: judge (FP64 accumulators), noisy and clean renders with their device times."""
     torch = _torch()
     H, W = int(cams[0].height), int(cams[0].width)
@@ -154,7 +166,7 @@ def eval_frames(r: Renderer, cams, noisy_spp, clean_spp, judge_spp, bounces, in_
         noisy = r.render(camera=cam, spp=noisy_spp, bounces=bounces, accum=False)
         clean = r.render(camera=cam, spp=clean_spp, bounces=bounces, accum=False, sample_base=100000)
         x = torch.empty((1, in_ch, H, W), device="cuda")
-        make_input(r, cam, noisy_spp, bounces, x[0])
+        make_input(r, cam, noisy_spp, bounces, x[0], hdr=hdr)
         out.append({"judge": judge, "noisy": noisy["rgb"], "clean": clean["rgb"], "x": x,
                     "noisy_ms": noisy["kernel_ms"], "clean_ms": clean["kernel_ms"]})
     return out
@@ -175,8 +187,8 @@ def evaluate(net: UNet, frames):
         e0.record(st)
         net.forward_device(x.data_ptr(), 1, H, W, y.data_ptr(), st.cuda_stream)
         e1.record(st)
-        _ffi.check(_ffi.lib().lg_f32_to_rgb8(C.c_void_p(y.data_ptr()), 1, H, W, C.c_void_p(u8.data_ptr()),
-                                            C.c_void_p(st.cuda_stream)))
+        to_u8 = _ffi.lib().lg_f32_tonemap_rgb8 if net.variant == "hdr" else _ffi.lib().lg_f32_to_rgb8
+        _ffi.check(to_u8(C.c_void_p(y.data_ptr()), 1, H, W, C.c_void_p(u8.data_ptr()), C.c_void_p(st.cuda_stream)))
         torch.cuda.synchronize()
         den = u8.cpu().numpy().reshape(H, W, 3)
         row = {"noisy_ms": f["noisy_ms"], "unet_ms": e0.elapsed_time(e1), "clean_ms": f["clean_ms"]}
@@ -221,27 +233,30 @@ def main(argv=None):
     ap.add_argument("--checkpoint", default="")
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--gbuffer", action="store_true", help="12-channel network on colour + G-buffer (train.py --gbuffer)")
+    ap.add_argument("--variant", default="ref", choices=["ref", "hdr"],
+                    help="ref: the reference network on u8/255 frames; hdr: ReLU, bilinear, log1p HDR radiance")
     a = ap.parse_args(argv)
     in_ch = 12 if a.gbuffer else 3
+    hdr = a.variant == "hdr"
     torch = _torch()
     t0 = time.time()
     sc = engine_scene(seed=7, width=a.width, height=a.height)
     r = Renderer(0)
     r.set_scene(sc)
     cams = [sc.camera.look_at(p, t) for p, t in orbit_poses(a.poses, seed=11, center=ENGINE_CENTER)]
-    noisy, clean = make_dataset(r, cams, a.noisy_spp, a.clean_spp, a.bounces, in_ch)
+    noisy, clean = make_dataset(r, cams, a.noisy_spp, a.clean_spp, a.bounces, in_ch, hdr)
     t_data = time.time() - t0
     perm = np.random.RandomState(a.seed).permutation(a.poses)
     val_idx, train_idx = perm[:a.val].tolist(), perm[a.val:].tolist()
     t1 = time.time()
-    frames = eval_frames(r, [cams[i] for i in val_idx], a.noisy_spp, a.clean_spp, a.judge_spp, a.bounces, in_ch)
+    frames = eval_frames(r, [cams[i] for i in val_idx], a.noisy_spp, a.clean_spp, a.judge_spp, a.bounces, in_ch, hdr)
     t_judge = time.time() - t1
     recipes = a.recipe or ["config:120:16:128:1e-4:1"]
     res = {"config": vars(a), "triangles": sc.n_tris, "train_poses": len(train_idx), "val_poses": len(val_idx),
            "data_seconds": t_data, "eval_render_seconds": t_judge, "recipes": {}}
     for spec in recipes:
         name, ep, bs, cr, lr, cpi = spec.split(":")
-        net = UNet(in_ch=in_ch)
+        net = UNet(in_ch=in_ch, variant=a.variant)
         net.set_params(he_init(a.seed, in_ch))
         t2 = time.time()
         best, best_val, hist = train(net, noisy, clean, train_idx, val_idx, int(ep), int(bs), int(cr), float(lr),
@@ -249,7 +264,7 @@ def main(argv=None):
         t_train = time.time() - t2
         net.set_params(best)
         if a.checkpoint:
-            save_checkpoint(best, f"{a.checkpoint}.{name}.pt", in_ch)
+            save_checkpoint(best, f"{a.checkpoint}.{name}.pt", in_ch, a.variant)
         agg, rows = evaluate(net, frames)
         res["recipes"][name] = {"spec": spec, "train_seconds": t_train, "best_val_l1": best_val,
                                 "history_tail": hist[-3:], "eval": agg, "per_pose": rows}

@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._ffi import check, lib, ptr
+from ._ffi import LG_UNET_HDR_VARIANT, LG_UNET_RELU, check, lib, ptr
 
 # state_dict keys and shapes of the reference UNet(base=32, in_ch).
 _BLOCKS = [("d1", None, 32), ("d2", 32, 64), ("d3", 64, 128), ("d4", 128, 256), ("u3", 384, 128), ("u2", 192, 64),
@@ -51,10 +51,18 @@ def unflatten(flat: np.ndarray, in_ch: int = 3) -> dict:
 
 
 class UNet:
-    def __init__(self, base: int = 32, in_ch: int = 3, act: str = "leaky"):
+    """variant "ref": the reference network (LeakyReLU 0.1, nearest upsampling,
+    [0,1] images, clamped residual); "hdr": ReLU, bilinear upsampling, HDR
+    radiance in and out through log1p/expm1 (the configuration-4 network).
+    act="relu" swaps only the activation of the reference variant."""
+
+    def __init__(self, base: int = 32, in_ch: int = 3, act: str = "leaky", variant: str = "ref"):
         self._h = C.c_void_p()
-        check(lib().lg_unet_create(base, in_ch, 0 if act == "leaky" else 1, C.byref(self._h)))
+        assert variant in ("ref", "hdr")
+        mode = LG_UNET_HDR_VARIANT if variant == "hdr" else (0 if act == "leaky" else LG_UNET_RELU)
+        check(lib().lg_unet_create(base, in_ch, mode, C.byref(self._h)))
         self.in_ch = in_ch
+        self.variant = variant
         self.n_params = int(lib().lg_unet_num_params(self._h))
         assert self.n_params == int(sum(np.prod(s) for _, s in param_shapes(in_ch)))
 
@@ -85,9 +93,10 @@ class UNet:
         """Loads a reference checkpoint dict {"model": state_dict, "base", "in_ch"} (ml/train.py:216)."""
         import torch
         ck = torch.load(path, map_location="cpu", weights_only=True)
-        if ck.get("base", 32) != 32 or ck.get("in_ch", 3) != self.in_ch:
-            raise ValueError(f"checkpoint is base={ck.get('base', 32)}, in_ch={ck.get('in_ch', 3)}; "
-                             f"this UNet is base=32, in_ch={self.in_ch}")
+        if ck.get("base", 32) != 32 or ck.get("in_ch", 3) != self.in_ch or ck.get("variant", "ref") != self.variant:
+            raise ValueError(f"checkpoint is base={ck.get('base', 32)}, in_ch={ck.get('in_ch', 3)}, "
+                             f"variant={ck.get('variant', 'ref')}; this UNet is base=32, in_ch={self.in_ch}, "
+                             f"variant={self.variant}")
         self.load_state_dict(ck["model"])
 
     def forward(self, x: np.ndarray) -> np.ndarray:
@@ -122,6 +131,14 @@ class UNet:
 
     def adam_reset(self) -> None:
         check(lib().lg_unet_adam_reset(self._h))
+
+    def denoise_hdr(self, radiance: np.ndarray) -> np.ndarray:
+        """HDR variant: (H,W,3) FP32 linear radiance -> (H,W,3), edge-padded to multiples of 8."""
+        assert self.variant == "hdr" and self.in_ch == 3
+        H, W = radiance.shape[:2]
+        ph, pw = (8 - H % 8) % 8, (8 - W % 8) % 8
+        x = np.pad(np.asarray(radiance, np.float32), ((0, ph), (0, pw), (0, 0)), mode="edge")
+        return self.forward(x.transpose(2, 0, 1)[None])[0].transpose(1, 2, 0)[:H, :W].copy()
 
     def denoise_rgb8(self, img: np.ndarray, albedo=None, normal=None, worldpos=None) -> np.ndarray:
         """tools/denoise.py:34-52: (H,W,3) u8 -> (H,W,3) u8.  A 12-channel

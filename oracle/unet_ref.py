@@ -8,6 +8,11 @@ reference's; pinned to the reference module by tests/golden/unet_golden.npz
   * forward_bf16(model, x): the same network with BF16 rounding at exactly the
     points where this project's tensor-core kernels round (inputs and weights
     of every conv, every stored activation), FP32 everywhere else.
+  * variant="hdr": the configuration-4 network the reference does not ship --
+    ReLU, bilinear 2x upsampling (align_corners=False), log1p applied to the
+    input and the residual taken in log space, output expm1(max(y, 0)).  Its
+    loss (hdr_loss) is L1 between max(y, 0) and log1p(target).  Only this
+    restatement defines it, so its parity is against this module alone.
 """
 from __future__ import annotations
 
@@ -28,10 +33,13 @@ class ConvBlock(nn.Module):
 
 
 class UNetRef(nn.Module):
-    """ml/train.py:51-75 (base 32, 3 input channels)."""
+    """ml/train.py:51-75 (base 32; 3 or 12 input channels); variant "hdr" as above."""
 
-    def __init__(self, base=32, in_ch=3, slope=0.1):
+    def __init__(self, base=32, in_ch=3, slope=0.1, variant="ref"):
         super().__init__()
+        assert variant in ("ref", "hdr")
+        self.variant = variant
+        slope = 0.0 if variant == "hdr" else slope
         self.slope = slope
         self.d1 = ConvBlock(in_ch, base, slope)
         self.d2 = ConvBlock(base, base * 2, slope)
@@ -42,9 +50,19 @@ class UNetRef(nn.Module):
         self.u1 = ConvBlock(base * 2 + base, base, slope)
         self.tail = nn.Conv2d(base, 3, 1)
 
-    def forward(self, x):
+    def _up(self, t):
+        if self.variant == "hdr":
+            return F.interpolate(t, scale_factor=2, mode="bilinear", align_corners=False)
+        return F.interpolate(t, scale_factor=2, mode="nearest")
+
+    def forward_log(self, x):
+        """hdr variant: max(log1p(x)[:, :3] + tail, 0) (the network output in log space)."""
+        assert self.variant == "hdr"
+        return torch.clamp(self._body(torch.log1p(x)), min=0.0)
+
+    def _body(self, x):
         pool = lambda t: F.max_pool2d(t, 2)
-        up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")
+        up = self._up
         d1 = self.d1(x)
         d2 = self.d2(pool(d1))
         d3 = self.d3(pool(d2))
@@ -52,7 +70,17 @@ class UNetRef(nn.Module):
         u3 = self.u3(torch.cat([up(d4), d3], 1))
         u2 = self.u2(torch.cat([up(u3), d2], 1))
         u1 = self.u1(torch.cat([up(u2), d1], 1))
-        return torch.clamp(x[:, :3] + self.tail(u1), 0.0, 1.0)
+        return x[:, :3] + self.tail(u1)
+
+    def forward(self, x):
+        if self.variant == "hdr":
+            return torch.expm1(self.forward_log(x))
+        return torch.clamp(self._body(x), 0.0, 1.0)
+
+
+def hdr_loss(model: UNetRef, x: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
+    """Training loss of the hdr variant: L1 in log1p space."""
+    return F.l1_loss(model.forward_log(x), torch.log1p(target))
 
 
 def param_shapes(model: nn.Module):
@@ -100,6 +128,9 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32) -> torch.
         return t.to(torch.bfloat16).to(dtype)
 
     x = x.to(dtype)
+    hdr = getattr(model, "variant", "ref") == "hdr"
+    if hdr:
+        x = torch.log1p(x)
 
     def conv(block_conv, t):
         return F.conv2d(_q(t), _q(block_conv.weight.to(dtype)), block_conv.bias.to(dtype), padding=1)
@@ -109,7 +140,10 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32) -> torch.
         return _q(F.leaky_relu(conv(b.net[2], t), s))
 
     pool = lambda t: F.max_pool2d(t, 2)
-    up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")
+    if hdr:  # interpolated from the stored (BF16) low-resolution output, stored again as BF16
+        up = lambda t: _q(F.interpolate(t, scale_factor=2, mode="bilinear", align_corners=False))
+    else:
+        up = lambda t: F.interpolate(t, scale_factor=2, mode="nearest")
     d1 = block(model.d1, x)
     d2 = block(model.d2, pool(d1))
     d3 = block(model.d3, pool(d2))
@@ -118,4 +152,6 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32) -> torch.
     u2 = block(model.u2, torch.cat([up(u3), d2], 1))
     u1 = block(model.u1, torch.cat([up(u2), d1], 1))
     tail = F.conv2d(u1, model.tail.weight.to(dtype), model.tail.bias.to(dtype))
+    if hdr:
+        return torch.expm1(torch.clamp(x[:, :3] + tail, min=0.0))
     return torch.clamp(x[:, :3] + tail, 0.0, 1.0)
