@@ -190,8 +190,13 @@ int lg_render(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, 
  * renderer until the next call; pointers are returned (any may be NULL). */
 int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, void* stream,
                      const uint8_t** d_rgb8, const float** d_accum, const double** d_accum64);
-/* n_jobs frames with per-job cameras and spp, tonemapped into rgb8_out
- * (n_jobs * W*H*3 bytes, host). */
+/* n_jobs frames (per-job camera, size, spp, bounces, sample_base) traced in
+ * ONE persistent launch: the (pixel, chunk of 8 samples) items of all frames
+ * share one work counter, so the GPU stays full across frames.  The job-table
+ * upload, clears, trace and tonemaps are replayed from a CUDA graph while the
+ * frame sizes and spp repeat.  rgb8_out receives the frames one after another
+ * (sum of W*H*3 bytes, host).  ms_per_job: the launch's device time
+ * apportioned to the frames by work items.  Same images as lg_render per job. */
 int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts* opts, int32_t n_jobs,
                     uint8_t* rgb8_out, float* ms_per_job);
 

@@ -119,6 +119,14 @@ struct lg_renderer
     // frame
     DevBuf accum, accum64, rgb, work, counters;
     int fw = 0, fh = 0;
+    // batched launches: job table (pinned host copy + device), frames, and the
+    // CUDA graph of the last batch shape (job table upload, clears, trace, tonemaps)
+    DevBuf batch_jobs, batch_acc, batch_rgb;
+    BatchJob* batch_host = nullptr;
+    int batch_host_cap = 0;
+    cudaGraphExec_t batch_exec = nullptr;
+    std::vector<long long> batch_key;
+    long long scene_gen = 0;  // bumped by every change a captured launch depends on
 };
 
 namespace
@@ -170,6 +178,7 @@ int upload_common(lg_renderer* r, const lg_scene_desc* d)
 {
     if (r->stream) cudaStreamSynchronize(r->stream);
     r->n_mats = d->n_mats;
+    ++r->scene_gen;
     clear_textures(r);  // a new scene starts untextured
     r->n_points = d->n_points;
     r->sun = d->sun;
@@ -577,6 +586,9 @@ void lg_renderer_destroy(lg_renderer* r)
     clear_textures(r);
     r->texs.release();
     r->gbuf.release();
+    if (r->batch_exec) cudaGraphExecDestroy(r->batch_exec);
+    if (r->batch_host) cudaFreeHost(r->batch_host);
+    for (DevBuf* b : {&r->batch_jobs, &r->batch_acc, &r->batch_rgb}) b->release();
     for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
         b->release();
@@ -708,6 +720,7 @@ int lg_renderer_set_texture(lg_renderer* r, int material, const uint8_t* rgba8, 
         r->tex_objs[m] = (unsigned long long)obj;
         ++r->n_textured;
     }
+    ++r->scene_gen;
     LG_TRY(r->texs.reserve((size_t)std::max(r->n_mats, 1) * sizeof(unsigned long long)));
     LG_TRY_CUDA(cudaMemcpy(r->texs.p, r->tex_objs.data(), (size_t)r->n_mats * sizeof(unsigned long long),
                            cudaMemcpyHostToDevice));
@@ -752,6 +765,7 @@ int lg_renderer_set_intersection(lg_renderer* r, int mode)
     if (wt == r->watertight) return LG_OK;
     DeviceGuard g(r->device);
     r->watertight = wt;
+    ++r->scene_gen;
     if (r->n_tris > 0)
     {
         LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), wt, r->stream));
@@ -819,19 +833,114 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
                     uint8_t* rgb8_out, float* ms_per_job)
 {
     if (!r || !cams || !opts || n_jobs < 0) return set_error(LG_ERR_INVALID, "bad argument");
+    if (n_jobs == 0) return LG_OK;
     DeviceGuard g(r->device);
-    size_t off = 0;
+    // Every frame's (pixel, chunk of 8 samples) items in one persistent launch,
+    // numbered frame after frame; frames go to consecutive accumulators.
+    std::vector<size_t> acc_off((size_t)n_jobs + 1, 0);
+    unsigned long long items = 0;
+    std::vector<unsigned long long> item_begin((size_t)n_jobs);
+    std::vector<long long> key;
+    key.reserve((size_t)n_jobs * 3 + 4);
     for (int j = 0; j < n_jobs; ++j)
     {
-        lg_render_stats st{};
-        LG_TRY(render_into_device(r, &cams[j], &opts[j], &st));
-        const size_t nval = (size_t)cams[j].width * cams[j].height * 3;
-        if (rgb8_out)
-            LG_TRY_CUDA(cudaMemcpyAsync(rgb8_out + off, r->rgb.p, nval, cudaMemcpyDeviceToHost, r->stream));
-        off += nval;
-        if (ms_per_job) ms_per_job[j] = st.kernel_ms;
+        const lg_camera& c = cams[j];
+        const lg_render_opts& o = opts[j];
+        if (c.width <= 0 || c.height <= 0) return set_error(LG_ERR_INVALID, "job %d: image size %dx%d", j, c.width, c.height);
+        if (o.spp < 0 || o.max_bounces < 0) return set_error(LG_ERR_INVALID, "job %d: spp/bounces must be >= 0", j);
+        if (o.flags & LG_RENDER_ACCUM64) return set_error(LG_ERR_INVALID, "job %d: FP64 accumulators are per-frame only", j);
+        acc_off[(size_t)j + 1] = acc_off[(size_t)j] + (size_t)c.width * c.height * 3;
+        item_begin[(size_t)j] = items;
+        const unsigned long long tiles = (unsigned long long)((c.width + 7) / 8) * ((c.height + 3) / 4);
+        items += tiles * (unsigned long long)((o.spp + 7) / 8) * 32ull;
+        key.push_back(c.width);
+        key.push_back(c.height);
+        key.push_back(o.spp);
     }
+    const size_t nval = acc_off[(size_t)n_jobs];
+    LG_TRY(r->batch_acc.reserve(nval * sizeof(float)));
+    LG_TRY(r->batch_rgb.reserve(nval));
+    LG_TRY(r->batch_jobs.reserve((size_t)n_jobs * sizeof(BatchJob)));
+    LG_TRY(r->work.reserve(256));
+    if (r->batch_host_cap < n_jobs)
+    {
+        if (r->batch_host) cudaFreeHost(r->batch_host);
+        r->batch_host = nullptr;
+        r->batch_host_cap = 0;
+        LG_TRY_CUDA(cudaMallocHost((void**)&r->batch_host, (size_t)n_jobs * sizeof(BatchJob)));
+        r->batch_host_cap = n_jobs;
+    }
+    // The job table is written into pinned memory that the graph copies from.
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    for (int j = 0; j < n_jobs; ++j)
+    {
+        BatchJob& b = r->batch_host[j];
+        b.cam = make_dev_cam(cams[j]);
+        b.item_begin = item_begin[(size_t)j];
+        b.accum = r->batch_acc.as<float>() + acc_off[(size_t)j];
+        b.spp = opts[j].spp;
+        b.max_bounces = opts[j].max_bounces;
+        b.sample_base = opts[j].sample_base;
+        b.n_chunks = (opts[j].spp + 7) / 8;
+        b.tiles_x = (cams[j].width + 7) / 8;
+        b.n_tiles = b.tiles_x * ((cams[j].height + 3) / 4);
+    }
+    // The graph depends on the frame shapes, the scene records, the buffers and the trace options.
+    const void* deps[] = {r->batch_acc.p, r->batch_rgb.p, r->batch_jobs.p, r->batch_host, r->wide.p, r->wide4.p,
+                          r->tv.p,        r->tris.p,      r->mats.p,       r->texs.p,     r->points.p, r->work.p};
+    for (const void* p : deps) key.push_back((long long)(uintptr_t)p);
+    key.push_back(r->bvh_width * 2 + (r->watertight ? 1 : 0));
+    key.push_back(r->scene_gen);
+    if (key != r->batch_key || !r->batch_exec)
+    {
+        if (r->batch_exec) cudaGraphExecDestroy(r->batch_exec);
+        r->batch_exec = nullptr;
+        r->batch_key.clear();
+        cudaStream_t st = r->stream;
+        LG_TRY_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaMemcpyAsync(r->batch_jobs.p, r->batch_host, (size_t)n_jobs * sizeof(BatchJob),
+                                        cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(r->batch_acc.p, 0, nval * sizeof(float), st);
+        if (e == cudaSuccess && r->n_nodes > 0 && items > 0)
+        {
+            TraceJob job{};
+            job.work64 = r->work.as<unsigned long long>();
+            job.jobs = r->batch_jobs.as<BatchJob>();
+            job.n_jobs = n_jobs;
+            job.total_items = items;
+            e = launch_trace_batch(dev_scene(r), job, r->sm_count, r->bvh_width, r->watertight, st);
+        }
+        for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)
+            e = launch_tonemap(r->batch_acc.as<float>() + acc_off[(size_t)j], r->batch_rgb.as<uint8_t>() + acc_off[(size_t)j],
+                               (long long)(acc_off[(size_t)j + 1] - acc_off[(size_t)j]), 1.0f / (float)opts[j].spp, st);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+        if (e == cudaSuccess) e = ec;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&r->batch_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess)
+        {
+            r->batch_exec = nullptr;
+            return set_error(LG_ERR_CUDA, "batched render graph: %s", cudaGetErrorString(e));
+        }
+        r->batch_key = key;
+    }
+    LG_TRY_CUDA(cudaEventRecord(r->ev0, r->stream));
+    LG_TRY_CUDA(cudaGraphLaunch(r->batch_exec, r->stream));
+    LG_TRY_CUDA(cudaEventRecord(r->ev1, r->stream));
+    if (rgb8_out) LG_TRY_CUDA(cudaMemcpyAsync(rgb8_out, r->batch_rgb.p, nval, cudaMemcpyDeviceToHost, r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    if (ms_per_job)
+    {
+        // One launch serves all frames: its time is apportioned by work items.
+        float ms = 0.0f;
+        LG_TRY_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
+        for (int j = 0; j < n_jobs; ++j)
+        {
+            const unsigned long long nj = (j + 1 < n_jobs ? item_begin[(size_t)j + 1] : items) - item_begin[(size_t)j];
+            ms_per_job[j] = items ? ms * (float)((double)nj / (double)items) : ms / (float)n_jobs;
+        }
+    }
     return LG_OK;
 }
 

@@ -633,7 +633,22 @@ struct PathState
     uint32_t rng;
     int px, py, k, n_this, bounce, li;  // li: -1 camera/bounce ray in flight, >= 0 shadow ray of light li
     unsigned pixel;                     // index of the pixel's first accumulator value
+    int job, max_bounces;               // batched launches: the frame this item belongs to
 };
+
+// Frame of a global work item in a batched launch: the last job whose
+// item_begin is <= item (jobs are in item order).
+__device__ __forceinline__ int find_job(const BatchJob* __restrict__ jobs, int n_jobs, unsigned long long item)
+{
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&jobs[mid].item_begin) <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 __device__ __forceinline__ void start_sample(PathState& st, const DevCam& cam)
 {
@@ -716,12 +731,15 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
 // the loop is one warp-wide traversal (camera, bounce or shadow ray per lane)
 // followed by a short state update.  Items are numbered chunk-major, then by
 // 8x4 pixel tile, so neighbouring lanes start on neighbouring pixels.
-template <bool kCount, bool kAcc64, int kWidth, bool kWT>
+// kBatch: several frames per launch (job.jobs), each item mapped to its frame
+// at refill; the frame's camera and bounce limit are read from the job table.
+template <bool kCount, bool kAcc64, int kWidth, bool kWT, bool kBatch>
 __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const unsigned long long total = (unsigned long long)job.n_tiles * job.n_chunks * 32ull;
+    const unsigned long long total =
+        kBatch ? job.total_items : (unsigned long long)job.n_tiles * job.n_chunks * 32ull;
     Counters cnt{0, 0, 0, 0, 0, 0};
     PathState st;
     bool active = false, exhausted = false;
@@ -738,25 +756,38 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
             if (base + __popc(need) >= total) exhausted = true;
             if (!active)
             {
-                const unsigned long long item = base + __popc(need & lt_mask);
+                unsigned long long item = base + __popc(need & lt_mask);
                 if (item < total)
                 {
+                    int n_tiles = job.n_tiles, tiles_x = job.tiles_x, spp = job.spp, sbase = job.sample_base;
+                    if (kBatch)
+                    {
+                        st.job = find_job(job.jobs, job.n_jobs, item);
+                        const BatchJob& b = job.jobs[st.job];
+                        item -= b.item_begin;  // item_begin is a multiple of 32
+                        n_tiles = b.n_tiles;
+                        tiles_x = b.tiles_x;
+                        spp = b.spp;
+                        sbase = b.sample_base;
+                        st.max_bounces = b.max_bounces;
+                    }
+                    const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
                     const unsigned j = (unsigned)(item & 31ull);
                     const unsigned long long tw = item >> 5;  // tile-wide item
-                    const int chunk = (int)(tw / (unsigned long long)job.n_tiles);
-                    const int tile = (int)(tw % (unsigned long long)job.n_tiles);
-                    st.px = (tile % job.tiles_x) * 8 + (int)(j & 7);
-                    st.py = (tile / job.tiles_x) * 4 + (int)(j >> 3);
-                    if (st.px < cam.width && st.py < cam.height)
+                    const int chunk = (int)(tw / (unsigned long long)n_tiles);
+                    const int tile = (int)(tw % (unsigned long long)n_tiles);
+                    st.px = (tile % tiles_x) * 8 + (int)(j & 7);
+                    st.py = (tile / tiles_x) * 4 + (int)(j >> 3);
+                    if (st.px < c.width && st.py < c.height)
                     {
                         const int first = chunk * 8;
-                        st.n_this = min(8, job.spp - first);
-                        const int sampleBase = job.sample_base + first;
+                        st.n_this = min(8, spp - first);
+                        const int sampleBase = sbase + first;
                         st.rng = (uint32_t)(st.px * 1973 + st.py * 9277 + sampleBase * 26699) | 1u;
                         st.sum = v3(0, 0, 0);
                         st.k = 0;
-                        st.pixel = (unsigned)((st.py * cam.width + st.px) * 3);
-                        start_sample(st, cam);
+                        st.pixel = (unsigned)((st.py * c.width + st.px) * 3);
+                        start_sample(st, c);
                         active = true;
                     }
                 }
@@ -768,11 +799,19 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
             float hitT, hitU, hitV;
             const int tri = kWidth == 4 ? traverse4<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt)
                                         : traverse<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
-            if (!advance(st, s, cam, job.max_bounces, tri, hitT, hitU, hitV))
+            const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
+            if (!advance(st, s, c, kBatch ? st.max_bounces : job.max_bounces, tri, hitT, hitU, hitV))
             {
                 active = false;
                 const unsigned i = st.pixel;
-                if (job.n_chunks == 1)
+                if (kBatch)
+                {
+                    float* acc = job.jobs[st.job].accum;
+                    atomicAdd(&acc[i + 0], st.sum.x);
+                    atomicAdd(&acc[i + 1], st.sum.y);
+                    atomicAdd(&acc[i + 2], st.sum.z);
+                }
+                else if (job.n_chunks == 1)
                 {
                     job.accum[i + 0] += st.sum.x;
                     job.accum[i + 1] += st.sum.y;
@@ -958,23 +997,34 @@ cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bo
     return cudaGetLastError();
 }
 
-template <bool kCount, bool kAcc64, int W, bool kWT>
+template <bool kCount, bool kAcc64, int W, bool kWT, bool kBatch = false>
 static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const TraceJob& job, int sm_count,
                                   cudaStream_t stream)
 {
-    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT>;
+    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT, kBatch>;
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, 0);
     if (e != cudaSuccess) return e;
-    const long long lanes = (long long)job.n_tiles * job.n_chunks * 32;
+    const long long lanes = kBatch ? (long long)job.total_items : (long long)job.n_tiles * job.n_chunks * 32;
     long long blocks = (long long)(per_sm < 1 ? 1 : per_sm) * sm_count;
     const long long useful = (lanes + kTraceThreads - 1) / kTraceThreads;
     if (blocks > useful) blocks = useful;
     if (blocks < 1) blocks = 1;
     e = cudaMemsetAsync(job.work64, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    trace_kernel<kCount, kAcc64, W, kWT><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
+    trace_kernel<kCount, kAcc64, W, kWT, kBatch><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
     return cudaGetLastError();
+}
+
+cudaError_t launch_trace_batch(const DevScene& s, const TraceJob& job, int sm_count, int width, bool watertight,
+                               cudaStream_t stream)
+{
+    const DevCam none{};
+    if (watertight)
+        return width == 4 ? launch_trace_t<false, false, 4, true, true>(s, none, job, sm_count, stream)
+                          : launch_trace_t<false, false, 2, true, true>(s, none, job, sm_count, stream);
+    return width == 4 ? launch_trace_t<false, false, 4, false, true>(s, none, job, sm_count, stream)
+                      : launch_trace_t<false, false, 2, false, true>(s, none, job, sm_count, stream);
 }
 
 template <int W, bool kWT>

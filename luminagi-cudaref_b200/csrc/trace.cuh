@@ -67,6 +67,17 @@ struct RenderCounters
     unsigned long long leaf_fetches;  // leaf-table entries read (8 B each)
 };
 
+// One frame of a batched launch: its camera and sampling, its accumulator,
+// and the number of the first of its (pixel, chunk) work items, which follow
+// the previous job's.
+struct BatchJob
+{
+    DevCam cam;
+    unsigned long long item_begin;
+    float* accum;  // W*H*3, added to
+    int spp, max_bounces, sample_base, n_chunks, tiles_x, n_tiles;
+};
+
 struct TraceJob
 {
     int spp, max_bounces, sample_base;
@@ -76,6 +87,10 @@ struct TraceJob
     double* accum64;       // optional
     unsigned long long* work64;  // work counter (zeroed by the launcher)
     RenderCounters* counters;  // optional
+    // batched launch (launch_trace_batch): every field above except work64 is taken from jobs[]
+    const BatchJob* jobs;
+    int n_jobs;
+    unsigned long long total_items;
 };
 
 // Camera set-up of RenderSceneCUDA (pathtracer.cu:654-663); tanf runs on the host as there.
@@ -99,6 +114,10 @@ cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bo
 
 cudaError_t launch_trace(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
                          int width, bool watertight, cudaStream_t stream);
+// Several frames (cameras, spp, bounces) in one persistent launch; job.jobs
+// (device) describes them, job.work64 is the shared work counter.
+cudaError_t launch_trace_batch(const DevScene& s, const TraceJob& job, int sm_count, int width, bool watertight,
+                               cudaStream_t stream);
 // Primary-hit G-buffer (albedo, encoded normal, box-normalised position), W*H*3 bytes each.
 cudaError_t launch_gbuffer(const DevScene& s, const DevCam& cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* d_albedo,
                            uint8_t* d_normal, uint8_t* d_worldpos, int width, bool watertight, cudaStream_t stream);

@@ -126,3 +126,25 @@ def test_gbuffer_vs_reference_gpu(small_engine_scene, width):
     for a, b in zip(ours, ref):
         assert float((a == b).all(axis=2).mean()) >= 0.999
     assert (ours[1] != 0).any() and (ours[2] != 0).any()
+
+
+@pytest.mark.parametrize("width,wt", [(4, False), (2, False), (4, True)])
+def test_batch_one_launch_matches_single_frames(box_scene, width, wt):
+    """lg_render_batch traces every frame in one persistent launch (replayed from
+    a CUDA graph); each frame must equal the frame rendered on its own."""
+    poses = [([-3, -3, 2], [0, 0, 1]), ([3, 3, 2.5], [0, 0, 1]), ([0.5, -3.5, 3.2], [1, 1, 0.5]),
+             ([-2, 2, 1], [2, -1, 1.5])]
+    spps, bounces = [1, 8, 20, 3], [0, 2, 1, 2]
+    with lumina.Renderer(0) as r:
+        r.set_scene(box_scene)
+        r.set_bvh_width(width)
+        if wt:
+            r.set_intersection("watertight")
+        for rep in range(2):  # the second batch (new cameras, same shapes) replays the captured graph
+            cams = [box_scene.camera.look_at(p, t) for p, t in (poses if rep == 0 else poses[::-1])]
+            imgs, ms = r.render_batch(cams, spps, bounces)
+            assert ms.shape == (4,) and (ms > 0).all()
+            for k, cam in enumerate(cams):
+                single = r.render(camera=cam, spp=spps[k], bounces=bounces[k])["rgb"]
+                same = float((imgs[k] == single).all(axis=2).mean())
+                assert same >= (1.0 if spps[k] <= 16 else 0.999), (rep, k, same)
