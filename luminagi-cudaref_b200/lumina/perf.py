@@ -3,6 +3,7 @@
     python -m lumina.perf unet  [--n 1] [--h 864] [--w 1728] [--reps 10]
     python -m lumina.perf trace [--spp 8] [--bounces 2] [--width 4] [--reps 2]
     python -m lumina.perf bvh   [--reps 5]
+    python -m lumina.perf batch [--poses 50] [--spp 8] [--bounces 2]
 
 Prints one JSON line.  Used for the profiles (run under ncu) and for quick
 A/B measurements; bench.py is the benchmark of record.
@@ -105,9 +106,31 @@ def bvh(a):
     return {"kernel": "lbvh", "triangles": n, "nodes": cnt.value, "device_ms": dev_ms, "host_io_ms": host_ms}
 
 
+def batch(a):
+    """Orbit poses of the engine scene: one batched launch (lg_render_batch,
+    graph-replayed) against one launch per frame, device time per frame."""
+    from .render import Renderer
+    from .scene import ENGINE_CENTER, engine_scene, orbit_poses
+    sc = engine_scene(seed=7)
+    r = Renderer(0)
+    r.set_scene(sc)
+    cams = [sc.camera.look_at(p, t) for p, t in orbit_poses(a.poses, seed=11, center=ENGINE_CENTER)]
+    n = len(cams)
+    spps, bounces = [a.spp] * n, [a.bounces] * n
+    r.render_batch(cams, spps, bounces)  # capture
+    _, ms = r.render_batch(cams, spps, bounces)
+    sep = [r.render(camera=c, spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for c in cams]
+    out = {"kernel": "trace (batched)", "poses": n, "spp": a.spp, "bounces": a.bounces,
+           "batch_ms_per_frame": float(ms.sum()) / n, "separate_ms_per_frame": float(np.sum(sep)) / n}
+    out["speedup"] = out["separate_ms_per_frame"] / out["batch_ms_per_frame"]
+    r.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["unet", "trace", "bvh"])
+    ap.add_argument("what", choices=["unet", "trace", "bvh", "batch"])
+    ap.add_argument("--poses", type=int, default=50)
     ap.add_argument("--n", type=int, default=1)
     ap.add_argument("--h", type=int, default=864)
     ap.add_argument("--w", type=int, default=1728)
@@ -116,7 +139,7 @@ def main(argv=None):
     ap.add_argument("--width", type=int, default=4)
     ap.add_argument("--reps", type=int, default=10)
     a = ap.parse_args(argv)
-    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh}[a.what](a)))
+    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch}[a.what](a)))
 
 
 if __name__ == "__main__":
