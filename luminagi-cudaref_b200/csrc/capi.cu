@@ -106,6 +106,7 @@ struct lg_renderer
     // scene
     int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0, root4 = 0;
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
+    int leaf_inline = 0;  // 4-wide leaf links carry (first, count)
     bool watertight = false;  // ray/triangle test: Moller-Trumbore (the reference's) or watertight
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
@@ -208,8 +209,10 @@ int finish_scene(lg_renderer* r)
     int root = 0, ni = 0, nl = 0, root4 = 0, n4 = 0;
     LG_TRY_CUDA(build_wide_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide.as<WideNode>(),
                                  r->leaves.as<int2>(), r->scratch.as<int>(), &root, &ni, &nl, r->stream));
-    LG_TRY_CUDA(build_wide4_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide4.as<Wide4Node>(),
-                                  r->scratch.as<int>(), &root4, &n4, r->stream));
+    int leaf_inline = 0;
+    LG_TRY_CUDA(build_wide4_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->n_tris, r->wide4.as<Wide4Node>(),
+                                  r->scratch.as<int>(), &root4, &n4, &leaf_inline, r->stream));
+    r->leaf_inline = leaf_inline;
     r->root4 = root4;
     LG_TRY_CUDA(cudaMemcpyAsync(&r->root_node, r->nodes.p, sizeof(lg_bvh_node), cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->watertight, r->stream));
@@ -245,6 +248,7 @@ DevScene dev_scene(const lg_renderer* r)
     s.root = r->root;
     s.nodes4 = r->wide4.as<Wide4Node>();
     s.root4 = r->root4;
+    s.leaf_inline = r->leaf_inline;
     s.sun = r->sun;
     return s;
 }

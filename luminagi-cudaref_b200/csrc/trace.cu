@@ -182,9 +182,20 @@ __device__ __forceinline__ void put_child(float (&lo)[3][4], float (&hi)[3][4], 
     ln[k] = link;
     ++k;
 }
+// Leaf links of the 4-wide records carry the leaf itself: ~(first << 4 |
+// count) for 1..15 triangles, so the traversal needs no leaf-table load; a
+// larger leaf (a run of equal Morton codes) is ~(leaf index << 4), count 0,
+// and is read from the table.  Scenes of 2^27 triangles or more keep ~leaf
+// index for every leaf (inline_ok = 0).
+__device__ __forceinline__ int leaf_link4(const lg_bvh_node& c, int leaf_index, int inline_ok)
+{
+    if (!inline_ok) return ~leaf_index;
+    return c.triCount < 16 ? ~((c.firstTri << 4) | c.triCount) : ~(leaf_index << 4);
+}
+
 __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ is4,
                              const int* __restrict__ dense4, const int* __restrict__ dense2,
-                             Wide4Node* __restrict__ out)
+                             Wide4Node* __restrict__ out, int inline_ok)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !is4[i]) return;
@@ -199,14 +210,14 @@ __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const
     for (int j = 0; j < 2; ++j)
     {
         const lg_bvh_node c = nodes[cs[j]];
-        if (c.triCount > 0) put_child(lo, hi, ln, k, c, ~dense2[cs[j]]);
+        if (c.triCount > 0) put_child(lo, hi, ln, k, c, leaf_link4(c, dense2[cs[j]], inline_ok));
         else
         {
             const int gs[2] = {c.left, c.right};
             for (int g = 0; g < 2; ++g)
             {
                 const lg_bvh_node gc = nodes[gs[g]];
-                put_child(lo, hi, ln, k, gc, gc.triCount > 0 ? ~dense2[gs[g]] : dense4[gs[g]]);
+                put_child(lo, hi, ln, k, gc, gc.triCount > 0 ? leaf_link4(gc, dense2[gs[g]], inline_ok) : dense4[gs[g]]);
             }
         }
     }
@@ -419,8 +430,22 @@ __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float 
         }
         else
         {
-            const int2 lf = __ldg(&s.leaves[~cur]);
-            if (kCount) { cnt.leaves++; }
+            int2 lf;
+            if (s.leaf_inline)
+            {
+                const int v = ~cur;
+                lf = make_int2(v >> 4, v & 15);
+                if (lf.y == 0)
+                {
+                    lf = __ldg(&s.leaves[lf.x]);
+                    if (kCount) { cnt.leaves++; }
+                }
+            }
+            else
+            {
+                lf = __ldg(&s.leaves[~cur]);
+                if (kCount) { cnt.leaves++; }
+            }
             bool done = false;
             for (int i = 0; i < lf.y; ++i)
             {
@@ -960,8 +985,9 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
     return cudaSuccess;
 }
 
-cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node* d_wide4, int* d_scratch,
-                              int* root4_host, int* n4_host, cudaStream_t stream)
+cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, Wide4Node* d_wide4,
+                              int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
+                              cudaStream_t stream)
 {
     // scratch: [is_internal | dense2 | block_sums] from build_wide_nodes, then [parent | is4 | dense4 | sums4]
     const int nb = (n_nodes + kScanTB - 1) / kScanTB;
@@ -976,7 +1002,9 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node
     count_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4);
     scan_sums_kernel<<<1, kScanTB, 0, stream>>>(sums4, nb);
     dense_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4, dense4);
-    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, d_wide4);
+    const int inline_ok = n_tris < (1 << 27) ? 1 : 0;
+    *leaf_inline_host = inline_ok;
+    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, d_wide4, inline_ok);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int root_is4 = 0, last_d = 0, last_v = 0;

@@ -38,6 +38,7 @@ struct DevScene
 {
     const Wide4Node* nodes4;   // 4-wide records (used when width == 4)
     int root4;
+    int leaf_inline;           // 4-wide leaf links carry (first, count); see wide4_kernel
     const WideNode* nodes;
     const int2* leaves;        // (first triangle, count)
     const float4* tv;          // 3 per triangle: v0 (w = material bits), e1 = v1-v0, e2 = v2-v0
@@ -106,8 +107,9 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
 // node at even depth becomes a record whose children are its grandchildren
 // (or its children, when those are leaves).  Must follow build_wide_nodes on
 // the same scratch (it reuses the leaf numbering).  Scratch: 5 * n_nodes ints.
-cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, Wide4Node* d_wide4, int* d_scratch,
-                              int* root4_host, int* n4_host, cudaStream_t stream);
+cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, Wide4Node* d_wide4,
+                              int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
+                              cudaStream_t stream);
 // Intersection records, 3 float4 per triangle (w of the first = material):
 // (v0, v1-v0, v2-v0) for Moller-Trumbore, (v0, v1, v2) for the watertight test.
 cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bool watertight, cudaStream_t stream);

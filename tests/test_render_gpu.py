@@ -148,3 +148,31 @@ def test_batch_one_launch_matches_single_frames(box_scene, width, wt):
                 single = r.render(camera=cam, spp=spps[k], bounces=bounces[k])["rgb"]
                 same = float((imgs[k] == single).all(axis=2).mean())
                 assert same >= (1.0 if spps[k] <= 16 else 0.999), (rep, k, same)
+
+
+def test_large_leaf_escape_vs_reference_gpu(box_scene):
+    """Leaves of more than 15 triangles (a run of equal Morton codes) take the
+    4-wide records' leaf-table escape; the frame must still match the reference."""
+    if not O.ref_available():
+        pytest.skip("reference oracle not built")
+    rng = np.random.default_rng(9)
+    n_fan = 40
+    fan = np.zeros(n_fan, box_scene.tris.dtype)
+    c = np.array([0.3, 0.2, 1.6])
+    for k in range(n_fan):  # triangles spun around one centroid: one Morton code, one leaf
+        a = rng.uniform(0, 2 * np.pi)
+        d = np.array([[np.cos(a), np.sin(a), 0.0], [np.cos(a + 2.1), np.sin(a + 2.1), 0.3],
+                      [np.cos(a + 4.2), np.sin(a + 4.2), -0.3]]) * 0.6
+        d -= d.mean(axis=0)
+        fan[k]["v"] = (c + d).astype(np.float32)
+        nrm = np.cross(d[1] - d[0], d[2] - d[0])
+        fan[k]["n"] = np.tile(nrm / np.linalg.norm(nrm), (3, 1)).astype(np.float32)
+        fan[k]["material"] = 0
+    tris = np.concatenate([box_scene.tris, fan])
+    sc = lumina.Scene(box_scene.camera, box_scene.sun, tris, box_scene.mat_albedo, box_scene.mat_emissive,
+                      box_scene.points)
+    nodes, otris, _, _ = O.oracle_build_bvh(sc.tris)
+    assert nodes["triCount"].max() >= 16
+    ours = render_ours(sc, nodes, otris, 8, 2, width=4)
+    ref_acc, _, _ = O.ref_render_gpu(sc, nodes, otris, 8, 2)
+    assert match_fraction(ours["accum"], ref_acc) >= 0.999
