@@ -231,3 +231,37 @@ def test_binary_scene_round_trip(tmp_path, small_engine_scene):
     with pytest.raises(lumina.LuminaError) as e:
         lumina.Scene.load_json(t)
     assert "truncated binary scene" in str(e.value)
+
+
+def test_split_parse_fuzz_matches_serial(tmp_path):
+    """Random byte edits inside the triangle array: the parallel split parse must
+    agree with the serial parse on success, triangles and error message."""
+    base = _big_json(12000).encode()
+    assert len(base) > 2 << 20
+    start = base.index(b'"triangles"')
+    rng = np.random.default_rng(11)
+    alphabet = b'{}[],:" 0123456789.-eE\\nx'
+    p = tmp_path / "fuzz.json"
+    outcomes = set()
+    for trial in range(60):
+        b = bytearray(base)
+        for _ in range(int(rng.integers(1, 4))):
+            pos = int(rng.integers(start, len(b)))
+            op = int(rng.integers(0, 3))
+            ch = alphabet[int(rng.integers(0, len(alphabet)))]
+            if op == 0:
+                b[pos] = ch
+            elif op == 1:
+                b.insert(pos, ch)
+            else:
+                del b[pos]
+        p.write_bytes(bytes(b))
+        res = []
+        for t in (1, 6):
+            try:
+                res.append(("ok", lumina.Scene.load_json(p, threads=t).tris.tobytes()))
+            except lumina.LuminaError as e:
+                res.append(("err", str(e)))
+        assert res[0] == res[1], (trial, res[0][0], res[1][0])
+        outcomes.add(res[0][0])
+    assert outcomes == {"ok", "err"}
