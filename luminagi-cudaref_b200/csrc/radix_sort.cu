@@ -31,23 +31,35 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const uint32_t* __restri
     for (int d = threadIdx.x; d < 256; d += kThreads) counts[(size_t)d * tiles + blockIdx.x] = h[d];
 }
 
-// Single-block exclusive scan over `total` counts (digit-major layout).
-__global__ void __launch_bounds__(1024) scan_kernel(uint32_t* __restrict__ counts, size_t total)
+// Single-block exclusive scan over `total` counts (digit-major layout).  Each
+// thread owns kScanItems consecutive counts per pass (a serial scan in
+// registers), so a pass covers 16K counts and a 1M-key sort needs 5 passes of
+// block synchronisation rather than 65.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 16;
+__global__ void __launch_bounds__(kScanThreads) scan_kernel(uint32_t* __restrict__ counts, size_t total)
 {
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (size_t base = 0; base < total; base += 1024)
+    for (size_t base = 0; base < total; base += (size_t)kScanThreads * kScanItems)
     {
-        size_t i = base + threadIdx.x;
-        uint32_t v = i < total ? counts[i] : 0u;
-        uint32_t x = v;
+        const size_t first = base + (size_t)threadIdx.x * kScanItems;
+        uint32_t v[kScanItems];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+        {
+            v[k] = first + k < total ? counts[first + k] : 0u;
+            sum += v[k];
+        }
+        uint32_t x = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1)
         {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
         if (lane == 31) warp_sums[warp] = x;
@@ -58,14 +70,19 @@ __global__ void __launch_bounds__(1024) scan_kernel(uint32_t* __restrict__ count
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1)
             {
-                uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
                 if (lane >= o) w += y;
             }
             warp_sums[lane] = w;  // inclusive
         }
         __syncthreads();
-        uint32_t excl = carry + (warp ? warp_sums[warp - 1] : 0u) + x - v;
-        if (i < total) counts[i] = excl;
+        uint32_t run = carry + (warp ? warp_sums[warp - 1] : 0u) + x - sum;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+        {
+            if (first + k < total) counts[first + k] = run;
+            run += v[k];
+        }
         __syncthreads();
         if (threadIdx.x == 0) carry += warp_sums[31];
         __syncthreads();
@@ -161,7 +178,7 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, size_t n, int begin
     {
         const int bits = (end_bit - shift) < 8 ? (end_bit - shift) : 8;
         hist_kernel<<<tiles, kThreads, 0, stream>>>(ki, n, shift, bits, s.counts, tiles);
-        scan_kernel<<<1, 1024, 0, stream>>>(s.counts, (size_t)256 * tiles);
+        scan_kernel<<<1, kScanThreads, 0, stream>>>(s.counts, (size_t)256 * tiles);
         scatter_kernel<<<tiles, kThreads, 0, stream>>>(ki, vi, ko, vo, n, shift, bits, s.counts, tiles);
         uint32_t* t = ki; ki = ko; ko = t;
         t = vi; vi = vo; vo = t;

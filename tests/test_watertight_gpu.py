@@ -52,7 +52,9 @@ def test_watertight_matches_mt_away_from_edges(box_scene):
     assert np.array_equal(again["accum"], mt["accum"])  # switching back restores the parity records
     close = np.abs(wt["accum"] - mt["accum"]) <= REL * np.maximum(np.abs(wt["accum"]), np.abs(mt["accum"])) + ABS
     frac = float(close.all(axis=2).mean())
-    same_hit = float(np.mean([(a == b).all(axis=2).mean() for a, b in zip(gb_mt, gb_wt)]))
+    # t, u, v come from different arithmetic, so 8-bit normals and positions may differ by one step
+    same_hit = float(np.mean([(np.abs(a.astype(int) - b.astype(int)) <= 1).all(axis=2).mean()
+                              for a, b in zip(gb_mt, gb_wt)]))
     print(f"watertight vs Moller-Trumbore: {frac:.5f} of pixels within 1e-3 (8 spp, 2 bounces); "
-          f"{same_hit:.5f} identical primary-hit G-buffer pixels")
-    assert frac >= 0.95 and same_hit >= 0.99
+          f"{same_hit:.5f} of primary-hit G-buffer pixels within one 8-bit step")
+    assert frac >= 0.95 and same_hit >= 0.999
