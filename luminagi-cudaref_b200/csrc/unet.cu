@@ -89,7 +89,7 @@ int pack_all_impl(lg_unet* u)
         const LayerDef& L = kLayers[i];
         LG_TRY(u->packed[i].ensure(conv_packed_elems(L.cin, L.cout) * sizeof(__nv_bfloat16)));
         LG_TRY_CUDA(conv_pack_weights((const float*)u->params.p + u->w_off[i], L.cout, layer_cin_real(u, i), L.cin,
-                                      (__nv_bfloat16*)u->packed[i].p, u->stream));
+                                      (__nv_bfloat16*)u->packed[i].p, u->stream, u->tile[i]));
     }
     u->packed_ok = true;
     return LG_OK;
@@ -108,6 +108,7 @@ ConvArgs base_args(lg_unet* u, int layer, int N, int H, int W)
     a.slope = u->slope;
     a.epilogue = kEpiStore;
     a.err = (int*)u->err.p;
+    a.tile = u->tile[layer];
     return a;
 }
 
@@ -143,7 +144,10 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
             a.log_hdr = u->log_hdr ? 1 : 0;
             a.final_out = d_y;
         }
+        const bool probe = layer == u->probe_layer;
+        if (probe) LG_TRY_CUDA(cudaEventRecord(u->probe_ev0, st));
         LG_TRY_CUDA(conv3x3_forward((const bf*)in, a, st));
+        if (probe) LG_TRY_CUDA(cudaEventRecord(u->probe_ev1, st));
         return LG_OK;
     };
     // encoder
@@ -233,6 +237,8 @@ void lg_unet_destroy(lg_unet* u)
         b->release();
     for (auto& b : u->packed_dg) b.release();
     for (auto& b : u->dz) b.release();
+    if (u->probe_ev0) cudaEventDestroy(u->probe_ev0);
+    if (u->probe_ev1) cudaEventDestroy(u->probe_ev1);
     if (u->stream) cudaStreamDestroy(u->stream);
     delete u;
 }

@@ -37,14 +37,12 @@ constexpr int kRows = 2;     // output rows per CTA
 constexpr int kHaloY = kRows + 2;
 constexpr int kThreads = 128;
 
-struct TileCfg
-{
-    int bn, kc, stages;
-};
+typedef ConvTile TileCfg;
 
-// Tile shape per layer: BN = min(Cout, 128), KC = 32 input channels per
-// K-block (16 when Cin is not a multiple of 32), stages to fill ~100 KB (two
-// CTAs per SM) for narrow layers or ~210 KB (one CTA per SM) for wide ones.
+// Default tile shape per layer: BN = min(Cout, 128), KC = 32 input channels
+// per K-block (16 when Cin is not a multiple of 32), stages to fill ~100 KB
+// (two CTAs per SM) for narrow layers or ~210 KB (one CTA per SM) for wide
+// ones.  The autotuner (lg_unet_autotune) may pick another compiled shape.
 TileCfg pick_cfg(int Cin, int Cout)
 {
     TileCfg c;
@@ -575,10 +573,26 @@ __global__ void from_blocked_kernel(const __nv_bfloat16* __restrict__ in, int N,
 
 size_t conv_packed_elems(int Cin, int Cout) { return (size_t)9 * Cin * Cout; }
 
-cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
-                              cudaStream_t stream)
+ConvTile conv_default_tile(int Cin, int Cout) { return pick_cfg(Cin, Cout); }
+
+// The shapes conv3x3_forward is compiled for.
+constexpr ConvTile kCompiledTiles[] = {{32, 16, 4},  {32, 32, 2},  {32, 32, 4},  {64, 16, 4},
+                                       {64, 32, 2},  {64, 32, 3},  {128, 16, 3}, {128, 32, 2}};
+
+int conv_tile_candidates(int Cin, int Cout, ConvTile* out, int max)
 {
-    const TileCfg c = pick_cfg(Cin, Cout);
+    int k = 0;
+    for (const ConvTile& t : kCompiledTiles)
+        if (k < max && t.bn <= Cout && Cout % t.bn == 0 && Cin % t.kc == 0) out[k++] = t;
+    return k;
+}
+
+static ConvTile resolve(ConvTile t, int Cin, int Cout) { return t.bn ? t : pick_cfg(Cin, Cout); }
+
+cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
+                              cudaStream_t stream, ConvTile tile)
+{
+    const TileCfg c = resolve(tile, Cin, Cout);
     const size_t total = conv_packed_elems(Cin, Cout);
     pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, Cin, c.bn, c.kc, d_packed,
                                                                      total);
@@ -586,9 +600,9 @@ cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin,
 }
 
 cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
-                                    __nv_bfloat16* d_packed, cudaStream_t stream)
+                                    __nv_bfloat16* d_packed, cudaStream_t stream, ConvTile tile)
 {
-    const TileCfg c = pick_cfg(Cout, ci_cnt);
+    const TileCfg c = resolve(tile, Cout, ci_cnt);
     const size_t total = conv_packed_elems(Cout, ci_cnt);
     pack_dgrad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, ci_lo, ci_cnt, c.bn,
                                                                            c.kc, d_packed, total);
@@ -604,13 +618,20 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
     if ((a.epilogue == kEpiBwdMask || a.epilogue == kEpiBwdSumPool || a.epilogue == kEpiBwdUnpool) && !a.ref)
         return cudaErrorInvalidValue;
     if (a.epilogue == kEpiBwdUnpool && !a.skip) return cudaErrorInvalidValue;
-    const TileCfg c = pick_cfg(a.Cin, a.Cout);
-    if (c.bn == 32 && c.kc == 16) return launch<32, 16, 4>(in, a, stream);
-    if (c.bn == 32 && c.kc == 32) return launch<32, 32, 2>(in, a, stream);
-    if (c.bn == 64 && c.kc == 32) return launch<64, 32, 3>(in, a, stream);
-    if (c.bn == 128 && c.kc == 32) return launch<128, 32, 2>(in, a, stream);
-    if (c.bn == 64 && c.kc == 16) return launch<64, 16, 4>(in, a, stream);
-    if (c.bn == 128 && c.kc == 16) return launch<128, 16, 3>(in, a, stream);
+    const TileCfg c = resolve(a.tile, a.Cin, a.Cout);
+    if (a.Cout % c.bn || a.Cin % c.kc) return cudaErrorInvalidValue;
+    const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    switch (key)
+    {
+    case 32164: return launch<32, 16, 4>(in, a, stream);
+    case 32322: return launch<32, 32, 2>(in, a, stream);
+    case 32324: return launch<32, 32, 4>(in, a, stream);
+    case 64164: return launch<64, 16, 4>(in, a, stream);
+    case 64322: return launch<64, 32, 2>(in, a, stream);
+    case 64323: return launch<64, 32, 3>(in, a, stream);
+    case 128163: return launch<128, 16, 3>(in, a, stream);
+    case 128322: return launch<128, 32, 2>(in, a, stream);
+    }
     return cudaErrorInvalidValue;
 }
 

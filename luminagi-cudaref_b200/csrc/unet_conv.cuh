@@ -30,6 +30,19 @@ enum ConvEpilogue : int
     kEpiBwdUnpool = 6,   // acc = d(pooled); route to the max of ref's 2x2 window, add skip, * act'(ref) -> out (2x)
 };
 
+// Tile shape of one convolution: BN output channels per CTA, KC input
+// channels per K-block, STAGES pipeline stages.  Packed weights depend on
+// (BN, KC), so a layer packs and launches with the same tile.  bn == 0 means
+// the default heuristic (conv_default_tile).
+struct ConvTile
+{
+    int bn, kc, stages;
+};
+ConvTile conv_default_tile(int Cin, int Cout);
+// The compiled tile shapes valid for a layer (Cout % bn == 0, Cin % kc == 0);
+// returns how many were written to out (at most max).
+int conv_tile_candidates(int Cin, int Cout, ConvTile* out, int max);
+
 struct ConvArgs
 {
     int N, H, W;         // spatial size of input and output
@@ -55,6 +68,7 @@ struct ConvArgs
     int ref_C, ref_coff;
     const __nv_bfloat16* skip;   // kEpiBwdUnpool: gradient arriving through the skip connection (2x res)
     int skip_C, skip_coff;
+    ConvTile tile;               // {0, 0, 0}: default; must match the tile the weights were packed with
 };
 
 // Bytes of packed weights for a layer (BF16).
@@ -62,13 +76,13 @@ size_t conv_packed_elems(int Cin, int Cout);
 // Packs PyTorch-layout FP32 weights w[Cout][Cin_real][3][3] into the layout
 // the kernel streams (input channels beyond Cin_real are zero).
 cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
-                              cudaStream_t stream);
+                              cudaStream_t stream, ConvTile tile = ConvTile{0, 0, 0});
 
 // Packs the input-gradient weights of a forward conv w[Cout][Cin_real][3][3]:
 // w'[ci][co][ky][kx] = w[co][ci][2-ky][2-kx] for ci in [ci_lo, ci_lo+ci_cnt),
 // as a convolution with Cin' = Cout input and ci_cnt output channels.
 cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
-                                    __nv_bfloat16* d_packed, cudaStream_t stream);
+                                    __nv_bfloat16* d_packed, cudaStream_t stream, ConvTile tile = ConvTile{0, 0, 0});
 
 // Launches the convolution reading `in` (blocked BF16, N x Cin x H x W).
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream);

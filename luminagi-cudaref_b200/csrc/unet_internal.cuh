@@ -73,6 +73,13 @@ struct lg_unet
     int gN = 0, gH = 0, gW = 0;
     Buf dz[14], gs1, gs2, gs3, tgt;
     Buf gup;  // bilinear mode: full-resolution gradient of an upsampled concat half
+    // tile shapes (lg::ConvTile; zero = the default heuristic) of the 14 convs and
+    // the 16 input-gradient convs, as chosen by lg_unet_autotune
+    lg::ConvTile tile[14] = {}, tile_dg[16] = {};
+    // autotuning: events recorded around one conv of the forward (probe_layer)
+    // or of the backward (probe_dgrad); -1 = none
+    int probe_layer = -1, probe_dgrad = -1;
+    cudaEvent_t probe_ev0 = nullptr, probe_ev1 = nullptr;
 };
 
 namespace lg

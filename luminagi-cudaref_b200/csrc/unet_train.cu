@@ -193,7 +193,7 @@ int pack_dgrad(lg_unet* u)
         const LayerDef& L = kLayers[d.layer];
         LG_TRY(u->packed_dg[k].ensure(conv_packed_elems(L.cout, d.ci_cnt) * sizeof(bf)));
         LG_TRY_CUDA(conv_pack_weights_dgrad((const float*)u->params.p + u->w_off[d.layer], L.cout, layer_cin_real(u, d.layer), d.ci_lo,
-                                            d.ci_cnt, (bf*)u->packed_dg[k].p, u->stream));
+                                            d.ci_cnt, (bf*)u->packed_dg[k].p, u->stream, u->tile_dg[k]));
     }
     u->packed_dg_ok = true;
     return LG_OK;
@@ -261,7 +261,11 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
         a.skip_C = skip_c;
         a.skip_coff = 0;
         a.err = (int*)u->err.p;
+        a.tile = u->tile_dg[k];
+        const bool probe = k == u->probe_dgrad;
+        if (probe) LG_TRY_CUDA(cudaEventRecord(u->probe_ev0, st));
         LG_TRY_CUDA(conv3x3_forward((const bf*)u->dz[d.layer].p, a, st));
+        if (probe) LG_TRY_CUDA(cudaEventRecord(u->probe_ev1, st));
         return LG_OK;
     };
     // decoder, from the output back
@@ -378,6 +382,97 @@ int lg_unet_adam_apply(lg_unet* u, float lr)
     if (!u->grads.p || !u->adam_m.p) return set_error(LG_ERR_INVALID, "no gradients yet: call lg_unet_loss_grad first");
     LG_TRY(adam_step(u, lr));
     return check_err(u);
+}
+
+int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_out)
+{
+    if (!u || n <= 0 || h <= 0 || w <= 0 || (h % 8) || (w % 8)) return set_error(LG_ERR_INVALID, "bad argument");
+    if (!u->probe_ev0)
+    {
+        LG_TRY_CUDA(cudaEventCreate(&u->probe_ev0));
+        LG_TRY_CUDA(cudaEventCreate(&u->probe_ev1));
+    }
+    // Inputs of the real shapes (values do not change the timing): x in [0,1), target 0.
+    const size_t xin = (size_t)n * u->in_ch * h * w, xout = (size_t)n * 3 * h * w;
+    Buf x, t, y;
+    LG_TRY(x.ensure(xin * sizeof(float)));
+    LG_TRY(t.ensure(xout * sizeof(float)));
+    LG_TRY(y.ensure(xout * sizeof(float)));
+    LG_TRY_CUDA(cudaMemsetAsync(x.p, 0, xin * sizeof(float), u->stream));
+    LG_TRY_CUDA(cudaMemsetAsync(t.p, 0, xout * sizeof(float), u->stream));
+    auto time_probe = [&](bool backward, float& best) -> int {
+        best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep)
+        {
+            if (backward) LG_TRY(loss_and_grads(u, (const float*)x.p, (const float*)t.p, n, h, w, nullptr));
+            else LG_TRY(unet_forward_device(u, (const float*)x.p, n, h, w, (float*)y.p));
+            LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+            float ms = 0.0f;
+            LG_TRY_CUDA(cudaEventElapsedTime(&ms, u->probe_ev0, u->probe_ev1));
+            if (rep > 0 && ms < best) best = ms;  // the first run warms the new shape
+        }
+        return LG_OK;
+    };
+    int rc = LG_OK;
+    const int n_sets = (flags & LG_UNET_TUNE_BACKWARD) ? 2 : 1;
+    for (int set = 0; set < n_sets && rc == LG_OK; ++set)
+    {
+        const bool bwd = set == 1;
+        const int count = bwd ? 16 : 14;
+        for (int i = 0; i < count && rc == LG_OK; ++i)
+        {
+            const int cin = bwd ? kLayers[kDgrad[i].layer].cout : kLayers[i].cin;
+            const int cout = bwd ? kDgrad[i].ci_cnt : kLayers[i].cout;
+            ConvTile cand[16];
+            const int nc = conv_tile_candidates(cin, cout, cand, 16);
+            ConvTile& slot = bwd ? u->tile_dg[i] : u->tile[i];
+            ConvTile best = conv_default_tile(cin, cout);
+            float best_ms = 1e30f;
+            (bwd ? u->probe_dgrad : u->probe_layer) = i;
+            for (int c = 0; c < nc && rc == LG_OK; ++c)
+            {
+                slot = cand[c];
+                u->packed_ok = false;
+                u->packed_dg_ok = false;
+                float ms = 0.0f;
+                rc = time_probe(bwd, ms);
+                if (rc == LG_OK && ms < best_ms)
+                {
+                    best_ms = ms;
+                    best = cand[c];
+                }
+            }
+            slot = best;
+            u->probe_layer = u->probe_dgrad = -1;
+        }
+    }
+    u->probe_layer = u->probe_dgrad = -1;
+    u->packed_ok = false;
+    u->packed_dg_ok = false;
+    // Autotuning ran training passes: leave the optimiser state and gradients as they were.
+    if (u->adam_m.p)
+    {
+        cudaMemsetAsync(u->adam_m.p, 0, u->n_params * sizeof(float), u->stream);
+        cudaMemsetAsync(u->adam_v.p, 0, u->n_params * sizeof(float), u->stream);
+    }
+    u->adam_t = 0;
+    if (rc == LG_OK) rc = unet_pack_all(u);
+    if (rc == LG_OK && tiles_out)
+        for (int i = 0; i < 30; ++i)
+        {
+            const ConvTile& tt = i < 14 ? u->tile[i] : u->tile_dg[i - 14];
+            const int cin = i < 14 ? kLayers[i].cin : kLayers[kDgrad[i - 14].layer].cout;
+            const int cout = i < 14 ? kLayers[i].cout : kDgrad[i - 14].ci_cnt;
+            const ConvTile r = tt.bn ? tt : conv_default_tile(cin, cout);
+            tiles_out[3 * i] = r.bn;
+            tiles_out[3 * i + 1] = r.kc;
+            tiles_out[3 * i + 2] = r.stages;
+        }
+    x.release();
+    t.release();
+    y.release();
+    if (rc == LG_OK) LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    return rc;
 }
 
 int lg_unet_adam_reset(lg_unet* u)

@@ -275,3 +275,35 @@ def test_unet_hdr_variant_gradients_match_torch_autograd():
     # and a few steps of training lower the loss
     losses = [loss] + [net.train_step(dx.data_ptr(), dt.data_ptr(), n, h, w, 1e-3) for _ in range(20)]
     assert losses[-1] < 0.8 * losses[0], losses[::5]
+
+
+def test_autotune_keeps_results():
+    """lg_unet_autotune picks per-layer tile shapes by timing; the network's
+    output and gradients must stay within the same bars against torch."""
+    flat = unet_ref.make_params(79)
+    net = lumina.UNet()
+    net.set_params(flat)
+    n, h, w = 2, 32, 144
+    x = np.random.default_rng(8).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
+    y0 = net.forward(x)
+    tiles = net.autotune(n, h, w, backward=True)
+    print("autotuned tiles (bn, kc, stages):", tiles)
+    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) for t in tiles)
+    y1 = net.forward(x)
+    assert np.array_equal(net.get_params(), flat)
+    m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
+    with torch.no_grad():
+        ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x)).numpy()
+        ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64).numpy()
+    floor = np.abs(ref_q - ref_q64)
+    for y in (y0, y1):
+        err = np.abs(y - ref_q)
+        assert err.mean() <= 2.0 * floor.mean() + 1e-4 and err.max() <= 2.0 * floor.max() + 2e-3
+    noisy, clean = _batch(n, h, w, 4)
+    dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
+    loss, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
+    mm = unet_ref.load_flat(unet_ref.UNetRef(), flat)
+    unet_ref.F.l1_loss(mm(torch.from_numpy(noisy)), torch.from_numpy(clean)).backward()
+    ref_g = np.concatenate([p.grad.numpy().ravel() for _, p in mm.named_parameters()])
+    cos = float(np.dot(g, ref_g) / (np.linalg.norm(g) * np.linalg.norm(ref_g)))
+    assert cos > 0.99
