@@ -171,6 +171,11 @@ int lg_renderer_set_bvh_width(lg_renderer* r, int width);
 #define LG_ISECT_MOLLER_TRUMBORE 0
 #define LG_ISECT_WATERTIGHT 1
 int lg_renderer_set_intersection(lg_renderer* r, int mode);
+/* Autotuner of the persistent trace launch: renders `cam` at spp/max_bounces
+ * with 1..4 resident blocks per SM, keeps the fastest for later frames and
+ * reports it (and its kernel time) through the optional outputs. */
+int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_bounces, int32_t* blocks_per_sm,
+                         float* ms);
 /* Diffuse texture of one material (load_texture_to_device + sample_albedo,
  * src/pathtracer.cu:553-579, 274-282): w x h RGBA8 host pixels, sampled as
  * sRGB with bilinear filtering and wrapping at uv (u, 1 - v).  rgba8 = NULL

@@ -108,6 +108,7 @@ struct lg_renderer
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
     int leaf_inline = 0;  // 4-wide leaf links carry (first, count)
     bool watertight = false;  // ray/triangle test: Moller-Trumbore (the reference's) or watertight
+    int trace_blocks_per_sm = 0;  // persistent trace grid (0 = occupancy maximum); see lg_renderer_autotune
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
@@ -279,6 +280,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.accum64 = acc64 ? r->accum64.as<double>() : nullptr;
         job.work64 = r->work.as<unsigned long long>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
+        job.blocks_per_sm = r->trace_blocks_per_sm;
         LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->watertight,
                                  r->stream));
     }
@@ -778,6 +780,43 @@ int lg_renderer_set_intersection(lg_renderer* r, int mode)
     return LG_OK;
 }
 
+int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_bounces, int32_t* blocks_per_sm_out,
+                         float* ms_out)
+{
+    if (!r || !cam || spp <= 0 || max_bounces < 0) return set_error(LG_ERR_INVALID, "bad argument");
+    DeviceGuard g(r->device);
+    const int saved = r->trace_blocks_per_sm;
+    const bool counting = r->counting;
+    r->counting = false;
+    int best = 0;
+    float best_ms = 1e30f;
+    int rc = LG_OK;
+    // Candidates: 1 .. 4 resident 256-thread blocks per SM (the kernel's register budget allows 4).
+    for (int bps = 1; bps <= 4 && rc == LG_OK; ++bps)
+    {
+        r->trace_blocks_per_sm = bps;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && rc == LG_OK; ++rep)
+        {
+            lg_render_opts o{spp, max_bounces, 0, 0};
+            lg_render_stats st{};
+            rc = render_into_device(r, cam, &o, &st);
+            if (rc == LG_OK && rep > 0) ms = std::min(ms, st.kernel_ms);
+        }
+        if (rc == LG_OK && ms < best_ms)
+        {
+            best_ms = ms;
+            best = bps;
+        }
+    }
+    r->counting = counting;
+    r->trace_blocks_per_sm = rc == LG_OK ? best : saved;
+    if (rc != LG_OK) return rc;
+    if (blocks_per_sm_out) *blocks_per_sm_out = best;
+    if (ms_out) *ms_out = best_ms;
+    return LG_OK;
+}
+
 int lg_renderer_set_counting(lg_renderer* r, int enable)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
@@ -894,6 +933,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
                           r->tv.p,        r->tris.p,      r->mats.p,       r->texs.p,     r->points.p, r->work.p};
     for (const void* p : deps) key.push_back((long long)(uintptr_t)p);
     key.push_back(r->bvh_width * 2 + (r->watertight ? 1 : 0));
+    key.push_back(r->trace_blocks_per_sm);
     key.push_back(r->scene_gen);
     if (key != r->batch_key || !r->batch_exec)
     {
@@ -912,6 +952,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
             job.jobs = r->batch_jobs.as<BatchJob>();
             job.n_jobs = n_jobs;
             job.total_items = items;
+            job.blocks_per_sm = r->trace_blocks_per_sm;
             e = launch_trace_batch(dev_scene(r), job, r->sm_count, r->bvh_width, r->watertight, st);
         }
         for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)

@@ -1033,6 +1033,7 @@ static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const Tr
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, 0);
     if (e != cudaSuccess) return e;
+    if (job.blocks_per_sm > 0 && job.blocks_per_sm < per_sm) per_sm = job.blocks_per_sm;
     const long long lanes = kBatch ? (long long)job.total_items : (long long)job.n_tiles * job.n_chunks * 32;
     long long blocks = (long long)(per_sm < 1 ? 1 : per_sm) * sm_count;
     const long long useful = (lanes + kTraceThreads - 1) / kTraceThreads;

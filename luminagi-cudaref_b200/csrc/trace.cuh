@@ -87,6 +87,7 @@ struct TraceJob
     float* accum;          // W*H*3, added to
     double* accum64;       // optional
     unsigned long long* work64;  // work counter (zeroed by the launcher)
+    int blocks_per_sm;     // persistent grid: resident blocks per SM (0 = as many as fit)
     RenderCounters* counters;  // optional
     // batched launch (launch_trace_batch): every field above except work64 is taken from jobs[]
     const BatchJob* jobs;

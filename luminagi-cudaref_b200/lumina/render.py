@@ -103,6 +103,13 @@ class Renderer:
         modes = {"mt": 0, "watertight": 1}
         check(lib().lg_renderer_set_intersection(self._h, modes[mode]))
 
+    def autotune(self, camera: Camera | None = None, spp: int = 8, bounces: int = 2):
+        """Picks the persistent trace grid (resident blocks per SM) by timing; returns (blocks_per_sm, ms)."""
+        cam = (camera if camera is not None else self.scene.camera).to_c()
+        b, ms = C.c_int32(0), C.c_float(0)
+        check(lib().lg_renderer_autotune(self._h, C.byref(cam), spp, bounces, C.byref(b), C.byref(ms)))
+        return int(b.value), float(ms.value)
+
     def set_counting(self, on: bool) -> None:
         check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))
 

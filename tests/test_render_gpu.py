@@ -176,3 +176,15 @@ def test_large_leaf_escape_vs_reference_gpu(box_scene):
     ours = render_ours(sc, nodes, otris, 8, 2, width=4)
     ref_acc, _, _ = O.ref_render_gpu(sc, nodes, otris, 8, 2)
     assert match_fraction(ours["accum"], ref_acc) >= 0.999
+
+
+def test_trace_grid_autotune(box_scene):
+    """lg_renderer_autotune picks the resident blocks per SM of the persistent
+    trace launch by timing; images do not depend on the grid."""
+    with lumina.Renderer(0) as r:
+        r.set_scene(box_scene)
+        before = r.render(spp=8, bounces=2)
+        bps, ms = r.autotune(spp=8, bounces=2)
+        assert 1 <= bps <= 4 and ms > 0
+        after = r.render(spp=8, bounces=2)
+    assert np.array_equal(before["accum"], after["accum"])
