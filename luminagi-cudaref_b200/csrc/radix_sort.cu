@@ -31,69 +31,51 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const uint32_t* __restri
     for (int d = threadIdx.x; d < 256; d += kThreads) counts[(size_t)d * tiles + blockIdx.x] = h[d];
 }
 
-// Single-block exclusive scan over `total` counts (digit-major layout).  Each
-// thread owns kScanItems consecutive counts per pass (a serial scan in
-// registers), so a pass covers 16K counts and a 1M-key sort needs 5 passes of
-// block synchronisation rather than 65.
-constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 16;
-__global__ void __launch_bounds__(kScanThreads) scan_kernel(uint32_t* __restrict__ counts, size_t total)
+// Exclusive scan of each digit's row of the [digit][tile] count table, one
+// block per digit (tiles is n / 4096, so a row is short), and the digit's
+// total.  The digits' own offsets (an exclusive scan of the 256 totals) are
+// added by every scatter block, so no single-block pass over the whole table
+// is needed.
+constexpr int kScanThreads = 256;
+__global__ void __launch_bounds__(kScanThreads) digit_scan_kernel(uint32_t* __restrict__ counts, int tiles,
+                                                                  uint32_t* __restrict__ digit_total)
 {
-    __shared__ uint32_t warp_sums[32];
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
+    __shared__ uint32_t warp_sums[kScanThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (size_t base = 0; base < total; base += (size_t)kScanThreads * kScanItems)
+    uint32_t* row = counts + (size_t)blockIdx.x * tiles;
+    const int per = (tiles + kScanThreads - 1) / kScanThreads;  // consecutive entries per thread
+    const int first = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (int k = 0; k < per; ++k)
+        if (first + k < tiles) sum += row[first + k];
+    uint32_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
     {
-        const size_t first = base + (size_t)threadIdx.x * kScanItems;
-        uint32_t v[kScanItems];
-        uint32_t sum = 0;
-#pragma unroll
-        for (int k = 0; k < kScanItems; ++k)
-        {
-            v[k] = first + k < total ? counts[first + k] : 0u;
-            sum += v[k];
-        }
-        uint32_t x = sum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1)
-        {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) warp_sums[warp] = x;
-        __syncthreads();
-        if (warp == 0)
-        {
-            uint32_t w = warp_sums[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1)
-            {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
-            }
-            warp_sums[lane] = w;  // inclusive
-        }
-        __syncthreads();
-        uint32_t run = carry + (warp ? warp_sums[warp - 1] : 0u) + x - sum;
-#pragma unroll
-        for (int k = 0; k < kScanItems; ++k)
-        {
-            if (first + k < total) counts[first + k] = run;
-            run += v[k];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) carry += warp_sums[31];
-        __syncthreads();
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
     }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += warp_sums[w];
+    uint32_t run = before + x - sum;
+    for (int k = 0; k < per; ++k)
+        if (first + k < tiles)
+        {
+            const uint32_t v = row[first + k];
+            row[first + k] = run;
+            run += v;
+        }
+    if (threadIdx.x == kScanThreads - 1) digit_total[blockIdx.x] = run;
 }
 
 __global__ void __launch_bounds__(kThreads) scatter_kernel(const uint32_t* __restrict__ keys_in,
                                                            const uint32_t* __restrict__ vals_in,
                                                            uint32_t* __restrict__ keys_out,
                                                            uint32_t* __restrict__ vals_out, size_t n, int shift,
-                                                           int bits, const uint32_t* __restrict__ offsets, int tiles)
+                                                           int bits, const uint32_t* __restrict__ offsets, int tiles,
+                                                           const uint32_t* __restrict__ digit_total)
 {
     __shared__ uint32_t digit_base[256];         // running position inside this tile
     __shared__ uint32_t global_base[256];
@@ -101,10 +83,24 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const uint32_t* __res
     __shared__ uint32_t round_total[256];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t mask = (1u << bits) - 1u;
-    for (int d = threadIdx.x; d < 256; d += kThreads)
+    // Digit offsets: exclusive scan of the 256 digit totals (one per thread).
+    static_assert(kThreads == 256, "one digit per thread");
     {
-        digit_base[d] = 0;
-        global_base[d] = offsets[(size_t)d * tiles + blockIdx.x];
+        const uint32_t t = digit_total[threadIdx.x];
+        uint32_t x = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) round_total[warp] = x;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int w = 0; w < warp; ++w) before += round_total[w];
+        digit_base[threadIdx.x] = 0;
+        global_base[threadIdx.x] = before + x - t + offsets[(size_t)threadIdx.x * tiles + blockIdx.x];
+        __syncthreads();
     }
     const size_t base = (size_t)blockIdx.x * kTile;
     const uint32_t lt_mask = (1u << lane) - 1u;
@@ -152,7 +148,7 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const uint32_t* __res
 size_t radix_sort_scratch_bytes(size_t n)
 {
     size_t t = tiles_for(n ? n : 1);
-    return align256(n * 4) * 2 + align256(256 * t * 4) + 256;
+    return align256(n * 4) * 2 + align256(256 * t * 4) + 256 * 4 + 256;
 }
 
 RadixSortScratch radix_sort_bind(void* base, size_t n)
@@ -164,6 +160,8 @@ RadixSortScratch radix_sort_bind(void* base, size_t n)
     s.vals_alt = (uint32_t*)p;
     p += align256(n * 4);
     s.counts = (uint32_t*)p;
+    p += align256(256 * tiles_for(n ? n : 1) * 4);
+    s.digit_total = (uint32_t*)p;
     s.capacity = n;
     return s;
 }
@@ -178,8 +176,9 @@ cudaError_t radix_sort_pairs(uint32_t* keys, uint32_t* vals, size_t n, int begin
     {
         const int bits = (end_bit - shift) < 8 ? (end_bit - shift) : 8;
         hist_kernel<<<tiles, kThreads, 0, stream>>>(ki, n, shift, bits, s.counts, tiles);
-        scan_kernel<<<1, kScanThreads, 0, stream>>>(s.counts, (size_t)256 * tiles);
-        scatter_kernel<<<tiles, kThreads, 0, stream>>>(ki, vi, ko, vo, n, shift, bits, s.counts, tiles);
+        digit_scan_kernel<<<256, kScanThreads, 0, stream>>>(s.counts, tiles, s.digit_total);
+        scatter_kernel<<<tiles, kThreads, 0, stream>>>(ki, vi, ko, vo, n, shift, bits, s.counts, tiles,
+                                                       s.digit_total);
         uint32_t* t = ki; ki = ko; ko = t;
         t = vi; vi = vo; vo = t;
     }

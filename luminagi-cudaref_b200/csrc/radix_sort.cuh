@@ -2,10 +2,12 @@
 //
 // One pass per 8-bit digit, three launches per pass:
 //   1. per-tile digit histogram (tile = 256 threads x kItems keys),
-//   2. exclusive scan of the digit-major [digit][tile] count table,
-//   3. stable scatter: keys of a tile are ranked in input order (warp
-//      match_any peers + per-warp digit counts), then written to
-//      base[digit][tile] + rank.
+//   2. exclusive scan of each digit's row of the [digit][tile] count table
+//      (one block per digit) and the digit totals,
+//   3. stable scatter: each block scans the 256 digit totals for the digit
+//      offsets; keys of a tile are ranked in input order (warp match_any
+//      peers + per-warp digit counts), then written to digit offset +
+//      row prefix[digit][tile] + rank.
 // Stability makes the result a total order on (key, input position), which
 // is what the BVH build relies on for a deterministic triangle order.
 #pragma once
@@ -21,6 +23,7 @@ struct RadixSortScratch
     uint32_t* keys_alt = nullptr;
     uint32_t* vals_alt = nullptr;
     uint32_t* counts = nullptr;  // 256 * tiles
+    uint32_t* digit_total = nullptr;  // 256
     size_t capacity = 0;         // elements
 };
 
