@@ -371,34 +371,6 @@ struct Counters
     unsigned long long closest, shadow, overflow, nodes, tris, leaves;
 };
 
-// Traversal stack of one thread.  The first kShStack entries live in shared
-// memory, stored entry-major across the block (entry i of thread t at
-// sh_base[i * kTraceThreads + t]), so the lanes of a warp touch 32 distinct
-// banks whatever their depths; deeper entries go to a local-memory tail that
-// only deep traversals reach.  Keeping the stack out of local memory removes
-// most of the L1 traffic the per-thread stack array caused.
-constexpr int kShStack = 24;
-struct TravStack
-{
-    int* sh;  // this thread's column: &s_stack[threadIdx]
-    int sp;
-    int tail[kStack - kShStack];
-    __device__ __forceinline__ explicit TravStack(int* column) : sh(column), sp(0) {}
-    __device__ __forceinline__ bool push(int v)
-    {
-        if (sp < kShStack) sh[sp * kTraceThreads] = v;
-        else if (sp < kStack) tail[sp - kShStack] = v;
-        else return false;
-        ++sp;
-        return true;
-    }
-    __device__ __forceinline__ int pop()
-    {
-        --sp;
-        return sp < kShStack ? sh[sp * kTraceThreads] : tail[sp - kShStack];
-    }
-};
-
 __device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
 {
     if (tb < ta)
@@ -411,11 +383,16 @@ __device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
 // The 4-wide form of the traversal below: one 128-byte record tests up to
 // four child boxes (same slab arithmetic); hit children are ordered by entry
 // distance, the nearest is entered and the rest stacked nearest-on-top.
+// Measured alternatives on the 64-spp engine frame (633 ms with this form):
+// a "while-while" loop (internal records until a leaf, then the warp's leaves
+// together) ran 745 ms, and a 24-entry shared-memory stack 675 ms (its 96 KB
+// per SM comes out of the L1 that caches the BVH records).
 template <bool kCount, bool kWT>
 __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
-                                         float& bestU, float& bestV, Counters& cnt, int* sh)
+                                         float& bestU, float& bestV, Counters& cnt)
 {
-    TravStack stk(sh);
+    int stack[kStack];
+    int sp = 0;
     int cur = s.root4;
     int bestTri = -1;
     bestT = tmax;
@@ -448,9 +425,9 @@ __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float 
             if (t0 != inf)
             {
                 // push farthest first so the nearest remaining is on top
-                if (t3 != inf && !stk.push(l3) && kCount) cnt.overflow++;
-                if (t2 != inf && !stk.push(l2) && kCount) cnt.overflow++;
-                if (t1 != inf && !stk.push(l1) && kCount) cnt.overflow++;
+                if (t3 != inf) { if (sp < kStack) stack[sp++] = l3; else if (kCount) cnt.overflow++; }
+                if (t2 != inf) { if (sp < kStack) stack[sp++] = l2; else if (kCount) cnt.overflow++; }
+                if (t1 != inf) { if (sp < kStack) stack[sp++] = l1; else if (kCount) cnt.overflow++; }
                 cur = l0;
                 continue;
             }
@@ -490,8 +467,8 @@ __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float 
             }
             if (done) break;
         }
-        if (stk.sp == 0) break;
-        cur = stk.pop();
+        if (sp == 0) break;
+        cur = stack[--sp];
     }
     return bestTri;
 }
@@ -504,9 +481,10 @@ __device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float 
 // Returns the hit triangle or -1; bestT/U/V as in traverse_closest.
 template <bool kCount, bool kWT>
 __device__ __forceinline__ int traverse(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
-                                        float& bestU, float& bestV, Counters& cnt, int* sh)
+                                        float& bestU, float& bestV, Counters& cnt)
 {
-    TravStack stk(sh);
+    int stack[kStack];
+    int sp = 0;
     int cur = s.root;
     int bestTri = -1;
     bestT = tmax;
@@ -528,7 +506,8 @@ __device__ __forceinline__ int traverse(const DevScene& s, const Ray& r, float t
             if (h0 && h1)
             {
                 const bool swap = t1 < t0;
-                if (!stk.push(swap ? ln.x : ln.y) && kCount) cnt.overflow++;
+                if (sp < kStack) stack[sp++] = swap ? ln.x : ln.y;
+                else if (kCount) cnt.overflow++;
                 cur = swap ? ln.y : ln.x;
                 continue;
             }
@@ -559,8 +538,8 @@ __device__ __forceinline__ int traverse(const DevScene& s, const Ray& r, float t
             }
             if (done) break;
         }
-        if (stk.sp == 0) break;
-        cur = stk.pop();
+        if (sp == 0) break;
+        cur = stack[--sp];
     }
     return bestTri;
 }
@@ -790,8 +769,6 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
     const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned long long total =
         kBatch ? job.total_items : (unsigned long long)job.n_tiles * job.n_chunks * 32ull;
-    __shared__ int s_stack[kShStack * kTraceThreads];
-    int* const stack_col = s_stack + threadIdx.x;
     Counters cnt{0, 0, 0, 0, 0, 0};
     PathState st;
     bool active = false, exhausted = false;
@@ -849,9 +826,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         if (active)
         {
             float hitT, hitU, hitV;
-            const int tri = kWidth == 4
-                                ? traverse4<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt, stack_col)
-                                : traverse<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt, stack_col);
+            const int tri = kWidth == 4 ? traverse4<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt)
+                                        : traverse<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
             const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
             if (!advance(st, s, c, kBatch ? st.max_bounces : job.max_bounces, tri, hitT, hitU, hitV))
             {
@@ -916,16 +892,14 @@ template <int kWidth, bool kWT>
 __global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExtent, uint8_t* __restrict__ albedo_out,
                                uint8_t* __restrict__ normal_out, uint8_t* __restrict__ worldpos_out)
 {
-    __shared__ int s_stack[kShStack * kTraceThreads];  // 16 x 16 = kTraceThreads threads
-    int* const stack_col = s_stack + threadIdx.y * blockDim.x + threadIdx.x;
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
     if (px >= cam.width || py >= cam.height) return;
     Ray r = primary_ray(cam, px, py, 0.5f, 0.5f);
     float hitT, hitU, hitV;
     Counters cnt{0, 0, 0, 0, 0, 0};
-    const int tri = kWidth == 4 ? traverse4<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt, stack_col)
-                                : traverse<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt, stack_col);
+    const int tri = kWidth == 4 ? traverse4<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt)
+                                : traverse<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt);
     const size_t i = ((size_t)py * cam.width + px) * 3;
     if (tri < 0)
     {
