@@ -44,6 +44,10 @@ sys.path.insert(0, str(ROOT / "luminagi-cudaref_b200"))
 import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
+# of an 8-spp engine frame: 376.9 MB / 65,366,791 rays
+# (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
+TRACE_DRAM_BYTES_PER_RAY = 376.92288e6 / 65366791
 
 
 def load_peaks():
@@ -387,7 +391,9 @@ def main():
             "e2e": {"value": rays * world / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_frame": e2e_s * 1e3},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": TRACE_DRAM_BYTES_PER_RAY * rays,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-spp launch, "
+                                           "scaled by rays", "working_set": "L2-resident (DRAM 5.8 B/ray)",
                          "peak_source": peak_kind, "kernel": "trace_kernel",
                          "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
             "gpu_launches": args.steps * 2,
