@@ -204,7 +204,7 @@ int finish_scene(lg_renderer* r)
     LG_TRY(r->leaves.reserve((size_t)r->n_nodes * sizeof(int2)));
     LG_TRY(r->tv.reserve((size_t)r->n_tris * 3 * sizeof(float4)));
     const size_t nb = (size_t)r->n_nodes / 1024 + 1;
-    size_t need = ((size_t)r->n_nodes * 6 + 2 * nb + 16) * sizeof(int);
+    size_t need = ((size_t)r->n_nodes * 11 + 2 * nb + 256) * sizeof(int);
     LG_TRY(r->scratch.reserve(need));
     LG_TRY(r->wide4.reserve(((size_t)r->n_nodes / 2 + 1) * sizeof(Wide4Node)));
     int root = 0, ni = 0, nl = 0, root4 = 0, n4 = 0;

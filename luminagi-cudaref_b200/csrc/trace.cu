@@ -35,6 +35,7 @@ namespace lg
 namespace
 {
 constexpr int kStack = 64;
+constexpr int kMaxLevels = 128;  // depth limit of the 4-wide collapse (the reference tree is at most ~31 deep)
 constexpr int kTraceThreads = 256;
 constexpr int kTraceMinBlocks = 4;
 
@@ -159,16 +160,62 @@ __global__ void parent_kernel(const lg_bvh_node* __restrict__ nodes, int n, int*
         parent[nd.right] = i;
     }
 }
-// is4[i] = internal node at even depth (depth by walking up; tree depth <= ~32).
-__global__ void even_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ parent,
-                            int* __restrict__ is4)
+// Depth of every node (BFS order: depths are non-decreasing along the array).
+__global__ void depth_kernel(int n, const int* __restrict__ parent, int* __restrict__ depth)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int d = 0;
     for (int a = i; a != 0; a = parent[a]) ++d;
-    is4[i] = (nodes[i].triCount == 0 && (d & 1) == 0) ? 1 : 0;
+    depth[i] = d;
 }
+__global__ void level_start_kernel(int n, const int* __restrict__ depth, int* __restrict__ level_start, int max_levels)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if ((i == 0 || depth[i] != depth[i - 1]) && depth[i] < max_levels) level_start[depth[i]] = i;
+}
+__device__ __forceinline__ float half_area(const lg_bvh_node& b)
+{
+    const float dx = b.bbMax[0] - b.bbMin[0], dy = b.bbMax[1] - b.bbMin[1], dz = b.bbMax[2] - b.bbMin[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+// Children of the 4-wide record rooted at internal node i (a record root,
+// is4[i] = 1), processed one BVH depth at a time from the root: start from
+// i's two children and, while fewer than four, replace the internal child of
+// largest surface area by its two children.  The record's internal children
+// become record roots themselves (they are deeper, so their level comes later).
+__global__ void select4_kernel(const lg_bvh_node* __restrict__ nodes, int lo, int hi, int* __restrict__ is4,
+                               int* __restrict__ sel)
+{
+    const int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= hi || !is4[i]) return;
+    const lg_bvh_node nd = nodes[i];
+    int c[4] = {nd.left, nd.right, -1, -1};
+    int k = 2;
+    while (k < 4)
+    {
+        int best = -1;
+        float best_a = -1.0f;
+        for (int j = 0; j < k; ++j)
+        {
+            const lg_bvh_node& cj = nodes[c[j]];
+            if (cj.triCount > 0) continue;
+            const float a = half_area(cj);
+            if (a > best_a) { best_a = a; best = j; }
+        }
+        if (best < 0) break;
+        const lg_bvh_node& cb = nodes[c[best]];
+        c[best] = cb.left;
+        c[k++] = cb.right;
+    }
+    for (int j = 0; j < 4; ++j)
+    {
+        sel[4 * i + j] = c[j];
+        if (c[j] >= 0 && nodes[c[j]].triCount == 0) is4[c[j]] = 1;
+    }
+}
+
 // Per-block totals, scan and dense numbering are shared with build_wide_nodes
 // (count_kernel / scan_sums_kernel / dense_kernel).
 __device__ __forceinline__ void put_child(float (&lo)[3][4], float (&hi)[3][4], int (&ln)[4], int& k,
@@ -195,31 +242,22 @@ __device__ __forceinline__ int leaf_link4(const lg_bvh_node& c, int leaf_index, 
 
 __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ is4,
                              const int* __restrict__ dense4, const int* __restrict__ dense2,
-                             Wide4Node* __restrict__ out, int inline_ok)
+                             const int* __restrict__ sel, Wide4Node* __restrict__ out, int inline_ok)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !is4[i]) return;
-    const lg_bvh_node nd = nodes[i];
     float lo[3][4], hi[3][4];
     int ln[4];
     for (int a = 0; a < 3; ++a)
         for (int k = 0; k < 4; ++k) { lo[a][k] = 1.0f; hi[a][k] = 0.0f; }
     for (int k = 0; k < 4; ++k) ln[k] = kEmptyLink;
     int k = 0;
-    const int cs[2] = {nd.left, nd.right};
-    for (int j = 0; j < 2; ++j)
+    for (int j = 0; j < 4; ++j)
     {
-        const lg_bvh_node c = nodes[cs[j]];
-        if (c.triCount > 0) put_child(lo, hi, ln, k, c, leaf_link4(c, dense2[cs[j]], inline_ok));
-        else
-        {
-            const int gs[2] = {c.left, c.right};
-            for (int g = 0; g < 2; ++g)
-            {
-                const lg_bvh_node gc = nodes[gs[g]];
-                put_child(lo, hi, ln, k, gc, gc.triCount > 0 ? leaf_link4(gc, dense2[gs[g]], inline_ok) : dense4[gs[g]]);
-            }
-        }
+        const int ci = sel[4 * i + j];
+        if (ci < 0) continue;
+        const lg_bvh_node c = nodes[ci];
+        put_child(lo, hi, ln, k, c, c.triCount > 0 ? leaf_link4(c, dense2[ci], inline_ok) : dense4[ci]);
     }
     Wide4Node w;
     w.lox = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
@@ -993,31 +1031,59 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tri
                               int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
                               cudaStream_t stream)
 {
-    // scratch: [is_internal | dense2 | block_sums] from build_wide_nodes, then [parent | is4 | dense4 | sums4]
+    // scratch: [is_internal | dense2 | block_sums] from build_wide_nodes, then
+    // [parent | is4 | dense4 | sums4 | depth | sel (4 per node) | level_start]
     const int nb = (n_nodes + kScanTB - 1) / kScanTB;
     const int* dense2 = d_scratch + n_nodes;
     int* parent = d_scratch + 2 * (size_t)n_nodes + nb + 8;
     int* is4 = parent + n_nodes;
     int* dense4 = is4 + n_nodes;
     int* sums4 = dense4 + n_nodes;
+    int* depth = sums4 + nb + 8;
+    int* sel = depth + n_nodes;
+    int* level_start = sel + 4 * (size_t)n_nodes;
     const int tb = 256, g = (n_nodes + tb - 1) / tb;
     parent_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, parent);
-    even_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, parent, is4);
+    depth_kernel<<<g, tb, 0, stream>>>(n_nodes, parent, depth);
+    level_start_kernel<<<g, tb, 0, stream>>>(n_nodes, depth, level_start, kMaxLevels);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    lg_bvh_node root{};
+    int levels = 0;
+    int starts[kMaxLevels + 1];
+    e = cudaMemcpyAsync(&root, d_nodes, sizeof(root), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&levels, depth + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    levels += 1;  // the last node has the largest depth
+    if (levels > kMaxLevels) return cudaErrorInvalidValue;
+    e = cudaMemcpyAsync(starts, level_start, sizeof(int) * levels, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(is4, 0, sizeof(int) * (size_t)n_nodes, stream);
+    static const int kOne = 1;
+    if (e == cudaSuccess && root.triCount == 0) e = cudaMemcpyAsync(is4, &kOne, sizeof(int), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    starts[levels] = n_nodes;
+    // Record roots and their children, one depth at a time from the top.
+    for (int d = 0; d + 1 < levels; ++d)
+    {
+        const int lo = starts[d], hi = starts[d + 1];
+        if (hi > lo) select4_kernel<<<(hi - lo + tb - 1) / tb, tb, 0, stream>>>(d_nodes, lo, hi, is4, sel);
+    }
     count_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4);
     scan_sums_kernel<<<1, kScanTB, 0, stream>>>(sums4, nb);
     dense_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4, dense4);
     const int inline_ok = n_tris < (1 << 27) ? 1 : 0;
     *leaf_inline_host = inline_ok;
-    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, d_wide4, inline_ok);
-    cudaError_t e = cudaGetLastError();
+    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, sel, d_wide4, inline_ok);
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    int root_is4 = 0, last_d = 0, last_v = 0;
-    e = cudaMemcpyAsync(&root_is4, is4, sizeof(int), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&last_d, dense4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    int last_d = 0, last_v = 0;
+    e = cudaMemcpyAsync(&last_d, dense4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&last_v, is4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
-    *root4_host = root_is4 ? 0 : ~0;
+    *root4_host = root.triCount == 0 ? 0 : ~0;
     *n4_host = last_v ? last_d + 1 : -1;  // count is only needed for sizing checks
     return cudaSuccess;
 }

@@ -104,10 +104,12 @@ DevCam make_dev_cam(const lg_camera& c);
 cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* d_wide, int2* d_leaves,
                              int* d_scratch, int* root_host, int* n_internal_host, int* n_leaves_host,
                              cudaStream_t stream);
-// Collapses the binary BVH (BFS order) into 4-wide records: every internal
-// node at even depth becomes a record whose children are its grandchildren
-// (or its children, when those are leaves).  Must follow build_wide_nodes on
-// the same scratch (it reuses the leaf numbering).  Scratch: 5 * n_nodes ints.
+// Collapses the binary BVH (BFS order) into 4-wide records, top-down: a
+// record starts from its node's two children and repeatedly opens the
+// internal child of largest surface area until it has four; the internal
+// children are the next records.  Records are numbered by the BFS rank of
+// their nodes (deterministic).  Must follow build_wide_nodes on the same
+// scratch (it reuses the leaf numbering).  Scratch: 11 * n_nodes + 256 ints.
 cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, Wide4Node* d_wide4,
                               int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
                               cudaStream_t stream);

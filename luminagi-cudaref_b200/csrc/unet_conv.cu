@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     __shared__ int s_fail;
 
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int n_cot = a.Cout / BN;
     const int x0 = blockIdx.x * kTileX;
     const int y0 = blockIdx.y * kRows;
