@@ -45,9 +45,9 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 376.9 MB / 65,366,791 rays
+# of an 8-spp engine frame: 359.8 MB / 65,366,791 rays
 # (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = 376.92288e6 / 65366791
+TRACE_DRAM_BYTES_PER_RAY = 359.814144e6 / 65366791
 
 
 def load_peaks():
@@ -393,7 +393,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": TRACE_DRAM_BYTES_PER_RAY * rays,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-spp launch, "
-                                           "scaled by rays", "working_set": "L2-resident (DRAM 5.8 B/ray)",
+                                           "scaled by rays", "working_set": "L2-resident (DRAM 5.5 B/ray)",
                          "peak_source": peak_kind, "kernel": "trace_kernel",
                          "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
             "gpu_launches": args.steps * 2,

@@ -160,7 +160,7 @@ int lg_renderer_set_scene_bvh(lg_renderer* r, const lg_scene_desc* scene, const 
 /* Copy back the device BVH (nodes_out may be NULL to query the count). */
 int lg_renderer_get_bvh(lg_renderer* r, lg_bvh_node* nodes_out, int32_t* n_nodes, lg_triangle* tris_out);
 int lg_renderer_set_counting(lg_renderer* r, int enable);
-/* Traversal records: 4 (default; two binary levels per 128-byte record) or 2
+/* Traversal records: 4 (default; up to four descendants per 128-byte record) or 2
  * (one binary node per 64-byte record).  Both traverse the same BVH. */
 int lg_renderer_set_bvh_width(lg_renderer* r, int width);
 /* Ray/triangle test.  LG_ISECT_MOLLER_TRUMBORE (default) is the reference's

@@ -421,7 +421,8 @@ __device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
 // The 4-wide form of the traversal below: one 128-byte record tests up to
 // four child boxes (same slab arithmetic); hit children are ordered by entry
 // distance, the nearest is entered and the rest stacked nearest-on-top.
-// Measured alternatives on the 64-spp engine frame (633 ms with this form):
+// Measured alternatives on the 64-spp engine frame (633 ms with this form and
+// records from the even-depth collapse; 596 ms with the surface-area collapse):
 // a "while-while" loop (internal records until a leaf, then the warp's leaves
 // together) ran 745 ms, and a 24-entry shared-memory stack 675 ms (its 96 KB
 // per SM comes out of the L1 that caches the BVH records).
