@@ -163,6 +163,20 @@ int lg_renderer_set_counting(lg_renderer* r, int enable);
 /* Traversal records: 4 (default; up to four descendants per 128-byte record) or 2
  * (one binary node per 64-byte record).  Both traverse the same BVH. */
 int lg_renderer_set_bvh_width(lg_renderer* r, int width);
+/* Topology of the tree the traversal records are built from.  Both use the
+ * leaves (triangle ranges and boxes) of the scene's BuildBVH tree, which
+ * lg_renderer_get_bvh still returns unchanged; any binary tree over those
+ * leaves gives the same closest hits (up to exact ties in t).
+ * LG_RENDER_TREE_BUILDBVH keeps BuildBVH's Morton-split topology.
+ * LG_RENDER_TREE_PLOC (default) regroups the leaves by PLOC (Meister and
+ * Bittner, HPG 2018): agglomerative clustering by union surface area, on the
+ * GPU, which makes traversal open fewer boxes.  A tree PLOC cannot regroup
+ * (leaves sharing a first triangle) keeps its own topology; get_render_tree
+ * reports the mode in use. */
+#define LG_RENDER_TREE_BUILDBVH 0
+#define LG_RENDER_TREE_PLOC 1
+int lg_renderer_set_render_tree(lg_renderer* r, int mode);
+int lg_renderer_get_render_tree(lg_renderer* r, int32_t* mode_used);
 /* Ray/triangle test.  LG_ISECT_MOLLER_TRUMBORE (default) is the reference's
  * ray_tri (src/pathtracer.cu:82-107) and the parity mode.
  * LG_ISECT_WATERTIGHT is the watertight test of Woop, Benthin and Wald (JCGT

@@ -15,6 +15,7 @@
 #include "bvh.h"
 #include "common.h"
 #include "lbvh.cuh"
+#include "render_tree.cuh"
 #include "scene.h"
 #include "trace.cuh"
 
@@ -107,6 +108,9 @@ struct lg_renderer
     int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0, root4 = 0;
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
     int leaf_inline = 0;  // 4-wide leaf links carry (first, count)
+    int tree_mode = LG_RENDER_TREE_PLOC;  // topology the traversal records are built from
+    int tree_used = -1;                   // the mode actually built (PLOC falls back to the BuildBVH tree)
+    DevBuf rnodes, rt_scratch;            // render tree (depth order) and its build scratch
     bool watertight = false;  // ray/triangle test: Moller-Trumbore (the reference's) or watertight
     int trace_blocks_per_sm = 0;  // persistent trace grid (0 = occupancy maximum); see lg_renderer_autotune
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
@@ -196,29 +200,53 @@ int upload_common(lg_renderer* r, const lg_scene_desc* d)
     return LG_OK;
 }
 
-// Wide nodes + intersection records from the device node/triangle arrays.
+// Traversal records (2- and 4-wide) from the render tree: the BuildBVH tree's
+// leaves under the topology tree_mode selects (render_tree.cu).
+int build_records(lg_renderer* r)
+{
+    const int n = r->n_nodes;
+    LG_TRY(r->wide.reserve((size_t)n * sizeof(WideNode)));
+    LG_TRY(r->leaves.reserve((size_t)n * sizeof(int2)));
+    LG_TRY(r->rnodes.reserve((size_t)n * sizeof(lg_bvh_node)));
+    LG_TRY(r->rt_scratch.reserve(render_tree_scratch_bytes(n, r->n_tris)));
+    int rc = build_render_tree(r->nodes.as<lg_bvh_node>(), n, r->n_tris, r->tree_mode, r->rnodes.as<lg_bvh_node>(),
+                               r->rt_scratch.p, r->rt_scratch.bytes, r->stream);
+    r->tree_used = r->tree_mode;
+    if (rc != LG_OK && r->tree_mode != LG_RENDER_TREE_BUILDBVH)
+    {
+        // e.g. leaves whose triangle ranges share a first triangle: keep the given topology
+        rc = build_render_tree(r->nodes.as<lg_bvh_node>(), n, r->n_tris, LG_RENDER_TREE_BUILDBVH,
+                               r->rnodes.as<lg_bvh_node>(), r->rt_scratch.p, r->rt_scratch.bytes, r->stream);
+        r->tree_used = LG_RENDER_TREE_BUILDBVH;
+    }
+    LG_TRY(rc);
+    const size_t nb = (size_t)n / 1024 + 1;
+    size_t need = ((size_t)n * 11 + 2 * nb + 256) * sizeof(int);
+    LG_TRY(r->scratch.reserve(need));
+    LG_TRY(r->wide4.reserve(((size_t)n / 2 + 1) * sizeof(Wide4Node)));
+    int root = 0, ni = 0, nl = 0, root4 = 0, n4 = 0;
+    LG_TRY_CUDA(build_wide_nodes(r->rnodes.as<lg_bvh_node>(), n, r->wide.as<WideNode>(), r->leaves.as<int2>(),
+                                 r->scratch.as<int>(), &root, &ni, &nl, r->stream));
+    int leaf_inline = 0;
+    LG_TRY_CUDA(build_wide4_nodes(r->rnodes.as<lg_bvh_node>(), n, r->n_tris, r->wide4.as<Wide4Node>(),
+                                  r->scratch.as<int>(), &root4, &n4, &leaf_inline, r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    r->leaf_inline = leaf_inline;
+    r->root4 = root4;
+    r->root = root;
+    ++r->scene_gen;
+    return LG_OK;
+}
+
+// Traversal records + intersection records from the device node/triangle arrays.
 int finish_scene(lg_renderer* r)
 {
     if (r->n_nodes == 0) { r->root = 0; return LG_OK; }
-    LG_TRY(r->wide.reserve((size_t)r->n_nodes * sizeof(WideNode)));
-    LG_TRY(r->leaves.reserve((size_t)r->n_nodes * sizeof(int2)));
     LG_TRY(r->tv.reserve((size_t)r->n_tris * 3 * sizeof(float4)));
-    const size_t nb = (size_t)r->n_nodes / 1024 + 1;
-    size_t need = ((size_t)r->n_nodes * 11 + 2 * nb + 256) * sizeof(int);
-    LG_TRY(r->scratch.reserve(need));
-    LG_TRY(r->wide4.reserve(((size_t)r->n_nodes / 2 + 1) * sizeof(Wide4Node)));
-    int root = 0, ni = 0, nl = 0, root4 = 0, n4 = 0;
-    LG_TRY_CUDA(build_wide_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->wide.as<WideNode>(),
-                                 r->leaves.as<int2>(), r->scratch.as<int>(), &root, &ni, &nl, r->stream));
-    int leaf_inline = 0;
-    LG_TRY_CUDA(build_wide4_nodes(r->nodes.as<lg_bvh_node>(), r->n_nodes, r->n_tris, r->wide4.as<Wide4Node>(),
-                                  r->scratch.as<int>(), &root4, &n4, &leaf_inline, r->stream));
-    r->leaf_inline = leaf_inline;
-    r->root4 = root4;
+    LG_TRY(build_records(r));
     LG_TRY_CUDA(cudaMemcpyAsync(&r->root_node, r->nodes.p, sizeof(lg_bvh_node), cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->watertight, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
-    r->root = root;
     return LG_OK;
 }
 
@@ -594,7 +622,7 @@ void lg_renderer_destroy(lg_renderer* r)
     r->gbuf.release();
     if (r->batch_exec) cudaGraphExecDestroy(r->batch_exec);
     if (r->batch_host) cudaFreeHost(r->batch_host);
-    for (DevBuf* b : {&r->batch_jobs, &r->batch_acc, &r->batch_rgb}) b->release();
+    for (DevBuf* b : {&r->batch_jobs, &r->batch_acc, &r->batch_rgb, &r->rnodes, &r->rt_scratch}) b->release();
     for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
         b->release();
@@ -814,6 +842,26 @@ int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_
     if (rc != LG_OK) return rc;
     if (blocks_per_sm_out) *blocks_per_sm_out = best;
     if (ms_out) *ms_out = best_ms;
+    return LG_OK;
+}
+
+int lg_renderer_set_render_tree(lg_renderer* r, int mode)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (mode != LG_RENDER_TREE_BUILDBVH && mode != LG_RENDER_TREE_PLOC)
+        return set_error(LG_ERR_INVALID, "render tree mode must be 0 (BuildBVH topology) or 1 (PLOC)");
+    if (mode == r->tree_mode) return LG_OK;
+    DeviceGuard g(r->device);
+    r->tree_mode = mode;
+    if (r->n_nodes == 0) return LG_OK;
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    return build_records(r);
+}
+
+int lg_renderer_get_render_tree(lg_renderer* r, int32_t* mode_used)
+{
+    if (!r || !mode_used) return set_error(LG_ERR_INVALID, "NULL argument");
+    *mode_used = r->tree_used;
     return LG_OK;
 }
 

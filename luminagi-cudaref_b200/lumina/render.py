@@ -110,6 +110,15 @@ class Renderer:
         check(lib().lg_renderer_autotune(self._h, C.byref(cam), spp, bounces, C.byref(b), C.byref(ms)))
         return int(b.value), float(ms.value)
 
+    def set_render_tree(self, mode: str) -> None:
+        """Topology of the traversal records: 'ploc' (default) or 'buildbvh' (same leaves either way)."""
+        check(lib().lg_renderer_set_render_tree(self._h, {"buildbvh": 0, "ploc": 1}[mode]))
+
+    def render_tree(self) -> str:
+        m = C.c_int32(-1)
+        check(lib().lg_renderer_get_render_tree(self._h, C.byref(m)))
+        return {0: "buildbvh", 1: "ploc"}.get(m.value, "none")
+
     def set_counting(self, on: bool) -> None:
         check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))
 

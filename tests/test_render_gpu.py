@@ -188,3 +188,44 @@ def test_trace_grid_autotune(box_scene):
         assert 1 <= bps <= 4 and ms > 0
         after = r.render(spp=8, bounces=2)
     assert np.array_equal(before["accum"], after["accum"])
+
+
+def _dfs_order(nodes):
+    """The same tree with its records in depth-first preorder (links remapped)."""
+    order, stack = [], [0]
+    while stack:
+        i = stack.pop()
+        order.append(i)
+        if nodes["triCount"][i] == 0:
+            stack += [int(nodes["right"][i]), int(nodes["left"][i])]
+    pos = np.empty(len(nodes), np.int64)
+    pos[np.array(order)] = np.arange(len(order))
+    out = nodes[np.array(order)].copy()
+    internal = out["triCount"] == 0
+    out["left"][internal] = pos[out["left"][internal]]
+    out["right"][internal] = pos[out["right"][internal]]
+    return out
+
+
+@pytest.mark.parametrize("tree", ["ploc", "buildbvh"])
+def test_render_tree_modes_and_dfs_input(small_engine_scene, tree):
+    """Traversal records from the PLOC-regrouped tree or from BuildBVH's own
+    topology, for a breadth-first and a depth-first caller array: every frame
+    must match the reference kernel on the reference tree."""
+    if not O.ref_available():
+        pytest.skip("reference oracle not built")
+    sc = small_engine_scene
+    nodes, tris, _, _ = O.oracle_build_bvh(sc.tris)
+    ref_acc, _, _ = O.ref_render_gpu(sc, nodes, tris, 8, 2)
+    s2 = lumina.Scene(sc.camera, sc.sun, tris, sc.mat_albedo, sc.mat_emissive, sc.points)
+    for arr in (nodes, _dfs_order(nodes)):
+        with lumina.Renderer(0) as r:
+            r.set_render_tree(tree)
+            r.set_scene_bvh(s2, arr)
+            assert r.render_tree() == tree
+            for width in (4, 2):
+                r.set_bvh_width(width)
+                ours = r.render(spp=8, bounces=2)
+                assert match_fraction(ours["accum"], ref_acc) >= 0.999, (tree, width)
+            got_nodes, _ = r.get_bvh()
+            assert got_nodes.tobytes() == np.ascontiguousarray(arr).tobytes()  # the caller's tree is kept as given
