@@ -278,11 +278,17 @@ int lg_unet_adam_reset(lg_unet* u);
 /* Autotuner: for each of the 14 convolutions (and, with
  * LG_UNET_TUNE_BACKWARD, the 16 input-gradient convolutions of training)
  * times every compiled tile shape (output channels per CTA, input channels
- * per K-block, pipeline stages) inside real passes at n x h x w and keeps the
- * fastest; weights are repacked to match.  tiles_out (may be NULL) receives 30
- * (bn, kc, stages) triples, forward layers first.  The Adam state is reset. */
+ * per K-block, pipeline stages) with each of the two kernels (one tile per
+ * CTA, or persistent and warp-specialised) inside real passes at n x h x w
+ * and keeps the fastest; weights are repacked to match.  tiles_out (may be
+ * NULL) receives 30 (bn, kc, stages, persistent) quadruples, forward layers
+ * first.  The Adam state is reset. */
 #define LG_UNET_TUNE_BACKWARD 1
 int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_out);
+/* Sets the 30 tile choices directly, in lg_unet_autotune's format; e.g. to
+ * reuse a tuning result without timing.  (0, 0, 0, p) is the default shape on
+ * the kernel p selects (0: one tile per CTA, 1: persistent). */
+int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles);
 /* One 3x3 convolution layer on device buffers in the channel-blocked BF16
  * layout ((n*C/8 + c/8)*H + y)*W + x)*8 + c%8: epilogue 0 writes act(conv+b)
  * into channels [out_coff, out_coff+cout) of d_out (and, if d_out2, the 2x2

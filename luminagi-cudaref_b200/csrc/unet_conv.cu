@@ -15,6 +15,7 @@
 // 2x2 max-pool (both rows are in the tile; x pairs are adjacent lanes),
 // nearest 2x upsample into a concat buffer, or the UNet tail (1x1 conv to
 // RGB + residual + clamp).  Operands are BF16, accumulation FP32.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -45,7 +46,7 @@ typedef ConvTile TileCfg;
 // ones.  The autotuner (lg_unet_autotune) may pick another compiled shape.
 TileCfg pick_cfg(int Cin, int Cout)
 {
-    TileCfg c;
+    TileCfg c{};
     c.bn = Cout < 128 ? Cout : 128;
     c.kc = (Cin % 32 == 0) ? 32 : 16;
     if (c.bn == 32) c.stages = c.kc == 16 ? 4 : 2;
@@ -202,6 +203,135 @@ __device__ __forceinline__ void bwd_epilogue(const ConvArgs& a, float (&v)[kRows
     }
 }
 
+// Epilogue of one output tile (2 rows x 128 pixels x BN channels of output
+// block ct): the accumulator at TMEM column `tmem` holds row r at columns
+// r*BN..r*BN+BN-1; lane p = pixel x0 + p.  The calling warp reads its quarter
+// of the lanes: `warp` (0..3) selects lanes 32*warp..32*warp+31 and
+// tid = 32*warp + lane is the pixel offset.
+template <int BN>
+__device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, int warp, int tid, int n, int ct,
+                                              int x0, int y0)
+{
+    const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
+    const int x = x0 + tid;
+    const bool xin = x < a.W;
+    if (a.epilogue == kEpiTail)
+    {
+        // BN == Cout == 32: whole pixel in this thread.
+        float o[kRows][3];
+#pragma unroll
+        for (int r = 0; r < kRows; ++r)
+        {
+            float v[32];
+            tc::tmem_ld16(lanebase + (uint32_t)(r * BN), v);
+            tc::tmem_ld16(lanebase + (uint32_t)(r * BN + 16), v + 16);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) v[c] = bf16r(act(v[c] + __ldg(&a.bias[c]), a.slope));
+            const int y = y0 + r;
+            if (a.out && xin && y < a.H)
+            {
+#pragma unroll
+                for (int b = 0; b < 4; ++b)
+                    *blk(a.out, a.out_C, a.H, a.W, n, (a.out_coff >> 3) + b, y, x) = pack8(v + 8 * b);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                float acc = __ldg(&a.tail_b[k]);
+#pragma unroll
+                for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&a.tail_w[k * 32 + c]), v[c], acc);
+                o[r][k] = acc;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kRows; ++r)
+        {
+            const int y = y0 + r;
+            if (!xin || y >= a.H) continue;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+            {
+                const size_t pi = (((size_t)n * a.resid_C + k) * a.H + y) * a.W + x;
+                const size_t po = (((size_t)n * 3 + k) * a.H + y) * a.W + x;
+                if (a.log_hdr) a.final_out[po] = expm1f(fmaxf(log1pf(a.resid[pi]) + o[r][k], 0.0f));
+                else a.final_out[po] = fminf(fmaxf(a.resid[pi] + o[r][k], 0.0f), 1.0f);
+            }
+        }
+    }
+    else
+    {
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16)
+        {
+            float v[kRows][16];
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) tc::tmem_ld16(lanebase + (uint32_t)(r * BN + c0), v[r]);
+            const int cg = ct * BN + c0;  // layer channel of v[.][0]
+            if (a.epilogue <= kEpiUpsample)
+            {
+#pragma unroll
+                for (int r = 0; r < kRows; ++r)
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + __ldg(&a.bias[cg + j]), a.slope));
+            }
+            const int b0 = (a.out_coff + cg) >> 3;
+            if (a.epilogue >= kEpiBwdMask)
+            {
+                bwd_epilogue(a, v, n, y0, x, cg, b0);
+            }
+            else if (a.epilogue == kEpiStore)
+            {
+#pragma unroll
+                for (int r = 0; r < kRows; ++r)
+                {
+                    const int y = y0 + r;
+                    if (xin && y < a.H)
+                    {
+                        *blk(a.out, a.out_C, a.H, a.W, n, b0, y, x) = pack8(v[r]);
+                        *blk(a.out, a.out_C, a.H, a.W, n, b0 + 1, y, x) = pack8(v[r] + 8);
+                    }
+                }
+                if (a.out2)
+                {
+                    float m[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                    {
+                        float t = fmaxf(v[0][j], v[1][j]);
+                        m[j] = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, 1));
+                    }
+                    const int H2 = a.H >> 1, W2 = a.W >> 1;
+                    if (((x & 1) == 0) && (x >> 1) < W2 && (y0 >> 1) < H2)
+                    {
+                        const int pb = (a.out2_coff + cg) >> 3;
+                        *blk(a.out2, a.out2_C, H2, W2, n, pb, y0 >> 1, x >> 1) = pack8(m);
+                        *blk(a.out2, a.out2_C, H2, W2, n, pb + 1, y0 >> 1, x >> 1) = pack8(m + 8);
+                    }
+                }
+            }
+            else  // kEpiUpsample: nearest 2x into a 2H x 2W buffer
+            {
+                const int H2 = a.H * 2, W2 = a.W * 2;
+#pragma unroll
+                for (int r = 0; r < kRows; ++r)
+                {
+                    const int y = y0 + r;
+                    if (!xin || y >= a.H) continue;
+                    const uint4 lo = pack8(v[r]), hi = pack8(v[r] + 8);
+#pragma unroll
+                    for (int i = 0; i < 2; ++i)
+#pragma unroll
+                        for (int jx = 0; jx < 2; ++jx)
+                        {
+                            *blk(a.out, a.out_C, H2, W2, n, b0, 2 * y + i, 2 * x + jx) = lo;
+                            *blk(a.out, a.out_C, H2, W2, n, b0 + 1, 2 * y + i, 2 * x + jx) = hi;
+                        }
+                }
+            }
+        }
+    }
+}
+
 template <int BN, int KC, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
 {
@@ -309,131 +439,207 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     const bool got = tc::mbar_wait(done, 0);
     if (!got && a.err) atomicExch(a.err, 2);
     tc::tc_fence_after();
-    if (got && !s_fail)
-    {
-        const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
-        const int x = x0 + tid;
-        const bool xin = x < a.W;
-        if (a.epilogue == kEpiTail)
-        {
-            // BN == Cout == 32: whole pixel in this thread.
-            float o[kRows][3];
-#pragma unroll
-            for (int r = 0; r < kRows; ++r)
-            {
-                float v[32];
-                tc::tmem_ld16(lanebase + (uint32_t)(r * BN), v);
-                tc::tmem_ld16(lanebase + (uint32_t)(r * BN + 16), v + 16);
-#pragma unroll
-                for (int c = 0; c < 32; ++c) v[c] = bf16r(act(v[c] + __ldg(&a.bias[c]), a.slope));
-                const int y = y0 + r;
-                if (a.out && xin && y < a.H)
-                {
-#pragma unroll
-                    for (int b = 0; b < 4; ++b)
-                        *blk(a.out, a.out_C, a.H, a.W, n, (a.out_coff >> 3) + b, y, x) = pack8(v + 8 * b);
-                }
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                {
-                    float acc = __ldg(&a.tail_b[k]);
-#pragma unroll
-                    for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&a.tail_w[k * 32 + c]), v[c], acc);
-                    o[r][k] = acc;
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < kRows; ++r)
-            {
-                const int y = y0 + r;
-                if (!xin || y >= a.H) continue;
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                {
-                    const size_t pi = (((size_t)n * a.resid_C + k) * a.H + y) * a.W + x;
-                    const size_t po = (((size_t)n * 3 + k) * a.H + y) * a.W + x;
-                    if (a.log_hdr) a.final_out[po] = expm1f(fmaxf(log1pf(a.resid[pi]) + o[r][k], 0.0f));
-                    else a.final_out[po] = fminf(fmaxf(a.resid[pi] + o[r][k], 0.0f), 1.0f);
-                }
-            }
-        }
-        else
-        {
-#pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16)
-            {
-                float v[kRows][16];
-#pragma unroll
-                for (int r = 0; r < kRows; ++r) tc::tmem_ld16(lanebase + (uint32_t)(r * BN + c0), v[r]);
-                const int cg = ct * BN + c0;  // layer channel of v[.][0]
-                if (a.epilogue <= kEpiUpsample)
-                {
-#pragma unroll
-                    for (int r = 0; r < kRows; ++r)
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + __ldg(&a.bias[cg + j]), a.slope));
-                }
-                const int b0 = (a.out_coff + cg) >> 3;
-                if (a.epilogue >= kEpiBwdMask)
-                {
-                    bwd_epilogue(a, v, n, y0, x, cg, b0);
-                }
-                else if (a.epilogue == kEpiStore)
-                {
-#pragma unroll
-                    for (int r = 0; r < kRows; ++r)
-                    {
-                        const int y = y0 + r;
-                        if (xin && y < a.H)
-                        {
-                            *blk(a.out, a.out_C, a.H, a.W, n, b0, y, x) = pack8(v[r]);
-                            *blk(a.out, a.out_C, a.H, a.W, n, b0 + 1, y, x) = pack8(v[r] + 8);
-                        }
-                    }
-                    if (a.out2)
-                    {
-                        float m[16];
-#pragma unroll
-                        for (int j = 0; j < 16; ++j)
-                        {
-                            float t = fmaxf(v[0][j], v[1][j]);
-                            m[j] = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, 1));
-                        }
-                        const int H2 = a.H >> 1, W2 = a.W >> 1;
-                        if (((x & 1) == 0) && (x >> 1) < W2 && (y0 >> 1) < H2)
-                        {
-                            const int pb = (a.out2_coff + cg) >> 3;
-                            *blk(a.out2, a.out2_C, H2, W2, n, pb, y0 >> 1, x >> 1) = pack8(m);
-                            *blk(a.out2, a.out2_C, H2, W2, n, pb + 1, y0 >> 1, x >> 1) = pack8(m + 8);
-                        }
-                    }
-                }
-                else  // kEpiUpsample: nearest 2x into a 2H x 2W buffer
-                {
-                    const int H2 = a.H * 2, W2 = a.W * 2;
-#pragma unroll
-                    for (int r = 0; r < kRows; ++r)
-                    {
-                        const int y = y0 + r;
-                        if (!xin || y >= a.H) continue;
-                        const uint4 lo = pack8(v[r]), hi = pack8(v[r] + 8);
-#pragma unroll
-                        for (int i = 0; i < 2; ++i)
-#pragma unroll
-                            for (int jx = 0; jx < 2; ++jx)
-                            {
-                                *blk(a.out, a.out_C, H2, W2, n, b0, 2 * y + i, 2 * x + jx) = lo;
-                                *blk(a.out, a.out_C, H2, W2, n, b0 + 1, 2 * y + i, 2 * x + jx) = hi;
-                            }
-                    }
-                }
-            }
-        }
-    }
+    if (got && !s_fail) tile_epilogue<BN>(a, tmem, warp, tid, n, ct, x0, y0);
+
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0)
     {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, kCols);
+    }
+}
+
+
+// Persistent, warp-specialised form of conv3x3_tc_kernel: one CTA per SM (two
+// for the smallest tiles) walks the output tiles in a grid-stride loop.
+//   warp 0 (one lane)  TMA loads of input halos and weight blocks into a
+//                      STAGES-deep ring (full/empty mbarriers);
+//   warp 1 (one lane)  tcgen05.mma into one of two TMEM accumulators (each two
+//                      rows x BN columns), committing the ring stage when its
+//                      MMAs retire and the accumulator when the tile is done;
+//   warps 2..5         the epilogue of tile i (tile_epilogue, each warp its
+//                      TMEM lane quarter) while tile i+1's loads and MMAs run.
+// Loads run ahead across tile boundaries; TMEM is allocated once per CTA.
+// The same packed weights, the same MMAs in the same order: results are
+// identical to conv3x3_tc_kernel's.
+constexpr int kPThreads = 192;
+template <int BN, int KC, int STAGES>
+__global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
+{
+    using S = Smem<BN, KC>;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * S::kStage);
+    uint64_t* empty = full + STAGES;
+    uint64_t* acc_full = empty + STAGES;  // [2]
+    uint64_t* acc_empty = acc_full + 2;   // [2]
+    uint64_t* done = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ volatile int s_fail;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n_cot = a.Cout / BN;
+    const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + kRows - 1) / kRows;
+    const int n_tiles = tiles_x * tiles_y * a.N * n_cot;
+    const int KB = a.Cin / KC;
+    constexpr uint32_t kCols = 4 * BN;  // two accumulators of two rows x BN FP32 columns
+    constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, BN);
+    constexpr uint32_t kLboA = kHaloY * kHaloX * 16;
+    constexpr uint32_t kLboB = BN * 16;
+    // tile t -> (n, ct, y0, x0); output blocks innermost so concurrent tiles share input rows
+    auto coords = [&](int t, int& n, int& ct, int& x0, int& y0) {
+        ct = t % n_cot;
+        t /= n_cot;
+        x0 = (t % tiles_x) * kTileX;
+        t /= tiles_x;
+        y0 = (t % tiles_y) * kRows;
+        n = t / tiles_y;
+    };
+    auto fail = [&](int code) {
+        s_fail = 1;
+        if (a.err) atomicExch(a.err, code);
+    };
+
+    if (warp == 1)
+    {
+        tc::tmem_alloc(tmem_slot, kCols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0)
+    {
+        s_fail = 0;
+        for (int s = 0; s < STAGES; ++s)
+        {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; ++b)
+        {
+            tc::mbar_init(&acc_full[b], 1);
+            tc::mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+        }
+        tc::mbar_init(done, 1);
+        tc::fence_mbar_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0)
+    {
+        if (lane == 0)
+        {
+            int it = 0;
+            for (int t = blockIdx.x; t < n_tiles && !s_fail; t += gridDim.x)
+            {
+                int n, ct, x0, y0;
+                coords(t, n, ct, x0, y0);
+                const __nv_bfloat16* wsrc = a.wpack + (size_t)ct * KB * (9 * KC * BN);
+                for (int kb = 0; kb < KB; ++kb, ++it)
+                {
+                    const int s = it % STAGES, u = it / STAGES;
+                    if (u > 0 && !tc::mbar_wait(&empty[s], (uint32_t)((u - 1) & 1)))
+                    {
+                        fail(3);
+                        break;
+                    }
+                    uint8_t* A = smem + s * S::kStage;
+                    uint8_t* B = A + S::kABytes;
+                    tc::mbar_expect_tx(&full[s], (uint32_t)(S::kABytes + S::kBBytes));
+                    tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
+                    tc::bulk_load(B, wsrc + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes, &full[s]);
+                }
+            }
+        }
+    }
+    else if (warp == 1)
+    {
+        if (lane == 0)
+        {
+            int it = 0, j = 0;
+            for (int t = blockIdx.x; t < n_tiles && !s_fail; t += gridDim.x, ++j)
+            {
+                const int b = j & 1, v = j >> 1;
+                if (v > 0 && !tc::mbar_wait(&acc_empty[b], (uint32_t)((v - 1) & 1)))
+                {
+                    fail(4);
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * 2 * BN);
+                bool ok = true;
+                for (int kb = 0; kb < KB; ++kb, ++it)
+                {
+                    const int s = it % STAGES;
+                    if (!tc::mbar_wait(&full[s], (uint32_t)((it / STAGES) & 1)))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const uint32_t abase = tc::smem_u32(smem + s * S::kStage);
+                    const uint32_t bbase = abase + S::kABytes;
+#pragma unroll 1
+                    for (int tap = 0; tap < 9; ++tap)
+                    {
+                        const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+                        for (int ks = 0; ks < KC / 16; ++ks)
+                        {
+                            const uint64_t bd =
+                                tc::smem_desc(bbase + (uint32_t)((tap * (KC / 8) + 2 * ks) * BN * 16), kLboB, 128);
+#pragma unroll
+                            for (int r = 0; r < kRows; ++r)
+                            {
+                                const uint32_t aoff =
+                                    (uint32_t)(2 * ks) * kLboA + (uint32_t)(((r + dy) * kHaloX + dx) * 16);
+                                const uint64_t ad = tc::smem_desc(abase + aoff, kLboA, 128);
+                                tc::mma_bf16(acc + (uint32_t)(r * BN), ad, bd, kIdesc, (kb | tap | ks) != 0 ? 1u : 0u);
+                            }
+                        }
+                    }
+                    tc::mma_commit(&empty[s]);  // frees the stage when these MMAs retire
+                }
+                if (!ok)
+                {
+                    fail(1);
+                    break;
+                }
+                tc::mma_commit(&acc_full[b]);
+            }
+            tc::mma_commit(done);  // completes when every MMA issued above has finished
+        }
+    }
+    else
+    {
+        const int q = warp & 3;  // the TMEM lane quarter this warp may read
+        int j = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++j)
+        {
+            const int b = j & 1, v = j >> 1;
+            if (!tc::mbar_wait(&acc_full[b], (uint32_t)(v & 1)))
+            {
+                fail(2);
+                break;
+            }
+            tc::tc_fence_after();
+            int n, ct, x0, y0;
+            coords(t, n, ct, x0, y0);
+            tile_epilogue<BN>(a, tmem + (uint32_t)(b * 2 * BN), q, q * 32 + lane, n, ct, x0, y0);
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&acc_empty[b]);
+        }
+    }
+    __syncthreads();
+    if (warp == 1)
+    {
+        bool drained = true;
+        if (lane == 0) drained = tc::mbar_wait(done, 0);
+        drained = __shfl_sync(0xffffffffu, drained ? 1 : 0, 0) != 0;
+        if (!drained && lane == 0 && a.err) atomicExch(a.err, 2);
         tc::tc_fence_after();
         tc::tmem_dealloc(tmem, kCols);
     }
@@ -472,6 +678,37 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+template <int BN, int KC, int STAGES>
+cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
+{
+    CUtensorMap m;
+    cudaError_t e = make_map(&m, in, a.N, a.Cin, a.H, a.W, KC);
+    if (e != cudaSuccess) return e;
+    const int smem = STAGES * Smem<BN, KC>::kStage + 1024 + 256;
+    static int per_sm = 0;
+    static int sm_count = 0;
+    if (per_sm == 0)
+    {
+        e = cudaFuncSetAttribute(conv3x3_tc_persistent<BN, KC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem);
+        if (e != cudaSuccess) return e;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_tc_persistent<BN, KC, STAGES>, kPThreads,
+                                                          smem);
+        if (e != cudaSuccess) return e;
+        // TMEM: each CTA holds 4*BN of the SM's 512 columns for its lifetime
+        const int tmem_fit = 512 / (4 * BN);
+        if (per_sm > tmem_fit) per_sm = tmem_fit;
+        if (per_sm < 1) per_sm = 1;
+    }
+    const long long tiles = (long long)((a.W + kTileX - 1) / kTileX) * ((a.H + kRows - 1) / kRows) * a.N * (a.Cout / BN);
+    const long long grid = std::min<long long>(tiles, (long long)per_sm * sm_count);
+    conv3x3_tc_persistent<BN, KC, STAGES><<<(unsigned)grid, kPThreads, smem, stream>>>(m, a);
+    return cudaGetLastError();
 }
 
 template <int BN, int KC, int STAGES>
@@ -576,8 +813,10 @@ size_t conv_packed_elems(int Cin, int Cout) { return (size_t)9 * Cin * Cout; }
 ConvTile conv_default_tile(int Cin, int Cout) { return pick_cfg(Cin, Cout); }
 
 // The shapes conv3x3_forward is compiled for.
-constexpr ConvTile kCompiledTiles[] = {{32, 16, 4},  {32, 32, 2},  {32, 32, 4},  {64, 16, 4},
-                                       {64, 32, 2},  {64, 32, 3},  {128, 16, 3}, {128, 32, 2}};
+constexpr ConvTile kCompiledTiles[] = {{32, 16, 4, 0},  {32, 32, 2, 0},  {32, 32, 4, 0},  {64, 16, 4, 0},
+                                       {64, 32, 2, 0},  {64, 32, 3, 0},  {128, 16, 3, 0}, {128, 32, 2, 0},
+                                       {32, 16, 4, 1},  {32, 32, 2, 1},  {32, 32, 4, 1},  {64, 16, 4, 1},
+                                       {64, 32, 2, 1},  {64, 32, 3, 1},  {128, 16, 3, 1}, {128, 32, 2, 1}};
 
 int conv_tile_candidates(int Cin, int Cout, ConvTile* out, int max)
 {
@@ -621,6 +860,19 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
     const TileCfg c = resolve(a.tile, a.Cin, a.Cout);
     if (a.Cout % c.bn || a.Cin % c.kc) return cudaErrorInvalidValue;
     const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    if (c.persist)
+        switch (key)
+        {
+        case 32164: return launch_persistent<32, 16, 4>(in, a, stream);
+        case 32322: return launch_persistent<32, 32, 2>(in, a, stream);
+        case 32324: return launch_persistent<32, 32, 4>(in, a, stream);
+        case 64164: return launch_persistent<64, 16, 4>(in, a, stream);
+        case 64322: return launch_persistent<64, 32, 2>(in, a, stream);
+        case 64323: return launch_persistent<64, 32, 3>(in, a, stream);
+        case 128163: return launch_persistent<128, 16, 3>(in, a, stream);
+        case 128322: return launch_persistent<128, 32, 2>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
     switch (key)
     {
     case 32164: return launch<32, 16, 4>(in, a, stream);

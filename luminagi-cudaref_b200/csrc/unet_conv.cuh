@@ -31,12 +31,13 @@ enum ConvEpilogue : int
 };
 
 // Tile shape of one convolution: BN output channels per CTA, KC input
-// channels per K-block, STAGES pipeline stages.  Packed weights depend on
+// channels per K-block, STAGES pipeline stages, and which kernel runs it.  Packed weights depend on
 // (BN, KC), so a layer packs and launches with the same tile.  bn == 0 means
 // the default heuristic (conv_default_tile).
 struct ConvTile
 {
     int bn, kc, stages;
+    int persist;  // 1: the persistent, warp-specialised kernel (same packing, same results)
 };
 ConvTile conv_default_tile(int Cin, int Cout);
 // The compiled tile shapes valid for a layer (Cout % bn == 0, Cin % kc == 0);

@@ -423,8 +423,8 @@ int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_
         {
             const int cin = bwd ? kLayers[kDgrad[i].layer].cout : kLayers[i].cin;
             const int cout = bwd ? kDgrad[i].ci_cnt : kLayers[i].cout;
-            ConvTile cand[16];
-            const int nc = conv_tile_candidates(cin, cout, cand, 16);
+            ConvTile cand[32];
+            const int nc = conv_tile_candidates(cin, cout, cand, 32);
             ConvTile& slot = bwd ? u->tile_dg[i] : u->tile[i];
             ConvTile best = conv_default_tile(cin, cout);
             float best_ms = 1e30f;
@@ -464,15 +464,52 @@ int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_
             const int cin = i < 14 ? kLayers[i].cin : kLayers[kDgrad[i - 14].layer].cout;
             const int cout = i < 14 ? kLayers[i].cout : kDgrad[i - 14].ci_cnt;
             const ConvTile r = tt.bn ? tt : conv_default_tile(cin, cout);
-            tiles_out[3 * i] = r.bn;
-            tiles_out[3 * i + 1] = r.kc;
-            tiles_out[3 * i + 2] = r.stages;
+            tiles_out[4 * i] = r.bn;
+            tiles_out[4 * i + 1] = r.kc;
+            tiles_out[4 * i + 2] = r.stages;
+            tiles_out[4 * i + 3] = r.persist;
         }
     x.release();
     t.release();
     y.release();
     if (rc == LG_OK) LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
     return rc;
+}
+
+int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
+{
+    if (!u || !tiles) return set_error(LG_ERR_INVALID, "NULL argument");
+    ConvTile fwd[14], bwd[16];
+    for (int i = 0; i < 30; ++i)
+    {
+        ConvTile t{tiles[4 * i], tiles[4 * i + 1], tiles[4 * i + 2], tiles[4 * i + 3] != 0 ? 1 : 0};
+        const bool back = i >= 14;
+        const int cin = back ? kLayers[kDgrad[i - 14].layer].cout : kLayers[i].cin;
+        const int cout = back ? kDgrad[i - 14].ci_cnt : kLayers[i].cout;
+        bool ok = false;
+        if (t.bn == 0)  // the default shape, on the kernel the fourth value selects
+        {
+            const int persist = t.persist;
+            t = conv_default_tile(cin, cout);
+            t.persist = persist;
+            ok = true;
+        }
+        ConvTile cand[32];
+        const int nc = conv_tile_candidates(cin, cout, cand, 32);
+        for (int c = 0; c < nc && !ok; ++c)
+            ok = cand[c].bn == t.bn && cand[c].kc == t.kc && cand[c].stages == t.stages && cand[c].persist == t.persist;
+        if (!ok)
+            return set_error(LG_ERR_INVALID, "conv %d: (%d, %d, %d, %d) is not a compiled tile for %d -> %d channels", i,
+                             t.bn, t.kc, t.stages, t.persist, cin, cout);
+        (back ? bwd[i - 14] : fwd[i]) = t;
+    }
+    for (int i = 0; i < 14; ++i) u->tile[i] = fwd[i];
+    for (int i = 0; i < 16; ++i) u->tile_dg[i] = bwd[i];
+    u->packed_ok = false;
+    u->packed_dg_ok = false;
+    LG_TRY(unet_pack_all(u));
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    return LG_OK;
 }
 
 int lg_unet_adam_reset(lg_unet* u)

@@ -288,7 +288,7 @@ def test_autotune_keeps_results():
     y0 = net.forward(x)
     tiles = net.autotune(n, h, w, backward=True)
     print("autotuned tiles (bn, kc, stages):", tiles)
-    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) for t in tiles)
+    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) and t[3] in (0, 1) for t in tiles)
     y1 = net.forward(x)
     assert np.array_equal(net.get_params(), flat)
     m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
@@ -307,3 +307,29 @@ def test_autotune_keeps_results():
     ref_g = np.concatenate([p.grad.numpy().ravel() for _, p in mm.named_parameters()])
     cos = float(np.dot(g, ref_g) / (np.linalg.norm(g) * np.linalg.norm(ref_g)))
     assert cos > 0.99
+
+
+def test_persistent_conv_kernel_is_bit_identical():
+    """Every conv on the persistent warp-specialised kernel (same tile shapes,
+    same MMAs in the same order) gives bit-identical outputs and loss to the
+    one-tile-per-CTA kernel; weight gradients use FP32 atomics, so they are
+    compared by cosine."""
+    flat = unet_ref.make_params(80)
+    n, h, w = 2, 40, 264  # partial tiles at the right and bottom edges, several tiles per CTA
+    x = np.random.default_rng(9).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
+    noisy, clean = _batch(n, h, w, 12)
+    dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
+    outs = []
+    for persist in (0, 1):
+        net = lumina.UNet()
+        net.set_params(flat)
+        net.set_tiles([(0, 0, 0, persist)] * 30)
+        y = net.forward(x)
+        loss, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
+        outs.append((y, loss, g))
+        net.close()
+    (y0, l0, g0), (y1, l1, g1) = outs
+    assert np.array_equal(y0, y1)
+    assert abs(l0 - l1) <= 1e-6 * max(1.0, abs(l0))
+    cos = float(np.dot(g0, g1) / (np.linalg.norm(g0) * np.linalg.norm(g1)))
+    assert cos > 0.9999
