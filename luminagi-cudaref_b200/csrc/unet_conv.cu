@@ -42,8 +42,8 @@ typedef ConvTile TileCfg;
 
 // Default tile shape per layer: BN = min(Cout, 128), KC = 32 input channels
 // per K-block (16 when Cin is not a multiple of 32), stages to fill ~100 KB
-// (two CTAs per SM) for narrow layers or ~210 KB (one CTA per SM) for wide
-// ones.  The autotuner (lg_unet_autotune) may pick another compiled shape.
+// for narrow layers or ~210 KB for wide ones, on the persistent kernel.  The
+// autotuner (lg_unet_autotune) may pick another compiled shape or kernel.
 TileCfg pick_cfg(int Cin, int Cout)
 {
     TileCfg c{};
@@ -52,6 +52,7 @@ TileCfg pick_cfg(int Cin, int Cout)
     if (c.bn == 32) c.stages = c.kc == 16 ? 4 : 2;
     else if (c.bn == 64) c.stages = 3;
     else c.stages = 2;
+    c.persist = 1;  // persistent kernel: 1.3-1.4x the one-tile-per-CTA kernel on the UNet layers
     return c;
 }
 

@@ -1,6 +1,6 @@
 """Device-timed micro-benchmarks of the library's kernels.
 
-    python -m lumina.perf unet  [--n 1] [--h 864] [--w 1728] [--reps 10]
+    python -m lumina.perf unet  [--n 1] [--h 864] [--w 1728] [--reps 10] [--kernel default|single|autotune]
     python -m lumina.perf trace [--spp 8] [--bounces 2] [--width 4] [--reps 2]
     python -m lumina.perf bvh   [--reps 5]
     python -m lumina.perf batch [--poses 50] [--spp 8] [--bounces 2]
@@ -26,6 +26,11 @@ def unet(a):
     from .unet import UNet
     net = UNet()
     net.set_params(np.random.default_rng(5).normal(0, 0.02, net.n_params).astype(np.float32))
+    tiles = None
+    if a.kernel == "single":
+        net.set_tiles([(0, 0, 0, 0)] * 30)
+    elif a.kernel == "autotune":
+        tiles = net.autotune(a.n, a.h, a.w)[:14]
     x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
     y = torch.empty_like(x)
     st = torch.cuda.current_stream()
@@ -40,7 +45,8 @@ def unet(a):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
     flops = 2 * 162240 * a.n * a.h * a.w
-    return {"kernel": "unet_forward", "n": a.n, "h": a.h, "w": a.w, "ms": ms, "tflops": flops / ms / 1e9}
+    return {"kernel": "unet_forward", "conv": a.kernel, "n": a.n, "h": a.h, "w": a.w, "ms": ms,
+            "tflops": flops / ms / 1e9, "tiles": tiles}
 
 
 def trace(a):
@@ -131,6 +137,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["unet", "trace", "bvh", "batch"])
     ap.add_argument("--poses", type=int, default=50)
+    ap.add_argument("--kernel", default="default", choices=["default", "single", "autotune"],
+                    help="unet: default tiles, the one-tile-per-CTA conv kernel, or autotuned tiles")
     ap.add_argument("--n", type=int, default=1)
     ap.add_argument("--h", type=int, default=864)
     ap.add_argument("--w", type=int, default=1728)
