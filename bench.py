@@ -11,9 +11,10 @@ counting pass) with ms/frame alongside.
   e2e       through the C ABI from host buffers: triangle upload from pinned
             memory, device LBVH build, render, tonemap and the 8-bit image read
             back, every step.
-  roofline  algorithmic bytes of the trace kernel (64 B per two-child BVH
-            record, 48 B per triangle test, 8 B per leaf entry, as counted)
-            over its event-timed duration, against the measured HBM copy peak.
+  roofline  algorithmic bytes of the trace kernel (112 B per 4-wide BVH
+            record: six planes of four boxes and four links; 48 B per triangle
+            test; 8 B per leaf-table entry; as counted) over its event-timed
+            duration, against the measured HBM copy peak.
             The scene (~200 MB) exceeds the 126 MB L2, so traffic is a mix of
             L2 and HBM.
   cpu_baseline  the reference's own trace code (oracle/_ref, compiled from its
@@ -45,9 +46,12 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 359.8 MB / 65,366,791 rays
+# of an 8-spp engine frame: 612.1 MB + 138.3 MB / 65,366,791 rays
 # (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = 359.814144e6 / 65366791
+TRACE_DRAM_BYTES_PER_RAY = 750.441984e6 / 65366791
+# Bytes one traversal step reads from a BVH record: 4-wide, six planes of
+# four boxes (96 B) and four links (16 B); 2-wide, the whole 64-B record.
+RECORD_BYTES = {4: 112, 2: 64}
 
 
 def load_peaks():
@@ -286,7 +290,7 @@ def main():
     c = r.render(spp=args.spp, bounces=args.bounces, accum=False, rgb=False)
     r.set_counting(False)
     rays = c["closest_rays"] + c["shadow_rays"]
-    algo_bytes = 64 * c["node_fetches"] + 48 * c["tri_tests"] + 8 * c["leaf_fetches"]
+    algo_bytes = RECORD_BYTES[4] * c["node_fetches"] + 48 * c["tri_tests"] + 8 * c["leaf_fetches"]
 
     import ctypes as C
     cam = scene.camera.to_c()
@@ -393,7 +397,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": TRACE_DRAM_BYTES_PER_RAY * rays,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-spp launch, "
-                                           "scaled by rays", "working_set": "L2-resident (DRAM 5.5 B/ray)",
+                                           "scaled by rays", "working_set": f"L2-resident (DRAM {TRACE_DRAM_BYTES_PER_RAY:.1f} B/ray)",
                          "peak_source": peak_kind, "kernel": "trace_kernel",
                          "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
             "gpu_launches": args.steps * 2,

@@ -190,6 +190,14 @@ int lg_renderer_set_intersection(lg_renderer* r, int mode);
  * reports it (and its kernel time) through the optional outputs. */
 int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_bounces, int32_t* blocks_per_sm,
                          float* ms);
+/* Ray refill of the persistent trace launch.  A warp steps its lanes' ray
+ * traversals one BVH record or leaf at a time; once `threshold` of its 32
+ * lanes have finished their rays, those lanes shade and start their next
+ * ray while the others keep traversing.  32 waits for the whole warp (one
+ * warp-wide traversal per path step).  Images do not depend on it. */
+#define LG_REFILL_DEFAULT 16
+int lg_renderer_set_refill_threshold(lg_renderer* r, int threshold);
+int lg_renderer_get_refill_threshold(const lg_renderer* r);
 /* Diffuse texture of one material (load_texture_to_device + sample_albedo,
  * src/pathtracer.cu:553-579, 274-282): w x h RGBA8 host pixels, sampled as
  * sRGB with bilinear filtering and wrapping at uv (u, 1 - v).  rgba8 = NULL

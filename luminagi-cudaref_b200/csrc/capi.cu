@@ -113,6 +113,7 @@ struct lg_renderer
     DevBuf rnodes, rt_scratch;            // render tree (depth order) and its build scratch
     bool watertight = false;  // ray/triangle test: Moller-Trumbore (the reference's) or watertight
     int trace_blocks_per_sm = 0;  // persistent trace grid (0 = occupancy maximum); see lg_renderer_autotune
+    int trace_refill = LG_REFILL_DEFAULT;  // finished rays per warp that trigger the path logic (1..32)
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
@@ -242,7 +243,7 @@ int build_records(lg_renderer* r)
 int finish_scene(lg_renderer* r)
 {
     if (r->n_nodes == 0) { r->root = 0; return LG_OK; }
-    LG_TRY(r->tv.reserve((size_t)r->n_tris * 3 * sizeof(float4)));
+    LG_TRY(r->tv.reserve((size_t)r->n_tris * kTriVec * sizeof(float4)));
     LG_TRY(build_records(r));
     LG_TRY_CUDA(cudaMemcpyAsync(&r->root_node, r->nodes.p, sizeof(lg_bvh_node), cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(prepare_triangles(r->tris.as<lg_triangle>(), r->n_tris, r->tv.as<float4>(), r->watertight, r->stream));
@@ -309,6 +310,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.work64 = r->work.as<unsigned long long>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
         job.blocks_per_sm = r->trace_blocks_per_sm;
+        job.refill_threshold = r->trace_refill;
         LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->watertight,
                                  r->stream));
     }
@@ -845,6 +847,20 @@ int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_
     return LG_OK;
 }
 
+int lg_renderer_set_refill_threshold(lg_renderer* r, int threshold)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (threshold < 1 || threshold > 32) return set_error(LG_ERR_INVALID, "refill threshold must be 1..32");
+    r->trace_refill = threshold;
+    return LG_OK;
+}
+
+int lg_renderer_get_refill_threshold(const lg_renderer* r)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    return r->trace_refill;
+}
+
 int lg_renderer_set_render_tree(lg_renderer* r, int mode)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
@@ -982,6 +998,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
     for (const void* p : deps) key.push_back((long long)(uintptr_t)p);
     key.push_back(r->bvh_width * 2 + (r->watertight ? 1 : 0));
     key.push_back(r->trace_blocks_per_sm);
+    key.push_back(r->trace_refill);
     key.push_back(r->scene_gen);
     if (key != r->batch_key || !r->batch_exec)
     {
@@ -1001,6 +1018,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
             job.n_jobs = n_jobs;
             job.total_items = items;
             job.blocks_per_sm = r->trace_blocks_per_sm;
+            job.refill_threshold = r->trace_refill;
             e = launch_trace_batch(dev_scene(r), job, r->sm_count, r->bvh_width, r->watertight, st);
         }
         for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)

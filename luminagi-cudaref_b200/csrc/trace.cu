@@ -6,24 +6,32 @@
 // Trumbore with |det| < 1e-6 culling (:82-107), slab test (:61-80), Lambert +
 // next-event estimation to the sun and point lights with a shadow ray even
 // at zero sun intensity (:230-272), Russian roulette from bounce 1 and
-// cosine-weighted bounces (:295-331).  Every FP32 expression keeps the
-// reference's operand order, so the compiler sees the same expressions.
+// cosine-weighted bounces (:295-331).  Every FP32 expression of the camera,
+// the triangle test and the shading keeps the reference's operand order, so
+// the compiler sees the same expressions.
 //
 // What is different (none of it changes which triangle a ray hits, except for
-// exact ties in t):
-//   * BVH records hold both children's boxes (WideNode), so one 64-byte fetch
-//     tests two boxes and traversal descends into the nearer child first and
-//     stacks the farther one; the reference pops children in fixed order and
-//     tests each box after a separate 40-byte fetch.
-//   * Triangle records for intersection are v0, e1, e2 as three float4
+// exact ties in t and rays within about an ulp of a box face):
+//   * BVH records hold up to four children's boxes (Wide4Node, 128 bytes),
+//     built from a render tree over the reference BVH's leaves; traversal
+//     enters the nearest hit child and stacks the others nearest-on-top; the
+//     reference pops children in fixed order and tests each box after a
+//     separate 40-byte fetch.  The 4-wide box test picks each axis's near and
+//     far planes by the sign of 1/d and evaluates them with fused
+//     multiply-adds (box4).  The 2-wide records (WideNode) keep the
+//     reference's slab arithmetic.
+//   * Triangle records for intersection are v0, e1, e2 as float4s
 //     (e1 = v1 - v0 is the same IEEE subtraction the reference does per test);
 //     normals are read from the 100-byte record only at the closest hit.
-//   * The path is a per-lane state machine around ONE traversal loop shared by
+//   * The path is a per-lane state machine around ONE traversal shared by
 //     camera, bounce and shadow rays; persistent warps refill idle lanes with
-//     (pixel, chunk of 8 samples) items from an atomic counter, so every loop
-//     iteration is a warp-wide traversal.  Chunk sums are added to the FP32
-//     accumulator atomically: the order of chunk additions (not their values)
-//     can differ from the reference's launch-per-chunk order.
+//     (pixel, chunk of 8 samples) items from an atomic counter.  The warp
+//     steps its lanes' traversals one record or leaf at a time, postpones
+//     leaves until every lane holds one, and lets lanes whose rays finished
+//     shade and start their next ray once enough of them have.  Chunk sums
+//     are added to the FP32 accumulator atomically: the order of chunk
+//     additions (not their values) can differ from the reference's
+//     launch-per-chunk order.
 #include <cstdint>
 
 #include <cuda_runtime.h>
@@ -248,8 +256,10 @@ __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const
     if (i >= n || !is4[i]) return;
     float lo[3][4], hi[3][4];
     int ln[4];
+    // An absent child gets the empty box [+inf, -inf], which box4 never hits.
+    const float inf = __int_as_float(0x7f800000);
     for (int a = 0; a < 3; ++a)
-        for (int k = 0; k < 4; ++k) { lo[a][k] = 1.0f; hi[a][k] = 0.0f; }
+        for (int k = 0; k < 4; ++k) { lo[a][k] = inf; hi[a][k] = -inf; }
     for (int k = 0; k < 4; ++k) ln[k] = kEmptyLink;
     int k = 0;
     for (int j = 0; j < 4; ++j)
@@ -276,17 +286,18 @@ __global__ void tri_prep_kernel(const lg_triangle* __restrict__ tris, int n, flo
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const lg_triangle t = tris[i];
-    tv[3 * i + 0] = make_float4(t.v[0][0], t.v[0][1], t.v[0][2], __int_as_float(t.material));
+    tv[kTriVec * i + 0] = make_float4(t.v[0][0], t.v[0][1], t.v[0][2], __int_as_float(t.material));
+    if (kTriVec > 3) tv[kTriVec * i + 3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (watertight)
     {
         // the watertight test needs the shared vertices themselves, not edges
-        tv[3 * i + 1] = make_float4(t.v[1][0], t.v[1][1], t.v[1][2], 0.0f);
-        tv[3 * i + 2] = make_float4(t.v[2][0], t.v[2][1], t.v[2][2], 0.0f);
+        tv[kTriVec * i + 1] = make_float4(t.v[1][0], t.v[1][1], t.v[1][2], 0.0f);
+        tv[kTriVec * i + 2] = make_float4(t.v[2][0], t.v[2][1], t.v[2][2], 0.0f);
         return;
     }
-    tv[3 * i + 1] = make_float4(__fsub_rn(t.v[1][0], t.v[0][0]), __fsub_rn(t.v[1][1], t.v[0][1]),
+    tv[kTriVec * i + 1] = make_float4(__fsub_rn(t.v[1][0], t.v[0][0]), __fsub_rn(t.v[1][1], t.v[0][1]),
                                 __fsub_rn(t.v[1][2], t.v[0][2]), 0.0f);
-    tv[3 * i + 2] = make_float4(__fsub_rn(t.v[2][0], t.v[0][0]), __fsub_rn(t.v[2][1], t.v[0][1]),
+    tv[kTriVec * i + 2] = make_float4(__fsub_rn(t.v[2][0], t.v[0][0]), __fsub_rn(t.v[2][1], t.v[0][1]),
                                 __fsub_rn(t.v[2][2], t.v[0][2]), 0.0f);
 }
 
@@ -313,14 +324,41 @@ __device__ __forceinline__ bool slab(const Ray& r, float mnx, float mxx, float m
     return true;
 }
 
+// 256-bit read-only load (sm_100): eight floats from a 32-byte aligned
+// address in one request, where two 128-bit loads would take two.
+__device__ __forceinline__ void ldg8(const void* p, float (&v)[8])
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "l"(p));
+}
+
+// The three float4s of triangle ti's intersection record.
+__device__ __forceinline__ void load_tri(const float4* __restrict__ tv, int ti, float4& a, float4& b, float4& c)
+{
+    const float4* p = tv + (size_t)kTriVec * ti;
+    if (kTriVec == 4)
+    {
+        float v[8];
+        ldg8(p, v);
+        a = make_float4(v[0], v[1], v[2], v[3]);
+        b = make_float4(v[4], v[5], v[6], v[7]);
+    }
+    else
+    {
+        a = __ldg(p);
+        b = __ldg(p + 1);
+    }
+    c = __ldg(p + 2);
+}
+
 // Moller-Trumbore (pathtracer.cu:82-107) on a precomputed (v0, e1, e2).
 __device__ __forceinline__ bool tri_hit(const Ray& r, const float4* __restrict__ tv, int ti, float tmax, float& outT,
                                         float& outU, float& outV)
 {
     constexpr float kEps = 1e-6f;
-    const float4 a = __ldg(&tv[3 * ti + 0]);
-    const float4 b = __ldg(&tv[3 * ti + 1]);
-    const float4 c = __ldg(&tv[3 * ti + 2]);
+    float4 a, b, c;
+    load_tri(tv, ti, a, b, c);
     const vec3 v0 = v3(a.x, a.y, a.z);
     const vec3 e1 = v3(b.x, b.y, b.z);
     const vec3 e2 = v3(c.x, c.y, c.z);
@@ -365,9 +403,8 @@ __device__ __forceinline__ bool tri_hit_wt(const Ray& r, const float4* __restric
     if (dz < 0.0f) { const int t = kx; kx = ky; ky = t; }
     const float Sz = __frcp_rn(dz);
     const float Sx = __fmul_rn(comp(r.d, kx), Sz), Sy = __fmul_rn(comp(r.d, ky), Sz);
-    const float4 a4 = __ldg(&tv[3 * ti + 0]);
-    const float4 b4 = __ldg(&tv[3 * ti + 1]);
-    const float4 c4 = __ldg(&tv[3 * ti + 2]);
+    float4 a4, b4, c4;
+    load_tri(tv, ti, a4, b4, c4);
     const vec3 A = v3(__fsub_rn(a4.x, r.o.x), __fsub_rn(a4.y, r.o.y), __fsub_rn(a4.z, r.o.z));
     const vec3 B = v3(__fsub_rn(b4.x, r.o.x), __fsub_rn(b4.y, r.o.y), __fsub_rn(b4.z, r.o.z));
     const vec3 C = v3(__fsub_rn(c4.x, r.o.x), __fsub_rn(c4.y, r.o.y), __fsub_rn(c4.z, r.o.z));
@@ -418,169 +455,229 @@ __device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
     }
 }
 
-// The 4-wide form of the traversal below: one 128-byte record tests up to
-// four child boxes (same slab arithmetic); hit children are ordered by entry
-// distance, the nearest is entered and the rest stacked nearest-on-top.
-// Measured alternatives on the 64-spp engine frame (633 ms with this form and
-// records from the even-depth collapse; 596 ms with the surface-area collapse):
-// a "while-while" loop (internal records until a leaf, then the warp's leaves
-// together) ran 745 ms, and a 24-entry shared-memory stack 675 ms (its 96 KB
-// per SM comes out of the L1 that caches the BVH records).
-template <bool kCount, bool kWT>
-__device__ __forceinline__ int traverse4(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
-                                         float& bestU, float& bestV, Counters& cnt)
+// Traversal state of one ray: the record or leaf link to visit next (kDone
+// once the stack is empty), a leaf postponed for testing (0 = none; leaf
+// links are negative), the stack depth, and the closest hit so far (t starts
+// at the ray's tmax).
+constexpr int kDone = kEmptyLink;  // also the link of an absent child
+struct Trav
 {
-    int stack[kStack];
-    int sp = 0;
-    int cur = s.root4;
-    int bestTri = -1;
-    bestT = tmax;
-    bestU = 0.0f;
-    bestV = 0.0f;
+    int cur, pend, sp, tri;
+    float t, u, v;
+};
+
+template <bool kCount>
+__device__ __forceinline__ void trav_begin(Trav& q, int root, float tmax, bool anyhit, Counters& cnt)
+{
+    q.cur = root;
+    q.pend = 0;
+    q.sp = 0;
+    q.tri = -1;
+    q.t = tmax;
+    q.u = 0.0f;
+    q.v = 0.0f;
     if (kCount) { if (anyhit) cnt.shadow++; else cnt.closest++; }
-    for (;;)
-    {
-        if (cur >= 0)
-        {
-            if (kCount) cnt.nodes++;
-            const Wide4Node* nd = &s.nodes4[cur];
-            const float4 lx = __ldg(&nd->lox), hx = __ldg(&nd->hix);
-            const float4 ly = __ldg(&nd->loy), hy = __ldg(&nd->hiy);
-            const float4 lz = __ldg(&nd->loz), hz = __ldg(&nd->hiz);
-            const int4 ln = __ldg(&nd->link);
-            const float inf = __int_as_float(0x7f800000);
-            float t0 = inf, t1 = inf, t2 = inf, t3 = inf;
-            float te;
-            if (ln.x != kEmptyLink && slab(r, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, bestT, te)) t0 = te;
-            if (ln.y != kEmptyLink && slab(r, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, bestT, te)) t1 = te;
-            if (ln.z != kEmptyLink && slab(r, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, bestT, te)) t2 = te;
-            if (ln.w != kEmptyLink && slab(r, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, bestT, te)) t3 = te;
-            int l0 = ln.x, l1 = ln.y, l2 = ln.z, l3 = ln.w;
-            cswap(t0, l0, t1, l1);
-            cswap(t2, l2, t3, l3);
-            cswap(t0, l0, t2, l2);
-            cswap(t1, l1, t3, l3);
-            cswap(t1, l1, t2, l2);
-            if (t0 != inf)
-            {
-                // push farthest first so the nearest remaining is on top
-                if (t3 != inf) { if (sp < kStack) stack[sp++] = l3; else if (kCount) cnt.overflow++; }
-                if (t2 != inf) { if (sp < kStack) stack[sp++] = l2; else if (kCount) cnt.overflow++; }
-                if (t1 != inf) { if (sp < kStack) stack[sp++] = l1; else if (kCount) cnt.overflow++; }
-                cur = l0;
-                continue;
-            }
-        }
-        else
-        {
-            int2 lf;
-            if (s.leaf_inline)
-            {
-                const int v = ~cur;
-                lf = make_int2(v >> 4, v & 15);
-                if (lf.y == 0)
-                {
-                    lf = __ldg(&s.leaves[lf.x]);
-                    if (kCount) { cnt.leaves++; }
-                }
-            }
-            else
-            {
-                lf = __ldg(&s.leaves[~cur]);
-                if (kCount) { cnt.leaves++; }
-            }
-            bool done = false;
-            for (int i = 0; i < lf.y; ++i)
-            {
-                const int ti = lf.x + i;
-                float tt, uu, vv;
-                if (kCount) cnt.tris++;
-                if (tri_test<kWT>(r, s.tv, ti, bestT, tt, uu, vv))
-                {
-                    bestT = tt;
-                    bestTri = ti;
-                    bestU = uu;
-                    bestV = vv;
-                    if (anyhit) { done = true; break; }
-                }
-            }
-            if (done) break;
-        }
-        if (sp == 0) break;
-        cur = stack[--sp];
-    }
-    return bestTri;
 }
 
-// One traversal loop serves closest-hit rays (traverse_closest, :109-160)
-// and shadow rays (traverse_occluded, :162-191): the nearer child is taken
-// first and the farther one stacked; a shadow ray stops at its first hit.
-// Keeping a single copy of this loop in the kernel lets lanes tracing
-// different kinds of rays execute it together and keeps the code small.
-// Returns the hit triangle or -1; bestT/U/V as in traverse_closest.
-template <bool kCount, bool kWT>
-__device__ __forceinline__ int traverse(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
-                                        float& bestU, float& bestV, Counters& cnt)
+__device__ __forceinline__ int pop(Trav& q, const int* stack) { return q.sp == 0 ? kDone : stack[--q.sp]; }
+
+// The four boxes of a 4-wide record against one ray.  Per axis the near
+// plane is the min plane when 1/d >= 0 and the max plane otherwise, so each
+// slab needs two fused multiply-adds, t = plane * (1/d) - o * (1/d), and no
+// min/max of the two; the near and far planes are fetched straight from the
+// record by the signs of 1/d.  The hit rule and the entry distance are the
+// reference's (pathtracer.cu:61-80): hit unless hi < max(lo, 0) or lo > tmax,
+// entry max(lo, 0) (tested as max(lo, 0) > tmax, the same for tmax >= 0; a
+// shadow ray with tmax < 0 can hit no triangle either way).  The rounding is
+// not the reference's (plane - o) * (1/d): a box boundary moves by about one
+// ulp of the ray origin, which changes which records are opened only for
+// rays passing within that distance of a box face.  Empty slots hold
+// [+inf, -inf] and always miss.  Children that miss get t = +inf.
+__device__ __forceinline__ int4 box4(const Wide4Node* nd, const Ray& r, float tmax, float& t0, float& t1, float& t2,
+                                     float& t3)
+{
+    const char* b = reinterpret_cast<const char*>(nd);
+    const int sx = (__float_as_int(r.inv_d.x) >> 31) & 16;
+    const int sy = (__float_as_int(r.inv_d.y) >> 31) & 16;
+    const int sz = (__float_as_int(r.inv_d.z) >> 31) & 16;
+    const float4 nx = __ldg(reinterpret_cast<const float4*>(b + 0 + sx));
+    const float4 fx = __ldg(reinterpret_cast<const float4*>(b + 16 - sx));
+    const float4 ny = __ldg(reinterpret_cast<const float4*>(b + 32 + sy));
+    const float4 fy = __ldg(reinterpret_cast<const float4*>(b + 48 - sy));
+    const float4 nz = __ldg(reinterpret_cast<const float4*>(b + 64 + sz));
+    const float4 fz = __ldg(reinterpret_cast<const float4*>(b + 80 - sz));
+    const int4 ln = __ldg(&nd->link);
+    const float ox = -(r.o.x * r.inv_d.x), oy = -(r.o.y * r.inv_d.y), oz = -(r.o.z * r.inv_d.z);
+    const float inf = __int_as_float(0x7f800000);
+    auto one = [&](float ax, float bx, float ay, float by, float az, float bz) {
+        const float l0 = fmaxf(fmaxf(fmaf(ax, r.inv_d.x, ox), fmaf(ay, r.inv_d.y, oy)), fmaxf(fmaf(az, r.inv_d.z, oz), 0.0f));
+        const float hi = fminf(fminf(fmaf(bx, r.inv_d.x, ox), fmaf(by, r.inv_d.y, oy)), fmaf(bz, r.inv_d.z, oz));
+        return (hi < l0 || l0 > tmax) ? inf : l0;
+    };
+    t0 = one(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x);
+    t1 = one(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y);
+    t2 = one(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z);
+    t3 = one(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w);
+    return ln;
+}
+
+// Visits record q.cur (>= 0).  4-wide: up to four child boxes; the hit
+// children are ordered by entry distance, the nearest becomes q.cur and the
+// rest are stacked nearest-on-top.  2-wide (traverse_closest, :109-160, for
+// one record): both children's boxes with the reference's slab arithmetic,
+// the nearer hit child first and the farther one stacked.  With no child hit
+// the next entry is popped (kDone when the stack is empty).
+// Measured alternatives on the 64-spp engine frame (633 ms with whole-ray
+// traversal and records from the even-depth collapse): a "while-while" loop
+// without speculation (internal records until every lane holds a leaf, then
+// the leaves) ran 745 ms, and a 24-entry shared-memory stack 675 ms (its
+// 96 KB per SM comes out of the L1 that caches the BVH records).
+template <int kWidth, bool kCount>
+__device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav& q, int* stack, Counters& cnt)
+{
+    if (kCount) cnt.nodes++;
+    const float inf = __int_as_float(0x7f800000);
+    if (kWidth == 4)
+    {
+        float t0, t1, t2, t3;
+        const int4 ln = box4(&s.nodes4[q.cur], r, q.t, t0, t1, t2, t3);
+        int l0 = ln.x, l1 = ln.y, l2 = ln.z, l3 = ln.w;
+        cswap(t0, l0, t1, l1);
+        cswap(t2, l2, t3, l3);
+        cswap(t0, l0, t2, l2);
+        cswap(t1, l1, t3, l3);
+        cswap(t1, l1, t2, l2);
+        if (t0 != inf)
+        {
+            // push farthest first so the nearest remaining is on top
+            if (t3 != inf) { if (q.sp < kStack) stack[q.sp++] = l3; else if (kCount) cnt.overflow++; }
+            if (t2 != inf) { if (q.sp < kStack) stack[q.sp++] = l2; else if (kCount) cnt.overflow++; }
+            if (t1 != inf) { if (q.sp < kStack) stack[q.sp++] = l1; else if (kCount) cnt.overflow++; }
+            q.cur = l0;
+            return;
+        }
+    }
+    else
+    {
+        const float4 xy0 = __ldg(&s.nodes[q.cur].xy0);
+        const float4 xy1 = __ldg(&s.nodes[q.cur].xy1);
+        const float4 z01 = __ldg(&s.nodes[q.cur].z01);
+        const int4 ln = __ldg(&s.nodes[q.cur].link);
+        float t0, t1;
+        const bool h0 = slab(r, xy0.x, xy0.y, xy0.z, xy0.w, z01.x, z01.y, q.t, t0);
+        const bool h1 = slab(r, xy1.x, xy1.y, xy1.z, xy1.w, z01.z, z01.w, q.t, t1);
+        if (h0 && h1)
+        {
+            const bool swap = t1 < t0;
+            if (q.sp < kStack) stack[q.sp++] = swap ? ln.x : ln.y;
+            else if (kCount) cnt.overflow++;
+            q.cur = swap ? ln.y : ln.x;
+            return;
+        }
+        if (h0 || h1)
+        {
+            q.cur = h0 ? ln.x : ln.y;
+            return;
+        }
+    }
+    q.cur = pop(q, stack);
+}
+
+// Tests every triangle of leaf `link` in order (strict < on t, as
+// traverse_closest's leaf loop).  4-wide leaf links carry (first, count) for
+// 1..15 triangles; larger leaves and 2-wide links index the leaf table.
+// Returns true when a shadow ray found an occluder.
+template <int kWidth, bool kCount, bool kWT>
+__device__ __forceinline__ bool leaf_step(const DevScene& s, const Ray& r, bool anyhit, int link, Trav& q,
+                                          Counters& cnt)
+{
+    int2 lf;
+    if (kWidth == 4 && s.leaf_inline)
+    {
+        const int v = ~link;
+        lf = make_int2(v >> 4, v & 15);
+        if (lf.y == 0)
+        {
+            lf = __ldg(&s.leaves[lf.x]);
+            if (kCount) { cnt.leaves++; }
+        }
+    }
+    else
+    {
+        lf = __ldg(&s.leaves[~link]);
+        if (kCount) { cnt.leaves++; }
+    }
+    for (int i = 0; i < lf.y; ++i)
+    {
+        const int ti = lf.x + i;
+        float tt, uu, vv;
+        if (kCount) cnt.tris++;
+        if (tri_test<kWT>(r, s.tv, ti, q.t, tt, uu, vv))
+        {
+            q.t = tt;
+            q.tri = ti;
+            q.u = uu;
+            q.v = vv;
+            if (anyhit) return true;
+        }
+    }
+    return false;
+}
+
+// A whole traversal of one ray, one record or leaf at a time: the closest
+// hit (triangle or -1) and its t, u, v, as traverse_closest returns them; a
+// shadow ray stops at its first hit.
+template <int kWidth, bool kCount, bool kWT>
+__device__ __forceinline__ int traverse_ray(const DevScene& s, const Ray& r, float tmax, bool anyhit, float& bestT,
+                                            float& bestU, float& bestV, Counters& cnt)
 {
     int stack[kStack];
-    int sp = 0;
-    int cur = s.root;
-    int bestTri = -1;
-    bestT = tmax;
-    bestU = 0.0f;
-    bestV = 0.0f;
-    if (kCount) { if (anyhit) cnt.shadow++; else cnt.closest++; }
-    for (;;)
+    Trav q;
+    trav_begin<kCount>(q, kWidth == 4 ? s.root4 : s.root, tmax, anyhit, cnt);
+    while (q.cur != kDone)
     {
-        if (cur >= 0)
-        {
-            if (kCount) cnt.nodes++;
-            const float4 xy0 = __ldg(&s.nodes[cur].xy0);
-            const float4 xy1 = __ldg(&s.nodes[cur].xy1);
-            const float4 z01 = __ldg(&s.nodes[cur].z01);
-            const int4 ln = __ldg(&s.nodes[cur].link);
-            float t0, t1;
-            const bool h0 = slab(r, xy0.x, xy0.y, xy0.z, xy0.w, z01.x, z01.y, bestT, t0);
-            const bool h1 = slab(r, xy1.x, xy1.y, xy1.z, xy1.w, z01.z, z01.w, bestT, t1);
-            if (h0 && h1)
-            {
-                const bool swap = t1 < t0;
-                if (sp < kStack) stack[sp++] = swap ? ln.x : ln.y;
-                else if (kCount) cnt.overflow++;
-                cur = swap ? ln.y : ln.x;
-                continue;
-            }
-            if (h0 || h1)
-            {
-                cur = h0 ? ln.x : ln.y;
-                continue;
-            }
-        }
+        if (q.cur >= 0) node_step<kWidth, kCount>(s, r, q, stack, cnt);
         else
         {
-            const int2 lf = __ldg(&s.leaves[~cur]);
-            if (kCount) { cnt.leaves++; }
-            bool done = false;
-            for (int i = 0; i < lf.y; ++i)
-            {
-                const int ti = lf.x + i;
-                float tt, uu, vv;
-                if (kCount) cnt.tris++;
-                if (tri_test<kWT>(r, s.tv, ti, bestT, tt, uu, vv))
-                {
-                    bestT = tt;
-                    bestTri = ti;
-                    bestU = uu;
-                    bestV = vv;
-                    if (anyhit) { done = true; break; }
-                }
-            }
-            if (done) break;
+            if (leaf_step<kWidth, kCount, kWT>(s, r, anyhit, q.cur, q, cnt)) break;
+            q.cur = pop(q, stack);
         }
-        if (sp == 0) break;
-        cur = stack[--sp];
     }
-    return bestTri;
+    bestT = q.t;
+    bestU = q.u;
+    bestV = q.v;
+    return q.tri;
+}
+
+// One warp-wide step of the persistent kernel's traversals, with leaves
+// postponed (Aila and Laine, "Understanding the Efficiency of Ray Traversal
+// on GPUs", HPG 2009): a lane that reaches a leaf sets it aside and keeps
+// visiting records from its stack while other lanes still look for a leaf;
+// once every lane with a ray in flight holds a leaf, the warp tests them
+// together.  The records visited past a postponed leaf would be culled by a
+// nearer hit in it only for closest-hit rays, and then only cost time: the
+// closest hit is the same (up to exact ties in t).  `busy` is this lane's
+// ray in flight; returns true when its traversal has finished.
+template <int kWidth, bool kCount, bool kWT>
+__device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool anyhit, bool busy, Trav& q,
+                                          int* stack, Counters& cnt)
+{
+    if (busy && q.pend == 0 && q.cur < 0 && q.cur != kDone)
+    {
+        q.pend = q.cur;
+        q.cur = pop(q, stack);
+    }
+    const bool fin = busy && q.pend == 0 && q.cur == kDone;
+    // every lane takes part in the vote, finished or idle ones included
+    if (__any_sync(0xffffffffu, busy && !fin && q.pend == 0))
+    {
+        if (busy && q.cur >= 0) node_step<kWidth, kCount>(s, r, q, stack, cnt);
+        return fin;
+    }
+    if (!busy || fin) return fin;
+    const int link = q.pend;
+    q.pend = 0;
+    return leaf_step<kWidth, kCount, kWT>(s, r, anyhit, link, q, cnt) || q.cur == kDone;
 }
 
 // xorshift32 / randf (pathtracer.cu:193-204).
@@ -749,7 +846,7 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
             if (dot(N, st.ray.d) > 0.0f) N = vmul(N, -1.0f);
             st.N = N;
             st.P = vadd(st.ray.o, vmul(st.ray.d, hitT));
-            const int mat = __float_as_int(__ldg(&s.tv[3 * tri].w));
+            const int mat = __float_as_int(__ldg(&s.tv[kTriVec * tri].w));
             st.albedo = hit_albedo(s, t, mat, w, hitU, hitV);
             st.color = v3(0, 0, 0);
         }
@@ -810,7 +907,11 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         kBatch ? job.total_items : (unsigned long long)job.n_tiles * job.n_chunks * 32ull;
     Counters cnt{0, 0, 0, 0, 0, 0};
     PathState st;
-    bool active = false, exhausted = false;
+    Trav q;
+    int stack[kStack];
+    const int root = kWidth == 4 ? s.root4 : s.root;
+    const int thresh = job.refill_threshold < 1 ? 1 : (job.refill_threshold > 32 ? 32 : job.refill_threshold);
+    bool active = false, exhausted = false, tdone = false;
     for (;;)
     {
         // Refill idle lanes with one atomic per warp.
@@ -856,19 +957,32 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
                         st.k = 0;
                         st.pixel = (unsigned)((st.py * c.width + st.px) * 3);
                         start_sample(st, c);
+                        trav_begin<kCount>(q, root, st.tmax, st.li >= 0, cnt);
+                        tdone = false;
                         active = true;
                     }
                 }
             }
         }
         if (!__any_sync(0xffffffffu, active)) break;
-        if (active)
+        // Lanes that stay idle for good (work exhausted) do not count towards
+        // the threshold; idle lanes that can still be refilled do.
+        const int idle_final = exhausted ? __popc(__ballot_sync(0xffffffffu, !active)) : 0;
+        for (;;)
         {
-            float hitT, hitU, hitV;
-            const int tri = kWidth == 4 ? traverse4<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt)
-                                        : traverse<kCount, kWT>(s, st.ray, st.tmax, st.li >= 0, hitT, hitU, hitV, cnt);
+            if (warp_step<kWidth, kCount, kWT>(s, st.ray, st.li >= 0, active && !tdone, q, stack, cnt)) tdone = true;
+            const unsigned busy = __ballot_sync(0xffffffffu, active && !tdone);
+            if (busy == 0 || 32 - __popc(busy) - idle_final >= thresh) break;
+        }
+        if (active && tdone)
+        {
             const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
-            if (!advance(st, s, c, kBatch ? st.max_bounces : job.max_bounces, tri, hitT, hitU, hitV))
+            if (advance(st, s, c, kBatch ? st.max_bounces : job.max_bounces, q.tri, q.t, q.u, q.v))
+            {
+                trav_begin<kCount>(q, root, st.tmax, st.li >= 0, cnt);
+                tdone = false;
+            }
+            else
             {
                 active = false;
                 const unsigned i = st.pixel;
@@ -937,8 +1051,7 @@ __global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExt
     Ray r = primary_ray(cam, px, py, 0.5f, 0.5f);
     float hitT, hitU, hitV;
     Counters cnt{0, 0, 0, 0, 0, 0};
-    const int tri = kWidth == 4 ? traverse4<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt)
-                                : traverse<false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt);
+    const int tri = traverse_ray<kWidth, false, kWT>(s, r, 1e30f, false, hitT, hitU, hitV, cnt);
     const size_t i = ((size_t)py * cam.width + px) * 3;
     if (tri < 0)
     {
@@ -955,7 +1068,7 @@ __global__ void gbuffer_kernel(DevScene s, DevCam cam, vec3 bbMin, vec3 bbInvExt
                           w * t.n[0][1] + hitU * t.n[1][1] + hitV * t.n[2][1],
                           w * t.n[0][2] + hitU * t.n[1][2] + hitV * t.n[2][2]));
     if (dot(N, r.d) > 0.0f) N = vmul(N, -1.0f);
-    const int mat = __float_as_int(__ldg(&s.tv[3 * tri].w));
+    const int mat = __float_as_int(__ldg(&s.tv[kTriVec * tri].w));
     const vec3 a = hit_albedo(s, t, mat, w, hitU, hitV);
     albedo_out[i + 0] = enc8(a.x);
     albedo_out[i + 1] = enc8(a.y);

@@ -24,7 +24,9 @@ static_assert(sizeof(WideNode) == 64, "WideNode is one 64-byte record");
 
 // A 4-wide node collapsed from two levels of the binary BVH: the boxes of up
 // to four children, struct-of-arrays in one 128-byte line (eight 16-byte
-// loads).  Links as in WideNode; kEmptyLink marks an absent child.
+// loads).  Links as in WideNode; an absent child has the empty box
+// [+inf, -inf] and the link kEmptyLink, which traversal treats as the end of
+// the ray's traversal, so even a box test that let it through reads nothing.
 struct alignas(16) Wide4Node
 {
     float4 lox, hix, loy, hiy, loz, hiz;  // child i in component i
@@ -32,7 +34,12 @@ struct alignas(16) Wide4Node
     int4 pad;
 };
 static_assert(sizeof(Wide4Node) == 128, "Wide4Node is one 128-byte line");
-constexpr int kEmptyLink = 0x7fffffff;
+constexpr int kEmptyLink = (int)0x80000000;
+
+// Intersection record of one triangle: kTriVec float4s, v0 (w = material
+// bits), e1 = v1 - v0, e2 = v2 - v0 (v0, v1, v2 in watertight mode), then
+// padding, so a record starts on a 32-byte boundary when kTriVec == 4.
+constexpr int kTriVec = 4;
 
 struct DevScene
 {
@@ -41,7 +48,7 @@ struct DevScene
     int leaf_inline;           // 4-wide leaf links carry (first, count); see wide4_kernel
     const WideNode* nodes;
     const int2* leaves;        // (first triangle, count)
-    const float4* tv;          // 3 per triangle: v0 (w = material bits), e1 = v1-v0, e2 = v2-v0
+    const float4* tv;          // kTriVec per triangle: v0 (w = material bits), e1 = v1-v0, e2 = v2-v0
     const lg_triangle* tris;   // shading data (normals), BVH order
     const float4* mats;        // albedo
     const unsigned long long* texs;  // per material: diffuse texture object or 0; nullptr when none is set
@@ -88,6 +95,7 @@ struct TraceJob
     double* accum64;       // optional
     unsigned long long* work64;  // work counter (zeroed by the launcher)
     int blocks_per_sm;     // persistent grid: resident blocks per SM (0 = as many as fit)
+    int refill_threshold;  // finished rays in a warp that trigger the path logic, 1..32
     RenderCounters* counters;  // optional
     // batched launch (launch_trace_batch): every field above except work64 is taken from jobs[]
     const BatchJob* jobs;

@@ -60,10 +60,19 @@ def trace(a):
     c = r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)
     r.set_counting(False)
     rays = c["closest_rays"] + c["shadow_rays"]
-    ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for _ in range(a.reps)]
-    return {"kernel": "trace", "spp": a.spp, "width": a.width, "ms": ms, "rays": rays,
-            "mrays_per_s": rays / min(ms) / 1e3, "nodes_per_ray": c["node_fetches"] / rays,
-            "tris_per_ray": c["tri_tests"] / rays}
+    out = {"kernel": "trace", "spp": a.spp, "width": a.width, "rays": rays,
+           "nodes_per_ray": c["node_fetches"] / rays, "tris_per_ray": c["tri_tests"] / rays}
+    sweep = {}
+    for th in (int(x) for x in str(a.refill).split(",")):
+        r.set_refill_threshold(th)
+        ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for _ in range(a.reps)]
+        sweep[th] = {"ms": ms, "mrays_per_s": rays / min(ms) / 1e3}
+    if len(sweep) == 1:
+        (th, v), = sweep.items()
+        out.update(refill=th, **v)
+    else:
+        out["refill"] = sweep
+    return out
 
 
 def bvh(a):
@@ -146,6 +155,7 @@ def main(argv=None):
     ap.add_argument("--bounces", type=int, default=2)
     ap.add_argument("--width", type=int, default=4)
     ap.add_argument("--reps", type=int, default=10)
+    ap.add_argument("--refill", default="16", help="trace: refill threshold(s), comma-separated")
     a = ap.parse_args(argv)
     print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch}[a.what](a)))
 

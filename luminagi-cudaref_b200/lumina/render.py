@@ -110,6 +110,13 @@ class Renderer:
         check(lib().lg_renderer_autotune(self._h, C.byref(cam), spp, bounces, C.byref(b), C.byref(ms)))
         return int(b.value), float(ms.value)
 
+    def set_refill_threshold(self, threshold: int) -> None:
+        """Finished rays per warp (1..32) after which those lanes shade and start their next ray."""
+        check(lib().lg_renderer_set_refill_threshold(self._h, int(threshold)))
+
+    def refill_threshold(self) -> int:
+        return int(lib().lg_renderer_get_refill_threshold(self._h))
+
     def set_render_tree(self, mode: str) -> None:
         """Topology of the traversal records: 'ploc' (default) or 'buildbvh' (same leaves either way)."""
         check(lib().lg_renderer_set_render_tree(self._h, {"buildbvh": 0, "ploc": 1}[mode]))
