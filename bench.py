@@ -46,9 +46,9 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 612.1 MB + 138.3 MB / 65,366,791 rays
+# of an 8-spp engine frame: 1,122.1 MB + 187.5 MB / 65,366,791 rays
 # (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = 750.441984e6 / 65366791
+TRACE_DRAM_BYTES_PER_RAY = 1309.551250e6 / 65366791
 # Bytes one traversal step reads from a BVH record: 4-wide, six planes of
 # four boxes (96 B) and four links (16 B); 2-wide, the whole 64-B record.
 RECORD_BYTES = {4: 112, 2: 64}

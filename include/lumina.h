@@ -163,18 +163,22 @@ int lg_renderer_set_counting(lg_renderer* r, int enable);
 /* Traversal records: 4 (default; up to four descendants per 128-byte record) or 2
  * (one binary node per 64-byte record).  Both traverse the same BVH. */
 int lg_renderer_set_bvh_width(lg_renderer* r, int width);
-/* Topology of the tree the traversal records are built from.  Both use the
- * leaves (triangle ranges and boxes) of the scene's BuildBVH tree, which
- * lg_renderer_get_bvh still returns unchanged; any binary tree over those
- * leaves gives the same closest hits (up to exact ties in t).
+/* The tree the traversal records are built from.  lg_renderer_get_bvh still
+ * returns the scene's BuildBVH tree unchanged, and every mode reports hits
+ * by BuildBVH's triangle order; any BVH over the same triangles gives the
+ * same closest hits (up to exact ties in t).
  * LG_RENDER_TREE_BUILDBVH keeps BuildBVH's Morton-split topology.
- * LG_RENDER_TREE_PLOC (default) regroups the leaves by PLOC (Meister and
- * Bittner, HPG 2018): agglomerative clustering by union surface area, on the
- * GPU, which makes traversal open fewer boxes.  A tree PLOC cannot regroup
- * (leaves sharing a first triangle) keeps its own topology; get_render_tree
- * reports the mode in use. */
+ * LG_RENDER_TREE_PLOC regroups BuildBVH's leaves (triangle ranges) by PLOC
+ * (Meister and Bittner, HPG 2018): agglomerative clustering by union surface
+ * area, on the GPU, which makes traversal open fewer boxes.  A tree PLOC
+ * cannot regroup (leaves sharing a first triangle) keeps its own topology.
+ * LG_RENDER_TREE_PLOC_TRIANGLES (default) clusters the triangles themselves
+ * by PLOC, one triangle per leaf (2T - 1 nodes): tighter leaves, 2.5x fewer
+ * triangle tests per ray.
+ * get_render_tree reports the mode in use. */
 #define LG_RENDER_TREE_BUILDBVH 0
 #define LG_RENDER_TREE_PLOC 1
+#define LG_RENDER_TREE_PLOC_TRIANGLES 2
 int lg_renderer_set_render_tree(lg_renderer* r, int mode);
 int lg_renderer_get_render_tree(lg_renderer* r, int32_t* mode_used);
 /* Ray/triangle test.  LG_ISECT_MOLLER_TRUMBORE (default) is the reference's
@@ -198,6 +202,13 @@ int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_
 #define LG_REFILL_DEFAULT 16
 int lg_renderer_set_refill_threshold(lg_renderer* r, int threshold);
 int lg_renderer_get_refill_threshold(const lg_renderer* r);
+/* Leaf postponement of the persistent trace launch.  A lane that reaches a
+ * BVH leaf holds it and keeps visiting records; the warp tests the held
+ * leaves together once at most `quorum` of its lanes are still looking for
+ * one (0 = all lanes hold a leaf or are done).  Images do not depend on it. */
+#define LG_LEAF_QUORUM_DEFAULT 8
+int lg_renderer_set_leaf_quorum(lg_renderer* r, int quorum);
+int lg_renderer_get_leaf_quorum(const lg_renderer* r);
 /* Diffuse texture of one material (load_texture_to_device + sample_albedo,
  * src/pathtracer.cu:553-579, 274-282): w x h RGBA8 host pixels, sampled as
  * sRGB with bilinear filtering and wrapping at uv (u, 1 - v).  rgba8 = NULL

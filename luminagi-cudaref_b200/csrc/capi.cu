@@ -108,12 +108,13 @@ struct lg_renderer
     int n_tris = 0, n_nodes = 0, n_mats = 0, n_points = 0, root = 0, root4 = 0;
     int bvh_width = 4;  // traversal records: 4-wide (default) or the 2-wide form
     int leaf_inline = 0;  // 4-wide leaf links carry (first, count)
-    int tree_mode = LG_RENDER_TREE_PLOC;  // topology the traversal records are built from
+    int tree_mode = LG_RENDER_TREE_PLOC_TRIANGLES;  // tree the traversal records are built from
     int tree_used = -1;                   // the mode actually built (PLOC falls back to the BuildBVH tree)
     DevBuf rnodes, rt_scratch;            // render tree (depth order) and its build scratch
     bool watertight = false;  // ray/triangle test: Moller-Trumbore (the reference's) or watertight
     int trace_blocks_per_sm = 0;  // persistent trace grid (0 = occupancy maximum); see lg_renderer_autotune
     int trace_refill = LG_REFILL_DEFAULT;  // finished rays per warp that trigger the path logic (1..32)
+    int trace_quorum = LG_LEAF_QUORUM_DEFAULT;  // searching lanes below which a warp tests its held leaves (0..31)
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
@@ -201,26 +202,30 @@ int upload_common(lg_renderer* r, const lg_scene_desc* d)
     return LG_OK;
 }
 
-// Traversal records (2- and 4-wide) from the render tree: the BuildBVH tree's
-// leaves under the topology tree_mode selects (render_tree.cu).
+// Traversal records (2- and 4-wide) from the render tree tree_mode selects
+// (render_tree.cu): PLOC over the triangles, PLOC over the BuildBVH tree's
+// leaves, or that tree itself.
 int build_records(lg_renderer* r)
 {
-    const int n = r->n_nodes;
-    LG_TRY(r->wide.reserve((size_t)n * sizeof(WideNode)));
-    LG_TRY(r->leaves.reserve((size_t)n * sizeof(int2)));
-    LG_TRY(r->rnodes.reserve((size_t)n * sizeof(lg_bvh_node)));
-    LG_TRY(r->rt_scratch.reserve(render_tree_scratch_bytes(n, r->n_tris)));
-    int rc = build_render_tree(r->nodes.as<lg_bvh_node>(), n, r->n_tris, r->tree_mode, r->rnodes.as<lg_bvh_node>(),
-                               r->rt_scratch.p, r->rt_scratch.bytes, r->stream);
-    r->tree_used = r->tree_mode;
-    if (rc != LG_OK && r->tree_mode != LG_RENDER_TREE_BUILDBVH)
+    const int nbvh = r->n_nodes;
+    const size_t cap = std::max((size_t)nbvh, 2 * (size_t)r->n_tris);  // nodes of any render tree
+    LG_TRY(r->wide.reserve(cap * sizeof(WideNode)));
+    LG_TRY(r->leaves.reserve(cap * sizeof(int2)));
+    LG_TRY(r->rnodes.reserve(cap * sizeof(lg_bvh_node)));
+    LG_TRY(r->rt_scratch.reserve(render_tree_scratch_bytes(nbvh, r->n_tris)));
+    int mode = r->tree_mode;
+    int rc = build_render_tree(r->nodes.as<lg_bvh_node>(), nbvh, r->tris.as<lg_triangle>(), r->n_tris, mode,
+                               r->rnodes.as<lg_bvh_node>(), r->rt_scratch.p, r->rt_scratch.bytes, r->stream);
+    if (rc != LG_OK && mode != LG_RENDER_TREE_BUILDBVH)
     {
         // e.g. leaves whose triangle ranges share a first triangle: keep the given topology
-        rc = build_render_tree(r->nodes.as<lg_bvh_node>(), n, r->n_tris, LG_RENDER_TREE_BUILDBVH,
+        mode = LG_RENDER_TREE_BUILDBVH;
+        rc = build_render_tree(r->nodes.as<lg_bvh_node>(), nbvh, r->tris.as<lg_triangle>(), r->n_tris, mode,
                                r->rnodes.as<lg_bvh_node>(), r->rt_scratch.p, r->rt_scratch.bytes, r->stream);
-        r->tree_used = LG_RENDER_TREE_BUILDBVH;
     }
     LG_TRY(rc);
+    r->tree_used = mode;
+    const int n = render_tree_nodes(nbvh, r->n_tris, mode);
     const size_t nb = (size_t)n / 1024 + 1;
     size_t need = ((size_t)n * 11 + 2 * nb + 256) * sizeof(int);
     LG_TRY(r->scratch.reserve(need));
@@ -311,6 +316,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
         job.blocks_per_sm = r->trace_blocks_per_sm;
         job.refill_threshold = r->trace_refill;
+        job.leaf_quorum = r->trace_quorum;
         LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->watertight,
                                  r->stream));
     }
@@ -861,11 +867,27 @@ int lg_renderer_get_refill_threshold(const lg_renderer* r)
     return r->trace_refill;
 }
 
+int lg_renderer_set_leaf_quorum(lg_renderer* r, int quorum)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (quorum < 0 || quorum > 31) return set_error(LG_ERR_INVALID, "leaf quorum must be 0..31");
+    r->trace_quorum = quorum;
+    return LG_OK;
+}
+
+int lg_renderer_get_leaf_quorum(const lg_renderer* r)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    return r->trace_quorum;
+}
+
 int lg_renderer_set_render_tree(lg_renderer* r, int mode)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
-    if (mode != LG_RENDER_TREE_BUILDBVH && mode != LG_RENDER_TREE_PLOC)
-        return set_error(LG_ERR_INVALID, "render tree mode must be 0 (BuildBVH topology) or 1 (PLOC)");
+    if (mode != LG_RENDER_TREE_BUILDBVH && mode != LG_RENDER_TREE_PLOC && mode != LG_RENDER_TREE_PLOC_TRIANGLES)
+        return set_error(LG_ERR_INVALID,
+                         "render tree mode must be 0 (BuildBVH topology), 1 (PLOC over its leaves) or 2 (PLOC over "
+                         "triangles)");
     if (mode == r->tree_mode) return LG_OK;
     DeviceGuard g(r->device);
     r->tree_mode = mode;
@@ -999,6 +1021,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
     key.push_back(r->bvh_width * 2 + (r->watertight ? 1 : 0));
     key.push_back(r->trace_blocks_per_sm);
     key.push_back(r->trace_refill);
+    key.push_back(r->trace_quorum);
     key.push_back(r->scene_gen);
     if (key != r->batch_key || !r->batch_exec)
     {
@@ -1019,6 +1042,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
             job.total_items = items;
             job.blocks_per_sm = r->trace_blocks_per_sm;
             job.refill_threshold = r->trace_refill;
+            job.leaf_quorum = r->trace_quorum;
             e = launch_trace_batch(dev_scene(r), job, r->sm_count, r->bvh_width, r->watertight, st);
         }
         for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)

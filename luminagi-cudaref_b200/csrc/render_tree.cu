@@ -16,8 +16,13 @@
 //     nearest neighbours merge into a new node, and the survivors are
 //     compacted in order.  The Morton tree splits at code bits; PLOC groups
 //     by actual box sizes, so traversal opens fewer boxes.
+//   * mode 2: PLOC over the triangles themselves (in their Morton order),
+//     one triangle per leaf: 2T - 1 nodes.  Leaves index the same triangle
+//     array, so nothing is reordered; any BVH over the triangles finds the
+//     same closest hits (up to exact ties in t).
 // Ties in the neighbour search go to the lower position and every numbering
 // comes from prefix sums, so both trees are deterministic.
+#include <algorithm>
 #include <cstdint>
 #include <vector>
 
@@ -192,6 +197,30 @@ __global__ void init_clusters_kernel(const lg_bvh_node* __restrict__ nodes, cons
     b.hi = make_float4(nd.bbMax[0], nd.bbMax[1], nd.bbMax[2], 0.0f);
     cbox[k] = b;
 }
+// Cluster t = triangle t (one-triangle leaf, node id t of the new tree).
+__global__ void init_tri_clusters_kernel(const lg_triangle* __restrict__ tris, int n_tris,
+                                         lg_bvh_node* __restrict__ tn, int* __restrict__ cid, Box* __restrict__ cbox)
+{
+    const int t = blockIdx.x * kTB + threadIdx.x;
+    if (t >= n_tris) return;
+    const lg_triangle tr = tris[t];
+    lg_bvh_node nd;
+    for (int a = 0; a < 3; ++a)
+    {
+        nd.bbMin[a] = fminf(fminf(tr.v[0][a], tr.v[1][a]), tr.v[2][a]);
+        nd.bbMax[a] = fmaxf(fmaxf(tr.v[0][a], tr.v[1][a]), tr.v[2][a]);
+    }
+    nd.left = -1;
+    nd.right = -1;
+    nd.firstTri = t;
+    nd.triCount = 1;
+    tn[t] = nd;
+    cid[t] = t;
+    Box b;
+    b.lo = make_float4(nd.bbMin[0], nd.bbMin[1], nd.bbMin[2], 0.0f);
+    b.hi = make_float4(nd.bbMax[0], nd.bbMax[1], nd.bbMax[2], 0.0f);
+    cbox[t] = b;
+}
 // Nearest neighbour within +-kRadius positions by union surface area; ties -> lower position.
 __global__ void __launch_bounds__(kTB) nn_kernel(const Box* __restrict__ cbox, int c, int* __restrict__ nn)
 {
@@ -274,10 +303,17 @@ struct Scratch
 };
 }  // namespace
 
+int render_tree_nodes(int n_nodes, int n_tris, int mode)
+{
+    return mode == 2 && n_tris > 0 ? 2 * n_tris - 1 : n_nodes;
+}
+
 size_t render_tree_scratch_bytes(int n_nodes, int n_tris)
 {
-    const size_t n = (size_t)(n_nodes > 0 ? n_nodes : 1), t = (size_t)(n_tris > 0 ? n_tris : 1);
-    const size_t L = (n + 1) / 2;
+    const size_t t = (size_t)(n_tris > 0 ? n_tris : 1);
+    // the larger of the modes: BuildBVH's n_nodes, or 2T - 1 one-triangle-leaf nodes
+    const size_t n = std::max((size_t)(n_nodes > 0 ? n_nodes : 1), 2 * t);
+    const size_t L = std::max((n + 1) / 2, t);
     size_t b = 0;
     b += a256(n * sizeof(lg_bvh_node));         // tn
     b += 4 * a256(n * 4);                       // parent, depth, ids, newpos
@@ -285,14 +321,16 @@ size_t render_tree_scratch_bytes(int n_nodes, int n_tris)
     b += 3 * a256(t * 4);                       // leaf_at, flag, pos
     b += 2 * (a256(L * 4) + a256(L * sizeof(Box)));  // cluster arrays (double buffered)
     b += 5 * a256(L * 4);                       // nn, mflag, midx, kflag, kpos
-    b += a256((t / kTB + 2) * 4) + 256;         // block sums, totals
+    b += a256((L / kTB + 2) * 4) + 256;         // block sums, totals
     return b + 1024;
 }
 
-int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int mode, lg_bvh_node* d_out,
-                      void* scratch, size_t scratch_bytes, cudaStream_t st)
+int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, const lg_triangle* d_tris, int n_tris, int mode,
+                      lg_bvh_node* d_out, void* scratch, size_t scratch_bytes, cudaStream_t st)
 {
     if (n_nodes <= 0) return LG_OK;
+    const int in_nodes = n_nodes;
+    n_nodes = render_tree_nodes(n_nodes, n_tris, mode);
     Scratch s{(char*)(((uintptr_t)scratch + 255) & ~(uintptr_t)255), (char*)scratch + scratch_bytes};
     lg_bvh_node* tn = s.take<lg_bvh_node>((size_t)n_nodes);
     int* parent = s.take<int>((size_t)n_nodes);
@@ -306,7 +344,7 @@ int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int m
     int root = 0;
     const int g = (n_nodes + kTB - 1) / kTB;
 
-    if (mode == 1 && n_nodes > 1)
+    if ((mode == 1 || mode == 2) && n_nodes > 1)
     {
         const int t = n_tris;
         int* leaf_at = s.take<int>((size_t)t);
@@ -325,15 +363,24 @@ int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int m
         int* sums = s.take<int>((size_t)t / kTB + 2);
         int* totals = s.take<int>(64);
         if (!sums || !totals) return set_error(LG_ERR_CAPACITY, "render tree: scratch too small");
-        LG_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)t, st));
-        leaf_at_kernel<<<g, kTB, 0, st>>>(d_nodes, n_nodes, leaf_at, flag);
-        LG_TRY_CUDA(excl_scan(flag, t, pos, sums, totals, st));
-        init_clusters_kernel<<<(t + kTB - 1) / kTB, kTB, 0, st>>>(d_nodes, leaf_at, flag, pos, t, tn, cid, cbox);
-        LG_TRY_CUDA(cudaGetLastError());
         int c = 0;
-        LG_TRY_CUDA(cudaMemcpyAsync(&c, totals, sizeof(int), cudaMemcpyDeviceToHost, st));
-        LG_TRY_CUDA(cudaStreamSynchronize(st));
-        if (c != L) return set_error(LG_ERR_INVALID, "render tree: %d leaves by range start, %d expected", c, L);
+        if (mode == 2)
+        {
+            init_tri_clusters_kernel<<<(t + kTB - 1) / kTB, kTB, 0, st>>>(d_tris, t, tn, cid, cbox);
+            LG_TRY_CUDA(cudaGetLastError());
+            c = t;
+        }
+        else
+        {
+            LG_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)t, st));
+            leaf_at_kernel<<<(in_nodes + kTB - 1) / kTB, kTB, 0, st>>>(d_nodes, in_nodes, leaf_at, flag);
+            LG_TRY_CUDA(excl_scan(flag, t, pos, sums, totals, st));
+            init_clusters_kernel<<<(t + kTB - 1) / kTB, kTB, 0, st>>>(d_nodes, leaf_at, flag, pos, t, tn, cid, cbox);
+            LG_TRY_CUDA(cudaGetLastError());
+            LG_TRY_CUDA(cudaMemcpyAsync(&c, totals, sizeof(int), cudaMemcpyDeviceToHost, st));
+            LG_TRY_CUDA(cudaStreamSynchronize(st));
+            if (c != L) return set_error(LG_ERR_INVALID, "render tree: %d leaves by range start, %d expected", c, L);
+        }
         int next_id = L;
         while (c > 1)
         {

@@ -484,40 +484,40 @@ __device__ __forceinline__ int pop(Trav& q, const int* stack) { return q.sp == 0
 // The four boxes of a 4-wide record against one ray.  Per axis the near
 // plane is the min plane when 1/d >= 0 and the max plane otherwise, so each
 // slab needs two fused multiply-adds, t = plane * (1/d) - o * (1/d), and no
-// min/max of the two; the near and far planes are fetched straight from the
-// record by the signs of 1/d.  The hit rule and the entry distance are the
-// reference's (pathtracer.cu:61-80): hit unless hi < max(lo, 0) or lo > tmax,
-// entry max(lo, 0) (tested as max(lo, 0) > tmax, the same for tmax >= 0; a
-// shadow ray with tmax < 0 can hit no triangle either way).  The rounding is
-// not the reference's (plane - o) * (1/d): a box boundary moves by about one
-// ulp of the ray origin, which changes which records are opened only for
-// rays passing within that distance of a box face.  Empty slots hold
-// [+inf, -inf] and always miss.  Children that miss get t = +inf.
+// min/max of the two; the record's planes come in one 256-bit load per axis
+// (four min planes, four max planes) and the signs of 1/d pick near and far.
+// The hit rule and the entry distance are the reference's
+// (pathtracer.cu:61-80): hit unless hi < max(lo, 0) or lo > tmax, entry
+// max(lo, 0) (tested as max(lo, 0) > tmax, the same for tmax >= 0; a shadow
+// ray with tmax < 0 can hit no triangle either way).  The rounding is not the
+// reference's (plane - o) * (1/d): a box boundary moves by about one ulp of
+// the ray origin, which changes which records are opened only for rays
+// passing within that distance of a box face.  Empty slots hold [+inf, -inf]
+// and always miss.  Children that miss get t = +inf.
 __device__ __forceinline__ int4 box4(const Wide4Node* nd, const Ray& r, float tmax, float& t0, float& t1, float& t2,
                                      float& t3)
 {
-    const char* b = reinterpret_cast<const char*>(nd);
-    const int sx = (__float_as_int(r.inv_d.x) >> 31) & 16;
-    const int sy = (__float_as_int(r.inv_d.y) >> 31) & 16;
-    const int sz = (__float_as_int(r.inv_d.z) >> 31) & 16;
-    const float4 nx = __ldg(reinterpret_cast<const float4*>(b + 0 + sx));
-    const float4 fx = __ldg(reinterpret_cast<const float4*>(b + 16 - sx));
-    const float4 ny = __ldg(reinterpret_cast<const float4*>(b + 32 + sy));
-    const float4 fy = __ldg(reinterpret_cast<const float4*>(b + 48 - sy));
-    const float4 nz = __ldg(reinterpret_cast<const float4*>(b + 64 + sz));
-    const float4 fz = __ldg(reinterpret_cast<const float4*>(b + 80 - sz));
+    float x[8], y[8], z[8];
+    ldg8(&nd->lox, x);
+    ldg8(&nd->loy, y);
+    ldg8(&nd->loz, z);
     const int4 ln = __ldg(&nd->link);
+    const bool sx = __float_as_int(r.inv_d.x) < 0, sy = __float_as_int(r.inv_d.y) < 0,
+               sz = __float_as_int(r.inv_d.z) < 0;
     const float ox = -(r.o.x * r.inv_d.x), oy = -(r.o.y * r.inv_d.y), oz = -(r.o.z * r.inv_d.z);
     const float inf = __int_as_float(0x7f800000);
-    auto one = [&](float ax, float bx, float ay, float by, float az, float bz) {
-        const float l0 = fmaxf(fmaxf(fmaf(ax, r.inv_d.x, ox), fmaf(ay, r.inv_d.y, oy)), fmaxf(fmaf(az, r.inv_d.z, oz), 0.0f));
-        const float hi = fminf(fminf(fmaf(bx, r.inv_d.x, ox), fmaf(by, r.inv_d.y, oy)), fmaf(bz, r.inv_d.z, oz));
+    auto one = [&](int k) {
+        const float nx = sx ? x[4 + k] : x[k], fx = sx ? x[k] : x[4 + k];
+        const float ny = sy ? y[4 + k] : y[k], fy = sy ? y[k] : y[4 + k];
+        const float nz = sz ? z[4 + k] : z[k], fz = sz ? z[k] : z[4 + k];
+        const float l0 = fmaxf(fmaxf(fmaf(nx, r.inv_d.x, ox), fmaf(ny, r.inv_d.y, oy)), fmaxf(fmaf(nz, r.inv_d.z, oz), 0.0f));
+        const float hi = fminf(fminf(fmaf(fx, r.inv_d.x, ox), fmaf(fy, r.inv_d.y, oy)), fmaf(fz, r.inv_d.z, oz));
         return (hi < l0 || l0 > tmax) ? inf : l0;
     };
-    t0 = one(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x);
-    t1 = one(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y);
-    t2 = one(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z);
-    t3 = one(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w);
+    t0 = one(0);
+    t1 = one(1);
+    t2 = one(2);
+    t3 = one(3);
     return ln;
 }
 
@@ -652,15 +652,18 @@ __device__ __forceinline__ int traverse_ray(const DevScene& s, const Ray& r, flo
 // One warp-wide step of the persistent kernel's traversals, with leaves
 // postponed (Aila and Laine, "Understanding the Efficiency of Ray Traversal
 // on GPUs", HPG 2009): a lane that reaches a leaf sets it aside and keeps
-// visiting records from its stack while other lanes still look for a leaf;
-// once every lane with a ray in flight holds a leaf, the warp tests them
-// together.  The records visited past a postponed leaf would be culled by a
-// nearer hit in it only for closest-hit rays, and then only cost time: the
-// closest hit is the same (up to exact ties in t).  `busy` is this lane's
-// ray in flight; returns true when its traversal has finished.
+// visiting records from its stack while other lanes still look for a leaf.
+// The warp visits records while more than `quorum` lanes are still looking
+// (or no lane holds a leaf), and otherwise tests the held leaves together;
+// quorum 0 waits for every lane, as in the paper.  Every step makes
+// progress: a record step has at least one searching lane, a leaf step at
+// least one held leaf.  The records visited past a postponed leaf would be
+// culled by a nearer hit in it only for closest-hit rays, and then only cost
+// time: the closest hit is the same (up to exact ties in t).  `busy` is this
+// lane's ray in flight; returns true when its traversal has finished.
 template <int kWidth, bool kCount, bool kWT>
-__device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool anyhit, bool busy, Trav& q,
-                                          int* stack, Counters& cnt)
+__device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool anyhit, bool busy, int quorum,
+                                          Trav& q, int* stack, Counters& cnt)
 {
     if (busy && q.pend == 0 && q.cur < 0 && q.cur != kDone)
     {
@@ -668,13 +671,16 @@ __device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool 
         q.cur = pop(q, stack);
     }
     const bool fin = busy && q.pend == 0 && q.cur == kDone;
-    // every lane takes part in the vote, finished or idle ones included
-    if (__any_sync(0xffffffffu, busy && !fin && q.pend == 0))
+    // every lane takes part in the votes, finished or idle ones included
+    const bool searching = busy && !fin && q.pend == 0;  // then q.cur >= 0
+    const unsigned n_searching = __popc(__ballot_sync(0xffffffffu, searching));
+    const bool holding = __any_sync(0xffffffffu, busy && !fin && q.pend != 0);
+    if (n_searching > (unsigned)quorum || !holding)
     {
         if (busy && q.cur >= 0) node_step<kWidth, kCount>(s, r, q, stack, cnt);
         return fin;
     }
-    if (!busy || fin) return fin;
+    if (!busy || fin || q.pend == 0) return fin;
     const int link = q.pend;
     q.pend = 0;
     return leaf_step<kWidth, kCount, kWT>(s, r, anyhit, link, q, cnt) || q.cur == kDone;
@@ -911,6 +917,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
     int stack[kStack];
     const int root = kWidth == 4 ? s.root4 : s.root;
     const int thresh = job.refill_threshold < 1 ? 1 : (job.refill_threshold > 32 ? 32 : job.refill_threshold);
+    const int quorum = job.leaf_quorum < 0 ? 0 : (job.leaf_quorum > 31 ? 31 : job.leaf_quorum);
     bool active = false, exhausted = false, tdone = false;
     for (;;)
     {
@@ -970,7 +977,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         const int idle_final = exhausted ? __popc(__ballot_sync(0xffffffffu, !active)) : 0;
         for (;;)
         {
-            if (warp_step<kWidth, kCount, kWT>(s, st.ray, st.li >= 0, active && !tdone, q, stack, cnt)) tdone = true;
+            if (warp_step<kWidth, kCount, kWT>(s, st.ray, st.li >= 0, active && !tdone, quorum, q, stack, cnt))
+                tdone = true;
             const unsigned busy = __ballot_sync(0xffffffffu, active && !tdone);
             if (busy == 0 || 32 - __popc(busy) - idle_final >= thresh) break;
         }

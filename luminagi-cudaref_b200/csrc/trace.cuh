@@ -96,6 +96,7 @@ struct TraceJob
     unsigned long long* work64;  // work counter (zeroed by the launcher)
     int blocks_per_sm;     // persistent grid: resident blocks per SM (0 = as many as fit)
     int refill_threshold;  // finished rays in a warp that trigger the path logic, 1..32
+    int leaf_quorum;       // lanes still searching for a leaf below which the warp tests held leaves, 0..31
     RenderCounters* counters;  // optional
     // batched launch (launch_trace_batch): every field above except work64 is taken from jobs[]
     const BatchJob* jobs;

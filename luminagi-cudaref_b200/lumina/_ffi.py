@@ -103,6 +103,8 @@ SIGNATURES = {
     "lg_renderer_set_render_tree": (_I, [_P, _I]),
     "lg_renderer_set_refill_threshold": (_I, [_P, _I]),
     "lg_renderer_get_refill_threshold": (_I, [_P]),
+    "lg_renderer_set_leaf_quorum": (_I, [_P, _I]),
+    "lg_renderer_get_leaf_quorum": (_I, [_P]),
     "lg_renderer_get_render_tree": (_I, [_P, C.POINTER(C.c_int32)]),
     "lg_renderer_autotune": (_I, [_P, C.POINTER(LgCamera), _I, _I, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "lg_renderer_set_texture": (_I, [_P, _I, _P, C.c_int32, C.c_int32]),

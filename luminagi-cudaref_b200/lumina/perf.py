@@ -56,22 +56,25 @@ def trace(a):
     r = Renderer(0)
     r.set_scene(sc)
     r.set_bvh_width(a.width)
+    r.set_render_tree(a.tree)
     r.set_counting(True)
     c = r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)
     r.set_counting(False)
     rays = c["closest_rays"] + c["shadow_rays"]
-    out = {"kernel": "trace", "spp": a.spp, "width": a.width, "rays": rays,
+    out = {"kernel": "trace", "spp": a.spp, "width": a.width, "tree": r.render_tree(), "rays": rays,
            "nodes_per_ray": c["node_fetches"] / rays, "tris_per_ray": c["tri_tests"] / rays}
     sweep = {}
-    for th in (int(x) for x in str(a.refill).split(",")):
-        r.set_refill_threshold(th)
-        ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for _ in range(a.reps)]
-        sweep[th] = {"ms": ms, "mrays_per_s": rays / min(ms) / 1e3}
+    for qu in (int(x) for x in str(a.quorum).split(",")):
+        r.set_leaf_quorum(qu)
+        for th in (int(x) for x in str(a.refill).split(",")):
+            r.set_refill_threshold(th)
+            ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for _ in range(a.reps)]
+            sweep[f"refill={th},quorum={qu}"] = {"ms": ms, "mrays_per_s": rays / min(ms) / 1e3}
     if len(sweep) == 1:
-        (th, v), = sweep.items()
-        out.update(refill=th, **v)
+        (k, v), = sweep.items()
+        out.update(schedule=k, **v)
     else:
-        out["refill"] = sweep
+        out["schedule"] = sweep
     return out
 
 
@@ -156,6 +159,8 @@ def main(argv=None):
     ap.add_argument("--width", type=int, default=4)
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--refill", default="16", help="trace: refill threshold(s), comma-separated")
+    ap.add_argument("--quorum", default="8", help="trace: leaf quorum(s), comma-separated")
+    ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)
     print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch}[a.what](a)))
 

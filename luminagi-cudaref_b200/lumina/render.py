@@ -117,14 +117,22 @@ class Renderer:
     def refill_threshold(self) -> int:
         return int(lib().lg_renderer_get_refill_threshold(self._h))
 
+    def set_leaf_quorum(self, quorum: int) -> None:
+        """Lanes still looking for a BVH leaf (0..31) below which a warp tests the leaves its lanes hold."""
+        check(lib().lg_renderer_set_leaf_quorum(self._h, int(quorum)))
+
+    def leaf_quorum(self) -> int:
+        return int(lib().lg_renderer_get_leaf_quorum(self._h))
+
     def set_render_tree(self, mode: str) -> None:
-        """Topology of the traversal records: 'ploc' (default) or 'buildbvh' (same leaves either way)."""
-        check(lib().lg_renderer_set_render_tree(self._h, {"buildbvh": 0, "ploc": 1}[mode]))
+        """Tree the traversal records come from: 'ploc_tris' (default; PLOC over the triangles, one per
+        leaf), 'ploc' (PLOC over BuildBVH's leaves) or 'buildbvh' (its own topology)."""
+        check(lib().lg_renderer_set_render_tree(self._h, {"buildbvh": 0, "ploc": 1, "ploc_tris": 2}[mode]))
 
     def render_tree(self) -> str:
         m = C.c_int32(-1)
         check(lib().lg_renderer_get_render_tree(self._h, C.byref(m)))
-        return {0: "buildbvh", 1: "ploc"}.get(m.value, "none")
+        return {0: "buildbvh", 1: "ploc", 2: "ploc_tris"}.get(m.value, "none")
 
     def set_counting(self, on: bool) -> None:
         check(lib().lg_renderer_set_counting(self._h, 1 if on else 0))

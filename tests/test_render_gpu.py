@@ -191,24 +191,33 @@ def test_trace_grid_autotune(box_scene):
 
 
 @pytest.mark.parametrize("width", [2, 4])
-def test_refill_threshold_does_not_change_images(small_engine_scene, width):
+def test_trace_schedule_does_not_change_images(small_engine_scene, width):
     """The warp refills lanes whose rays finished once `threshold` of them
-    have; every ray's result is independent of that schedule.  At 8 spp each
-    pixel is one (pixel, chunk) item, so the accumulators are bit-identical."""
+    have, and tests held leaves once at most `quorum` lanes still look for
+    one.  At 8 spp each pixel is one (pixel, chunk) item, so the accumulator
+    of a pixel is one sum and depends only on its rays' hits."""
     out = {}
     with lumina.Renderer(0) as r:
         r.set_scene(small_engine_scene)
         r.set_bvh_width(width)
-        assert r.refill_threshold() == 16
-        for th in (32, 1, 7, 16):
+        assert r.refill_threshold() == 16 and r.leaf_quorum() == 8
+        for th, qu in ((32, 0), (1, 0), (7, 3), (16, 8), (16, 31), (32, 31)):
             r.set_refill_threshold(th)
-            out[th] = r.render(spp=8, bounces=2)["accum"]
-        with pytest.raises(lumina.LuminaError):
-            r.set_refill_threshold(0)
-        with pytest.raises(lumina.LuminaError):
-            r.set_refill_threshold(33)
-    for th in (1, 7, 16):
-        assert np.array_equal(out[th], out[32]), th
+            r.set_leaf_quorum(qu)
+            out[th, qu] = r.render(spp=8, bounces=2)["accum"]
+        for bad in (0, 33):
+            with pytest.raises(lumina.LuminaError):
+                r.set_refill_threshold(bad)
+        for bad in (-1, 32):
+            with pytest.raises(lumina.LuminaError):
+                r.set_leaf_quorum(bad)
+    # the refill threshold only reschedules whole rays: bit-identical
+    assert np.array_equal(out[1, 0], out[32, 0])
+    # the quorum changes when a ray's held leaves are tested relative to its
+    # record visits, hence which records its current hit culls; the closest
+    # hit can differ only for exact ties and rays grazing a box face
+    for k in out:
+        assert match_fraction(out[k], out[32, 0]) >= 0.9999, k
 
 
 def test_engine_full_frame_vs_reference_gpu():
@@ -242,11 +251,12 @@ def _dfs_order(nodes):
     return out
 
 
-@pytest.mark.parametrize("tree", ["ploc", "buildbvh"])
+@pytest.mark.parametrize("tree", ["ploc_tris", "ploc", "buildbvh"])
 def test_render_tree_modes_and_dfs_input(small_engine_scene, tree):
-    """Traversal records from the PLOC-regrouped tree or from BuildBVH's own
-    topology, for a breadth-first and a depth-first caller array: every frame
-    must match the reference kernel on the reference tree."""
+    """Traversal records from PLOC over the triangles, from the PLOC-regrouped
+    BuildBVH leaves or from BuildBVH's own topology, for a breadth-first and a
+    depth-first caller array: every frame must match the reference kernel on
+    the reference tree."""
     if not O.ref_available():
         pytest.skip("reference oracle not built")
     sc = small_engine_scene
