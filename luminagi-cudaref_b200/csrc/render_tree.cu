@@ -38,7 +38,7 @@ namespace lg
 namespace
 {
 constexpr int kTB = 256;
-constexpr int kRadius = 16;  // PLOC search radius (positions on either side)
+constexpr int kRadius = 8;  // PLOC search radius (positions on either side); 8 measured 1% faster to trace than 16 or 32
 
 size_t a256(size_t b) { return (b + 255) & ~(size_t)255; }
 
