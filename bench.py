@@ -11,10 +11,10 @@ counting pass) with ms/frame alongside.
   e2e       through the C ABI from host buffers: triangle upload from pinned
             memory, device LBVH build, render, tonemap and the 8-bit image read
             back, every step.
-  roofline  algorithmic bytes of the trace kernel (112 B per 4-wide BVH
-            record: six planes of four boxes and four links; 48 B per triangle
-            test; 8 B per leaf-table entry; as counted) over its event-timed
-            duration, against the measured HBM copy peak.
+  roofline  algorithmic bytes of the trace kernel (56 B per 4-wide BVH
+            record: grid origin and steps, 24 one-byte planes, four links;
+            48 B per triangle test; 8 B per leaf-table entry; as counted) over
+            its event-timed duration, against the measured HBM copy peak.
             The scene (~200 MB) exceeds the 126 MB L2, so traffic is a mix of
             L2 and HBM.
   cpu_baseline  the reference's own trace code (oracle/_ref, compiled from its
@@ -46,12 +46,13 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 1,122.1 MB + 187.5 MB / 65,366,791 rays
+# of an 8-spp engine frame: 470.0 MB + 63.1 MB / 65,366,791 rays
 # (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = 1309.551250e6 / 65366791
-# Bytes one traversal step reads from a BVH record: 4-wide, six planes of
-# four boxes (96 B) and four links (16 B); 2-wide, the whole 64-B record.
-RECORD_BYTES = {4: 112, 2: 64}
+TRACE_DRAM_BYTES_PER_RAY = 533.148672e6 / 65366791
+# Bytes one traversal step uses from a BVH record: 4-wide, the grid origin and
+# steps (16 B), 24 one-byte planes and four links (16 B); 2-wide, the whole
+# 64-B record.
+RECORD_BYTES = {4: 56, 2: 64}
 
 
 def load_peaks():

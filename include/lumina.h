@@ -160,8 +160,10 @@ int lg_renderer_set_scene_bvh(lg_renderer* r, const lg_scene_desc* scene, const 
 /* Copy back the device BVH (nodes_out may be NULL to query the count). */
 int lg_renderer_get_bvh(lg_renderer* r, lg_bvh_node* nodes_out, int32_t* n_nodes, lg_triangle* tris_out);
 int lg_renderer_set_counting(lg_renderer* r, int enable);
-/* Traversal records: 4 (default; up to four descendants per 128-byte record) or 2
- * (one binary node per 64-byte record).  Both traverse the same BVH. */
+/* Traversal records: 4 (default; up to four descendants per 64-byte record,
+ * their boxes quantized to 8 bits per plane and rounded outwards) or 2 (one
+ * binary node per 64-byte record, exact boxes and the reference's slab test).
+ * Both traverse the same render tree. */
 int lg_renderer_set_bvh_width(lg_renderer* r, int width);
 /* The tree the traversal records are built from.  lg_renderer_get_bvh still
  * returns the scene's BuildBVH tree unchanged, and every mode reports hits

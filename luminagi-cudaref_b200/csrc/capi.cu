@@ -210,7 +210,7 @@ int build_records(lg_renderer* r)
     const int nbvh = r->n_nodes;
     const size_t cap = std::max((size_t)nbvh, 2 * (size_t)r->n_tris);  // nodes of any render tree
     LG_TRY(r->wide.reserve(cap * sizeof(WideNode)));
-    LG_TRY(r->leaves.reserve(cap * sizeof(int2)));
+    LG_TRY(r->leaves.reserve((cap + 1) * sizeof(int2)));  // + the empty leaf of absent 4-wide children
     LG_TRY(r->rnodes.reserve(cap * sizeof(lg_bvh_node)));
     LG_TRY(r->rt_scratch.reserve(render_tree_scratch_bytes(nbvh, r->n_tris)));
     int mode = r->tree_mode;
@@ -234,7 +234,10 @@ int build_records(lg_renderer* r)
     LG_TRY_CUDA(build_wide_nodes(r->rnodes.as<lg_bvh_node>(), n, r->wide.as<WideNode>(), r->leaves.as<int2>(),
                                  r->scratch.as<int>(), &root, &ni, &nl, r->stream));
     int leaf_inline = 0;
-    LG_TRY_CUDA(build_wide4_nodes(r->rnodes.as<lg_bvh_node>(), n, r->n_tris, r->wide4.as<Wide4Node>(),
+    static const int2 kEmptyLeaf = {0, 0};
+    LG_TRY_CUDA(cudaMemcpyAsync(r->leaves.as<int2>() + nl, &kEmptyLeaf, sizeof(int2), cudaMemcpyHostToDevice,
+                                r->stream));
+    LG_TRY_CUDA(build_wide4_nodes(r->rnodes.as<lg_bvh_node>(), n, r->n_tris, nl, r->wide4.as<Wide4Node>(),
                                   r->scratch.as<int>(), &root4, &n4, &leaf_inline, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
     r->leaf_inline = leaf_inline;

@@ -11,15 +11,16 @@
 // the compiler sees the same expressions.
 //
 // What is different (none of it changes which triangle a ray hits, except for
-// exact ties in t and rays within about an ulp of a box face):
-//   * BVH records hold up to four children's boxes (Wide4Node, 128 bytes),
-//     built from a render tree over the reference BVH's leaves; traversal
-//     enters the nearest hit child and stacks the others nearest-on-top; the
-//     reference pops children in fixed order and tests each box after a
-//     separate 40-byte fetch.  The 4-wide box test picks each axis's near and
-//     far planes by the sign of 1/d and evaluates them with fused
-//     multiply-adds (box4).  The 2-wide records (WideNode) keep the
-//     reference's slab arithmetic.
+// exact ties in t and rays within rounding distance of a box face):
+//   * BVH records hold up to four children's boxes (Wide4Node, 64 bytes, the
+//     planes quantized to 8 bits on a per-record grid, rounded outwards),
+//     built from a render tree over the same triangles; traversal enters the
+//     nearest hit child and stacks the others nearest-on-top; the reference
+//     pops children in fixed order and tests each box after a separate
+//     40-byte fetch.  The 4-wide box test picks each axis's near and far
+//     planes by the sign of 1/d and evaluates them with fused multiply-adds
+//     (box4).  The 2-wide records (WideNode) keep the reference's exact boxes
+//     and slab arithmetic.
 //   * Triangle records for intersection are v0, e1, e2 as float4s
 //     (e1 = v1 - v0 is the same IEEE subtraction the reference does per test);
 //     normals are read from the 100-byte record only at the closest hit.
@@ -248,19 +249,46 @@ __device__ __forceinline__ int leaf_link4(const lg_bvh_node& c, int leaf_index, 
     return c.triCount < 16 ? ~((c.firstTri << 4) | c.triCount) : ~(leaf_index << 4);
 }
 
+// Grid of one axis of a quantized record over its nk children's planes:
+// step 2^E with the record's extent within 252 steps and at least two ulps of
+// its coordinates, origin one step below its min rounded down, planes one
+// step outside each child's exact box (floor for min, ceil for max).
+__device__ void quantize_axis(const float (&lo)[4], const float (&hi)[4], int nk, float& origin, float& step_out,
+                              uint32_t& qlo, uint32_t& qhi)
+{
+    float pl = lo[0], ph = hi[0];
+    for (int k = 1; k < nk; ++k) { pl = fminf(pl, lo[k]); ph = fmaxf(ph, hi[k]); }
+    const double ext = (double)ph - (double)pl;
+    const double m = fmax(fabs((double)pl), fabs((double)ph));
+    int E = -126;
+    if (ext > 0.0) E = max(E, (int)ceil(log2(ext / 252.0)));
+    if (m > 0.0) E = max(E, ilogb(m) - 22);
+    E = min(E, 127);
+    const double step = ldexp(1.0, E);
+    origin = __double2float_rd((double)pl - step);
+    step_out = (float)step;  // a power of two in the normal range: exact
+    qlo = 0xffffffffu;  // absent children: 255 / 0
+    qhi = 0u;
+    for (int k = 0; k < nk; ++k)
+    {
+        const int ql = min(255, max(0, (int)floor(((double)lo[k] - (double)origin) / step) - 1));
+        const int qh = min(255, max(0, (int)ceil(((double)hi[k] - (double)origin) / step) + 1));
+        qlo = (qlo & ~(0xffu << (8 * k))) | ((uint32_t)ql << (8 * k));
+        qhi |= (uint32_t)qh << (8 * k);
+    }
+}
+
 __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const int* __restrict__ is4,
                              const int* __restrict__ dense4, const int* __restrict__ dense2,
-                             const int* __restrict__ sel, Wide4Node* __restrict__ out, int inline_ok)
+                             const int* __restrict__ sel, Wide4Node* __restrict__ out, int inline_ok, int null_link)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !is4[i]) return;
     float lo[3][4], hi[3][4];
     int ln[4];
-    // An absent child gets the empty box [+inf, -inf], which box4 never hits.
-    const float inf = __int_as_float(0x7f800000);
     for (int a = 0; a < 3; ++a)
-        for (int k = 0; k < 4; ++k) { lo[a][k] = inf; hi[a][k] = -inf; }
-    for (int k = 0; k < 4; ++k) ln[k] = kEmptyLink;
+        for (int k = 0; k < 4; ++k) { lo[a][k] = 0.0f; hi[a][k] = 0.0f; }
+    for (int k = 0; k < 4; ++k) ln[k] = null_link;
     int k = 0;
     for (int j = 0; j < 4; ++j)
     {
@@ -270,14 +298,8 @@ __global__ void wide4_kernel(const lg_bvh_node* __restrict__ nodes, int n, const
         put_child(lo, hi, ln, k, c, c.triCount > 0 ? leaf_link4(c, dense2[ci], inline_ok) : dense4[ci]);
     }
     Wide4Node w;
-    w.lox = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
-    w.hix = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
-    w.loy = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
-    w.hiy = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
-    w.loz = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
-    w.hiz = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
-    w.link = make_int4(ln[0], ln[1], ln[2], ln[3]);
-    w.pad = make_int4(0, 0, 0, 0);
+    for (int a = 0; a < 3; ++a) quantize_axis(lo[a], hi[a], k, w.o[a], w.step[a], w.qlo[a], w.qhi[a]);
+    for (int j = 0; j < 4; ++j) w.link[j] = ln[j];
     out[dense4[i]] = w;
 }
 
@@ -459,7 +481,7 @@ __device__ __forceinline__ void cswap(float& ta, int& la, float& tb, int& lb)
 // once the stack is empty), a leaf postponed for testing (0 = none; leaf
 // links are negative), the stack depth, and the closest hit so far (t starts
 // at the ray's tmax).
-constexpr int kDone = kEmptyLink;  // also the link of an absent child
+constexpr int kDone = (int)0x80000000;  // no leaf or record link takes this value
 struct Trav
 {
     int cur, pend, sp, tri;
@@ -481,37 +503,43 @@ __device__ __forceinline__ void trav_begin(Trav& q, int root, float tmax, bool a
 
 __device__ __forceinline__ int pop(Trav& q, const int* stack) { return q.sp == 0 ? kDone : stack[--q.sp]; }
 
-// The four boxes of a 4-wide record against one ray.  Per axis the near
-// plane is the min plane when 1/d >= 0 and the max plane otherwise, so each
-// slab needs two fused multiply-adds, t = plane * (1/d) - o * (1/d), and no
-// min/max of the two; the record's planes come in one 256-bit load per axis
-// (four min planes, four max planes) and the signs of 1/d pick near and far.
-// The hit rule and the entry distance are the reference's
-// (pathtracer.cu:61-80): hit unless hi < max(lo, 0) or lo > tmax, entry
-// max(lo, 0) (tested as max(lo, 0) > tmax, the same for tmax >= 0; a shadow
-// ray with tmax < 0 can hit no triangle either way).  The rounding is not the
-// reference's (plane - o) * (1/d): a box boundary moves by about one ulp of
-// the ray origin, which changes which records are opened only for rays
-// passing within that distance of a box face.  Empty slots hold [+inf, -inf]
-// and always miss.  Children that miss get t = +inf.
+// The four boxes of a quantized 4-wide record against one ray.  Per axis,
+// t(q) = q * (step / d) + (origin - o) / d: the step is a power of two, so
+// the first product is exact, and each plane costs a byte extraction (as the
+// float 2^23 + q, minus 2^23, exactly) and one fused multiply-add.  The near
+// plane is the min plane when 1/d >= 0 and the max plane otherwise; the signs
+// of 1/d pick the byte words.  Hit rule and entry distance are the
+// reference's (pathtracer.cu:61-80): hit unless hi < max(lo, 0) or lo > tmax
+// (tested as max(lo, 0) > tmax, the same for tmax >= 0), entry max(lo, 0).
+// The quantized boxes enclose the exact ones with a step to spare, which
+// covers the rounding of these products.  Children that miss get t = +inf.
+__device__ __forceinline__ float qplane(uint32_t w, int k)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (unsigned)k)) - 8388608.0f;
+}
 __device__ __forceinline__ int4 box4(const Wide4Node* nd, const Ray& r, float tmax, float& t0, float& t1, float& t2,
                                      float& t3)
 {
-    float x[8], y[8], z[8];
-    ldg8(&nd->lox, x);
-    ldg8(&nd->loy, y);
-    ldg8(&nd->loz, z);
-    const int4 ln = __ldg(&nd->link);
+    // a = o[3], step[3], qlo[0..1]; b = qlo[2], qhi[3], link[4]
+    float a[8], b[8];
+    ldg8(nd, a);
+    ldg8(reinterpret_cast<const char*>(nd) + 32, b);
+    const int4 ln = make_int4(__float_as_int(b[4]), __float_as_int(b[5]), __float_as_int(b[6]), __float_as_int(b[7]));
+    const float ix = a[3] * r.inv_d.x, iy = a[4] * r.inv_d.y, iz = a[5] * r.inv_d.z;
+    const float bx = (a[0] - r.o.x) * r.inv_d.x, by = (a[1] - r.o.y) * r.inv_d.y, bz = (a[2] - r.o.z) * r.inv_d.z;
     const bool sx = __float_as_int(r.inv_d.x) < 0, sy = __float_as_int(r.inv_d.y) < 0,
                sz = __float_as_int(r.inv_d.z) < 0;
-    const float ox = -(r.o.x * r.inv_d.x), oy = -(r.o.y * r.inv_d.y), oz = -(r.o.z * r.inv_d.z);
+    const uint32_t qlx = __float_as_uint(a[6]), qly = __float_as_uint(a[7]), qlz = __float_as_uint(b[0]);
+    const uint32_t qhx = __float_as_uint(b[1]), qhy = __float_as_uint(b[2]), qhz = __float_as_uint(b[3]);
+    const uint32_t nx = sx ? qhx : qlx, fx = sx ? qlx : qhx;
+    const uint32_t ny = sy ? qhy : qly, fy = sy ? qly : qhy;
+    const uint32_t nz = sz ? qhz : qlz, fz = sz ? qlz : qhz;
     const float inf = __int_as_float(0x7f800000);
     auto one = [&](int k) {
-        const float nx = sx ? x[4 + k] : x[k], fx = sx ? x[k] : x[4 + k];
-        const float ny = sy ? y[4 + k] : y[k], fy = sy ? y[k] : y[4 + k];
-        const float nz = sz ? z[4 + k] : z[k], fz = sz ? z[k] : z[4 + k];
-        const float l0 = fmaxf(fmaxf(fmaf(nx, r.inv_d.x, ox), fmaf(ny, r.inv_d.y, oy)), fmaxf(fmaf(nz, r.inv_d.z, oz), 0.0f));
-        const float hi = fminf(fminf(fmaf(fx, r.inv_d.x, ox), fmaf(fy, r.inv_d.y, oy)), fmaf(fz, r.inv_d.z, oz));
+        const float l0 = fmaxf(fmaxf(fmaf(qplane(nx, k), ix, bx), fmaf(qplane(ny, k), iy, by)),
+                               fmaxf(fmaf(qplane(nz, k), iz, bz), 0.0f));
+        const float hi = fminf(fminf(fmaf(qplane(fx, k), ix, bx), fmaf(qplane(fy, k), iy, by)),
+                               fmaf(qplane(fz, k), iz, bz));
         return (hi < l0 || l0 > tmax) ? inf : l0;
     };
     t0 = one(0);
@@ -1149,7 +1177,7 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
     return cudaSuccess;
 }
 
-cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, Wide4Node* d_wide4,
+cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int null_leaf, Wide4Node* d_wide4,
                               int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
                               cudaStream_t stream)
 {
@@ -1197,7 +1225,8 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tri
     dense_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4, dense4);
     const int inline_ok = n_tris < (1 << 27) ? 1 : 0;
     *leaf_inline_host = inline_ok;
-    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, sel, d_wide4, inline_ok);
+    const int null_link = inline_ok ? ~(null_leaf << 4) : ~null_leaf;
+    wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, sel, d_wide4, inline_ok, null_link);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     int last_d = 0, last_v = 0;

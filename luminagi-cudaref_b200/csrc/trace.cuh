@@ -22,19 +22,24 @@ struct alignas(16) WideNode
 };
 static_assert(sizeof(WideNode) == 64, "WideNode is one 64-byte record");
 
-// A 4-wide node collapsed from two levels of the binary BVH: the boxes of up
-// to four children, struct-of-arrays in one 128-byte line (eight 16-byte
-// loads).  Links as in WideNode; an absent child has the empty box
-// [+inf, -inf] and the link kEmptyLink, which traversal treats as the end of
-// the ray's traversal, so even a box test that let it through reads nothing.
-struct alignas(16) Wide4Node
+// A 4-wide record: up to four children of a render-tree node, their boxes
+// quantized to 8 bits per plane on a per-record grid (64 B, two 32-byte
+// loads).  Per axis a the grid has origin o[a] and a power-of-two step
+// step[a]; child k's min plane is o[a] + q * step[a] for q = byte k of
+// qlo[a], its max plane likewise from qhi[a].  Quantized planes lie at least
+// one step outside the child's exact box, so every ray that enters the exact
+// box enters the quantized one.  An absent child has qlo = 255, qhi = 0 (an
+// inverted box) and a link to an empty leaf, so even a test that let it
+// through costs one visit of a leaf with no triangles.  Links as in WideNode.
+struct alignas(32) Wide4Node
 {
-    float4 lox, hix, loy, hiy, loz, hiz;  // child i in component i
-    int4 link;
-    int4 pad;
+    float o[3];
+    float step[3];
+    uint32_t qlo[3];
+    uint32_t qhi[3];
+    int link[4];
 };
-static_assert(sizeof(Wide4Node) == 128, "Wide4Node is one 128-byte line");
-constexpr int kEmptyLink = (int)0x80000000;
+static_assert(sizeof(Wide4Node) == 64, "Wide4Node is two 32-byte halves");
 
 // Intersection record of one triangle: kTriVec float4s, v0 (w = material
 // bits), e1 = v1 - v0, e2 = v2 - v0 (v0, v1, v2 in watertight mode), then
@@ -119,7 +124,8 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
 // children are the next records.  Records are numbered by the BFS rank of
 // their nodes (deterministic).  Must follow build_wide_nodes on the same
 // scratch (it reuses the leaf numbering).  Scratch: 11 * n_nodes + 256 ints.
-cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, Wide4Node* d_wide4,
+// null_leaf: the index of a leaf-table entry (0, 0) for absent children.
+cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int null_leaf, Wide4Node* d_wide4,
                               int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
                               cudaStream_t stream);
 // Intersection records, 3 float4 per triangle (w of the first = material):
