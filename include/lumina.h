@@ -201,14 +201,14 @@ int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_
  * lanes have finished their rays, those lanes shade and start their next
  * ray while the others keep traversing.  32 waits for the whole warp (one
  * warp-wide traversal per path step).  Images do not depend on it. */
-#define LG_REFILL_DEFAULT 16
+#define LG_REFILL_DEFAULT 12
 int lg_renderer_set_refill_threshold(lg_renderer* r, int threshold);
 int lg_renderer_get_refill_threshold(const lg_renderer* r);
 /* Leaf postponement of the persistent trace launch.  A lane that reaches a
  * BVH leaf holds it and keeps visiting records; the warp tests the held
  * leaves together once at most `quorum` of its lanes are still looking for
  * one (0 = all lanes hold a leaf or are done).  Images do not depend on it. */
-#define LG_LEAF_QUORUM_DEFAULT 8
+#define LG_LEAF_QUORUM_DEFAULT 12
 int lg_renderer_set_leaf_quorum(lg_renderer* r, int quorum);
 int lg_renderer_get_leaf_quorum(const lg_renderer* r);
 /* Diffuse texture of one material (load_texture_to_device + sample_albedo,

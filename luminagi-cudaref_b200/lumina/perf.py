@@ -158,8 +158,8 @@ def main(argv=None):
     ap.add_argument("--bounces", type=int, default=2)
     ap.add_argument("--width", type=int, default=4)
     ap.add_argument("--reps", type=int, default=10)
-    ap.add_argument("--refill", default="16", help="trace: refill threshold(s), comma-separated")
-    ap.add_argument("--quorum", default="8", help="trace: leaf quorum(s), comma-separated")
+    ap.add_argument("--refill", default="12", help="trace: refill threshold(s), comma-separated")
+    ap.add_argument("--quorum", default="12", help="trace: leaf quorum(s), comma-separated")
     ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)
     print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch}[a.what](a)))

@@ -200,7 +200,7 @@ def test_trace_schedule_does_not_change_images(small_engine_scene, width):
     with lumina.Renderer(0) as r:
         r.set_scene(small_engine_scene)
         r.set_bvh_width(width)
-        assert r.refill_threshold() == 16 and r.leaf_quorum() == 8
+        assert r.refill_threshold() == 12 and r.leaf_quorum() == 12
         for th, qu in ((32, 0), (1, 0), (7, 3), (16, 8), (16, 31), (32, 31)):
             r.set_refill_threshold(th)
             r.set_leaf_quorum(qu)
