@@ -46,9 +46,9 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 470.0 MB + 63.1 MB / 65,366,791 rays
+# of an 8-spp engine frame: 479.4 MB + 60.2 MB / 65,366,791 rays
 # (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = 533.148672e6 / 65366791
+TRACE_DRAM_BYTES_PER_RAY = 539.592704e6 / 65366791
 # Bytes one traversal step uses from a BVH record: 4-wide, the grid origin and
 # steps (16 B), 24 one-byte planes and four links (16 B); 2-wide, the whole
 # 64-B record.
