@@ -211,6 +211,13 @@ int lg_renderer_get_refill_threshold(const lg_renderer* r);
 #define LG_LEAF_QUORUM_DEFAULT 12
 int lg_renderer_set_leaf_quorum(lg_renderer* r, int quorum);
 int lg_renderer_get_leaf_quorum(const lg_renderer* r);
+/* Autotuner of the trace schedule: renders `cam` at spp/max_bounces with each
+ * pair of refill threshold (8, 12, 16, 24) and leaf quorum (4, 8, 12, 16),
+ * keeps the fastest pair for later frames and reports it (and its kernel
+ * time) through the optional outputs.  Images do not depend on the choice
+ * beyond exact ties. */
+int lg_renderer_autotune_schedule(lg_renderer* r, const lg_camera* cam, int spp, int max_bounces,
+                                  int32_t* refill, int32_t* quorum, float* ms);
 /* Diffuse texture of one material (load_texture_to_device + sample_albedo,
  * src/pathtracer.cu:553-579, 274-282): w x h RGBA8 host pixels, sampled as
  * sRGB with bilinear filtering and wrapping at uv (u, 1 - v).  rgba8 = NULL

@@ -856,6 +856,51 @@ int lg_renderer_autotune(lg_renderer* r, const lg_camera* cam, int spp, int max_
     return LG_OK;
 }
 
+int lg_renderer_autotune_schedule(lg_renderer* r, const lg_camera* cam, int spp, int max_bounces,
+                                  int32_t* refill_out, int32_t* quorum_out, float* ms_out)
+{
+    if (!r || !cam || spp <= 0 || max_bounces < 0) return set_error(LG_ERR_INVALID, "bad argument");
+    DeviceGuard g(r->device);
+    const int saved_refill = r->trace_refill, saved_quorum = r->trace_quorum;
+    const bool counting = r->counting;
+    r->counting = false;
+    // Candidates around the engine-scene optimum (refill 12, quorum 12); one
+    // untimed render, then the fastest of two timed ones per pair.
+    static const int kRefill[] = {8, 12, 16, 24};
+    static const int kQuorum[] = {4, 8, 12, 16};
+    int best_refill = saved_refill, best_quorum = saved_quorum;
+    float best_ms = 1e30f;
+    int rc = LG_OK;
+    for (int fi = 0; fi < 4 && rc == LG_OK; ++fi)
+        for (int qi = 0; qi < 4 && rc == LG_OK; ++qi)
+        {
+            r->trace_refill = kRefill[fi];
+            r->trace_quorum = kQuorum[qi];
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && rc == LG_OK; ++rep)
+            {
+                lg_render_opts o{spp, max_bounces, 0, 0};
+                lg_render_stats st{};
+                rc = render_into_device(r, cam, &o, &st);
+                if (rc == LG_OK && rep > 0) ms = std::min(ms, st.kernel_ms);
+            }
+            if (rc == LG_OK && ms < best_ms)
+            {
+                best_ms = ms;
+                best_refill = kRefill[fi];
+                best_quorum = kQuorum[qi];
+            }
+        }
+    r->counting = counting;
+    r->trace_refill = rc == LG_OK ? best_refill : saved_refill;
+    r->trace_quorum = rc == LG_OK ? best_quorum : saved_quorum;
+    if (rc != LG_OK) return rc;
+    if (refill_out) *refill_out = best_refill;
+    if (quorum_out) *quorum_out = best_quorum;
+    if (ms_out) *ms_out = best_ms;
+    return LG_OK;
+}
+
 int lg_renderer_set_refill_threshold(lg_renderer* r, int threshold)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");

@@ -107,6 +107,8 @@ SIGNATURES = {
     "lg_renderer_get_leaf_quorum": (_I, [_P]),
     "lg_renderer_get_render_tree": (_I, [_P, C.POINTER(C.c_int32)]),
     "lg_renderer_autotune": (_I, [_P, C.POINTER(LgCamera), _I, _I, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "lg_renderer_autotune_schedule": (_I, [_P, C.POINTER(LgCamera), _I, _I, C.POINTER(C.c_int32),
+                                           C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "lg_renderer_set_texture": (_I, [_P, _I, _P, C.c_int32, C.c_int32]),
     "lg_renderer_load_textures": (_I, [_P, _P, C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "lg_render": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, _P, C.POINTER(LgRenderStats)]),

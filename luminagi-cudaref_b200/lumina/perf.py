@@ -135,10 +135,16 @@ def batch(a):
     cams = [sc.camera.look_at(p, t) for p, t in orbit_poses(a.poses, seed=11, center=ENGINE_CENTER)]
     n = len(cams)
     spps, bounces = [a.spp] * n, [a.bounces] * n
+    tuned = None
+    if a.tune:
+        # the persistent launch's occupancy and schedule, tuned on the first pose
+        bps, _ = r.autotune(camera=cams[0], spp=a.spp, bounces=a.bounces)
+        refill, quorum, _ = r.autotune_schedule(camera=cams[0], spp=a.spp, bounces=a.bounces)
+        tuned = {"blocks_per_sm": bps, "refill": refill, "quorum": quorum}
     r.render_batch(cams, spps, bounces)  # capture
     _, ms = r.render_batch(cams, spps, bounces)
     sep = [r.render(camera=c, spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for c in cams]
-    out = {"kernel": "trace (batched)", "poses": n, "spp": a.spp, "bounces": a.bounces,
+    out = {"kernel": "trace (batched)", "poses": n, "spp": a.spp, "bounces": a.bounces, "tuned": tuned,
            "batch_ms_per_frame": float(ms.sum()) / n, "separate_ms_per_frame": float(np.sum(sep)) / n}
     out["speedup"] = out["separate_ms_per_frame"] / out["batch_ms_per_frame"]
     r.close()
@@ -160,6 +166,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--refill", default="12", help="trace: refill threshold(s), comma-separated")
     ap.add_argument("--quorum", default="12", help="trace: leaf quorum(s), comma-separated")
+    ap.add_argument("--tune", type=int, default=1, help="batch: autotune the launch and schedule first (1/0)")
     ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)
     print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch}[a.what](a)))

@@ -110,6 +110,14 @@ class Renderer:
         check(lib().lg_renderer_autotune(self._h, C.byref(cam), spp, bounces, C.byref(b), C.byref(ms)))
         return int(b.value), float(ms.value)
 
+    def autotune_schedule(self, camera: Camera | None = None, spp: int = 8, bounces: int = 2):
+        """Picks the refill threshold and leaf quorum by timing; returns (refill, quorum, ms)."""
+        cam = (camera if camera is not None else self.scene.camera).to_c()
+        f, q, ms = C.c_int32(0), C.c_int32(0), C.c_float(0)
+        check(lib().lg_renderer_autotune_schedule(self._h, C.byref(cam), spp, bounces, C.byref(f), C.byref(q),
+                                                  C.byref(ms)))
+        return int(f.value), int(q.value), float(ms.value)
+
     def set_refill_threshold(self, threshold: int) -> None:
         """Finished rays per warp (1..32) after which those lanes shade and start their next ray."""
         check(lib().lg_renderer_set_refill_threshold(self._h, int(threshold)))

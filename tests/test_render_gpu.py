@@ -190,6 +190,20 @@ def test_trace_grid_autotune(box_scene):
     assert np.array_equal(before["accum"], after["accum"])
 
 
+def test_schedule_autotune(small_engine_scene):
+    """lg_renderer_autotune_schedule times refill thresholds and leaf quorums
+    on the caller's camera and keeps the fastest pair; the image matches the
+    one rendered before tuning (the quorum may change exact ties only)."""
+    with lumina.Renderer(0) as r:
+        r.set_scene(small_engine_scene)
+        before = r.render(spp=8, bounces=2)
+        refill, quorum, ms = r.autotune_schedule(spp=8, bounces=2)
+        assert refill in (8, 12, 16, 24) and quorum in (4, 8, 12, 16) and ms > 0
+        assert (r.refill_threshold(), r.leaf_quorum()) == (refill, quorum)
+        after = r.render(spp=8, bounces=2)
+    assert match_fraction(after["accum"], before["accum"]) >= 0.9999
+
+
 @pytest.mark.parametrize("width", [2, 4])
 def test_trace_schedule_does_not_change_images(small_engine_scene, width):
     """The warp refills lanes whose rays finished once `threshold` of them
