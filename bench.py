@@ -285,6 +285,8 @@ def main():
     r = lumina.Renderer(dev)
     r.set_scene(scene)
     nodes_dev, tris_dev = r.get_bvh()
+    cfg["trace"] = {"records": "4-wide, 8-bit quantized planes, 64 B", "render_tree": r.render_tree(),
+                    "refill_threshold": r.refill_threshold(), "leaf_quorum": r.leaf_quorum()}
 
     # counting pass (not timed)
     r.set_counting(True)
