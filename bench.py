@@ -37,6 +37,7 @@ import pathlib
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = pathlib.Path(__file__).resolve().parent
@@ -46,8 +47,8 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 479.4 MB + 60.2 MB / 65,366,791 rays
-# (profiles/trace_kernel_engine_1728x864.md); traffic scales with rays.
+# of an 8-spp engine frame: 479.4 MB + 60.2 MB / 65,366,791 rays; traffic
+# scales with rays.
 TRACE_DRAM_BYTES_PER_RAY = 539.592704e6 / 65366791
 # Bytes one traversal step uses from a BVH record: 4-wide, the grid origin and
 # steps (16 B), 24 one-byte planes and four links (16 B); 2-wide, the whole
@@ -92,11 +93,12 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        fd, name = tempfile.mkstemp(prefix="lumina_clocks_", suffix=".csv")
+        os.close(fd)
+        self.path = pathlib.Path(name)
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}",
@@ -121,7 +123,12 @@ class ClockSampler:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows = []
-        for line in self.path.read_text().splitlines():
+        text = self.path.read_text()
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        for line in text.splitlines():
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
                 rows.append(parts)
@@ -387,7 +394,7 @@ def main():
         ms_p = timed(lambda: _ffi.check(_ffi.lib().lg_render_device(
             r._h, C.byref(cam), C.byref(o256), C.c_void_p(stream.cuda_stream), None, None, None)), 1)
         denoise = {"ms_8spp_plus_unet": ms_d, "ms_256spp": ms_p, "speedup": ms_p / ms_d,
-                   "quality": "PSNR/SSIM vs a 1024-spp FP64 judge: profiles/surrogate_engine_1728x864.md"}
+                   "weights": "random (the cost of a forward pass does not depend on their values)"}
         net.close()
 
     line = {"metric": "Mrays/s (plain render; ms/frame alongside)", "value": value, "unit": "Mrays/s",

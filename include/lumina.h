@@ -122,8 +122,14 @@ int lg_build_bvh_device(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* 
  * GPU that loads it, so at most LG_NOALLOC_MAX_TRIS triangles are accepted
  * (larger inputs return LG_ERR_CAPACITY).  The first call on a device looks
  * up the array's address for that device; make it before any stream capture.
- * All calls share the one array: calls whose work overlaps on the GPU (other
- * threads, other streams) race and must be serialised by the caller. */
+ * Under lazy module loading (CUDA's default since 12.2) that first call is
+ * also when the array is loaded and its 14 MB are taken from the device, so
+ * a host that reserves all device memory for its own allocator should make
+ * one call on each device before it does (or set CUDA_MODULE_LOADING=EAGER).
+ * Every call synchronises `stream` before it returns: it reads the node count
+ * back to the host.  All calls share the one array: calls whose work overlaps
+ * on the GPU (other threads, other streams) race and must be serialised by
+ * the caller. */
 #define LG_NOALLOC_MAX_TRIS 65536
 int lg_build_bvh_device_noalloc(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* d_nodes_out,
                                 int32_t* n_nodes_out, int32_t* d_perm_out, lg_triangle* d_tris_out, void* stream);

@@ -117,6 +117,10 @@ struct lg_renderer
     int trace_quorum = LG_LEAF_QUORUM_DEFAULT;  // searching lanes below which a warp tests its held leaves (0..31)
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
+    // Traversal-stack overflow word (DevScene::fault) and its pinned host
+    // copy, refreshed by an asynchronous copy after every trace launch.
+    DevBuf fault;
+    unsigned* fault_host = nullptr;
     // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
     std::vector<cudaArray_t> tex_arrays;
     std::vector<unsigned long long> tex_objs;  // cudaTextureObject_t, 0 = untextured
@@ -288,7 +292,31 @@ DevScene dev_scene(const lg_renderer* r)
     s.root4 = r->root4;
     s.leaf_inline = r->leaf_inline;
     s.sun = r->sun;
+    s.fault = r->fault.as<unsigned>();
     return s;
+}
+
+// Queues a copy of the device fault word into its pinned host copy, after
+// the launches already on `st`.
+cudaError_t post_fault(lg_renderer* r, cudaStream_t st)
+{
+    return cudaMemcpyAsync(r->fault_host, r->fault.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+}
+
+// Reports a traversal-stack overflow recorded by a finished launch and clears
+// the word.  The fast path reads the pinned copy only; a set word is rare, and
+// then the stream is drained first so no copy still in flight can set it again.
+int take_fault(lg_renderer* r)
+{
+    if (!*(volatile unsigned*)r->fault_host) return LG_OK;
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    LG_TRY_CUDA(cudaMemsetAsync(r->fault.p, 0, sizeof(unsigned), r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    *(volatile unsigned*)r->fault_host = 0u;
+    return set_error(LG_ERR_DEVICE,
+                     "traversal stack overflow: the BVH is deeper than the %d-entry traversal stack holds, so "
+                     "some subtrees were skipped and the image is incomplete",
+                     kTraceStack);
 }
 
 int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* o, lg_render_stats* stats)
@@ -326,9 +354,11 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
     const float inv = 1.0f / (float)o->spp;
     LG_TRY_CUDA(launch_tonemap(r->accum.as<float>(), r->rgb.as<uint8_t>(), nval, inv, r->stream));
     LG_TRY_CUDA(cudaEventRecord(r->ev1, r->stream));
+    LG_TRY_CUDA(post_fault(r, r->stream));
     if (stats)
     {
-        LG_TRY_CUDA(cudaEventSynchronize(r->ev1));
+        LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+        LG_TRY(take_fault(r));
         float ms = 0.0f;
         LG_TRY_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
         stats->kernel_ms = ms;
@@ -613,10 +643,19 @@ int lg_renderer_create(int device, lg_renderer** out)
     r->device = device;
     cudaDeviceGetAttribute(&r->sm_count, cudaDevAttrMultiProcessorCount, device);
     if ((e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&r->ev0)) != cudaSuccess || (e = cudaEventCreate(&r->ev1)) != cudaSuccess)
+        (e = cudaEventCreate(&r->ev0)) != cudaSuccess || (e = cudaEventCreate(&r->ev1)) != cudaSuccess ||
+        (e = cudaMallocHost((void**)&r->fault_host, sizeof(unsigned))) != cudaSuccess)
     {
         lg_renderer_destroy(r);
         return set_error(LG_ERR_CUDA, "renderer init: %s", cudaGetErrorString(e));
+    }
+    *r->fault_host = 0u;
+    if (r->fault.reserve(sizeof(unsigned)) != LG_OK ||
+        (e = cudaMemsetAsync(r->fault.p, 0, sizeof(unsigned), r->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(r->stream)) != cudaSuccess)
+    {
+        lg_renderer_destroy(r);
+        return set_error(LG_ERR_CUDA, "renderer init: fault word: %s", cudaGetErrorString(e));
     }
     *out = r;
     return LG_OK;
@@ -633,6 +672,8 @@ void lg_renderer_destroy(lg_renderer* r)
     r->gbuf.release();
     if (r->batch_exec) cudaGraphExecDestroy(r->batch_exec);
     if (r->batch_host) cudaFreeHost(r->batch_host);
+    if (r->fault_host) cudaFreeHost(r->fault_host);
+    r->fault.release();
     for (DevBuf* b : {&r->batch_jobs, &r->batch_acc, &r->batch_rgb, &r->rnodes, &r->rt_scratch}) b->release();
     for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
@@ -981,6 +1022,8 @@ int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
     DeviceGuard g(r->device);
+    // An overflow in an earlier asynchronous frame is reported here.
+    LG_TRY(take_fault(r));
     // Order the renderer's stream after the caller's stream.
     if (stream)
     {
@@ -999,7 +1042,11 @@ int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
         cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
         cudaEventDestroy(ev);
     }
-    else LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    else
+    {
+        LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+        LG_TRY(take_fault(r));
+    }
     if (d_rgb8) *d_rgb8 = r->rgb.as<uint8_t>();
     if (d_accum) *d_accum = r->accum.as<float>();
     if (d_accum64) *d_accum64 = (o->flags & LG_RENDER_ACCUM64) ? r->accum64.as<double>() : nullptr;
@@ -1096,6 +1143,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
         for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)
             e = launch_tonemap(r->batch_acc.as<float>() + acc_off[(size_t)j], r->batch_rgb.as<uint8_t>() + acc_off[(size_t)j],
                                (long long)(acc_off[(size_t)j + 1] - acc_off[(size_t)j]), 1.0f / (float)opts[j].spp, st);
+        if (e == cudaSuccess) e = post_fault(r, st);
         cudaGraph_t graph = nullptr;
         const cudaError_t ec = cudaStreamEndCapture(st, &graph);
         if (e == cudaSuccess) e = ec;
@@ -1113,6 +1161,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
     LG_TRY_CUDA(cudaEventRecord(r->ev1, r->stream));
     if (rgb8_out) LG_TRY_CUDA(cudaMemcpyAsync(rgb8_out, r->batch_rgb.p, nval, cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    LG_TRY(take_fault(r));
     if (ms_per_job)
     {
         // One launch serves all frames: its time is apportioned by work items.
@@ -1152,11 +1201,13 @@ int lg_render_gbuffer(lg_renderer* r, const lg_camera* cam, uint8_t* albedo, uin
         const vec3 inv = v3(1.0f / std::max(ext.x, 1e-6f), 1.0f / std::max(ext.y, 1e-6f), 1.0f / std::max(ext.z, 1e-6f));
         LG_TRY_CUDA(launch_gbuffer(dev_scene(r), make_dev_cam(*cam), bbMin, inv, base, base + n, base + 2 * n,
                                    r->bvh_width, r->watertight, r->stream));
+        LG_TRY_CUDA(post_fault(r, r->stream));
     }
     if (albedo) LG_TRY_CUDA(cudaMemcpyAsync(albedo, base, n, cudaMemcpyDeviceToHost, r->stream));
     if (normal) LG_TRY_CUDA(cudaMemcpyAsync(normal, base + n, n, cudaMemcpyDeviceToHost, r->stream));
     if (worldpos) LG_TRY_CUDA(cudaMemcpyAsync(worldpos, base + 2 * n, n, cudaMemcpyDeviceToHost, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    LG_TRY(take_fault(r));
     return LG_OK;
 }
 

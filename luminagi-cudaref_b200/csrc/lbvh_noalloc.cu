@@ -8,10 +8,15 @@
 // device memory up front through its own allocator leaves no room for
 // allocations it does not control.  lg_build_bvh_device_noalloc() serves
 // them: its scratch is one fixed array in device global memory, defined
-// below and loaded with the library, so the call itself allocates nothing.
+// below, so the build itself allocates nothing.
 //
 // The array holds LG_NOALLOC_MAX_TRIS triangles' worth of scratch (about
-// 14 MB); every GPU that loads the library keeps it until the process exits.
+// 14 MB); every GPU that loads it keeps it until the process exits.  When it
+// is loaded depends on CUDA's module loading: eagerly (CUDA_MODULE_LOADING=
+// EAGER) with the library's other device code at context creation; lazily
+// (the default since CUDA 12.2) on the first call on each device, when its
+// address is looked up.  A host that later reserves all device memory for
+// its own allocator should therefore make one call on each device first.
 #include <cstdint>
 #include <mutex>
 
@@ -31,13 +36,14 @@ constexpr size_t kNoAllocScratchBytes = 14u << 20;
 // cudaGetSymbolAddress (see scratch_on_device).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch, resolved once per device with that
-// device current.  The first call of the entry point on a device does this.
+// Device address of g_noalloc_scratch, looked up with the device current on
+// the first call on that device and kept once found.  A failed lookup (e.g.
+// no memory left for a lazily loaded module) is not kept: the next call on
+// that device tries again.
 struct DeviceSlot
 {
-    std::once_flag once;
+    std::mutex mu;
     void* ptr = nullptr;
-    cudaError_t err = cudaSuccess;
 };
 DeviceSlot g_slots[64];
 
@@ -47,9 +53,18 @@ int scratch_on_device(void** out)
     LG_TRY_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return lg::set_error(LG_ERR_INVALID, "device ordinal %d not supported", dev);
     DeviceSlot& s = g_slots[dev];
-    std::call_once(s.once, [&] { s.err = cudaGetSymbolAddress(&s.ptr, g_noalloc_scratch); });
-    if (s.err != cudaSuccess)
-        return lg::set_error(LG_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch): %s", cudaGetErrorString(s.err));
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.ptr)
+    {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+        {
+            cudaGetLastError();  // the lookup's error is reported here, not left to a later call
+            return lg::set_error(LG_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch): %s", cudaGetErrorString(e));
+        }
+        s.ptr = p;
+    }
     *out = s.ptr;
     return LG_OK;
 }

@@ -60,14 +60,18 @@ void reserve_triangles(std::vector<Triangle>& v, size_t n)
     if (e > a) ::madvise(reinterpret_cast<void*>(a), e - a, MADV_HUGEPAGE);
 #endif
 }
+// n default-valued records (Triangle{}: zero vertices, normals and uvs,
+// material 0).  The value-initialisation writes every page once on the
+// calling thread, which is where the huge-page hint above pays.
 void size_triangles(std::vector<Triangle>& v, size_t n)
 {
     reserve_triangles(v, n);
+    v.clear();
     v.resize(n);
 }
 
-// Copies n triangle records with up to 16 host threads (the destination pages
-// are faulted by the copy; spreading it over threads spreads the faults).
+// Copies n triangle records with up to 16 host threads (the pages are
+// already faulted in by size_triangles; the threads split the copy itself).
 void copy_triangles(Triangle* dst, const void* src, size_t n)
 {
     const size_t bytes = n * sizeof(Triangle);
@@ -679,7 +683,6 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
             if (v.peek() != '[') v.fail("triangles must be an array");
             const size_t n = tri_starts.size();
             size_triangles(out.triangles, n);
-            std::fill(out.triangles.begin(), out.triangles.end(), Triangle{});
             int nt = nt_all;
             const size_t min_per_thread = 16384;
             if ((size_t)nt > n / min_per_thread + 1) nt = (int)(n / min_per_thread + 1);

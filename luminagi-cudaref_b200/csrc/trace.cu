@@ -43,7 +43,7 @@ namespace lg
 {
 namespace
 {
-constexpr int kStack = 64;
+constexpr int kStack = kTraceStack;
 constexpr int kMaxLevels = 128;  // depth limit of the 4-wide collapse (the reference tree is at most ~31 deep)
 constexpr int kTraceThreads = 256;
 constexpr int kTraceMinBlocks = 4;
@@ -503,6 +503,21 @@ __device__ __forceinline__ void trav_begin(Trav& q, int root, float tmax, bool a
 
 __device__ __forceinline__ int pop(Trav& q, const int* stack) { return q.sp == 0 ? kDone : stack[--q.sp]; }
 
+// Stacks `link`; a push past kStack entries is dropped and flags the scene's
+// fault word (the host turns it into LG_ERR_DEVICE), so a tree too deep for
+// the stack never yields a silently incomplete image.
+template <bool kCount>
+__device__ __forceinline__ void push(Trav& q, int* stack, int link, const DevScene& s, Counters& cnt)
+{
+    if (q.sp < kStack)
+    {
+        stack[q.sp++] = link;
+        return;
+    }
+    if (kCount) cnt.overflow++;
+    *s.fault = 1u;
+}
+
 // The four boxes of a quantized 4-wide record against one ray.  Per axis,
 // t(q) = q * (step / d) + (origin - o) / d: the step is a power of two, so
 // the first product is exact, and each plane costs a byte-to-float
@@ -581,9 +596,9 @@ __device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav&
         if (t0 != inf)
         {
             // push farthest first so the nearest remaining is on top
-            if (t3 != inf) { if (q.sp < kStack) stack[q.sp++] = l3; else if (kCount) cnt.overflow++; }
-            if (t2 != inf) { if (q.sp < kStack) stack[q.sp++] = l2; else if (kCount) cnt.overflow++; }
-            if (t1 != inf) { if (q.sp < kStack) stack[q.sp++] = l1; else if (kCount) cnt.overflow++; }
+            if (t3 != inf) push<kCount>(q, stack, l3, s, cnt);
+            if (t2 != inf) push<kCount>(q, stack, l2, s, cnt);
+            if (t1 != inf) push<kCount>(q, stack, l1, s, cnt);
             q.cur = l0;
             return;
         }
@@ -600,8 +615,7 @@ __device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav&
         if (h0 && h1)
         {
             const bool swap = t1 < t0;
-            if (q.sp < kStack) stack[q.sp++] = swap ? ln.x : ln.y;
-            else if (kCount) cnt.overflow++;
+            push<kCount>(q, stack, swap ? ln.x : ln.y, s, cnt);
             q.cur = swap ? ln.y : ln.x;
             return;
         }
@@ -832,6 +846,7 @@ struct PathState
     Ray ray;
     float tmax;
     vec3 L, throughput, P, N, albedo, color, contrib, sum;
+    double sum64x, sum64y, sum64z;  // judge images only: the same chunk sum, each sample added in FP64
     uint32_t rng;
     int px, py, k, n_this, bounce, li;  // li: -1 camera/bounce ray in flight, >= 0 shadow ray of light li
     unsigned pixel;                     // index of the pixel's first accumulator value
@@ -865,7 +880,9 @@ __device__ __forceinline__ void start_sample(PathState& st, const DevCam& cam)
 }
 
 // Consumes the result of the ray in flight and sets up the next one.
-// Returns false when the chunk's last sample has finished.
+// Returns false when the chunk's last sample has finished.  kAcc64: every
+// sample's radiance is also added to an FP64 chunk sum.
+template <bool kAcc64>
 __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const DevCam& cam, int maxBounces, int tri,
                                         float hitT, float hitU, float hitV)
 {
@@ -923,6 +940,12 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
         }
     }
     st.sum = vadd(st.sum, st.L);
+    if (kAcc64)
+    {
+        st.sum64x += (double)st.L.x;
+        st.sum64y += (double)st.L.y;
+        st.sum64z += (double)st.L.z;
+    }
     if (++st.k == st.n_this) return false;
     start_sample(st, cam);
     return true;
@@ -992,6 +1015,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
                         const int sampleBase = sbase + first;
                         st.rng = (uint32_t)(st.px * 1973 + st.py * 9277 + sampleBase * 26699) | 1u;
                         st.sum = v3(0, 0, 0);
+                        st.sum64x = st.sum64y = st.sum64z = 0.0;
                         st.k = 0;
                         st.pixel = (unsigned)((st.py * c.width + st.px) * 3);
                         start_sample(st, c);
@@ -1016,7 +1040,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         if (active && tdone)
         {
             const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
-            if (advance(st, s, c, kBatch ? st.max_bounces : job.max_bounces, q.tri, q.t, q.u, q.v))
+            if (advance<kAcc64>(st, s, c, kBatch ? st.max_bounces : job.max_bounces, q.tri, q.t, q.u, q.v))
             {
                 trav_begin<kCount>(q, root, st.tmax, st.li >= 0, cnt);
                 tdone = false;
@@ -1046,9 +1070,9 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
                 }
                 if (kAcc64)
                 {
-                    atomicAdd(&job.accum64[i + 0], (double)st.sum.x);
-                    atomicAdd(&job.accum64[i + 1], (double)st.sum.y);
-                    atomicAdd(&job.accum64[i + 2], (double)st.sum.z);
+                    atomicAdd(&job.accum64[i + 0], st.sum64x);
+                    atomicAdd(&job.accum64[i + 1], st.sum64y);
+                    atomicAdd(&job.accum64[i + 2], st.sum64z);
                 }
             }
         }

@@ -46,6 +46,9 @@ static_assert(sizeof(Wide4Node) == 64, "Wide4Node is two 32-byte halves");
 // padding, so a record starts on a 32-byte boundary when kTriVec == 4.
 constexpr int kTriVec = 4;
 
+// Entries of a ray's traversal stack (per thread, local memory).
+constexpr int kTraceStack = 64;
+
 struct DevScene
 {
     const Wide4Node* nodes4;   // 4-wide records (used when width == 4)
@@ -61,6 +64,11 @@ struct DevScene
     int n_points;
     int root;                  // root link (0 = internal record 0, < 0 = leaf)
     lg_dir_light sun;
+    // Set to 1 by any traversal that had to drop a stack push (the tree is
+    // deeper than the stack allows and the image would be incomplete).  It
+    // stays set until the host reads and clears it; the store only runs on
+    // overflow, so the check costs nothing otherwise.
+    unsigned* fault;
 };
 
 struct DevCam

@@ -5,6 +5,7 @@ Known answers: the reference's published numbers for its shipped renders
 PSNR 34.52 / 42.04 / 49.57 dB, MAD 3.25 / 1.39 / 0.51, SSIM 0.815 / 0.964 /
 0.991 (three decimals) -- checked when the reference checkout is present,
 plus closed-form cases that always run."""
+import os
 import pathlib
 
 import numpy as np
@@ -12,7 +13,8 @@ import pytest
 
 from lumina import metrics as M
 
-EVAL = pathlib.Path("/root/reference/ml/eval")
+# The reference checkout (same variable as oracle/Makefile); its shipped renders sit under ml/eval.
+EVAL = pathlib.Path(os.environ.get("REF", "/root/reference")) / "ml" / "eval"
 KAT = [("noisy_8", 34.52, 3.25, 0.815), ("denoised", 42.04, 1.39, 0.964), ("clean_256", 49.57, 0.51, 0.991)]
 
 

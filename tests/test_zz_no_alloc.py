@@ -30,18 +30,24 @@ def _soup(n, seed):
     return t
 
 
-def _build(fn_name, d_tris, n, torch):
+def _build(fn_name, d_tris, n, torch, out="separate"):
+    """Calls fn_name through the C ABI; out selects where the reordered
+    triangles go: a separate buffer, nowhere (NULL), or back into d_tris."""
     d_nodes = torch.zeros(max(2 * n - 1, 1) * NODE_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
     d_perm = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
     d_out = torch.zeros(max(n, 1) * TRI_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    out_ptr = {"separate": C.c_void_p(d_out.data_ptr()), "none": None,
+               "inplace": C.c_void_p(d_tris.data_ptr())}[out]
     count = C.c_int32(-1)
     stream = torch.cuda.current_stream().cuda_stream
     fn = getattr(_ffi.lib(), fn_name)
     _ffi.check(fn(C.c_void_p(d_tris.data_ptr()), n, C.c_void_p(d_nodes.data_ptr()), C.byref(count),
-                  C.c_void_p(d_perm.data_ptr()), C.c_void_p(d_out.data_ptr()), C.c_void_p(stream)))
+                  C.c_void_p(d_perm.data_ptr()), out_ptr, C.c_void_p(stream)))
     torch.cuda.synchronize()
     nodes = d_nodes.cpu().numpy().view(NODE_DTYPE)[: count.value]
-    return nodes, d_perm.cpu().numpy()[:n], d_out.cpu().numpy().view(TRI_DTYPE)[:n]
+    tris_out = {"separate": d_out, "none": None, "inplace": d_tris}[out]
+    tris_np = tris_out.cpu().numpy().view(TRI_DTYPE)[:n] if tris_out is not None else None
+    return nodes, d_perm.cpu().numpy()[:n], tris_np
 
 
 def test_noalloc_build_matches_allocating_build_twice():
@@ -70,3 +76,22 @@ def test_noalloc_build_rejects_oversize_input():
                                                 C.byref(count), None, None, None)
     assert rc == _ffi.LG_ERR_CAPACITY
     assert b"limit" in _ffi.lib().lg_last_error()
+
+
+def test_noalloc_build_at_the_limit_in_every_output_layout():
+    """LG_NOALLOC_MAX_TRIS triangles, with the reordered triangles written to a
+    separate buffer, not written (NULL), and written back over the input: the
+    last two stage the sorted triangles inside the fixed array, its largest
+    layout.  Nodes and permutation must equal the allocating build's, and the
+    in-place triangles its separate output."""
+    torch = pytest.importorskip("torch")
+    n = LG_NOALLOC_MAX_TRIS
+    tris = _soup(n, 11)
+    src = torch.from_numpy(tris.view(np.uint8).copy()).cuda()
+    ref = _build("lg_build_bvh_device", src.clone(), n, torch)
+    for out in ("none", "inplace", "separate"):
+        got = _build("lg_build_bvh_device_noalloc", src.clone(), n, torch, out=out)
+        assert got[0].tobytes() == ref[0].tobytes(), out
+        assert (got[1] == ref[1]).all(), out
+        if got[2] is not None:
+            assert got[2].tobytes() == ref[2].tobytes(), out
