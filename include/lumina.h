@@ -14,6 +14,7 @@
  *   lg_build_bvh            BuildBVH                      src/bvh.cpp:164-211
  *   lg_build_bvh_device     BuildBVH, device-resident in/out
  *   lg_renderer_*, lg_render RenderSceneCUDA              src/pathtracer.cu:581-757
+ *   lg_render_sorted        RenderSceneCUDASorted         src/pathtracer.cu:759-909 (cuda_ref --sort)
  *   lg_render_batch         cuda_ref --batch job loop     src/main.cpp:158-190
  *   lg_tonemap_device       tonemap_kernel                src/pathtracer.cu:413-429
  *   lg_look_at              overwrite_camera              src/main.cpp:29-59
@@ -138,6 +139,7 @@ int lg_build_bvh_device_noalloc(const lg_triangle* d_tris, int32_t n_tris, lg_bv
 typedef struct lg_renderer lg_renderer;
 
 #define LG_RENDER_ACCUM64 1u   /* keep an FP64 per-pixel accumulator (judge images) */
+#define LG_RENDER_NO_RAY_SORT 2u /* lg_render_sorted only: same launches, rays left in pixel order */
 
 typedef struct {
     int32_t spp;           /* samples per pixel (chunks of 8 share one RNG stream, as in the reference) */
@@ -243,6 +245,21 @@ int lg_render(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, 
  * renderer until the next call; pointers are returned (any may be NULL). */
 int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, void* stream,
                      const uint8_t** d_rgb8, const float** d_accum, const double** d_accum64);
+/* The reference's ray-sorted render (RenderSceneCUDASorted,
+ * src/pathtracer.cu:431-547 and 759-909; the CLI's --sort), with its own
+ * estimator: per sample, a camera ray per pixel seeded (px*1973 + py*9277 +
+ * (sample_base + sample)*26699) | 1; the rays sorted stably by a 30-bit
+ * Morton code of their direction; per bounce every live ray traced, its
+ * throughput x direct light (sun and point lights, a shadow ray each) added
+ * to its pixel, and its next ray (cosine-weighted, no Russian roulette)
+ * sorted again.  Draws after the camera jitter come from the RNG state of
+ * the ray's sorted slot, as in the reference, so the sort order is part of
+ * the image.  opts->flags may hold LG_RENDER_NO_RAY_SORT (rays stay in pixel
+ * order: the same launches without the sorts, a different image of the same
+ * estimator).  rgb8 / accum: host buffers as lg_render; stats->kernel_ms is
+ * the device time of every launch of the frame. */
+int lg_render_sorted(lg_renderer* r, const lg_camera* cam, const lg_render_opts* opts, uint8_t* rgb8, float* accum,
+                     lg_render_stats* stats);
 /* n_jobs frames (per-job camera, size, spp, bounces, sample_base) traced in
  * ONE persistent launch: the (pixel, chunk of 8 samples) items of all frames
  * share one work counter, so the GPU stays full across frames.  The job-table
@@ -352,6 +369,15 @@ int lg_f32_tonemap_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, 
  * (n_crops x 3 x crop x crop). */
 int lg_gather_crops(const float* d_images, int n_images, int h, int w, const int32_t* img_idx, const int32_t* ys,
                     const int32_t* xs, int n_crops, int crop, float* d_out, void* stream);
+
+/* ---- measurement ----
+ * No counterpart in the reference.  Read bandwidth of one memory level on
+ * `device`, in GB/s, for roofline denominators: level 2 reads a `bytes`
+ * buffer (choose one that fits in L2) `passes` times with L2-only loads;
+ * level 1 has every block read the same `bytes` region (at most 48 KB)
+ * `passes` times through the read-only L1 path.  Allocates and frees its
+ * own buffers; synchronous. */
+int lg_measure_read_bandwidth(int device, int level, int64_t bytes, int passes, double* gbs);
 
 /* ---- image output ---- */
 int lg_write_png(const char* path, int32_t w, int32_t h, const uint8_t* rgb8);

@@ -18,6 +18,7 @@
 #include "render_tree.cuh"
 #include "scene.h"
 #include "trace.cuh"
+#include "wavefront.cuh"
 
 namespace lg
 {
@@ -121,6 +122,7 @@ struct lg_renderer
     // copy, refreshed by an asynchronous copy after every trace launch.
     DevBuf fault;
     unsigned* fault_host = nullptr;
+    DevBuf wf_scratch;  // ray-sorted render: rays, keys, slots, RNG states, sort buffers
     // diffuse textures, per material (load_texture_to_device, pathtracer.cu:553-579)
     std::vector<cudaArray_t> tex_arrays;
     std::vector<unsigned long long> tex_objs;  // cudaTextureObject_t, 0 = untextured
@@ -674,7 +676,8 @@ void lg_renderer_destroy(lg_renderer* r)
     if (r->batch_host) cudaFreeHost(r->batch_host);
     if (r->fault_host) cudaFreeHost(r->fault_host);
     r->fault.release();
-    for (DevBuf* b : {&r->batch_jobs, &r->batch_acc, &r->batch_rgb, &r->rnodes, &r->rt_scratch}) b->release();
+    for (DevBuf* b : {&r->batch_jobs, &r->batch_acc, &r->batch_rgb, &r->rnodes, &r->rt_scratch, &r->wf_scratch})
+        b->release();
     for (DevBuf* b : {&r->tris, &r->tris_in, &r->nodes, &r->wide, &r->wide4, &r->leaves, &r->tv, &r->mats, &r->points,
                       &r->scratch, &r->accum, &r->accum64, &r->rgb, &r->work, &r->counters})
         b->release();
@@ -1053,6 +1056,64 @@ int lg_render_device(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
     return LG_OK;
 }
 
+int lg_render_sorted(lg_renderer* r, const lg_camera* cam, const lg_render_opts* o, uint8_t* rgb8, float* accum,
+                     lg_render_stats* stats)
+{
+    if (!r || !cam || !o) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (cam->width <= 0 || cam->height <= 0) return set_error(LG_ERR_INVALID, "image size %dx%d", cam->width, cam->height);
+    if ((long long)cam->width * cam->height > (1ll << 30)) return set_error(LG_ERR_INVALID, "image too large");
+    if (o->spp < 0 || o->max_bounces < 0) return set_error(LG_ERR_INVALID, "spp/bounces must be >= 0");
+    if (o->flags & LG_RENDER_ACCUM64) return set_error(LG_ERR_INVALID, "the ray-sorted render has no FP64 accumulator");
+    DeviceGuard g(r->device);
+    LG_TRY(take_fault(r));
+    LG_TRY(ensure_frame(r, cam->width, cam->height, false));
+    const int npix = cam->width * cam->height;
+    const long long nval = (long long)npix * 3;
+    LG_TRY(r->wf_scratch.reserve(wavefront_scratch_bytes(npix)));
+    LG_TRY_CUDA(cudaMemsetAsync(r->accum.p, 0, (size_t)nval * sizeof(float), r->stream));
+    if (r->counting) LG_TRY_CUDA(cudaMemsetAsync(r->counters.p, 0, sizeof(RenderCounters), r->stream));
+    LG_TRY_CUDA(cudaEventRecord(r->ev0, r->stream));
+    if (o->spp > 0 && r->n_nodes > 0)
+    {
+        WavefrontJob job;
+        job.spp = o->spp;
+        job.max_bounces = o->max_bounces;
+        job.sample_base = o->sample_base;
+        job.sort = (o->flags & LG_RENDER_NO_RAY_SORT) == 0;
+        job.width = r->bvh_width;
+        job.watertight = r->watertight;
+        job.accum = r->accum.as<float>();
+        job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
+        LG_TRY_CUDA(launch_wavefront_frame(dev_scene(r), make_dev_cam(*cam), job, r->wf_scratch.p,
+                                           r->wf_scratch.bytes, r->stream));
+    }
+    LG_TRY_CUDA(launch_tonemap(r->accum.as<float>(), r->rgb.as<uint8_t>(), nval, 1.0f / (float)o->spp, r->stream));
+    LG_TRY_CUDA(cudaEventRecord(r->ev1, r->stream));
+    LG_TRY_CUDA(post_fault(r, r->stream));
+    if (rgb8) LG_TRY_CUDA(cudaMemcpyAsync(rgb8, r->rgb.p, (size_t)nval, cudaMemcpyDeviceToHost, r->stream));
+    if (accum) LG_TRY_CUDA(cudaMemcpyAsync(accum, r->accum.p, (size_t)nval * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
+    LG_TRY(take_fault(r));
+    if (stats)
+    {
+        float ms = 0.0f;
+        LG_TRY_CUDA(cudaEventElapsedTime(&ms, r->ev0, r->ev1));
+        *stats = lg_render_stats{};
+        stats->kernel_ms = ms;
+        if (r->counting)
+        {
+            RenderCounters c;
+            LG_TRY_CUDA(cudaMemcpy(&c, r->counters.p, sizeof c, cudaMemcpyDeviceToHost));
+            stats->closest_rays = c.closest_rays;
+            stats->shadow_rays = c.shadow_rays;
+            stats->node_fetches = c.node_fetches;
+            stats->tri_tests = c.tri_tests;
+            stats->leaf_fetches = c.leaf_fetches;
+        }
+    }
+    return LG_OK;
+}
+
 int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts* opts, int32_t n_jobs,
                     uint8_t* rgb8_out, float* ms_per_job)
 {
@@ -1285,6 +1346,42 @@ lg_scene_desc desc_of(const Scene& s, std::vector<float>& alb)
     d.n_points = (int32_t)s.points.size();
     return d;
 }
+
+// A renderer holding `scene` with the caller's BVH and the scene's textures
+// resolved against assetRoot, reported as the reference reports them
+// (pathtracer.cu:597-613).  Returns LG_OK or the failing call's status.
+int open_renderer(const Scene& scene, const Bvh& bvh, const std::string& assetRoot, lg_scene_desc& d,
+                  std::vector<float>& alb, lg_renderer** out)
+{
+    d = desc_of(scene, alb);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int rc = lg_renderer_create(dev, out);
+    if (rc == LG_OK)
+        rc = lg_renderer_set_scene_bvh(*out, &d, reinterpret_cast<const lg_bvh_node*>(bvh.nodes.data()),
+                                       (int32_t)bvh.nodes.size());
+    if (rc != LG_OK) return rc;
+    int loaded = 0, missing = 0;
+    for (size_t m = 0; m < scene.materials.size() && rc == LG_OK; ++m)
+    {
+        const std::string& rel = scene.materials[m].diffuseTex;
+        if (rel.empty()) continue;
+        const std::string full = assetRoot + "/" + rel;
+        int32_t w = 0, h = 0;
+        uint8_t* px = nullptr;
+        if (lg_image_load(full.c_str(), &w, &h, &px) != LG_OK)
+        {
+            std::fprintf(stderr, "  texture not found: %s\n", full.c_str());
+            ++missing;
+            continue;
+        }
+        rc = lg_renderer_set_texture(*out, (int)m, px, w, h);
+        lg_image_free(px);
+        ++loaded;
+    }
+    std::printf("textures: %d loaded, %d missing (of %zu materials)\n", loaded, missing, scene.materials.size());
+    return rc;
+}
 }  // namespace
 
 // Same signature as the reference (declared in its main.cpp:19-24).  The
@@ -1300,37 +1397,9 @@ void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& asse
     for (auto* v : {outAlbedo, outNormal, outWorldPos})
         if (v) v->assign((size_t)outW * outH * 3, 0);
     std::vector<float> alb;
-    lg_scene_desc d = desc_of(scene, alb);
+    lg_scene_desc d{};
     lg_renderer* r = nullptr;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int rc = lg_renderer_create(dev, &r);
-    if (rc == LG_OK)
-        rc = lg_renderer_set_scene_bvh(r, &d, reinterpret_cast<const lg_bvh_node*>(bvh.nodes.data()),
-                                       (int32_t)bvh.nodes.size());
-    if (rc == LG_OK)
-    {
-        // Textures resolved against assetRoot and reported as the reference does (pathtracer.cu:597-613).
-        int loaded = 0, missing = 0;
-        for (size_t m = 0; m < scene.materials.size() && rc == LG_OK; ++m)
-        {
-            const std::string& rel = scene.materials[m].diffuseTex;
-            if (rel.empty()) continue;
-            const std::string full = assetRoot + "/" + rel;
-            int32_t w = 0, h = 0;
-            uint8_t* px = nullptr;
-            if (lg_image_load(full.c_str(), &w, &h, &px) != LG_OK)
-            {
-                std::fprintf(stderr, "  texture not found: %s\n", full.c_str());
-                ++missing;
-                continue;
-            }
-            rc = lg_renderer_set_texture(r, (int)m, px, w, h);
-            lg_image_free(px);
-            ++loaded;
-        }
-        std::printf("textures: %d loaded, %d missing (of %zu materials)\n", loaded, missing, scene.materials.size());
-    }
+    int rc = open_renderer(scene, bvh, assetRoot, d, alb, &r);
     lg_render_stats st{};
     if (rc == LG_OK)
     {
@@ -1348,5 +1417,31 @@ void RenderSceneCUDA(const Scene& scene, const Bvh& bvh, const std::string& asse
         rc = lg_render_gbuffer(r, &cam, outAlbedo->data(), outNormal->data(), outWorldPos->data());
         if (rc != LG_OK) std::fprintf(stderr, "gbuffer failed: %s\n", lg_last_error());
     }
+    lg_renderer_destroy(r);
+}
+
+// Same signature as the reference (declared in its main.cpp:25-27; defined
+// at pathtracer.cu:759-909): the ray-sorted render, lg_render_sorted.
+void RenderSceneCUDASorted(const Scene& scene, const Bvh& bvh, const std::string& assetRoot, int spp, int maxBounces,
+                           std::vector<uint8_t>& outRGB, int& outW, int& outH)
+{
+    outW = scene.camera.imageWidth;
+    outH = scene.camera.imageHeight;
+    outRGB.assign((size_t)outW * outH * 3, 0);
+    std::vector<float> alb;
+    lg_scene_desc d{};
+    lg_renderer* r = nullptr;
+    int rc = open_renderer(scene, bvh, assetRoot, d, alb, &r);
+    lg_render_stats st{};
+    if (rc == LG_OK)
+    {
+        lg_render_opts o{spp, maxBounces, 0, 0};
+        lg_camera cam = d.camera;
+        rc = lg_render_sorted(r, &cam, &o, outRGB.data(), nullptr, &st);
+    }
+    if (rc != LG_OK) std::fprintf(stderr, "render failed: %s\n", lg_last_error());
+    else
+        std::printf("kernel (sorted): %.1f ms  (%d x %d, %d spp, %d bounces, %zu tris)\n", st.kernel_ms, outW, outH,
+                    spp, maxBounces, scene.triangles.size());
     lg_renderer_destroy(r);
 }

@@ -10,7 +10,10 @@
 // "render: ...", "wrote ...", "[k/n] ... render=... ms") and the exit codes
 // (1 usage, 2 scene load, 3 PNG write) follow main.cpp:93-229.  The scene is
 // uploaded and its BVH built on the device once; batch jobs only change the
-// camera.  --sort is accepted and ignored (one trace path serves both).
+// camera.  --sort renders the single frame with the ray-sorted wavefront
+// (lg_render_sorted, RenderSceneCUDASorted's semantics: per-sample seeding,
+// no Russian roulette, rays sorted by direction between bounces) and prints
+// "kernel (sorted): ..."; batch jobs ignore it, as main.cpp:158-190 does.
 // Diffuse textures resolve against --asset-root (default: the scene file's
 // grandparent directory, main.cpp:140-141).  --gbuffer also writes <stem>.albedo.png, <stem>.normal.png and
 // <stem>.worldpos.png (main.cpp:177-184, 220-227).  --hdr additionally writes
@@ -123,7 +126,7 @@ int main(int argc, char** argv)
     std::string assetRoot;
     std::string batchFile;
     int spp = 64, bounces = 2, device = 0;
-    bool gbuffer = false;
+    bool gbuffer = false, useSort = false;
     bool haveCamPos = false, haveCamTgt = false;
     float camPos[3] = {0, 0, 0}, camTgt[3] = {0, 0, 0};
 
@@ -143,7 +146,7 @@ int main(int argc, char** argv)
         else if (a == "-o" && i + 1 < argc) pngPath = argv[++i];
         else if (a == "--hdr" && i + 1 < argc) hdrPath = argv[++i];
         else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
-        else if (a == "--sort") { /* one trace path serves both */ }
+        else if (a == "--sort") useSort = true;
         else if (a == "--gbuffer") gbuffer = true;
         else if (a == "--cam-pos") haveCamPos = read_vec3(i, camPos);
         else if (a == "--cam-target") haveCamTgt = read_vec3(i, camTgt);
@@ -230,15 +233,17 @@ int main(int argc, char** argv)
     lg_render_opts o{spp, bounces, 0, 0};
     lg_render_stats st{};
     auto t2 = std::chrono::steady_clock::now();
-    if (lg_render(r, &desc.camera, &o, rgb.data(), hdrPath.empty() ? nullptr : accum.data(), nullptr, &st) != LG_OK)
+    const int rrc = useSort ? lg_render_sorted(r, &desc.camera, &o, rgb.data(), hdrPath.empty() ? nullptr : accum.data(), &st)
+                            : lg_render(r, &desc.camera, &o, rgb.data(), hdrPath.empty() ? nullptr : accum.data(), nullptr, &st);
+    if (rrc != LG_OK)
     {
         std::fprintf(stderr, "%s\n", lg_last_error());
         lg_renderer_destroy(r);
         lg_scene_destroy(scene);
         return 4;
     }
-    std::printf("kernel: %.1f ms  (%d x %d, %d spp, %d bounces, %d tris)\n", st.kernel_ms, W, H, spp, bounces,
-                desc.n_tris);
+    std::printf("kernel%s: %.1f ms  (%d x %d, %d spp, %d bounces, %d tris)\n", useSort ? " (sorted)" : "",
+                st.kernel_ms, W, H, spp, bounces, desc.n_tris);
     std::printf("render: %.1f ms (%d x %d)\n", ms_since(t2), W, H);
     if (gbuffer)
     {

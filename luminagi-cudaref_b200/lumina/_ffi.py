@@ -25,6 +25,7 @@ LG_ERR_NOMEM = -5
 LG_ERR_DEVICE = -6
 LG_ERR_CAPACITY = -7
 LG_RENDER_ACCUM64 = 1
+LG_RENDER_NO_RAY_SORT = 2
 LG_ISECT_MOLLER_TRUMBORE = 0
 LG_ISECT_WATERTIGHT = 1
 LG_UNET_RELU, LG_UNET_BILINEAR, LG_UNET_LOG_HDR, LG_UNET_HDR_VARIANT = 1, 2, 4, 7
@@ -112,6 +113,8 @@ SIGNATURES = {
     "lg_renderer_set_texture": (_I, [_P, _I, _P, C.c_int32, C.c_int32]),
     "lg_renderer_load_textures": (_I, [_P, _P, C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "lg_render": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, _P, C.POINTER(LgRenderStats)]),
+    "lg_measure_read_bandwidth": (_I, [C.c_int, C.c_int, C.c_int64, C.c_int, C.POINTER(C.c_double)]),
+    "lg_render_sorted": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, C.POINTER(LgRenderStats)]),
     "lg_render_device": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, C.POINTER(_P), C.POINTER(_P),
                               C.POINTER(_P)]),
     "lg_render_batch": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), C.c_int32, _P, _P]),

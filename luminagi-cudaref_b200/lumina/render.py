@@ -5,8 +5,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._ffi import (LG_RENDER_ACCUM64, NODE_DTYPE, TRI_DTYPE, LgCamera, LgRenderOpts, LgRenderStats, check, lib,
-                   ptr)
+from ._ffi import (LG_RENDER_ACCUM64, LG_RENDER_NO_RAY_SORT, NODE_DTYPE, TRI_DTYPE, LgCamera, LgRenderOpts,
+                   LgRenderStats, check, lib, ptr)
 from .scene import Camera, Scene
 
 
@@ -160,6 +160,25 @@ class Renderer:
         check(lib().lg_render(self._h, C.byref(c), C.byref(o), ptr(out_rgb), ptr(out_acc), ptr(out_acc64),
                               C.byref(st)))
         return {"rgb": out_rgb, "accum": out_acc, "accum64": out_acc64, "kernel_ms": st.kernel_ms,
+                "closest_rays": int(st.closest_rays), "shadow_rays": int(st.shadow_rays),
+                "node_fetches": int(st.node_fetches), "tri_tests": int(st.tri_tests),
+                "leaf_fetches": int(st.leaf_fetches)}
+
+    def render_sorted(self, camera: Camera | None = None, spp: int = 1, bounces: int = 0, sample_base: int = 0,
+                      sort: bool = True):
+        """The reference's ray-sorted render (RenderSceneCUDASorted; cuda_ref --sort): per-sample
+        seeding, rays sorted by direction between bounces, no Russian roulette.  sort=False keeps the
+        rays in pixel order (same launches without the sorts).  Returns dict(rgb, accum, kernel_ms,
+        closest_rays, shadow_rays, ...) as render()."""
+        cam = camera if camera is not None else self.scene.camera
+        c = cam.to_c()
+        W, H = int(cam.width), int(cam.height)
+        o = LgRenderOpts(spp, bounces, sample_base, 0 if sort else LG_RENDER_NO_RAY_SORT)
+        out_rgb = np.zeros((H, W, 3), np.uint8)
+        out_acc = np.zeros((H, W, 3), np.float32)
+        st = LgRenderStats()
+        check(lib().lg_render_sorted(self._h, C.byref(c), C.byref(o), ptr(out_rgb), ptr(out_acc), C.byref(st)))
+        return {"rgb": out_rgb, "accum": out_acc, "kernel_ms": st.kernel_ms,
                 "closest_rays": int(st.closest_rays), "shadow_rays": int(st.shadow_rays),
                 "node_fetches": int(st.node_fetches), "tri_tests": int(st.tri_tests),
                 "leaf_fetches": int(st.leaf_fetches)}

@@ -186,8 +186,10 @@ def ref_trace_cpu(scene, nodes, tris, spp, bounces, row_start=0, row_step=1, thr
     return acc
 
 
-def ref_render_gpu(scene, nodes, tris, spp, bounces, camera=None):
-    """The reference kernels on the GPU; returns (accum (H,W,3) f32, rgb (H,W,3) u8, kernel ms)."""
+def ref_render_gpu(scene, nodes, tris, spp, bounces, camera=None, sorted_path=False):
+    """The reference kernels on the GPU; returns (accum (H,W,3) f32, rgb (H,W,3) u8, kernel ms).
+    sorted_path: its ray-sorted render (RenderSceneCUDASorted, pathtracer.cu:759-909) instead of
+    accumulate_kernel."""
     cam = camera if camera is not None else scene.camera
     H, W = int(cam.height), int(cam.width)
     acc = np.zeros((H, W, 3), np.float32)
@@ -200,8 +202,9 @@ def ref_render_gpu(scene, nodes, tris, spp, bounces, camera=None):
     alb = np.ascontiguousarray(scene.mat_albedo, np.float32)
     emi = np.ascontiguousarray(scene.mat_emissive, np.float32)
     pts = np.ascontiguousarray(scene.points, POINT_DTYPE)
-    rc = rlib().ref_render_gpu(_p(nodes), len(nodes), _p(tris), len(tris), _p(alb), _p(emi), len(alb), _p(pts),
-                               len(pts), _p(sun), C.byref(c), spp, bounces, _p(acc), _p(rgb), C.byref(ms))
+    fn = rlib().ref_render_sorted_gpu if sorted_path else rlib().ref_render_gpu
+    rc = fn(_p(nodes), len(nodes), _p(tris), len(tris), _p(alb), _p(emi), len(alb), _p(pts),
+            len(pts), _p(sun), C.byref(c), spp, bounces, _p(acc), _p(rgb), C.byref(ms))
     if rc != 0:
         raise RuntimeError(f"reference GPU render failed with CUDA error {rc}")
     return acc, rgb, ms.value

@@ -292,6 +292,110 @@ done:
 #undef RCHK
 }
 
+// ---- The reference's ray-sorted render, launched as RenderSceneCUDASorted
+// launches it (pathtracer.cu:838-890: per sample gen_primary_kernel, a
+// thrust::sort_by_key of the rays by direction key, then per bounce
+// trace_and_bounce_kernel and a sort of the next rays), reading back the FP32
+// accumulator it never returns.  Untextured scenes; node buffer padded to
+// 255 nodes because trace_and_bounce_kernel stages nodes[0..254] into shared
+// memory (pathtracer.cu:492-494).
+int ref_render_sorted_gpu(const BvhNode* nodes, int nNodes, const Triangle* tris, int nTris, const float* matAlbedo,
+                          const float* matEmissive, int nMats, const PointLight* points, int nPoints,
+                          const DirectionalLight* sun, const CameraDesc* camDesc, int spp, int maxBounces,
+                          float* accumHost, uint8_t* rgbHost, float* kernelMs)
+{
+#define RCHK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { rc = (int)e_; goto done; } } while (0)
+    int rc = 0;
+    std::vector<DeviceMaterial> mats = make_mats(matAlbedo, matEmissive, nMats);
+    const CameraGPU cam = make_cam(*camDesc);
+    const int W = cam.width, H = cam.height, N = W * H;
+    const int nPad = nNodes < kShmemBvhNodes ? kShmemBvhNodes : nNodes;
+    BvhNode* d_nodes = nullptr;
+    Triangle* d_tris = nullptr;
+    DeviceMaterial* d_mats = nullptr;
+    PointLight* d_points = nullptr;
+    float* d_accum = nullptr;
+    uint8_t* d_image = nullptr;
+    SortedRay *d_raysA = nullptr, *d_raysB = nullptr;
+    uint32_t *d_keysA = nullptr, *d_keysB = nullptr, *d_rng = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    DeviceScene s{};
+    dim3 block2d(16, 16);
+    dim3 grid2d((W + 15) / 16, (H + 15) / 16);
+    const int grid1d = (N + 255) / 256;
+    RCHK(cudaMalloc(&d_nodes, (size_t)nPad * sizeof(BvhNode)));
+    RCHK(cudaMemset(d_nodes, 0, (size_t)nPad * sizeof(BvhNode)));
+    RCHK(cudaMemcpy(d_nodes, nodes, (size_t)nNodes * sizeof(BvhNode), cudaMemcpyHostToDevice));
+    RCHK(cudaMalloc(&d_tris, (size_t)(nTris > 0 ? nTris : 1) * sizeof(Triangle)));
+    if (nTris) RCHK(cudaMemcpy(d_tris, tris, (size_t)nTris * sizeof(Triangle), cudaMemcpyHostToDevice));
+    RCHK(cudaMalloc(&d_mats, (size_t)(nMats > 0 ? nMats : 1) * sizeof(DeviceMaterial)));
+    if (nMats) RCHK(cudaMemcpy(d_mats, mats.data(), (size_t)nMats * sizeof(DeviceMaterial), cudaMemcpyHostToDevice));
+    if (nPoints)
+    {
+        RCHK(cudaMalloc(&d_points, (size_t)nPoints * sizeof(PointLight)));
+        RCHK(cudaMemcpy(d_points, points, (size_t)nPoints * sizeof(PointLight), cudaMemcpyHostToDevice));
+    }
+    RCHK(cudaMalloc(&d_accum, (size_t)N * 3 * sizeof(float)));
+    RCHK(cudaMemset(d_accum, 0, (size_t)N * 3 * sizeof(float)));
+    RCHK(cudaMalloc(&d_image, (size_t)N * 3));
+    RCHK(cudaMalloc(&d_raysA, (size_t)N * sizeof(SortedRay)));
+    RCHK(cudaMalloc(&d_raysB, (size_t)N * sizeof(SortedRay)));
+    RCHK(cudaMalloc(&d_keysA, (size_t)N * sizeof(uint32_t)));
+    RCHK(cudaMalloc(&d_keysB, (size_t)N * sizeof(uint32_t)));
+    RCHK(cudaMalloc(&d_rng, (size_t)N * sizeof(uint32_t)));
+    s.nodes = d_nodes;
+    s.tris = d_tris;
+    s.mats = d_mats;
+    s.points = d_points;
+    s.numPoints = nPoints;
+    s.sun = *sun;
+    RCHK(cudaEventCreate(&t0));
+    RCHK(cudaEventCreate(&t1));
+    RCHK(cudaEventRecord(t0));
+    for (int sample = 0; sample < spp; ++sample)
+    {
+        gen_primary_kernel<<<grid2d, block2d>>>(cam, d_raysA, d_keysA, d_rng, sample);
+        RCHK(cudaGetLastError());
+        thrust::sort_by_key(thrust::device_ptr<uint32_t>(d_keysA), thrust::device_ptr<uint32_t>(d_keysA + N),
+                            thrust::device_ptr<SortedRay>(d_raysA));
+        for (int b = 0; b <= maxBounces; ++b)
+        {
+            const bool last = (b == maxBounces);
+            trace_and_bounce_kernel<<<grid1d, 256>>>(s, d_raysA, (uint32_t)N, d_accum, last ? nullptr : d_raysB,
+                                                      last ? nullptr : d_keysB, d_rng, last);
+            RCHK(cudaGetLastError());
+            if (last) break;
+            thrust::sort_by_key(thrust::device_ptr<uint32_t>(d_keysB), thrust::device_ptr<uint32_t>(d_keysB + N),
+                                thrust::device_ptr<SortedRay>(d_raysB));
+            std::swap(d_raysA, d_raysB);
+            std::swap(d_keysA, d_keysB);
+        }
+    }
+    tonemap_kernel<<<grid2d, block2d>>>(d_accum, d_image, W, H, 1.0f / (float)spp);
+    RCHK(cudaGetLastError());
+    RCHK(cudaEventRecord(t1));
+    RCHK(cudaEventSynchronize(t1));
+    if (kernelMs) RCHK(cudaEventElapsedTime(kernelMs, t0, t1));
+    if (accumHost) RCHK(cudaMemcpy(accumHost, d_accum, (size_t)N * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+    if (rgbHost) RCHK(cudaMemcpy(rgbHost, d_image, (size_t)N * 3, cudaMemcpyDeviceToHost));
+done:
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    cudaFree(d_nodes);
+    cudaFree(d_tris);
+    cudaFree(d_mats);
+    cudaFree(d_points);
+    cudaFree(d_accum);
+    cudaFree(d_image);
+    cudaFree(d_raysA);
+    cudaFree(d_raysB);
+    cudaFree(d_keysA);
+    cudaFree(d_keysB);
+    cudaFree(d_rng);
+    return rc;
+#undef RCHK
+}
+
 // ---- G-buffer with the reference gbuffer_kernel, box from the root node as
 // RenderSceneCUDA computes it (pathtracer.cu:726-747).  Node buffer padded as above.
 int ref_gbuffer_gpu(const BvhNode* nodes, int nNodes, const Triangle* tris, int nTris, const float* matAlbedo,
