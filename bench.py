@@ -11,21 +11,31 @@ counting pass) with ms/frame alongside.
   e2e       through the C ABI from host buffers: triangle upload from pinned
             memory, device LBVH build, render, tonemap and the 8-bit image read
             back, every step.
-  roofline  algorithmic bytes of the trace kernel (56 B per 4-wide BVH
-            record: grid origin and steps, 24 one-byte planes, four links;
-            48 B per triangle test; 8 B per leaf-table entry; as counted) over
-            its event-timed duration, against the measured HBM copy peak.
-            The scene (~200 MB) exceeds the 126 MB L2, so traffic is a mix of
-            L2 and HBM.
+  roofline  algorithmic bytes of the trace kernel (64 B per 4-wide BVH
+            record, both 32-byte halves as loaded; 48 B per triangle test;
+            8 B per leaf-table entry; as counted) over its event-timed
+            duration, against the L2 read bandwidth measured in this run
+            (lg_measure_read_bandwidth: a 32 MB buffer, L2-only loads).  The
+            hot arrays (records ~22 MB, triangle records ~67 MB) stay
+            L2-resident across frames: DRAM moves ~8 B per ray.  L1 and HBM
+            fractions ride along.
+  ref_gpu   the reference's accumulate_kernel compiled for sm_100a
+            (oracle/_ref) on the same frame and BVH, timed with CUDA events
+            as RenderSceneCUDA times it: the reference design on this GPU.
+  sorted    the ray-sorted render (RenderSceneCUDASorted semantics) of the
+            same frame: this library with and without its ray sort, and the
+            reference's sorted kernels on this GPU.
   cpu_baseline  the reference's own trace code (oracle/_ref, compiled from its
-            sources for the host) with OpenMP on all host cores, on a bounded
-            sample of rows; rays counted by the oracle on the same rows.
+            sources for the host) with OpenMP on all host cores, on a fixed
+            sample of rows (every CPU_ROW_STEP-th row; the reference arm uses
+            the same rows); rays counted by the oracle on the same rows.
   ingest    scene-file load times: this library on scene.json and on the
             binary scene file, and the reference's LoadSceneJSON on the same
             JSON (host only).
 
 --impl reference times only that CPU path (the reference renderer has no
-other CPU path) and prints its line.  Multi-GPU: replicas (each rank renders
+other CPU path) on the same rows, over the reference's own BuildBVH, and
+prints its line.  Multi-GPU: replicas (each rank renders
 its own frame; no collective), value summed over ranks.
 """
 from __future__ import annotations
@@ -50,10 +60,20 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # of an 8-spp engine frame: 479.4 MB + 60.2 MB / 65,366,791 rays; traffic
 # scales with rays.
 TRACE_DRAM_BYTES_PER_RAY = 539.592704e6 / 65366791
-# Bytes one traversal step uses from a BVH record: 4-wide, the grid origin and
-# steps (16 B), 24 one-byte planes and four links (16 B); 2-wide, the whole
-# 64-B record.
-RECORD_BYTES = {4: 56, 2: 64}
+# Bytes one traversal step loads from a BVH record: both 32-byte halves of a
+# 4-wide record (grid origin, steps, 24 one-byte planes, four links, 8 B of
+# padding), or the whole 64-byte 2-wide record.
+RECORD_BYTES = {4: 64, 2: 64}
+# Rows of the CPU sample: every CPU_ROW_STEP-th row of the frame, the same in
+# the cpu_baseline leg and the reference arm.
+CPU_ROW_STEP = 24
+# Local-memory (stack and spill) bytes per traced ray of trace_kernel, from one
+# ncu capture of an 8-spp engine frame (lmem load + store sectors x 32 B /
+# rays); the waste to cut.
+TRACE_LOCAL_BYTES_PER_RAY = None
+# L2 probe: buffer size (fits in L2) and passes.
+L2_PROBE_BYTES = 32 << 20
+L1_PROBE_BYTES = 16 << 10
 
 
 def load_peaks():
@@ -75,7 +95,10 @@ def parse_args():
     ap.add_argument("--scene", default="engine", choices=["engine", "box"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-denoise", action="store_true", help="skip the 8spp+UNet vs 256spp timing")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the baseline sample")
+    ap.add_argument("--cpu-row-step", type=int, default=CPU_ROW_STEP,
+                    help="CPU sample: every N-th row of the frame (cpu_baseline and the reference arm)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference kernels on this GPU (ref_gpu, sorted)")
     ap.add_argument("--no-ingest", action="store_true", help="skip the scene-file load timing")
     return ap.parse_args()
 
@@ -142,27 +165,30 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_baseline(scene, nodes, tris, spp, bounces, target_s, impl_kind="reference"):
-    """Reference trace code on the host cores over a row sample, scaled to Mrays/s."""
+def sample_rays(scene, nodes, tris, spp, bounces, step):
+    """Rays (closest + shadow) the frame's sampled rows trace, counted by the
+    oracle on the same paths (the counts are deterministic)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
-    cam = scene.camera
-    H = int(cam.height)
+    _, cnt = O.oracle_render(scene, nodes, tris, spp, bounces, row_start=0, row_step=step,
+                             threads=os.cpu_count() or 1)
+    return cnt["closest_rays"] + cnt["shadow_rays"]
+
+
+def cpu_baseline(scene, nodes, tris, spp, bounces, step=CPU_ROW_STEP, rays=None):
+    """The reference's trace code on all host cores over every step-th row,
+    as Mrays/s and scaled to a full frame."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    H = int(scene.camera.height)
     use_ref = O.ref_available()
     threads = os.cpu_count() or 1
     run = O.ref_trace_cpu if use_ref else (lambda *a, **k: O.oracle_render(*a, **k)[0])
-    # calibrate on one row
-    t = time.perf_counter()
-    run(scene, nodes, tris, spp, bounces, row_start=H // 2, row_step=H, threads=threads)
-    per_row = max(time.perf_counter() - t, 1e-3)
-    # rows are spread over `threads` cores (one row per task)
-    rows = int(max(2 * threads, min(H, target_s * threads / per_row * 0.9)))
-    step = max(1, H // rows)
+    if rays is None:
+        rays = sample_rays(scene, nodes, tris, spp, bounces, step)
     t = time.perf_counter()
     run(scene, nodes, tris, spp, bounces, row_start=0, row_step=step, threads=threads)
     dt = time.perf_counter() - t
-    _, cnt = O.oracle_render(scene, nodes, tris, spp, bounces, row_start=0, row_step=step, threads=threads)
-    rays = cnt["closest_rays"] + cnt["shadow_rays"]
     n_rows = len(range(0, H, step))
     return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": threads,
             "kind": "reference" if use_ref else "port",
@@ -248,6 +274,30 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def reference_designs_on_gpu(scene, spp, bounces, ours_kernel_ms, r):
+    """The reference's kernels compiled for sm_100a (oracle/_ref) on the same
+    frame, over the reference's own BuildBVH: accumulate_kernel (the plain
+    render) and the ray-sorted path, each timed with CUDA events around its
+    launches as the reference times them; plus this library's sorted render
+    with and without its ray sort.  Second of two runs each."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    if not O.ref_available():
+        return None, None
+    nodes, tris = O.ref_build_bvh(scene.tris)
+    plain = [O.ref_render_gpu(scene, nodes, tris, spp, bounces)[2] for _ in range(2)][-1]
+    ref_gpu = {"ms_per_frame": plain, "ours_kernel_ms": ours_kernel_ms, "speedup": plain / ours_kernel_ms,
+               "what": "reference accumulate_kernel + tonemap_kernel, sm_100a build, same frame and BVH"}
+    srt = [O.ref_render_gpu(scene, nodes, tris, spp, bounces, sorted_path=True)[2] for _ in range(2)][-1]
+    ours = [r.render_sorted(spp=spp, bounces=bounces)["kernel_ms"] for _ in range(2)][-1]
+    ours_nosort = [r.render_sorted(spp=spp, bounces=bounces, sort=False)["kernel_ms"] for _ in range(2)][-1]
+    sorted_cmp = {"ref_ms_per_frame": srt, "ours_ms_per_frame": ours, "ours_ms_without_ray_sort": ours_nosort,
+                  "speedup_vs_ref": srt / ours,
+                  "what": "RenderSceneCUDASorted semantics (per-sample seeding, rays sorted by direction "
+                          "between bounces, no Russian roulette); the reference's sorted kernels vs lg_render_sorted"}
+    return ref_gpu, sorted_cmp
+
+
 def main():
     args = parse_args()
     world, rank, local, dist = dist_setup(args)
@@ -256,7 +306,8 @@ def main():
     cfg = {"workload": workload, "triangles": scene.n_tris, "width": int(scene.camera.width),
            "height": int(scene.camera.height), "spp": args.spp, "bounces": args.bounces,
            "rng": "xorshift32 per (pixel, chunk of 8 samples), reference seeding",
-           "l2": "scene + frame buffers (~330 MB) exceed the 126 MB L2; no flush needed",
+           "l2": "no flush: the BVH records (~22 MB) and triangle records (~67 MB) stay L2-resident across "
+                 "frames, as they would across a renderer's frames; DRAM moves ~8 B per ray",
            "parallelism": f"replicas x{world}"}
 
     if args.impl == "reference":
@@ -264,10 +315,11 @@ def main():
             return
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
-        nodes, tris, _, _ = O.oracle_build_bvh(scene.tris)
+        nodes, tris = O.ref_build_bvh(scene.tris)  # the reference's own BuildBVH
+        rays = sample_rays(scene, nodes, tris, args.spp, args.bounces, args.cpu_row_step)
         vals = []
         for i in range(args.warmup + args.steps):
-            b = cpu_baseline(scene, nodes, tris, args.spp, args.bounces, args.cpu_seconds / 2)
+            b = cpu_baseline(scene, nodes, tris, args.spp, args.bounces, args.cpu_row_step, rays)
             if i >= args.warmup:
                 vals.append(b)
         v = statistics.median([b["value"] for b in vals])
@@ -279,9 +331,13 @@ def main():
                 "data": "synthetic (seeded procedural scene)", "config": cfg,
                 "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": b["cores"], "kind": b["kind"],
                                  "sample": b["sample"]},
-                "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "ms_per_step_note": "each step traces the sampled rows; ms_per_step is that time scaled to the "
+                                    "full frame"}
         print(json.dumps(line))
         return
+
+    import ctypes as C
 
     import torch
     import lumina
@@ -289,6 +345,10 @@ def main():
 
     torch.cuda.set_device(local)
     dev = local
+    # Cache read bandwidths of this GPU (the trace kernel's roofline denominators).
+    l2_gbs, l1_gbs = C.c_double(0), C.c_double(0)
+    _ffi.check(_ffi.lib().lg_measure_read_bandwidth(dev, 2, L2_PROBE_BYTES, 40, C.byref(l2_gbs)))
+    _ffi.check(_ffi.lib().lg_measure_read_bandwidth(dev, 1, L1_PROBE_BYTES, 400, C.byref(l1_gbs)))
     r = lumina.Renderer(dev)
     r.set_scene(scene)
     nodes_dev, tris_dev = r.get_bvh()
@@ -302,7 +362,6 @@ def main():
     rays = c["closest_rays"] + c["shadow_rays"]
     algo_bytes = RECORD_BYTES[4] * c["node_fetches"] + 48 * c["tri_tests"] + 8 * c["leaf_fetches"]
 
-    import ctypes as C
     cam = scene.camera.to_c()
     opts = _ffi.LgRenderOpts(args.spp, args.bounces, 0, 0)
     stream = torch.cuda.current_stream(dev)
@@ -397,6 +456,20 @@ def main():
                    "weights": "random (the cost of a forward pass does not depend on their values)"}
         net.close()
 
+    traffic = TRACE_DRAM_BYTES_PER_RAY * rays
+    roof = {"bound": "l2", "achieved": achieved, "peak": l2_gbs.value, "unit": "GB/s",
+            "frac": achieved / l2_gbs.value, "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-spp launch, scaled by rays",
+            "peak_source": f"measured in this run: L2 read bandwidth, {L2_PROBE_BYTES >> 20} MB buffer, "
+                           "ld.global.cg (lg_measure_read_bandwidth)",
+            "l1_peak": l1_gbs.value, "l1_frac": achieved / l1_gbs.value,
+            "hbm_peak": peaks["hbm_gbs"], "hbm_frac": achieved / peaks["hbm_gbs"], "hbm_peak_source": peak_kind,
+            "dram_bytes_per_ray": TRACE_DRAM_BYTES_PER_RAY, "kernel": "trace_kernel",
+            "algorithmic_bytes_per_launch": algo_bytes, "algorithmic_bytes_per_ray": algo_bytes / rays,
+            "kernel_ms": kernel_ms,
+            "limiter": "instruction issue, not memory (ncu: issue slots ~70% busy, L1 data pipe ~50%)"}
+    if TRACE_LOCAL_BYTES_PER_RAY is not None:
+        roof["local_bytes_per_ray"] = TRACE_LOCAL_BYTES_PER_RAY
     line = {"metric": "Mrays/s (plain render; ms/frame alongside)", "value": value, "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -404,21 +477,24 @@ def main():
             "rays_per_frame": rays, "ms_per_frame": ms_step,
             "e2e": {"value": rays * world / e2e_s / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_frame": e2e_s * 1e3},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": TRACE_DRAM_BYTES_PER_RAY * rays,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of an 8-spp launch, "
-                                           "scaled by rays", "working_set": f"L2-resident (DRAM {TRACE_DRAM_BYTES_PER_RAY:.1f} B/ray)",
-                         "peak_source": peak_kind, "kernel": "trace_kernel",
-                         "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms": kernel_ms},
+            "roofline": roof,
             "gpu_launches": args.steps * 2,
             "clocks": clk.summary()}
     if denoise:
         line["denoise"] = denoise
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        try:
+            ref_gpu, sorted_cmp = reference_designs_on_gpu(scene, args.spp, args.bounces, kernel_ms, r)
+            if ref_gpu:
+                line["ref_gpu"] = ref_gpu
+                line["sorted"] = sorted_cmp
+        except Exception as e:  # the oracle libraries are test infrastructure; report, don't fail
+            line["ref_gpu"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_ingest:
         line["ingest"] = ingest_timing(scene, with_reference=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(scene, nodes_dev, tris_dev, args.spp, args.bounces, args.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline(scene, nodes_dev, tris_dev, args.spp, args.bounces, args.cpu_row_step)
         except Exception as e:  # the oracle libraries are test infrastructure; report, don't fail
             line["cpu_baseline"] = {"value": None, "error": str(e)}
     r.close()

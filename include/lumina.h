@@ -219,6 +219,16 @@ int lg_renderer_get_refill_threshold(const lg_renderer* r);
 #define LG_LEAF_QUORUM_DEFAULT 12
 int lg_renderer_set_leaf_quorum(lg_renderer* r, int quorum);
 int lg_renderer_get_leaf_quorum(const lg_renderer* r);
+/* Shared-memory copy of the top of the BVH: each block of the persistent
+ * trace launch copies the first `n` 4-wide records (BFS order: the top levels,
+ * which every ray visits first) into shared memory at start and reads them
+ * from there (64 B each; at most LG_TOP_RECORDS_MAX, 0 = off).  The
+ * reference stages its first 255 binary nodes the same way
+ * (src/pathtracer.cu:44-50, 338-342).  Images do not depend on it. */
+#define LG_TOP_RECORDS_DEFAULT 0
+#define LG_TOP_RECORDS_MAX 1024
+int lg_renderer_set_top_records(lg_renderer* r, int n);
+int lg_renderer_get_top_records(const lg_renderer* r);
 /* Autotuner of the trace schedule: renders `cam` at spp/max_bounces with each
  * pair of refill threshold (8, 12, 16, 24) and leaf quorum (4, 8, 12, 16),
  * keeps the fastest pair for later frames and reports it (and its kernel
@@ -326,6 +336,14 @@ int lg_unet_loss_grad(lg_unet* u, const float* d_x, const float* d_target, int n
 int lg_unet_adam_apply(lg_unet* u, float lr);
 /* Clears the Adam moments and step count. */
 int lg_unet_adam_reset(lg_unet* u);
+/* No counterpart in the reference (which calls exit(1) on any CUDA error,
+ * src/pathtracer.cu:17-20).  Checks the failure path of the tensor-core
+ * kernels: a probe kernel waits, with the same bounded wait they use, on an
+ * mbarrier that nothing arrives at; after limit_ns (1 us .. 2 s) it sets the
+ * network's error word as a convolution whose wait ran out would, and the
+ * call returns LG_ERR_DEVICE ("... wait timeout 3").  Nothing is left in
+ * flight, so the network stays usable: the next call clears the word. */
+int lg_unet_wait_selftest(lg_unet* u, int64_t limit_ns);
 /* Autotuner: for each of the 14 convolutions (and, with
  * LG_UNET_TUNE_BACKWARD, the 16 input-gradient convolutions of training)
  * times every compiled tile shape (output channels per CTA, input channels

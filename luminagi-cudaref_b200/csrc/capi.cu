@@ -116,6 +116,8 @@ struct lg_renderer
     int trace_blocks_per_sm = 0;  // persistent trace grid (0 = occupancy maximum); see lg_renderer_autotune
     int trace_refill = LG_REFILL_DEFAULT;  // finished rays per warp that trigger the path logic (1..32)
     int trace_quorum = LG_LEAF_QUORUM_DEFAULT;  // searching lanes below which a warp tests its held leaves (0..31)
+    int trace_top = LG_TOP_RECORDS_DEFAULT;     // 4-wide records each trace block keeps in shared memory
+    int n4 = 0;                                 // 4-wide records of the current scene
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     // Traversal-stack overflow word (DevScene::fault) and its pinned host
@@ -248,6 +250,7 @@ int build_records(lg_renderer* r)
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
     r->leaf_inline = leaf_inline;
     r->root4 = root4;
+    r->n4 = root4 >= 0 ? n4 : 0;
     r->root = root;
     ++r->scene_gen;
     return LG_OK;
@@ -292,6 +295,7 @@ DevScene dev_scene(const lg_renderer* r)
     s.root = r->root;
     s.nodes4 = r->wide4.as<Wide4Node>();
     s.root4 = r->root4;
+    s.n4 = r->n4;
     s.leaf_inline = r->leaf_inline;
     s.sun = r->sun;
     s.fault = r->fault.as<unsigned>();
@@ -350,6 +354,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.blocks_per_sm = r->trace_blocks_per_sm;
         job.refill_threshold = r->trace_refill;
         job.leaf_quorum = r->trace_quorum;
+        job.top_records = r->trace_top;
         LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->watertight,
                                  r->stream));
     }
@@ -973,6 +978,20 @@ int lg_renderer_get_leaf_quorum(const lg_renderer* r)
     return r->trace_quorum;
 }
 
+int lg_renderer_set_top_records(lg_renderer* r, int n)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    if (n < 0 || n > LG_TOP_RECORDS_MAX) return set_error(LG_ERR_INVALID, "top records must be 0..%d", LG_TOP_RECORDS_MAX);
+    r->trace_top = n;
+    return LG_OK;
+}
+
+int lg_renderer_get_top_records(const lg_renderer* r)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    return r->trace_top;
+}
+
 int lg_renderer_set_render_tree(lg_renderer* r, int mode)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
@@ -1178,6 +1197,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
     key.push_back(r->trace_blocks_per_sm);
     key.push_back(r->trace_refill);
     key.push_back(r->trace_quorum);
+    key.push_back(r->trace_top);
     key.push_back(r->scene_gen);
     if (key != r->batch_key || !r->batch_exec)
     {
@@ -1199,6 +1219,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
             job.blocks_per_sm = r->trace_blocks_per_sm;
             job.refill_threshold = r->trace_refill;
             job.leaf_quorum = r->trace_quorum;
+            job.top_records = r->trace_top;
             e = launch_trace_batch(dev_scene(r), job, r->sm_count, r->bvh_width, r->watertight, st);
         }
         for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)

@@ -33,6 +33,7 @@
 //     are added to the FP32 accumulator atomically: the order of chunk
 //     additions (not their values) can differ from the reference's
 //     launch-per-chunk order.
+#include <algorithm>
 #include <cstdint>
 
 #include <cuda_runtime.h>
@@ -326,12 +327,17 @@ __global__ void tri_prep_kernel(const lg_triangle* __restrict__ tris, int n, flo
 
 // Per-lane path state of the chunk being traced (accumulate_kernel's sample
 // loop, :352-358, and trace_path, :295-331, unrolled into a state machine).
+// Each unoccluded light's throughput x contribution goes straight into the
+// chunk sum, where the reference first sums the lights of a bounce, then the
+// bounces of a sample, then the samples: the same terms added in another
+// FP32 order (rounding-level differences), with two vec3s less live state
+// across the traversal.
 struct PathState
 {
     Ray ray;
     float tmax;
-    vec3 L, throughput, P, N, albedo, color, contrib, sum;
-    double sum64x, sum64y, sum64z;  // judge images only: the same chunk sum, each sample added in FP64
+    vec3 throughput, P, N, albedo, contrib, sum;
+    double sum64x, sum64y, sum64z;  // judge images only: the same terms added in FP64
     uint32_t rng;
     int px, py, k, n_this, bounce, li;  // li: -1 camera/bounce ray in flight, >= 0 shadow ray of light li
     unsigned pixel;                     // index of the pixel's first accumulator value
@@ -354,7 +360,6 @@ __device__ __forceinline__ int find_job(const BatchJob* __restrict__ jobs, int n
 
 __device__ __forceinline__ void start_sample(PathState& st, const DevCam& cam)
 {
-    st.L = v3(0, 0, 0);
     st.throughput = v3(1, 1, 1);
     st.bounce = 0;
     st.li = -1;
@@ -366,7 +371,7 @@ __device__ __forceinline__ void start_sample(PathState& st, const DevCam& cam)
 
 // Consumes the result of the ray in flight and sets up the next one.
 // Returns false when the chunk's last sample has finished.  kAcc64: every
-// sample's radiance is also added to an FP64 chunk sum.
+// radiance term is also multiplied and added in FP64.
 template <bool kAcc64>
 __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const DevCam& cam, int maxBounces, int tri,
                                         float hitT, float hitU, float hitV)
@@ -387,12 +392,18 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
             st.P = vadd(st.ray.o, vmul(st.ray.d, hitT));
             const int mat = __float_as_int(__ldg(&s.tv[kTriVec * tri].w));
             st.albedo = hit_albedo(s, t, mat, w, hitU, hitV);
-            st.color = v3(0, 0, 0);
         }
     }
     else if (tri < 0)
     {
-        st.color = vadd(st.color, st.contrib);  // light li unoccluded
+        // light li unoccluded
+        st.sum = vadd(st.sum, vhad(st.throughput, st.contrib));
+        if (kAcc64)
+        {
+            st.sum64x += (double)st.throughput.x * (double)st.contrib.x;
+            st.sum64y += (double)st.throughput.y * (double)st.contrib.y;
+            st.sum64z += (double)st.throughput.z * (double)st.contrib.z;
+        }
     }
     if (!path_done)
     {
@@ -402,7 +413,6 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
                 st.li = next;
                 return true;
             }
-        st.L = vadd(st.L, vhad(st.throughput, st.color));
         if (st.bounce == maxBounces) path_done = true;
         else
         {
@@ -424,13 +434,6 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
             }
         }
     }
-    st.sum = vadd(st.sum, st.L);
-    if (kAcc64)
-    {
-        st.sum64x += (double)st.L.x;
-        st.sum64y += (double)st.L.y;
-        st.sum64z += (double)st.L.z;
-    }
     if (++st.k == st.n_this) return false;
     start_sample(st, cam);
     return true;
@@ -446,6 +449,14 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
 template <bool kCount, bool kAcc64, int kWidth, bool kWT, bool kBatch>
 __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
 {
+    // The top of the tree (the first top_n records in BFS order), copied once
+    // per block into dynamic shared memory; every ray starts there.
+    extern __shared__ __align__(32) float4 smem_top[];
+    const Wide4Node* s_top = reinterpret_cast<const Wide4Node*>(smem_top);
+    const int top_n = kWidth == 4 ? min(job.top_records, s.n4) : 0;
+    for (int i = threadIdx.x; i < top_n * 4; i += kTraceThreads)
+        smem_top[i] = __ldg(reinterpret_cast<const float4*>(s.nodes4) + i);
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned long long total =
@@ -517,7 +528,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         const int idle_final = exhausted ? __popc(__ballot_sync(0xffffffffu, !active)) : 0;
         for (;;)
         {
-            if (warp_step<kWidth, kCount, kWT>(s, st.ray, st.li >= 0, active && !tdone, quorum, q, stack, cnt))
+            if (warp_step<kWidth, kCount, kWT>(s, st.ray, st.li >= 0, active && !tdone, quorum, q, stack, cnt, s_top,
+                                               top_n))
                 tdone = true;
             const unsigned busy = __ballot_sync(0xffffffffu, active && !tdone);
             if (busy == 0 || 32 - __popc(busy) - idle_final >= thresh) break;
@@ -747,7 +759,9 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tri
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
     *root4_host = root.triCount == 0 ? 0 : ~0;
-    *n4_host = last_v ? last_d + 1 : -1;  // count is only needed for sizing checks
+    // dense4 of the last node: its rank among record roots if it is one, else
+    // its rank among the others (so the roots before it number n - 1 - rank)
+    *n4_host = last_v ? last_d + 1 : (n_nodes - 1 - last_d);
     return cudaSuccess;
 }
 
@@ -763,8 +777,12 @@ static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const Tr
                                   cudaStream_t stream)
 {
     const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT, kBatch>;
+    const int top_n = W == 4 ? std::min(std::max(job.top_records, 0), s.n4) : 0;
+    const size_t smem = (size_t)top_n * sizeof(Wide4Node);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kTraceThreads, smem);
     if (e != cudaSuccess) return e;
     if (job.blocks_per_sm > 0 && job.blocks_per_sm < per_sm) per_sm = job.blocks_per_sm;
     const long long lanes = kBatch ? (long long)job.total_items : (long long)job.n_tiles * job.n_chunks * 32;
@@ -774,7 +792,7 @@ static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const Tr
     if (blocks < 1) blocks = 1;
     e = cudaMemsetAsync(job.work64, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    trace_kernel<kCount, kAcc64, W, kWT, kBatch><<<(int)blocks, kTraceThreads, 0, stream>>>(s, cam, job);
+    trace_kernel<kCount, kAcc64, W, kWT, kBatch><<<(int)blocks, kTraceThreads, smem, stream>>>(s, cam, job);
     return cudaGetLastError();
 }
 

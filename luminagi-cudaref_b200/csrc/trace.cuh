@@ -53,6 +53,7 @@ struct DevScene
 {
     const Wide4Node* nodes4;   // 4-wide records (used when width == 4)
     int root4;
+    int n4;                    // number of 4-wide records
     int leaf_inline;           // 4-wide leaf links carry (first, count); see wide4_kernel
     const WideNode* nodes;
     const int2* leaves;        // (first triangle, count)
@@ -110,6 +111,7 @@ struct TraceJob
     int blocks_per_sm;     // persistent grid: resident blocks per SM (0 = as many as fit)
     int refill_threshold;  // finished rays in a warp that trigger the path logic, 1..32
     int leaf_quorum;       // lanes still searching for a leaf below which the warp tests held leaves, 0..31
+    int top_records;       // 4-wide records (the first in BFS order) each block keeps in shared memory, 0 = none
     RenderCounters* counters;  // optional
     // batched launch (launch_trace_batch): every field above except work64 is taken from jobs[]
     const BatchJob* jobs;

@@ -219,13 +219,28 @@ __device__ __forceinline__ float qplane(uint32_t w, int k)
     // subtracting 2^23
     return (float)((w >> (8 * k)) & 0xffu);
 }
-__device__ __forceinline__ int4 box4(const Wide4Node* nd, const Ray& r, float tmax, float& t0, float& t1, float& t2,
-                                     float& t3)
+// The two 32-byte halves of 4-wide record i: a = o[3], step[3], qlo[0..1];
+// b = qlo[2], qhi[3], link[4].  Records below top_n come from the block's
+// shared-memory copy of the top of the tree (the first records in BFS
+// order), the others through the read-only path.
+__device__ __forceinline__ void load_rec4(const DevScene& s, const Wide4Node* s_top, int top_n, int i, float (&a)[8],
+                                          float (&b)[8])
 {
-    // a = o[3], step[3], qlo[0..1]; b = qlo[2], qhi[3], link[4]
-    float a[8], b[8];
-    ldg8(nd, a);
-    ldg8(reinterpret_cast<const char*>(nd) + 32, b);
+    if (i < top_n)
+    {
+        const float4* p = reinterpret_cast<const float4*>(s_top + i);
+        const float4 x = p[0], y = p[1], z = p[2], w = p[3];
+        a[0] = x.x; a[1] = x.y; a[2] = x.z; a[3] = x.w; a[4] = y.x; a[5] = y.y; a[6] = y.z; a[7] = y.w;
+        b[0] = z.x; b[1] = z.y; b[2] = z.z; b[3] = z.w; b[4] = w.x; b[5] = w.y; b[6] = w.z; b[7] = w.w;
+        return;
+    }
+    ldg8(&s.nodes4[i], a);
+    ldg8(reinterpret_cast<const char*>(&s.nodes4[i]) + 32, b);
+}
+
+__device__ __forceinline__ int4 box4(const float (&a)[8], const float (&b)[8], const Ray& r, float tmax, float& t0,
+                                     float& t1, float& t2, float& t3)
+{
     const int4 ln = make_int4(__float_as_int(b[4]), __float_as_int(b[5]), __float_as_int(b[6]), __float_as_int(b[7]));
     const float ix = a[3] * r.inv_d.x, iy = a[4] * r.inv_d.y, iz = a[5] * r.inv_d.z;
     const float bx = (a[0] - r.o.x) * r.inv_d.x, by = (a[1] - r.o.y) * r.inv_d.y, bz = (a[2] - r.o.z) * r.inv_d.z;
@@ -263,14 +278,17 @@ __device__ __forceinline__ int4 box4(const Wide4Node* nd, const Ray& r, float tm
 // the leaves) ran 745 ms, and a 24-entry shared-memory stack 675 ms (its
 // 96 KB per SM comes out of the L1 that caches the BVH records).
 template <int kWidth, bool kCount>
-__device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav& q, int* stack, Counters& cnt)
+__device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav& q, int* stack, Counters& cnt,
+                                          const Wide4Node* s_top = nullptr, int top_n = 0)
 {
     if (kCount) cnt.nodes++;
     const float inf = __int_as_float(0x7f800000);
     if (kWidth == 4)
     {
         float t0, t1, t2, t3;
-        const int4 ln = box4(&s.nodes4[q.cur], r, q.t, t0, t1, t2, t3);
+        float a[8], b[8];
+        load_rec4(s, s_top, top_n, q.cur, a, b);
+        const int4 ln = box4(a, b, r, q.t, t0, t1, t2, t3);
         int l0 = ln.x, l1 = ln.y, l2 = ln.z, l3 = ln.w;
         cswap(t0, l0, t1, l1);
         cswap(t2, l2, t3, l3);
@@ -392,7 +410,7 @@ __device__ __forceinline__ int traverse_ray(const DevScene& s, const Ray& r, flo
 // lane's ray in flight; returns true when its traversal has finished.
 template <int kWidth, bool kCount, bool kWT>
 __device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool anyhit, bool busy, int quorum,
-                                          Trav& q, int* stack, Counters& cnt)
+                                          Trav& q, int* stack, Counters& cnt, const Wide4Node* s_top, int top_n)
 {
     if (busy && q.pend == 0 && q.cur < 0 && q.cur != kDone)
     {
@@ -406,7 +424,7 @@ __device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool 
     const bool holding = __any_sync(0xffffffffu, busy && !fin && q.pend != 0);
     if (n_searching > (unsigned)quorum || !holding)
     {
-        if (busy && q.cur >= 0) node_step<kWidth, kCount>(s, r, q, stack, cnt);
+        if (busy && q.cur >= 0) node_step<kWidth, kCount>(s, r, q, stack, cnt, s_top, top_n);
         return fin;
     }
     if (!busy || fin || q.pend == 0) return fin;

@@ -298,6 +298,21 @@ int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, fl
     return LG_OK;
 }
 
+int lg_unet_wait_selftest(lg_unet* u, int64_t limit_ns)
+{
+    if (!u) return set_error(LG_ERR_INVALID, "NULL argument");
+    if (limit_ns < 1000 || limit_ns > 2000000000ll)
+        return set_error(LG_ERR_INVALID, "wait limit must be 1 us .. 2 s (got %lld ns)", (long long)limit_ns);
+    LG_TRY(u->err.ensure(sizeof(int)));
+    LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), u->stream));
+    LG_TRY_CUDA(launch_wait_probe((int*)u->err.p, (unsigned long long)limit_ns, u->stream));
+    LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
+    int err = 0;
+    LG_TRY_CUDA(cudaMemcpy(&err, u->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return set_error(LG_ERR_DEVICE, "convolution kernel reported wait timeout %d", err);
+    return LG_OK;
+}
+
 int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y)
 {
     if (!u || !x || !y) return set_error(LG_ERR_INVALID, "NULL argument");

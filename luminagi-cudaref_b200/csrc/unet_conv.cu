@@ -902,4 +902,24 @@ cudaError_t from_blocked_bf16(const __nv_bfloat16* in, int N, int C, int H, int 
     from_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(in, N, C, H, W, out);
     return cudaGetLastError();
 }
+namespace
+{
+__global__ void wait_probe_kernel(int* err, unsigned long long limit_ns)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0)
+    {
+        tc::mbar_init(&bar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !tc::mbar_wait(&bar, 0, limit_ns)) atomicExch(err, 3);
+}
+}  // namespace
+
+cudaError_t launch_wait_probe(int* err, unsigned long long limit_ns, cudaStream_t stream)
+{
+    wait_probe_kernel<<<1, 32, 0, stream>>>(err, limit_ns);
+    return cudaGetLastError();
+}
 }  // namespace lg

@@ -88,6 +88,13 @@ cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, in
 // Launches the convolution reading `in` (blocked BF16, N x Cin x H x W).
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream);
 
+// The bounded wait of the convolution kernels (tc::mbar_wait) on an mbarrier
+// that nothing arrives at: after limit_ns the probe stores 3 in *err, as a
+// convolution kernel whose wait ran out stores its code, and returns.  It
+// issues no TMA copy or MMA, so nothing is left in flight; the context stays
+// usable.  Exercises the error path (device flag -> host status) on demand.
+cudaError_t launch_wait_probe(int* err, unsigned long long limit_ns, cudaStream_t stream);
+
 // FP32 NCHW (C channels) -> blocked BF16 with Cpad channels (zero padded);
 // log1p_in applies log1p to every value first (the HDR variant's input).
 cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,

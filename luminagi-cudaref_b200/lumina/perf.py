@@ -64,12 +64,17 @@ def trace(a):
     out = {"kernel": "trace", "spp": a.spp, "width": a.width, "tree": r.render_tree(), "rays": rays,
            "nodes_per_ray": c["node_fetches"] / rays, "tris_per_ray": c["tri_tests"] / rays}
     sweep = {}
-    for qu in (int(x) for x in str(a.quorum).split(",")):
-        r.set_leaf_quorum(qu)
-        for th in (int(x) for x in str(a.refill).split(",")):
-            r.set_refill_threshold(th)
-            ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"] for _ in range(a.reps)]
-            sweep[f"refill={th},quorum={qu}"] = {"ms": ms, "mrays_per_s": rays / min(ms) / 1e3}
+    for top in (int(x) for x in str(a.top).split(",")):
+        if hasattr(r, "set_top_records"):
+            r.set_top_records(top)
+        for qu in (int(x) for x in str(a.quorum).split(",")):
+            r.set_leaf_quorum(qu)
+            for th in (int(x) for x in str(a.refill).split(",")):
+                r.set_refill_threshold(th)
+                r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)
+                ms = [r.render(spp=a.spp, bounces=a.bounces, accum=False, rgb=False)["kernel_ms"]
+                      for _ in range(a.reps)]
+                sweep[f"refill={th},quorum={qu},top={top}"] = {"ms": ms, "mrays_per_s": rays / min(ms) / 1e3}
     if len(sweep) == 1:
         (k, v), = sweep.items()
         out.update(schedule=k, **v)
@@ -166,6 +171,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--refill", default="12", help="trace: refill threshold(s), comma-separated")
     ap.add_argument("--quorum", default="12", help="trace: leaf quorum(s), comma-separated")
+    ap.add_argument("--top", default="0", help="trace: top records kept in shared memory, comma-separated")
     ap.add_argument("--tune", type=int, default=1, help="batch: autotune the launch and schedule first (1/0)")
     ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)

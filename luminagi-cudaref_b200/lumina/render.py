@@ -132,6 +132,13 @@ class Renderer:
     def leaf_quorum(self) -> int:
         return int(lib().lg_renderer_get_leaf_quorum(self._h))
 
+    def set_top_records(self, n: int) -> None:
+        """4-wide BVH records (the top of the tree) each trace block keeps in shared memory; 0 = off."""
+        check(lib().lg_renderer_set_top_records(self._h, int(n)))
+
+    def top_records(self) -> int:
+        return int(lib().lg_renderer_get_top_records(self._h))
+
     def set_render_tree(self, mode: str) -> None:
         """Tree the traversal records come from: 'ploc_tris' (default; PLOC over the triangles, one per
         leaf), 'ploc' (PLOC over BuildBVH's leaves) or 'buildbvh' (its own topology)."""

@@ -241,10 +241,40 @@ def _sphere_uv(v):
                     -1)
 
 
+def look_at_f32(pos, target, camera_to_world=None):
+    """overwrite_camera (reference main.cpp:29-59) in float32 numpy, the same
+    single-precision operations in the same order as lg_look_at, so the two
+    agree bit for bit (checked by a test); lets the scene generators run
+    without the CUDA library.  Returns (pos, camera_to_world) or None when
+    |target - pos| < 1e-8 (the reference leaves the camera unchanged)."""
+    f = np.float32
+    p = np.asarray(pos, np.float32).reshape(3)
+    t = np.asarray(target, np.float32).reshape(3)
+    fx, fy, fz = f(t[0] - p[0]), f(t[1] - p[1]), f(t[2] - p[2])
+    fl = np.sqrt(f(f(f(fx * fx) + f(fy * fy)) + f(fz * fz)))
+    if fl < f(1e-8):
+        return None
+    fx, fy, fz = f(fx / fl), f(fy / fl), f(fz / fl)
+    lx, ly, lz = f(-fy), fx, f(0.0)
+    ll = np.sqrt(f(f(f(lx * lx) + f(ly * ly)) + f(lz * lz)))
+    if ll < f(1e-6):
+        lx, ly, lz, ll = f(0.0), f(1.0), f(0.0), f(1.0)
+    lx, ly, lz = f(lx / ll), f(ly / ll), f(lz / ll)
+    ux = f(f(fy * lz) - f(fz * ly))
+    uy = f(f(fz * lx) - f(fx * lz))
+    uz = f(f(fx * ly) - f(fy * lx))
+    m = np.array(camera_to_world if camera_to_world is not None else np.eye(4).ravel(), np.float32).copy()
+    m[0:4] = [fx, fy, fz, 0]
+    m[4:8] = [lx, ly, lz, 0]
+    m[8:12] = [ux, uy, uz, 0]
+    m[12:16] = [p[0], p[1], p[2], 1]
+    return p.copy(), m
+
+
 def look_at_camera(pos, target, width, height, fov=60.0, aspect=None) -> Camera:
-    base = Camera(np.zeros(3, np.float32), np.eye(4, dtype=np.float32).ravel(), fov,
-                  float(aspect if aspect is not None else width / height), 0.1, 1000.0, width, height)
-    return base.look_at(pos, target)
+    """A pinhole camera at pos looking at target (overwrite_camera's frame)."""
+    p, m = look_at_f32(pos, target)
+    return Camera(p, m, fov, float(aspect if aspect is not None else width / height), 0.1, 1000.0, width, height)
 
 
 def box_scene(seed: int = 1, width: int = 512, height: int = 256, sphere_subdiv: int = 4) -> Scene:

@@ -60,7 +60,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), str(ROOT / "bench.py"), "--impl", "reference",
            "--gpus", "2", "--steps", "1", "--warmup", "0", "--scene", "box", "--spp", "1", "--bounces", "0",
-           "--cpu-seconds", "0.5"]
+           "--cpu-row-step", "16"]
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]

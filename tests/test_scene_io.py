@@ -134,6 +134,23 @@ def test_look_at_matches_reference_formula():
     assert np.allclose(m[8:11], np.cross(f, l), atol=1e-6) and np.allclose(m[12:15], [1, 2, 3])
 
 
+def test_numpy_look_at_is_bit_identical_to_the_library():
+    """The scene generators' float32 restatement of overwrite_camera equals
+    lg_look_at bit for bit (so generated scenes need no CUDA library)."""
+    from lumina.scene import look_at_f32
+    rng = np.random.default_rng(3)
+    poses = [([1.0, 2.0, 3.0], [4.0, -2.0, 3.5]), ([0, 0, 0], [0, 0, 5.0]), ([0, 0, 0], [0, 0, -1.0]),
+             ([20.0, -6.0, 5.0], [0.3, 0.1, 1.7])]
+    poses += [(rng.uniform(-30, 30, 3), rng.uniform(-30, 30, 3)) for _ in range(200)]
+    base = lumina.Camera(np.zeros(3, np.float32), np.eye(4, dtype=np.float32).ravel(), 60.0, 2.0, 0.1, 1000.0,
+                         64, 32)
+    for pos, tgt in poses:
+        lib_cam = base.look_at(pos, tgt)
+        p, m = look_at_f32(pos, tgt, base.camera_to_world)
+        assert lib_cam.camera_to_world.tobytes() == m.tobytes(), (pos, tgt)
+        assert lib_cam.pos.tobytes() == p.tobytes()
+
+
 def test_abi_exports_every_declared_symbol():
     header = (ROOT / "include" / "lumina.h").read_text()
     declared = set(re.findall(r"\b(lg_[a-z0-9_]+)\s*\(", header))

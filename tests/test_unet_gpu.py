@@ -172,6 +172,57 @@ def test_unet_gradients_match_torch_autograd(in_ch):
     assert all(c > 0.98 and r < 0.25 for c, r, _ in worst), worst[:4]
 
 
+def _grad_errors(flat, g, model, noisy, clean, dtype):
+    """Per-tensor (cosine, relative L2) of the kernels' gradients g against
+    autograd through unet_ref.forward_bf16 in `dtype`."""
+    m = unet_ref.load_flat(model, flat).to(dtype)
+    out = unet_ref.forward_bf16(m, torch.from_numpy(noisy), dtype=dtype)
+    F.l1_loss(out, torch.from_numpy(clean).to(dtype)).backward()
+    off, res = 0, {}
+    for k, p in m.named_parameters():
+        gn = g[off:off + p.numel()].astype(np.float64)
+        off += p.numel()
+        gr = p.grad.double().numpy().ravel()
+        cos = float(np.dot(gn, gr) / (np.linalg.norm(gn) * np.linalg.norm(gr) + 1e-30))
+        rel = float(np.linalg.norm(gn - gr) / (np.linalg.norm(gr) + 1e-30))
+        res[k] = (cos, rel)
+    return res
+
+
+@pytest.mark.parametrize("in_ch", [3, 12])
+def test_unet_gradients_match_bf16_emulated_autograd(in_ch):
+    """Gradients vs autograd through the BF16-emulated restatement, which
+    rounds activations and weights where the kernels do, and (through the
+    casts' backward) the activation gradients where the kernels store them.
+    The emulation in FP32 against the same emulation in FP64 gives the noise
+    floor of that rounding (a value near a BF16 rounding boundary can go
+    either way); per tensor the kernels' relative L2 error against the FP64
+    emulation must stay within 3x that floor + 1%, and the cosine above
+    0.998."""
+    model = lambda: unet_ref.UNetRef(in_ch=in_ch)
+    flat = unet_ref.make_params(21, model())
+    net = lumina.UNet(in_ch=in_ch)
+    net.set_params(flat)
+    n, h, w = 2, 32, 48
+    noisy, clean = _batch(n, h, w, 4, in_ch)
+    dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
+    _, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
+    ours = _grad_errors(flat, g, model(), noisy, clean, torch.float64)
+    g32 = np.concatenate([p.ravel() for p in _autograd_bf16(flat, model(), noisy, clean, torch.float32)])
+    floor = _grad_errors(flat, g32, model(), noisy, clean, torch.float64)
+    worst = sorted(((ours[k][1] - 3 * floor[k][1], ours[k], floor[k], k) for k in ours), reverse=True)
+    print("worst tensors (excess, (cos, rel) ours vs emulation, (cos, rel) FP32 vs FP64 emulation):", worst[:4])
+    for _, (cos, rel), (_, frel), k in worst:
+        assert cos > 0.998 and rel <= 3 * frel + 0.01, (k, cos, rel, frel)
+
+
+def _autograd_bf16(flat, model, noisy, clean, dtype):
+    m = unet_ref.load_flat(model, flat).to(dtype)
+    out = unet_ref.forward_bf16(m, torch.from_numpy(noisy), dtype=dtype)
+    F.l1_loss(out, torch.from_numpy(clean).to(dtype)).backward()
+    return [p.grad.double().numpy().ravel() for p in m.parameters()]
+
+
 def test_unet_adam_step_and_training_reduces_loss():
     flat = unet_ref.make_params(22)
     net = lumina.UNet()
