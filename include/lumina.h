@@ -225,6 +225,13 @@ int lg_renderer_get_leaf_quorum(const lg_renderer* r);
  * from there (64 B each; at most LG_TOP_RECORDS_MAX, 0 = off).  The
  * reference stages its first 255 binary nodes the same way
  * (src/pathtracer.cu:44-50, 338-342).  Images do not depend on it. */
+/* Persisting-L2 access window (the reference's CUDAREF_L2_PIN knob,
+ * src/pathtracer.cu:675-693): with enable, the renderer's launches mark their
+ * accesses to the 4-wide BVH records as persisting in L2 (up to the device's
+ * persisting maximum, which this call also sets aside for the process).
+ * Images do not depend on it.  The C++ RenderSceneCUDA drop-in turns it on
+ * when the environment has CUDAREF_L2_PIN=1, as the reference does. */
+int lg_renderer_set_l2_window(lg_renderer* r, int enable);
 #define LG_TOP_RECORDS_DEFAULT 0
 #define LG_TOP_RECORDS_MAX 1024
 int lg_renderer_set_top_records(lg_renderer* r, int n);
@@ -347,16 +354,19 @@ int lg_unet_wait_selftest(lg_unet* u, int64_t limit_ns);
 /* Autotuner: for each of the 14 convolutions (and, with
  * LG_UNET_TUNE_BACKWARD, the 16 input-gradient convolutions of training)
  * times every compiled tile shape (output channels per CTA, input channels
- * per K-block, pipeline stages) with each of the two kernels (one tile per
- * CTA, or persistent and warp-specialised) inside real passes at n x h x w
- * and keeps the fastest; weights are repacked to match.  tiles_out (may be
- * NULL) receives 30 (bn, kc, stages, persistent) quadruples, forward layers
- * first.  The Adam state is reset. */
+ * per K-block, pipeline stages) with each of the kernels (0: one tile per
+ * CTA; 1: persistent and warp-specialised; 2: persistent with the layer's
+ * weights resident in shared memory, for layers with one output block whose
+ * weights fit beside the pipeline) inside real passes at n x h x w and keeps
+ * the fastest; weights are repacked to match.  tiles_out (may be NULL)
+ * receives 30 (bn, kc, stages, kernel) quadruples, forward layers first.
+ * The Adam state is reset. */
 #define LG_UNET_TUNE_BACKWARD 1
 int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_out);
 /* Sets the 30 tile choices directly, in lg_unet_autotune's format; e.g. to
  * reuse a tuning result without timing.  (0, 0, 0, p) is the default shape on
- * the kernel p selects (0: one tile per CTA, 1: persistent). */
+ * the kernel p selects (0: one tile per CTA, 1: persistent; 2 only with an
+ * explicit shape compiled for it). */
 int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles);
 /* One 3x3 convolution layer on device buffers in the channel-blocked BF16
  * layout ((n*C/8 + c/8)*H + y)*W + x)*8 + c%8: epilogue 0 writes act(conv+b)

@@ -118,6 +118,7 @@ struct lg_renderer
     int trace_quorum = LG_LEAF_QUORUM_DEFAULT;  // searching lanes below which a warp tests its held leaves (0..31)
     int trace_top = LG_TOP_RECORDS_DEFAULT;     // 4-wide records each trace block keeps in shared memory
     int n4 = 0;                                 // 4-wide records of the current scene
+    bool l2_window = false;                     // persisting-L2 access window over the 4-wide records
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
     // Traversal-stack overflow word (DevScene::fault) and its pinned host
@@ -162,6 +163,8 @@ struct DeviceGuard
         if (prev >= 0 && cur != prev) cudaSetDevice(prev);
     }
 };
+
+int apply_l2_window(lg_renderer* r);
 
 int validate_scene(const lg_scene_desc* d)
 {
@@ -253,7 +256,7 @@ int build_records(lg_renderer* r)
     r->n4 = root4 >= 0 ? n4 : 0;
     r->root = root;
     ++r->scene_gen;
-    return LG_OK;
+    return r->l2_window ? apply_l2_window(r) : LG_OK;
 }
 
 // Traversal records + intersection records from the device node/triangle arrays.
@@ -300,6 +303,32 @@ DevScene dev_scene(const lg_renderer* r)
     s.sun = r->sun;
     s.fault = r->fault.as<unsigned>();
     return s;
+}
+
+// The renderer stream's access-policy window: with l2_window, accesses of
+// its launches to the 4-wide records (up to the device's persisting-L2
+// maximum) are marked persisting, and the context's persisting L2 set-aside
+// is raised to that size (a per-process setting, released at exit);
+// otherwise no window.
+int apply_l2_window(lg_renderer* r)
+{
+    cudaStreamAttrValue attr{};
+    if (r->l2_window && r->n4 > 0)
+    {
+        int maxp = 0;
+        LG_TRY_CUDA(cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, r->device));
+        int maxw = 0;
+        LG_TRY_CUDA(cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, r->device));
+        const size_t bytes = std::min({(size_t)r->n4 * sizeof(Wide4Node), (size_t)maxp, (size_t)maxw});
+        LG_TRY_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, bytes));
+        attr.accessPolicyWindow.base_ptr = r->wide4.p;
+        attr.accessPolicyWindow.num_bytes = bytes;
+        attr.accessPolicyWindow.hitRatio = 1.0f;
+        attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    }
+    LG_TRY_CUDA(cudaStreamSetAttribute(r->stream, cudaStreamAttributeAccessPolicyWindow, &attr));
+    return LG_OK;
 }
 
 // Queues a copy of the device fault word into its pinned host copy, after
@@ -978,6 +1007,15 @@ int lg_renderer_get_leaf_quorum(const lg_renderer* r)
     return r->trace_quorum;
 }
 
+int lg_renderer_set_l2_window(lg_renderer* r, int enable)
+{
+    if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
+    DeviceGuard g(r->device);
+    r->l2_window = enable != 0;
+    ++r->scene_gen;  // captured batch graphs carry the stream's window
+    return apply_l2_window(r);
+}
+
 int lg_renderer_set_top_records(lg_renderer* r, int n)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
@@ -1378,6 +1416,10 @@ int open_renderer(const Scene& scene, const Bvh& bvh, const std::string& assetRo
     int dev = 0;
     cudaGetDevice(&dev);
     int rc = lg_renderer_create(dev, out);
+    // CUDAREF_L2_PIN=1: the reference's knob for a persisting-L2 window over
+    // the BVH (pathtracer.cu:675-693)
+    const char* pin = std::getenv("CUDAREF_L2_PIN");
+    if (rc == LG_OK && pin && std::atoi(pin)) rc = lg_renderer_set_l2_window(*out, 1);
     if (rc == LG_OK)
         rc = lg_renderer_set_scene_bvh(*out, &d, reinterpret_cast<const lg_bvh_node*>(bvh.nodes.data()),
                                        (int32_t)bvh.nodes.size());

@@ -464,19 +464,37 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 // Loads run ahead across tile boundaries; TMEM is allocated once per CTA.
 // The same packed weights, the same MMAs in the same order: results are
 // identical to conv3x3_tc_kernel's.
+// RESW (layers with one output block, Cout == BN): every K-block's weights
+// are copied into shared memory once per CTA, so a ring stage holds only the
+// input halo, and more stages fit; the weights are the same for every tile.
 constexpr int kPThreads = 192;
-template <int BN, int KC, int STAGES>
+template <int BN, int KC, bool RESW>
+struct PSmem
+{
+    using S = Smem<BN, KC>;
+    static constexpr int kStage = RESW ? ((S::kABytes + 1023) / 1024) * 1024 : S::kStage;
+    static constexpr int kBarBytes = 1024;  // mbarriers and the TMEM slot, after the ring
+    // dynamic shared memory of a launch with KB K-blocks (1024 B for aligning the base)
+    static constexpr int bytes(int stages, int KB)
+    {
+        return stages * kStage + kBarBytes + (RESW ? KB * S::kBBytes : 0) + 1024;
+    }
+};
+template <int BN, int KC, int STAGES, bool RESW>
 __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
 {
     using S = Smem<BN, KC>;
+    using P = PSmem<BN, KC, RESW>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * S::kStage);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * P::kStage);
     uint64_t* empty = full + STAGES;
     uint64_t* acc_full = empty + STAGES;  // [2]
     uint64_t* acc_empty = acc_full + 2;   // [2]
     uint64_t* done = acc_empty + 2;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* wfull = done + 1;  // RESW: the resident weights have landed
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wfull + 1);
+    uint8_t* wres = smem + STAGES * P::kStage + P::kBarBytes;  // RESW: KB x 9 x KC x BN weights
     __shared__ volatile int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -521,6 +539,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
             tc::mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
         }
         tc::mbar_init(done, 1);
+        tc::mbar_init(wfull, 1);
         tc::fence_mbar_init();
     }
     tc::tc_fence_before();
@@ -532,6 +551,14 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
     {
         if (lane == 0)
         {
+            if (RESW)
+            {
+                // all K-blocks of the single output block, one bulk copy each
+                tc::mbar_expect_tx(wfull, (uint32_t)(KB * S::kBBytes));
+                for (int kb = 0; kb < KB; ++kb)
+                    tc::bulk_load(wres + kb * S::kBBytes, a.wpack + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes,
+                                  wfull);
+            }
             int it = 0;
             for (int t = blockIdx.x; t < n_tiles && !s_fail; t += gridDim.x)
             {
@@ -546,11 +573,19 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                         fail(3);
                         break;
                     }
-                    uint8_t* A = smem + s * S::kStage;
-                    uint8_t* B = A + S::kABytes;
-                    tc::mbar_expect_tx(&full[s], (uint32_t)(S::kABytes + S::kBBytes));
-                    tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
-                    tc::bulk_load(B, wsrc + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes, &full[s]);
+                    uint8_t* A = smem + s * P::kStage;
+                    if (RESW)
+                    {
+                        tc::mbar_expect_tx(&full[s], (uint32_t)S::kABytes);
+                        tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
+                    }
+                    else
+                    {
+                        uint8_t* B = A + S::kABytes;
+                        tc::mbar_expect_tx(&full[s], (uint32_t)(S::kABytes + S::kBBytes));
+                        tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
+                        tc::bulk_load(B, wsrc + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes, &full[s]);
+                    }
                 }
             }
         }
@@ -560,6 +595,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
         if (lane == 0)
         {
             int it = 0, j = 0;
+            if (RESW && !tc::mbar_wait(wfull, 0)) fail(5);
             for (int t = blockIdx.x; t < n_tiles && !s_fail; t += gridDim.x, ++j)
             {
                 const int b = j & 1, v = j >> 1;
@@ -580,8 +616,9 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                         break;
                     }
                     tc::tc_fence_after();
-                    const uint32_t abase = tc::smem_u32(smem + s * S::kStage);
-                    const uint32_t bbase = abase + S::kABytes;
+                    const uint32_t abase = tc::smem_u32(smem + s * P::kStage);
+                    const uint32_t bbase =
+                        RESW ? tc::smem_u32(wres) + (uint32_t)(kb * S::kBBytes) : abase + (uint32_t)S::kABytes;
 #pragma unroll 1
                     for (int tap = 0; tap < 9; ++tap)
                     {
@@ -681,34 +718,44 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-template <int BN, int KC, int STAGES>
+// Dynamic shared memory a CTA may use on sm_100: 227 KB less 1 KB of headroom
+// for the kernel's static shared memory.
+constexpr int kMaxSmem = 226 * 1024;
+
+template <int BN, int KC, int STAGES, bool RESW = false>
 cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
 {
+    const int KB = a.Cin / KC;
+    if (RESW && a.Cout != BN) return cudaErrorInvalidValue;  // one output block only
+    const int smem = PSmem<BN, KC, RESW>::bytes(STAGES, KB);
+    if (smem > kMaxSmem) return cudaErrorInvalidValue;
     CUtensorMap m;
     cudaError_t e = make_map(&m, in, a.N, a.Cin, a.H, a.W, KC);
     if (e != cudaSuccess) return e;
-    const int smem = STAGES * Smem<BN, KC>::kStage + 1024 + 256;
-    static int per_sm = 0;
+    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW>;
+    // The resident-weights form's smem depends on KB: size the attribute for
+    // the largest launch it may see and query occupancy per launch size.
+    static bool attr_done = false;
     static int sm_count = 0;
-    if (per_sm == 0)
+    if (!attr_done)
     {
-        e = cudaFuncSetAttribute(conv3x3_tc_persistent<BN, KC, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem);
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
         if (e != cudaSuccess) return e;
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3x3_tc_persistent<BN, KC, STAGES>, kPThreads,
-                                                          smem);
-        if (e != cudaSuccess) return e;
-        // TMEM: each CTA holds 4*BN of the SM's 512 columns for its lifetime
-        const int tmem_fit = 512 / (4 * BN);
-        if (per_sm > tmem_fit) per_sm = tmem_fit;
-        if (per_sm < 1) per_sm = 1;
+        attr_done = true;
     }
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPThreads, smem);
+    if (e != cudaSuccess) return e;
+    // TMEM: each CTA holds 4*BN of the SM's 512 columns for its lifetime
+    const int tmem_fit = 512 / (4 * BN);
+    if (per_sm > tmem_fit) per_sm = tmem_fit;
+    if (per_sm < 1) per_sm = 1;
     const long long tiles = (long long)((a.W + kTileX - 1) / kTileX) * ((a.H + kRows - 1) / kRows) * a.N * (a.Cout / BN);
     const long long grid = std::min<long long>(tiles, (long long)per_sm * sm_count);
-    conv3x3_tc_persistent<BN, KC, STAGES><<<(unsigned)grid, kPThreads, smem, stream>>>(m, a);
+    fn<<<(unsigned)grid, kPThreads, smem, stream>>>(m, a);
     return cudaGetLastError();
 }
 
@@ -817,13 +864,26 @@ ConvTile conv_default_tile(int Cin, int Cout) { return pick_cfg(Cin, Cout); }
 constexpr ConvTile kCompiledTiles[] = {{32, 16, 4, 0},  {32, 32, 2, 0},  {32, 32, 4, 0},  {64, 16, 4, 0},
                                        {64, 32, 2, 0},  {64, 32, 3, 0},  {128, 16, 3, 0}, {128, 32, 2, 0},
                                        {32, 16, 4, 1},  {32, 32, 2, 1},  {32, 32, 4, 1},  {64, 16, 4, 1},
-                                       {64, 32, 2, 1},  {64, 32, 3, 1},  {128, 16, 3, 1}, {128, 32, 2, 1}};
+                                       {64, 32, 2, 1},  {64, 32, 3, 1},  {128, 16, 3, 1}, {128, 32, 2, 1},
+                                       {32, 16, 10, 2}, {32, 32, 2, 2},  {32, 32, 5, 2},  {32, 32, 6, 2},
+                                       {64, 32, 3, 2},  {64, 32, 4, 2}};
+
+// Shared memory of a tile shape's launch for a layer with Cin input channels.
+int tile_smem(const ConvTile& t, int Cin)
+{
+    const int KB = Cin / t.kc;
+    const int a = 4 * 130 * t.kc * 2, b = 9 * t.kc * t.bn * 2;
+    if (t.persist == 2) return t.stages * (((a + 1023) / 1024) * 1024) + 1024 + KB * b + 1024;
+    return t.stages * (((a + b + 1023) / 1024) * 1024) + 1024 + 1024;
+}
 
 int conv_tile_candidates(int Cin, int Cout, ConvTile* out, int max)
 {
     int k = 0;
     for (const ConvTile& t : kCompiledTiles)
-        if (k < max && t.bn <= Cout && Cout % t.bn == 0 && Cin % t.kc == 0) out[k++] = t;
+        if (k < max && t.bn <= Cout && Cout % t.bn == 0 && Cin % t.kc == 0 &&
+            (t.persist != 2 || (t.bn == Cout && tile_smem(t, Cin) <= kMaxSmem)))
+            out[k++] = t;
     return k;
 }
 
@@ -861,6 +921,17 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
     const TileCfg c = resolve(a.tile, a.Cin, a.Cout);
     if (a.Cout % c.bn || a.Cin % c.kc) return cudaErrorInvalidValue;
     const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    if (c.persist == 2)
+        switch (key)
+        {
+        case 32170: return launch_persistent<32, 16, 10, true>(in, a, stream);
+        case 32322: return launch_persistent<32, 32, 2, true>(in, a, stream);
+        case 32325: return launch_persistent<32, 32, 5, true>(in, a, stream);
+        case 32326: return launch_persistent<32, 32, 6, true>(in, a, stream);
+        case 64323: return launch_persistent<64, 32, 3, true>(in, a, stream);
+        case 64324: return launch_persistent<64, 32, 4, true>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
     if (c.persist)
         switch (key)
         {

@@ -482,7 +482,9 @@ int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
     ConvTile fwd[14], bwd[16];
     for (int i = 0; i < 30; ++i)
     {
-        ConvTile t{tiles[4 * i], tiles[4 * i + 1], tiles[4 * i + 2], tiles[4 * i + 3] != 0 ? 1 : 0};
+        const int p4 = tiles[4 * i + 3];
+        if (p4 < 0 || p4 > 2) return set_error(LG_ERR_INVALID, "conv %d: kernel choice %d is not 0, 1 or 2", i, p4);
+        ConvTile t{tiles[4 * i], tiles[4 * i + 1], tiles[4 * i + 2], p4};
         const bool back = i >= 14;
         const int cin = back ? kLayers[kDgrad[i - 14].layer].cout : kLayers[i].cin;
         const int cout = back ? kDgrad[i - 14].ci_cnt : kLayers[i].cout;
@@ -492,7 +494,7 @@ int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
             const int persist = t.persist;
             t = conv_default_tile(cin, cout);
             t.persist = persist;
-            ok = true;
+            ok = persist != 2;  // the resident-weights kernel is compiled for some shapes only
         }
         ConvTile cand[32];
         const int nc = conv_tile_candidates(cin, cout, cand, 32);

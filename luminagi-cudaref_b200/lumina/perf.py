@@ -20,6 +20,12 @@ def _events(torch):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
+# Forward convs (d1a .. u1b) on the persistent kernel with resident weights
+# where the layer has one output block and its weights fit beside the ring.
+RESIDENT_TILES = [(32, 16, 10, 2), (32, 32, 6, 2), (64, 32, 4, 2), (64, 32, 4, 2)] + [(0, 0, 0, 1)] * 7 + \
+                 [(64, 32, 4, 2), (32, 32, 5, 2), (32, 32, 6, 2)]
+
+
 def unet(a):
     import torch
 
@@ -29,6 +35,8 @@ def unet(a):
     tiles = None
     if a.kernel == "single":
         net.set_tiles([(0, 0, 0, 0)] * 30)
+    elif a.kernel == "resident":
+        net.set_tiles(RESIDENT_TILES + [(0, 0, 0, 1)] * 16)
     elif a.kernel == "autotune":
         tiles = net.autotune(a.n, a.h, a.w)[:14]
     x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
@@ -64,6 +72,9 @@ def trace(a):
     out = {"kernel": "trace", "spp": a.spp, "width": a.width, "tree": r.render_tree(), "rays": rays,
            "nodes_per_ray": c["node_fetches"] / rays, "tris_per_ray": c["tri_tests"] / rays}
     sweep = {}
+    if a.l2win:
+        r.set_l2_window(True)
+        out["l2_window"] = True
     for top in (int(x) for x in str(a.top).split(",")):
         if hasattr(r, "set_top_records"):
             r.set_top_records(top)
@@ -160,8 +171,9 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["unet", "trace", "bvh", "batch"])
     ap.add_argument("--poses", type=int, default=50)
-    ap.add_argument("--kernel", default="default", choices=["default", "single", "autotune"],
-                    help="unet: default tiles, the one-tile-per-CTA conv kernel, or autotuned tiles")
+    ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "autotune"],
+                    help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
+                         "single-block layers, or autotuned tiles")
     ap.add_argument("--n", type=int, default=1)
     ap.add_argument("--h", type=int, default=864)
     ap.add_argument("--w", type=int, default=1728)
@@ -172,6 +184,7 @@ def main(argv=None):
     ap.add_argument("--refill", default="12", help="trace: refill threshold(s), comma-separated")
     ap.add_argument("--quorum", default="12", help="trace: leaf quorum(s), comma-separated")
     ap.add_argument("--top", default="0", help="trace: top records kept in shared memory, comma-separated")
+    ap.add_argument("--l2win", type=int, default=0, help="trace: persisting-L2 window over the BVH records (1/0)")
     ap.add_argument("--tune", type=int, default=1, help="batch: autotune the launch and schedule first (1/0)")
     ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)

@@ -132,6 +132,10 @@ class Renderer:
     def leaf_quorum(self) -> int:
         return int(lib().lg_renderer_get_leaf_quorum(self._h))
 
+    def set_l2_window(self, enable: bool) -> None:
+        """Persisting-L2 access window over the 4-wide BVH records (the reference's CUDAREF_L2_PIN)."""
+        check(lib().lg_renderer_set_l2_window(self._h, 1 if enable else 0))
+
     def set_top_records(self, n: int) -> None:
         """4-wide BVH records (the top of the tree) each trace block keeps in shared memory; 0 = off."""
         check(lib().lg_renderer_set_top_records(self._h, int(n)))

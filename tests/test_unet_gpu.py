@@ -384,3 +384,32 @@ def test_persistent_conv_kernel_is_bit_identical():
     assert abs(l0 - l1) <= 1e-6 * max(1.0, abs(l0))
     cos = float(np.dot(g0, g1) / (np.linalg.norm(g0) * np.linalg.norm(g1)))
     assert cos > 0.9999
+
+
+# Forward convs in order (d1a .. u1b) with the resident-weights kernel where
+# the layer has one output block and its weights fit beside the ring.
+RESIDENT_TILES = [(32, 16, 10, 2), (32, 32, 6, 2), (64, 32, 4, 2), (64, 32, 4, 2)] + [(0, 0, 0, 1)] * 7 + \
+                 [(64, 32, 4, 2), (32, 32, 5, 2), (32, 32, 6, 2)]
+
+
+def test_resident_weight_conv_kernel_is_bit_identical():
+    """The persistent kernel with the weights resident in shared memory (one
+    copy per CTA instead of one per ring stage) runs the same MMAs in the
+    same order: outputs and loss are bit-identical to the plain persistent
+    kernel's, at batch 1 and 2, with partial edge tiles."""
+    flat = unet_ref.make_params(81)
+    for n, h, w in ((1, 40, 264), (2, 64, 136)):
+        x = np.random.default_rng(10).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
+        noisy, clean = _batch(n, h, w, 13)
+        dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
+        outs = []
+        for tiles in ([(0, 0, 0, 1)] * 30, RESIDENT_TILES + [(0, 0, 0, 1)] * 16):
+            net = lumina.UNet()
+            net.set_params(flat)
+            net.set_tiles(tiles)
+            y = net.forward(x)
+            loss, _ = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
+            outs.append((y, loss))
+            net.close()
+        assert np.array_equal(outs[0][0], outs[1][0])
+        assert outs[0][1] == outs[1][1]
