@@ -446,14 +446,15 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
 // 8x4 pixel tile, so neighbouring lanes start on neighbouring pixels.
 // kBatch: several frames per launch (job.jobs), each item mapped to its frame
 // at refill; the frame's camera and bounce limit are read from the job table.
-template <bool kCount, bool kAcc64, int kWidth, bool kWT, bool kBatch>
+template <bool kCount, bool kAcc64, int kWidth, bool kWT, bool kBatch, bool kTop = false>
 __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
 {
-    // The top of the tree (the first top_n records in BFS order), copied once
-    // per block into dynamic shared memory; every ray starts there.
+    // kTop: the top of the tree (the first top_n records in BFS order), copied
+    // once per block into dynamic shared memory; every ray starts there.  The
+    // other instantiations carry no trace of it (top_n is the constant 0).
     extern __shared__ __align__(32) float4 smem_top[];
     const Wide4Node* s_top = reinterpret_cast<const Wide4Node*>(smem_top);
-    const int top_n = kWidth == 4 ? min(job.top_records, s.n4) : 0;
+    const int top_n = (kTop && kWidth == 4) ? min(job.top_records, s.n4) : 0;
     for (int i = threadIdx.x; i < top_n * 4; i += kTraceThreads)
         smem_top[i] = __ldg(reinterpret_cast<const float4*>(s.nodes4) + i);
     __syncthreads();
@@ -772,12 +773,12 @@ cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bo
     return cudaGetLastError();
 }
 
-template <bool kCount, bool kAcc64, int W, bool kWT, bool kBatch = false>
+template <bool kCount, bool kAcc64, int W, bool kWT, bool kBatch = false, bool kTop = false>
 static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const TraceJob& job, int sm_count,
                                   cudaStream_t stream)
 {
-    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT, kBatch>;
-    const int top_n = W == 4 ? std::min(std::max(job.top_records, 0), s.n4) : 0;
+    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT, kBatch, kTop>;
+    const int top_n = (kTop && W == 4) ? std::min(std::max(job.top_records, 0), s.n4) : 0;
     const size_t smem = (size_t)top_n * sizeof(Wide4Node);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -792,7 +793,7 @@ static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const Tr
     if (blocks < 1) blocks = 1;
     e = cudaMemsetAsync(job.work64, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    trace_kernel<kCount, kAcc64, W, kWT, kBatch><<<(int)blocks, kTraceThreads, smem, stream>>>(s, cam, job);
+    trace_kernel<kCount, kAcc64, W, kWT, kBatch, kTop><<<(int)blocks, kTraceThreads, smem, stream>>>(s, cam, job);
     return cudaGetLastError();
 }
 
@@ -800,6 +801,9 @@ cudaError_t launch_trace_batch(const DevScene& s, const TraceJob& job, int sm_co
                                cudaStream_t stream)
 {
     const DevCam none{};
+    if (width == 4 && job.top_records > 0)
+        return watertight ? launch_trace_t<false, false, 4, true, true, true>(s, none, job, sm_count, stream)
+                          : launch_trace_t<false, false, 4, false, true, true>(s, none, job, sm_count, stream);
     if (watertight)
         return width == 4 ? launch_trace_t<false, false, 4, true, true>(s, none, job, sm_count, stream)
                           : launch_trace_t<false, false, 2, true, true>(s, none, job, sm_count, stream);
@@ -811,6 +815,10 @@ template <int W, bool kWT>
 static cudaError_t launch_trace_w(const DevScene& s, const DevCam& cam, const TraceJob& job, bool count, int sm_count,
                                  cudaStream_t stream)
 {
+    // the shared-memory top records serve the plain 4-wide frames (they change no result, so
+    // counting and FP64 frames run without them)
+    if (W == 4 && job.top_records > 0 && !count && !job.accum64)
+        return launch_trace_t<false, false, W, kWT, false, true>(s, cam, job, sm_count, stream);
     if (count)
         return job.accum64 ? launch_trace_t<true, true, W, kWT>(s, cam, job, sm_count, stream)
                            : launch_trace_t<true, false, W, kWT>(s, cam, job, sm_count, stream);

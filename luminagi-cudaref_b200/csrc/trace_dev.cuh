@@ -226,7 +226,7 @@ __device__ __forceinline__ float qplane(uint32_t w, int k)
 __device__ __forceinline__ void load_rec4(const DevScene& s, const Wide4Node* s_top, int top_n, int i, float (&a)[8],
                                           float (&b)[8])
 {
-    if (i < top_n)
+    if ((unsigned)i < (unsigned)top_n)  // never true when top_n is the constant 0
     {
         const float4* p = reinterpret_cast<const float4*>(s_top + i);
         const float4 x = p[0], y = p[1], z = p[2], w = p[3];

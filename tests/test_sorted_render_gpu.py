@@ -71,15 +71,15 @@ def test_sort_only_reorders_work_without_bounces(box_scene):
     """With no bounce, no draw follows the camera jitter, so the sort cannot
     change the image: sorted and unsorted give the same accumulator bits, and
     the persistent trace kernel (one sample: its chunk seed is the sample
-    seed) the same image up to exact ties in t, which its traversal order may
-    break differently."""
+    seed) the same image within the render bar (the two kernels may contract
+    the same FP32 expressions into FMAs differently)."""
     with lumina.Renderer(0) as r:
         r.set_scene(box_scene)
         a = r.render_sorted(spp=1, bounces=0)["accum"]
         b = r.render_sorted(spp=1, bounces=0, sort=False)["accum"]
         c = r.render(spp=1, bounces=0)["accum"]
     assert np.array_equal(a, b)
-    assert match_fraction(a, c, rel=0.0, abs_=0.0) >= 0.9999
+    assert match_fraction(a, c) >= 0.9999
 
 
 def test_sorted_counts_and_estimator(box_scene):
