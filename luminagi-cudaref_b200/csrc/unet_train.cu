@@ -234,8 +234,13 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
         a.Cin_real = layer_cin_real(u, L);
         a.dw = G + u->w_off[L];
         a.err = (int*)u->err.p;
+        LG_TRY(u->wpart.ensure(conv3x3_wgrad_partial_floats(N, a.H, a.Cout, a.Cin, a.Cin_real, u->sm_count) *
+                               sizeof(float)));
+        LG_TRY(u->bpart.ensure(conv_bias_grad_partial_floats(a.Cout) * sizeof(float)));
+        a.partial = (float*)u->wpart.p;
         LG_TRY_CUDA(conv3x3_wgrad((const bf*)u->dz[L].p, (const bf*)in_of[L], a, u->sm_count, st));
-        LG_TRY_CUDA(conv_bias_grad((const bf*)u->dz[L].p, N, kLayers[L].cout, hs[lv], ws[lv], G + u->b_off[L], st));
+        LG_TRY_CUDA(conv_bias_grad((const bf*)u->dz[L].p, N, kLayers[L].cout, hs[lv], ws[lv], G + u->b_off[L],
+                                   (float*)u->bpart.p, st));
         return LG_OK;
     };
     auto dgrad = [&](int k, void* out, int out_c, const void* ref, int ref_c, int ref_coff, const void* skip,

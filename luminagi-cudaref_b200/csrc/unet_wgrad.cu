@@ -9,8 +9,10 @@
 // MMA's MN-major no-swizzle layout with K = pixels.  One CTA owns one kernel
 // row ky and all three kx taps: the X box is 130 pixels wide and tap kx reads
 // it 16*kx bytes further on, accumulating into three TMEM tiles.  Each CTA
-// sums a chunk of image rows and adds its partial dW to global memory with
-// FP32 atomics.
+// sums a chunk of image rows and stores its partial dW in a scratch slice of
+// its own; a second pass adds the chunks' partials to dW in chunk order, so
+// gradients (and training) are bit-reproducible.
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -144,35 +146,40 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::mma_commit(done);
     }
     __syncwarp();
+    // This CTA's slice of the scratch: chunk blockIdx.x of [chunk][Cout][Cin_real][3][3].
+    float* part = a.partial + (size_t)blockIdx.x * a.Cout * a.Cin_real * 9;
+    const int co = co0 + tid;  // TMEM lane = output channel
+    bool have = false;
     if (steps > 0)
     {
         const bool got = tc::mbar_wait(done, 0);
         if (!got && a.err) atomicExch(a.err, 4);
         tc::tc_fence_after();
-        const int co = co0 + tid;  // TMEM lane = output channel
-        if (got && !s_fail)
-        {
-            const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-            for (int dx = 0; dx < 3; ++dx)
-#pragma unroll 1
-                for (int c0 = 0; c0 < BNW; c0 += 16)
-                {
-                    float v[16];
-                    tc::tmem_ld16(lanebase + (uint32_t)(dx * BNW + c0), v);
-                    if (co < a.Cout)
-                    {
-#pragma unroll
-                        for (int j = 0; j < 16; ++j)
-                        {
-                            const int ci = ci0 + c0 + j;
-                            if (ci < a.Cin_real)
-                                atomicAdd(&a.dw[(((size_t)co * a.Cin_real + ci) * 3 + ky) * 3 + dx], v[j]);
-                        }
-                    }
-                }
-        }
+        have = got && !s_fail;
     }
+    const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int dx = 0; dx < 3; ++dx)
+#pragma unroll 1
+        for (int c0 = 0; c0 < BNW; c0 += 16)
+        {
+            float v[16];
+            if (have) tc::tmem_ld16(lanebase + (uint32_t)(dx * BNW + c0), v);
+            else
+            {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = 0.0f;  // an empty chunk (or a failed one) adds zeros
+            }
+            if (co < a.Cout)
+            {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                    const int ci = ci0 + c0 + j;
+                    if (ci < a.Cin_real) part[(((size_t)co * a.Cin_real + ci) * 3 + ky) * 3 + dx] = v[j];
+                }
+            }
+        }
     tc::tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -213,6 +220,33 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// dw[e] += partial[0][e] + partial[1][e] + ... in chunk order.
+__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int chunks, size_t n, float* __restrict__ dw)
+{
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    {
+        float s = 0.0f;
+        for (int c = 0; c < chunks; ++c) s += partial[(size_t)c * n + e];
+        dw[e] += s;
+    }
+}
+
+// Row chunks of a launch: about two CTAs per SM over the (ky, input block,
+// output block) grid, at most one per image row.
+int wgrad_chunks(int N, int H, int Cout, int Cin, int bnw, int sm_count, int* rows_per_cta)
+{
+    const int cot = (Cout + 127) / 128, cit = Cin / bnw;
+    const int rows = N * H;
+    int chunks = (2 * sm_count) / (3 * cit * cot);
+    if (chunks < 1) chunks = 1;
+    if (chunks > rows) chunks = rows;
+    const int rpc = (rows + chunks - 1) / chunks;
+    if (rows_per_cta) *rows_per_cta = rpc;
+    return (rows + rpc - 1) / rpc;
+}
+
+int wgrad_bnw(int Cin) { return Cin % 128 == 0 ? 128 : Cin % 64 == 0 ? 64 : Cin % 32 == 0 ? 32 : 16; }
+
 template <int BNW>
 cudaError_t launch_w(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
                      cudaStream_t stream)
@@ -232,19 +266,22 @@ cudaError_t launch_w(const __nv_bfloat16* dz, const __nv_bfloat16* x, const Wgra
     }
     WgradArgs b = a;
     const int cot = (a.Cout + 127) / 128, cit = a.Cin / BNW;
-    const int rows = a.N * a.H;
-    int chunks = (2 * sm_count) / (3 * cit * cot);
-    if (chunks < 1) chunks = 1;
-    if (chunks > rows) chunks = rows;
-    b.rows_per_cta = (rows + chunks - 1) / chunks;
-    chunks = (rows + b.rows_per_cta - 1) / b.rows_per_cta;
+    const int chunks = wgrad_chunks(a.N, a.H, a.Cout, a.Cin, BNW, sm_count, &b.rows_per_cta);
     dim3 grid(chunks, 3 * cit, cot);
     wgrad_kernel<BNW><<<grid, kThreads, smem, stream>>>(mdz, mx, b);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t n = (size_t)a.Cout * a.Cin_real * 9;
+    wgrad_reduce_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 1184), 256, 0, stream>>>(b.partial, chunks, n,
+                                                                                               a.dw);
     return cudaGetLastError();
 }
 
-__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW, float* __restrict__ db)
+constexpr int kBiasBlocks = 64;  // blocks per 8-channel group; each writes its own partial
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW,
+                                 float* __restrict__ partial)
 {
+    __shared__ float warp_sum[8][8];
     // block (c-block, chunk): 8 channels of a range of pixels
     const int cb = blockIdx.y;
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -262,21 +299,46 @@ __global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, in
             acc[2 * i + 1] += f.y;
         }
     }
+    const int warp = threadIdx.x >> 5;
 #pragma unroll
     for (int i = 0; i < 8; ++i)
     {
         float v = acc[i];
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&db[cb * 8 + i], v);
+        if ((threadIdx.x & 31) == 0) warp_sum[warp][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8)
+    {
+        float s = 0.0f;
+        for (int w = 0; w < 8; ++w) s += warp_sum[w][threadIdx.x];  // warps in order
+        partial[((size_t)cb * kBiasBlocks + blockIdx.x) * 8 + threadIdx.x] = s;
     }
 }
+
+// db[c] += the kBiasBlocks partials of channel c, in block order.
+__global__ void bias_reduce_kernel(const float* __restrict__ partial, int C, float* __restrict__ db)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= C) return;
+    const int cb = c >> 3, i = c & 7;
+    float s = 0.0f;
+    for (int b = 0; b < kBiasBlocks; ++b) s += partial[((size_t)cb * kBiasBlocks + b) * 8 + i];
+    db[c] += s;
+}
 }  // namespace
+
+size_t conv3x3_wgrad_partial_floats(int N, int H, int Cout, int Cin, int Cin_real, int sm_count)
+{
+    const int chunks = wgrad_chunks(N, H, Cout, Cin, wgrad_bnw(Cin), sm_count, nullptr);
+    return (size_t)chunks * Cout * Cin_real * 9;
+}
 
 cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
                           cudaStream_t stream)
 {
-    if (a.Cout % 32 || a.Cin % 16) return cudaErrorInvalidValue;
-    const int bnw = a.Cin % 128 == 0 ? 128 : a.Cin % 64 == 0 ? 64 : a.Cin % 32 == 0 ? 32 : 16;
+    if (a.Cout % 32 || a.Cin % 16 || !a.partial) return cudaErrorInvalidValue;
+    const int bnw = wgrad_bnw(a.Cin);
     switch (bnw)
     {
     case 128: return launch_w<128>(dz, x, a, sm_count, stream);
@@ -286,10 +348,17 @@ cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const
     }
 }
 
-cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, cudaStream_t stream)
+size_t conv_bias_grad_partial_floats(int C) { return (size_t)(C / 8) * kBiasBlocks * 8; }
+
+cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, float* partial,
+                           cudaStream_t stream)
 {
-    dim3 grid(64, C / 8);
-    bias_grad_kernel<<<grid, 256, 0, stream>>>(dz, N, C, H * W, db);
+    if (!partial || C % 8) return cudaErrorInvalidValue;
+    dim3 grid(kBiasBlocks, C / 8);
+    bias_grad_kernel<<<grid, 256, 0, stream>>>(dz, N, C, H * W, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    bias_reduce_kernel<<<(C + 255) / 256, 256, 0, stream>>>(partial, C, db);
     return cudaGetLastError();
 }
 }  // namespace lg

@@ -14,11 +14,20 @@ struct WgradArgs
     int rows_per_cta;  // set by the launcher
     float* dw;      // [Cout][Cin_real][3][3], added to
     int* err;
+    // Scratch of conv3x3_wgrad_partial_floats() floats: each CTA stores its
+    // partial sums there and one pass adds them to dw in chunk order, so the
+    // gradient does not depend on the order the CTAs finish in.
+    float* partial;
 };
 
+// Floats of WgradArgs::partial the launch for this layer shape needs.
+size_t conv3x3_wgrad_partial_floats(int N, int H, int Cout, int Cin, int Cin_real, int sm_count);
 // dW += sum over pixels of dZ (x) shifted X; both blocked BF16 at N x C x H x W.
 cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
                           cudaStream_t stream);
-// db += sum over pixels of dZ.
-cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, cudaStream_t stream);
+// Floats of scratch conv_bias_grad needs for C channels.
+size_t conv_bias_grad_partial_floats(int C);
+// db += sum over pixels of dZ, summed in a fixed order through `partial`.
+cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, float* partial,
+                           cudaStream_t stream);
 }  // namespace lg

@@ -4,6 +4,7 @@
     python -m lumina.perf trace [--spp 8] [--bounces 2] [--width 4] [--reps 2]
     python -m lumina.perf bvh   [--reps 5]
     python -m lumina.perf batch [--poses 50] [--spp 8] [--bounces 2]
+    python -m lumina.perf membench
 
 Prints one JSON line.  Used for the profiles (run under ncu) and for quick
 A/B measurements; bench.py is the benchmark of record.
@@ -167,9 +168,26 @@ def batch(a):
     return out
 
 
+def membench(a):
+    """Read bandwidth of the L2 (buffers of 8-96 MB, L2-only loads) and of L1
+    (every block re-reading a 16 KB region), lg_measure_read_bandwidth."""
+    import ctypes as C
+
+    from . import _ffi
+    out = {"kernel": "membench", "l2_gbs": {}, "l1_gbs": {}}
+    g = C.c_double(0)
+    for mb in (8, 16, 32, 48, 64, 96):
+        _ffi.check(_ffi.lib().lg_measure_read_bandwidth(0, 2, mb << 20, 40, C.byref(g)))
+        out["l2_gbs"][f"{mb}MB"] = g.value
+    for kb in (4, 16, 32):
+        _ffi.check(_ffi.lib().lg_measure_read_bandwidth(0, 1, kb << 10, 400, C.byref(g)))
+        out["l1_gbs"][f"{kb}KB"] = g.value
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["unet", "trace", "bvh", "batch"])
+    ap.add_argument("what", choices=["unet", "trace", "bvh", "batch", "membench"])
     ap.add_argument("--poses", type=int, default=50)
     ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "autotune"],
                     help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
@@ -188,7 +206,7 @@ def main(argv=None):
     ap.add_argument("--tune", type=int, default=1, help="batch: autotune the launch and schedule first (1/0)")
     ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)
-    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch}[a.what](a)))
+    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch, "membench": membench}[a.what](a)))
 
 
 if __name__ == "__main__":
