@@ -232,6 +232,14 @@ int lg_renderer_get_leaf_quorum(const lg_renderer* r);
  * Images do not depend on it.  The C++ RenderSceneCUDA drop-in turns it on
  * when the environment has CUDAREF_L2_PIN=1, as the reference does. */
 int lg_renderer_set_l2_window(lg_renderer* r, int enable);
+/* No counterpart in the reference (whose traversal drops pushes past its
+ * 64-entry stack without a word, src/pathtracer.cu:142, 184).  The most
+ * traversal-stack entries any ray can need over the current scene's records
+ * (computed when they are built: per root-to-record path, the sum of each
+ * record's children less one) and the stack's capacity.  When the bound fits,
+ * frames are traced without per-push checks; otherwise every push is checked
+ * and one that does not fit makes the render return LG_ERR_DEVICE. */
+int lg_renderer_get_stack_bound(const lg_renderer* r, int32_t* bound, int32_t* capacity);
 #define LG_TOP_RECORDS_DEFAULT 0
 #define LG_TOP_RECORDS_MAX 1024
 int lg_renderer_set_top_records(lg_renderer* r, int n);

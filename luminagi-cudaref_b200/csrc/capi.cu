@@ -118,6 +118,7 @@ struct lg_renderer
     int trace_quorum = LG_LEAF_QUORUM_DEFAULT;  // searching lanes below which a warp tests its held leaves (0..31)
     int trace_top = LG_TOP_RECORDS_DEFAULT;     // 4-wide records each trace block keeps in shared memory
     int n4 = 0;                                 // 4-wide records of the current scene
+    int stack4 = 1 << 30, stack2 = 1 << 30;     // traversal-stack bounds of the records (build_wide4_nodes)
     bool l2_window = false;                     // persisting-L2 access window over the 4-wide records
     lg_bvh_node root_node{};  // host copy of the BVH root (scene box for the G-buffer)
     DevBuf gbuf;              // G-buffer images (3 x W*H*3 bytes)
@@ -249,7 +250,7 @@ int build_records(lg_renderer* r)
     LG_TRY_CUDA(cudaMemcpyAsync(r->leaves.as<int2>() + nl, &kEmptyLeaf, sizeof(int2), cudaMemcpyHostToDevice,
                                 r->stream));
     LG_TRY_CUDA(build_wide4_nodes(r->rnodes.as<lg_bvh_node>(), n, r->n_tris, nl, r->wide4.as<Wide4Node>(),
-                                  r->scratch.as<int>(), &root4, &n4, &leaf_inline, r->stream));
+                                  r->scratch.as<int>(), &root4, &n4, &leaf_inline, &r->stack4, &r->stack2, r->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(r->stream));
     r->leaf_inline = leaf_inline;
     r->root4 = root4;
@@ -331,6 +332,14 @@ int apply_l2_window(lg_renderer* r)
     return LG_OK;
 }
 
+// True when no traversal over the current records can need more than the
+// traversal stack's entries (the bound build_wide4_nodes computed), so the
+// trace launches may leave out the per-push check.
+bool stack_safe(const lg_renderer* r)
+{
+    return (r->bvh_width == 4 ? r->stack4 : r->stack2) <= kTraceStack;
+}
+
 // Queues a copy of the device fault word into its pinned host copy, after
 // the launches already on `st`.
 cudaError_t post_fault(lg_renderer* r, cudaStream_t st)
@@ -384,6 +393,7 @@ int render_into_device(lg_renderer* r, const lg_camera* cam, const lg_render_opt
         job.refill_threshold = r->trace_refill;
         job.leaf_quorum = r->trace_quorum;
         job.top_records = r->trace_top;
+        job.stack_safe = stack_safe(r);
         LG_TRY_CUDA(launch_trace(s, make_dev_cam(*cam), job, r->counting, r->sm_count, r->bvh_width, r->watertight,
                                  r->stream));
     }
@@ -1007,6 +1017,14 @@ int lg_renderer_get_leaf_quorum(const lg_renderer* r)
     return r->trace_quorum;
 }
 
+int lg_renderer_get_stack_bound(const lg_renderer* r, int32_t* bound, int32_t* capacity)
+{
+    if (!r || !bound || !capacity) return set_error(LG_ERR_INVALID, "NULL argument");
+    *bound = r->n_nodes ? (r->bvh_width == 4 ? r->stack4 : r->stack2) : 0;
+    *capacity = kTraceStack;
+    return LG_OK;
+}
+
 int lg_renderer_set_l2_window(lg_renderer* r, int enable)
 {
     if (!r) return set_error(LG_ERR_INVALID, "NULL renderer");
@@ -1258,6 +1276,7 @@ int lg_render_batch(lg_renderer* r, const lg_camera* cams, const lg_render_opts*
             job.refill_threshold = r->trace_refill;
             job.leaf_quorum = r->trace_quorum;
             job.top_records = r->trace_top;
+            job.stack_safe = stack_safe(r);
             e = launch_trace_batch(dev_scene(r), job, r->sm_count, r->bvh_width, r->watertight, st);
         }
         for (int j = 0; j < n_jobs && e == cudaSuccess; ++j)

@@ -194,8 +194,11 @@ __device__ __forceinline__ float half_area(const lg_bvh_node& b)
 // i's two children and, while fewer than four, replace the internal child of
 // largest surface area by its two children.  The record's internal children
 // become record roots themselves (they are deeper, so their level comes later).
+// rb[i]: stack entries a ray may hold when it reaches record root i (set by
+// the record above it; 0 at the root); *bound receives the largest value a
+// visit can leave, rb[i] + (children of i) - 1.
 __global__ void select4_kernel(const lg_bvh_node* __restrict__ nodes, int lo, int hi, int* __restrict__ is4,
-                               int* __restrict__ sel)
+                               int* __restrict__ sel, int* __restrict__ rb, int* __restrict__ bound)
 {
     const int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= hi || !is4[i]) return;
@@ -218,10 +221,16 @@ __global__ void select4_kernel(const lg_bvh_node* __restrict__ nodes, int lo, in
         c[best] = cb.left;
         c[k++] = cb.right;
     }
+    const int here = rb[i] + k - 1;
+    atomicMax(bound, here);
     for (int j = 0; j < 4; ++j)
     {
         sel[4 * i + j] = c[j];
-        if (c[j] >= 0 && nodes[c[j]].triCount == 0) is4[c[j]] = 1;
+        if (c[j] >= 0 && nodes[c[j]].triCount == 0)
+        {
+            is4[c[j]] = 1;
+            rb[c[j]] = here;
+        }
     }
 }
 
@@ -446,7 +455,7 @@ __device__ __forceinline__ bool advance(PathState& st, const DevScene& s, const 
 // 8x4 pixel tile, so neighbouring lanes start on neighbouring pixels.
 // kBatch: several frames per launch (job.jobs), each item mapped to its frame
 // at refill; the frame's camera and bounce limit are read from the job table.
-template <bool kCount, bool kAcc64, int kWidth, bool kWT, bool kBatch, bool kTop = false>
+template <bool kCount, bool kAcc64, int kWidth, bool kWT, bool kBatch, bool kTop = false, bool kChecked = true>
 __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(DevScene s, DevCam cam, TraceJob job)
 {
     // kTop: the top of the tree (the first top_n records in BFS order), copied
@@ -529,8 +538,8 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         const int idle_final = exhausted ? __popc(__ballot_sync(0xffffffffu, !active)) : 0;
         for (;;)
         {
-            if (warp_step<kWidth, kCount, kWT>(s, st.ray, st.li >= 0, active && !tdone, quorum, q, stack, cnt, s_top,
-                                               top_n))
+            if (warp_step<kWidth, kCount, kWT, kChecked>(s, st.ray, st.li >= 0, active && !tdone, quorum, q, stack,
+                                                         cnt, s_top, top_n))
                 tdone = true;
             const unsigned busy = __ballot_sync(0xffffffffu, active && !tdone);
             if (busy == 0 || 32 - __popc(busy) - idle_final >= thresh) break;
@@ -704,7 +713,7 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
 
 cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int null_leaf, Wide4Node* d_wide4,
                               int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
-                              cudaStream_t stream)
+                              int* stack4_host, int* stack2_host, cudaStream_t stream)
 {
     // scratch: [is_internal | dense2 | block_sums] from build_wide_nodes, then
     // [parent | is4 | dense4 | sums4 | depth | sel (4 per node) | level_start]
@@ -733,6 +742,12 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tri
     levels += 1;  // the last node has the largest depth
     if (levels > kMaxLevels) return cudaErrorInvalidValue;
     e = cudaMemcpyAsync(starts, level_start, sizeof(int) * levels, cudaMemcpyDeviceToHost, stream);
+    // the depth array is free from here on: it holds the records' stack counts
+    // (rb, root 0); the bound goes after the level table
+    int* rb = depth;
+    int* bound = level_start + kMaxLevels + 1;
+    if (e == cudaSuccess) e = cudaMemsetAsync(rb, 0, sizeof(int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bound, 0, sizeof(int), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(is4, 0, sizeof(int) * (size_t)n_nodes, stream);
     static const int kOne = 1;
     if (e == cudaSuccess && root.triCount == 0) e = cudaMemcpyAsync(is4, &kOne, sizeof(int), cudaMemcpyHostToDevice, stream);
@@ -743,7 +758,8 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tri
     for (int d = 0; d + 1 < levels; ++d)
     {
         const int lo = starts[d], hi = starts[d + 1];
-        if (hi > lo) select4_kernel<<<(hi - lo + tb - 1) / tb, tb, 0, stream>>>(d_nodes, lo, hi, is4, sel);
+        if (hi > lo)
+            select4_kernel<<<(hi - lo + tb - 1) / tb, tb, 0, stream>>>(d_nodes, lo, hi, is4, sel, rb, bound);
     }
     count_kernel<<<nb, kScanTB, 0, stream>>>(is4, n_nodes, sums4);
     scan_sums_kernel<<<1, kScanTB, 0, stream>>>(sums4, nb);
@@ -754,15 +770,18 @@ cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tri
     wide4_kernel<<<g, tb, 0, stream>>>(d_nodes, n_nodes, is4, dense4, dense2, sel, d_wide4, inline_ok, null_link);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    int last_d = 0, last_v = 0;
+    int last_d = 0, last_v = 0, stack4 = 0;
     e = cudaMemcpyAsync(&last_d, dense4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&last_v, is4 + n_nodes - 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&stack4, bound, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return e;
     *root4_host = root.triCount == 0 ? 0 : ~0;
     // dense4 of the last node: its rank among record roots if it is one, else
     // its rank among the others (so the roots before it number n - 1 - rank)
     *n4_host = last_v ? last_d + 1 : (n_nodes - 1 - last_d);
+    *stack4_host = stack4;
+    *stack2_host = levels - 1;  // one entry per internal ancestor, plus the deepest internal node's own push
     return cudaSuccess;
 }
 
@@ -773,11 +792,11 @@ cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bo
     return cudaGetLastError();
 }
 
-template <bool kCount, bool kAcc64, int W, bool kWT, bool kBatch = false, bool kTop = false>
+template <bool kCount, bool kAcc64, int W, bool kWT, bool kBatch = false, bool kTop = false, bool kChecked = true>
 static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const TraceJob& job, int sm_count,
                                   cudaStream_t stream)
 {
-    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT, kBatch, kTop>;
+    const void* fn = (const void*)trace_kernel<kCount, kAcc64, W, kWT, kBatch, kTop, kChecked>;
     const int top_n = (kTop && W == 4) ? std::min(std::max(job.top_records, 0), s.n4) : 0;
     const size_t smem = (size_t)top_n * sizeof(Wide4Node);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -793,7 +812,8 @@ static cudaError_t launch_trace_t(const DevScene& s, const DevCam& cam, const Tr
     if (blocks < 1) blocks = 1;
     e = cudaMemsetAsync(job.work64, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
-    trace_kernel<kCount, kAcc64, W, kWT, kBatch, kTop><<<(int)blocks, kTraceThreads, smem, stream>>>(s, cam, job);
+    trace_kernel<kCount, kAcc64, W, kWT, kBatch, kTop, kChecked><<<(int)blocks, kTraceThreads, smem, stream>>>(s, cam,
+                                                                                                          job);
     return cudaGetLastError();
 }
 
@@ -804,6 +824,14 @@ cudaError_t launch_trace_batch(const DevScene& s, const TraceJob& job, int sm_co
     if (width == 4 && job.top_records > 0)
         return watertight ? launch_trace_t<false, false, 4, true, true, true>(s, none, job, sm_count, stream)
                           : launch_trace_t<false, false, 4, false, true, true>(s, none, job, sm_count, stream);
+    if (job.stack_safe)
+    {
+        if (watertight)
+            return width == 4 ? launch_trace_t<false, false, 4, true, true, false, false>(s, none, job, sm_count, stream)
+                              : launch_trace_t<false, false, 2, true, true, false, false>(s, none, job, sm_count, stream);
+        return width == 4 ? launch_trace_t<false, false, 4, false, true, false, false>(s, none, job, sm_count, stream)
+                          : launch_trace_t<false, false, 2, false, true, false, false>(s, none, job, sm_count, stream);
+    }
     if (watertight)
         return width == 4 ? launch_trace_t<false, false, 4, true, true>(s, none, job, sm_count, stream)
                           : launch_trace_t<false, false, 2, true, true>(s, none, job, sm_count, stream);
@@ -819,6 +847,10 @@ static cudaError_t launch_trace_w(const DevScene& s, const DevCam& cam, const Tr
     // counting and FP64 frames run without them)
     if (W == 4 && job.top_records > 0 && !count && !job.accum64)
         return launch_trace_t<false, false, W, kWT, false, true>(s, cam, job, sm_count, stream);
+    // trees whose stack bound fits: no push checks (counting runs keep them, and count overflows)
+    if (job.stack_safe && !count)
+        return job.accum64 ? launch_trace_t<false, true, W, kWT, false, false, false>(s, cam, job, sm_count, stream)
+                           : launch_trace_t<false, false, W, kWT, false, false, false>(s, cam, job, sm_count, stream);
     if (count)
         return job.accum64 ? launch_trace_t<true, true, W, kWT>(s, cam, job, sm_count, stream)
                            : launch_trace_t<true, false, W, kWT>(s, cam, job, sm_count, stream);

@@ -46,8 +46,9 @@ static_assert(sizeof(Wide4Node) == 64, "Wide4Node is two 32-byte halves");
 // padding, so a record starts on a 32-byte boundary when kTriVec == 4.
 constexpr int kTriVec = 4;
 
-// Entries of a ray's traversal stack (per thread, local memory).
-constexpr int kTraceStack = 64;
+// Entries of a ray's traversal stack (per thread, local memory; entries a
+// traversal does not reach cost nothing).
+constexpr int kTraceStack = 96;
 
 struct DevScene
 {
@@ -112,6 +113,7 @@ struct TraceJob
     int refill_threshold;  // finished rays in a warp that trigger the path logic, 1..32
     int leaf_quorum;       // lanes still searching for a leaf below which the warp tests held leaves, 0..31
     int top_records;       // 4-wide records (the first in BFS order) each block keeps in shared memory, 0 = none
+    int stack_safe;        // 1: the records' stack bound fits kTraceStack, launch without push checks
     RenderCounters* counters;  // optional
     // batched launch (launch_trace_batch): every field above except work64 is taken from jobs[]
     const BatchJob* jobs;
@@ -135,9 +137,14 @@ cudaError_t build_wide_nodes(const lg_bvh_node* d_nodes, int n_nodes, WideNode* 
 // their nodes (deterministic).  Must follow build_wide_nodes on the same
 // scratch (it reuses the leaf numbering).  Scratch: 11 * n_nodes + 256 ints.
 // null_leaf: the index of a leaf-table entry (0, 0) for absent children.
+// stack4_host / stack2_host: the most traversal-stack entries any ray can
+// need over the 4-wide records (the largest sum, over a root-to-record path,
+// of each record's child count less one: a visit stacks at most the hit
+// children it does not enter, and entries above a popped one are gone) and
+// over the 2-wide ones (the deepest internal node's depth + 1).
 cudaError_t build_wide4_nodes(const lg_bvh_node* d_nodes, int n_nodes, int n_tris, int null_leaf, Wide4Node* d_wide4,
                               int* d_scratch, int* root4_host, int* n4_host, int* leaf_inline_host,
-                              cudaStream_t stream);
+                              int* stack4_host, int* stack2_host, cudaStream_t stream);
 // Intersection records, 3 float4 per triangle (w of the first = material):
 // (v0, v1-v0, v2-v0) for Moller-Trumbore, (v0, v1, v2) for the watertight test.
 cudaError_t prepare_triangles(const lg_triangle* d_tris, int n, float4* d_tv, bool watertight, cudaStream_t stream);

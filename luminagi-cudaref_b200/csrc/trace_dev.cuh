@@ -189,10 +189,17 @@ __device__ __forceinline__ int pop(Trav& q, const int* stack) { return q.sp == 0
 
 // Stacks `link`; a push past kStack entries is dropped and flags the scene's
 // fault word (the host turns it into LG_ERR_DEVICE), so a tree too deep for
-// the stack never yields a silently incomplete image.
-template <bool kCount>
+// the stack never yields a silently incomplete image.  kChecked = false is
+// for trees whose stack bound (computed when their records are built) fits
+// in kStack: no traversal over them can overflow, so the test is left out.
+template <bool kCount, bool kChecked = true>
 __device__ __forceinline__ void push(Trav& q, int* stack, int link, const DevScene& s, Counters& cnt)
 {
+    if (!kChecked)
+    {
+        stack[q.sp++] = link;
+        return;
+    }
     if (q.sp < kStack)
     {
         stack[q.sp++] = link;
@@ -277,7 +284,7 @@ __device__ __forceinline__ int4 box4(const float (&a)[8], const float (&b)[8], c
 // without speculation (internal records until every lane holds a leaf, then
 // the leaves) ran 745 ms, and a 24-entry shared-memory stack 675 ms (its
 // 96 KB per SM comes out of the L1 that caches the BVH records).
-template <int kWidth, bool kCount>
+template <int kWidth, bool kCount, bool kChecked = true>
 __device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav& q, int* stack, Counters& cnt,
                                           const Wide4Node* s_top = nullptr, int top_n = 0)
 {
@@ -298,9 +305,9 @@ __device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav&
         if (t0 != inf)
         {
             // push farthest first so the nearest remaining is on top
-            if (t3 != inf) push<kCount>(q, stack, l3, s, cnt);
-            if (t2 != inf) push<kCount>(q, stack, l2, s, cnt);
-            if (t1 != inf) push<kCount>(q, stack, l1, s, cnt);
+            if (t3 != inf) push<kCount, kChecked>(q, stack, l3, s, cnt);
+            if (t2 != inf) push<kCount, kChecked>(q, stack, l2, s, cnt);
+            if (t1 != inf) push<kCount, kChecked>(q, stack, l1, s, cnt);
             q.cur = l0;
             return;
         }
@@ -317,7 +324,7 @@ __device__ __forceinline__ void node_step(const DevScene& s, const Ray& r, Trav&
         if (h0 && h1)
         {
             const bool swap = t1 < t0;
-            push<kCount>(q, stack, swap ? ln.x : ln.y, s, cnt);
+            push<kCount, kChecked>(q, stack, swap ? ln.x : ln.y, s, cnt);
             q.cur = swap ? ln.y : ln.x;
             return;
         }
@@ -408,7 +415,7 @@ __device__ __forceinline__ int traverse_ray(const DevScene& s, const Ray& r, flo
 // culled by a nearer hit in it only for closest-hit rays, and then only cost
 // time: the closest hit is the same (up to exact ties in t).  `busy` is this
 // lane's ray in flight; returns true when its traversal has finished.
-template <int kWidth, bool kCount, bool kWT>
+template <int kWidth, bool kCount, bool kWT, bool kChecked = true>
 __device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool anyhit, bool busy, int quorum,
                                           Trav& q, int* stack, Counters& cnt, const Wide4Node* s_top, int top_n)
 {
@@ -424,7 +431,7 @@ __device__ __forceinline__ bool warp_step(const DevScene& s, const Ray& r, bool 
     const bool holding = __any_sync(0xffffffffu, busy && !fin && q.pend != 0);
     if (n_searching > (unsigned)quorum || !holding)
     {
-        if (busy && q.cur >= 0) node_step<kWidth, kCount>(s, r, q, stack, cnt, s_top, top_n);
+        if (busy && q.cur >= 0) node_step<kWidth, kCount, kChecked>(s, r, q, stack, cnt, s_top, top_n);
         return fin;
     }
     if (!busy || fin || q.pend == 0) return fin;

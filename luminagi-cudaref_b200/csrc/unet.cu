@@ -233,7 +233,7 @@ void lg_unet_destroy(lg_unet* u)
     for (auto& b : u->packed) b.release();
     for (Buf* b : {&u->x0, &u->t1, &u->cat1, &u->p1, &u->t2, &u->cat2, &u->p2, &u->t3, &u->cat3, &u->p3, &u->t4,
                    &u->t5, &u->t6, &u->t7, &u->u1, &u->xin, &u->yout, &u->err, &u->grads, &u->adam_m, &u->adam_v,
-                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt, &u->lo7, &u->lo9, &u->lo11, &u->gup, &u->wpart, &u->bpart})
+                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt, &u->lo7, &u->lo9, &u->lo11, &u->gup, &u->wpart, &u->bpart, &u->tpart})
         b->release();
     for (auto& b : u->packed_dg) b.release();
     for (auto& b : u->dz) b.release();

@@ -56,10 +56,10 @@ TileCfg pick_cfg(int Cin, int Cout)
     return c;
 }
 
-template <int BN, int KC>
+template <int BN, int KC, int ROWS = kRows>
 struct Smem
 {
-    static constexpr int kABytes = kHaloY * kHaloX * KC * 2;
+    static constexpr int kABytes = (ROWS + 2) * kHaloX * KC * 2;
     static constexpr int kBBytes = 9 * KC * BN * 2;
     static constexpr int kStage = ((kABytes + kBBytes + 1023) / 1024) * 1024;
 };
@@ -467,11 +467,14 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 // RESW (layers with one output block, Cout == BN): every K-block's weights
 // are copied into shared memory once per CTA, so a ring stage holds only the
 // input halo, and more stages fit; the weights are the same for every tile.
+// ROWS (2 or 4, persistent kernel only): output rows per tile; a 4-row tile
+// reads a 6-row halo for four rows of MMAs (each weight block feeds four M
+// tiles) and hands the epilogue two 2-row sub-tiles.
 constexpr int kPThreads = 192;
-template <int BN, int KC, bool RESW>
+template <int BN, int KC, bool RESW, int ROWS = kRows>
 struct PSmem
 {
-    using S = Smem<BN, KC>;
+    using S = Smem<BN, KC, ROWS>;
     static constexpr int kStage = RESW ? ((S::kABytes + 1023) / 1024) * 1024 : S::kStage;
     static constexpr int kBarBytes = 1024;  // mbarriers and the TMEM slot, after the ring
     // dynamic shared memory of a launch with KB K-blocks (1024 B for aligning the base)
@@ -480,11 +483,12 @@ struct PSmem
         return stages * kStage + kBarBytes + (RESW ? KB * S::kBBytes : 0) + 1024;
     }
 };
-template <int BN, int KC, int STAGES, bool RESW>
+template <int BN, int KC, int STAGES, bool RESW, int ROWS = kRows>
 __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
 {
-    using S = Smem<BN, KC>;
-    using P = PSmem<BN, KC, RESW>;
+    static_assert(ROWS == 2 || ROWS == 4, "2- or 4-row tiles");
+    using S = Smem<BN, KC, ROWS>;
+    using P = PSmem<BN, KC, RESW, ROWS>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * P::kStage);
@@ -499,12 +503,14 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int n_cot = a.Cout / BN;
-    const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + kRows - 1) / kRows;
+    const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + ROWS - 1) / ROWS;
     const int n_tiles = tiles_x * tiles_y * a.N * n_cot;
     const int KB = a.Cin / KC;
-    constexpr uint32_t kCols = 4 * BN;  // two accumulators of two rows x BN FP32 columns
+    constexpr uint32_t kAccCols = ROWS * BN;   // one accumulator: ROWS rows x BN FP32 columns
+    constexpr uint32_t kCols = 2 * kAccCols;  // two of them (a power of two >= 32 for BN >= 16)
+    static_assert(kCols <= 512, "two accumulators must fit in TMEM");
     constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, BN);
-    constexpr uint32_t kLboA = kHaloY * kHaloX * 16;
+    constexpr uint32_t kLboA = (ROWS + 2) * kHaloX * 16;
     constexpr uint32_t kLboB = BN * 16;
     // tile t -> (n, ct, y0, x0); output blocks innermost so concurrent tiles share input rows
     auto coords = [&](int t, int& n, int& ct, int& x0, int& y0) {
@@ -512,7 +518,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
         t /= n_cot;
         x0 = (t % tiles_x) * kTileX;
         t /= tiles_x;
-        y0 = (t % tiles_y) * kRows;
+        y0 = (t % tiles_y) * ROWS;
         n = t / tiles_y;
     };
     auto fail = [&](int code) {
@@ -605,7 +611,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t acc = tmem + (uint32_t)(b * 2 * BN);
+                const uint32_t acc = tmem + (uint32_t)b * kAccCols;
                 bool ok = true;
                 for (int kb = 0; kb < KB; ++kb, ++it)
                 {
@@ -629,7 +635,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                             const uint64_t bd =
                                 tc::smem_desc(bbase + (uint32_t)((tap * (KC / 8) + 2 * ks) * BN * 16), kLboB, 128);
 #pragma unroll
-                            for (int r = 0; r < kRows; ++r)
+                            for (int r = 0; r < ROWS; ++r)
                             {
                                 const uint32_t aoff =
                                     (uint32_t)(2 * ks) * kLboA + (uint32_t)(((r + dy) * kHaloX + dx) * 16);
@@ -665,7 +671,10 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
             tc::tc_fence_after();
             int n, ct, x0, y0;
             coords(t, n, ct, x0, y0);
-            tile_epilogue<BN>(a, tmem + (uint32_t)(b * 2 * BN), q, q * 32 + lane, n, ct, x0, y0);
+#pragma unroll 1
+            for (int sub = 0; sub < ROWS / 2; ++sub)  // 2-row sub-tiles
+                tile_epilogue<BN>(a, tmem + (uint32_t)b * kAccCols + (uint32_t)(sub * 2 * BN), q, q * 32 + lane, n,
+                                  ct, x0, y0 + 2 * sub);
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&acc_empty[b]);
@@ -704,13 +713,14 @@ EncodeTiledFn encode_fn()
 
 // 5-D map over a blocked BF16 tensor: (8 channels, W, H, C/8, N), box
 // (8, 130, 4, KC/8, 1).
-cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int KC)
+cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int KC,
+                     int halo_y = kHaloY)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)(C / 8), (cuuint64_t)N};
     cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)(C / 8) * H * W * 16};
-    cuuint32_t box[5] = {8, (cuuint32_t)kHaloX, (cuuint32_t)kHaloY, (cuuint32_t)(KC / 8), 1};
+    cuuint32_t box[5] = {8, (cuuint32_t)kHaloX, (cuuint32_t)halo_y, (cuuint32_t)(KC / 8), 1};
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)base, dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -722,17 +732,17 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
 // for the kernel's static shared memory.
 constexpr int kMaxSmem = 226 * 1024;
 
-template <int BN, int KC, int STAGES, bool RESW = false>
+template <int BN, int KC, int STAGES, bool RESW = false, int ROWS = kRows>
 cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
 {
     const int KB = a.Cin / KC;
     if (RESW && a.Cout != BN) return cudaErrorInvalidValue;  // one output block only
-    const int smem = PSmem<BN, KC, RESW>::bytes(STAGES, KB);
+    const int smem = PSmem<BN, KC, RESW, ROWS>::bytes(STAGES, KB);
     if (smem > kMaxSmem) return cudaErrorInvalidValue;
     CUtensorMap m;
-    cudaError_t e = make_map(&m, in, a.N, a.Cin, a.H, a.W, KC);
+    cudaError_t e = make_map(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2);
     if (e != cudaSuccess) return e;
-    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW>;
+    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW, ROWS>;
     // The resident-weights form's smem depends on KB: size the attribute for
     // the largest launch it may see and query occupancy per launch size.
     static bool attr_done = false;
@@ -749,11 +759,11 @@ cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaSt
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPThreads, smem);
     if (e != cudaSuccess) return e;
-    // TMEM: each CTA holds 4*BN of the SM's 512 columns for its lifetime
-    const int tmem_fit = 512 / (4 * BN);
+    // TMEM: each CTA holds 2*ROWS*BN of the SM's 512 columns for its lifetime
+    const int tmem_fit = 512 / (2 * ROWS * BN);
     if (per_sm > tmem_fit) per_sm = tmem_fit;
     if (per_sm < 1) per_sm = 1;
-    const long long tiles = (long long)((a.W + kTileX - 1) / kTileX) * ((a.H + kRows - 1) / kRows) * a.N * (a.Cout / BN);
+    const long long tiles = (long long)((a.W + kTileX - 1) / kTileX) * ((a.H + ROWS - 1) / ROWS) * a.N * (a.Cout / BN);
     const long long grid = std::min<long long>(tiles, (long long)per_sm * sm_count);
     fn<<<(unsigned)grid, kPThreads, smem, stream>>>(m, a);
     return cudaGetLastError();
@@ -866,14 +876,15 @@ constexpr ConvTile kCompiledTiles[] = {{32, 16, 4, 0},  {32, 32, 2, 0},  {32, 32
                                        {32, 16, 4, 1},  {32, 32, 2, 1},  {32, 32, 4, 1},  {64, 16, 4, 1},
                                        {64, 32, 2, 1},  {64, 32, 3, 1},  {128, 16, 3, 1}, {128, 32, 2, 1},
                                        {32, 16, 10, 2}, {32, 32, 2, 2},  {32, 32, 5, 2},  {32, 32, 6, 2},
-                                       {64, 32, 3, 2},  {64, 32, 4, 2}};
+                                       {64, 32, 3, 2},  {64, 32, 4, 2},  {32, 16, 8, 3},  {32, 32, 3, 3},
+                                       {32, 32, 4, 3},  {64, 32, 3, 3}};
 
 // Shared memory of a tile shape's launch for a layer with Cin input channels.
 int tile_smem(const ConvTile& t, int Cin)
 {
     const int KB = Cin / t.kc;
-    const int a = 4 * 130 * t.kc * 2, b = 9 * t.kc * t.bn * 2;
-    if (t.persist == 2) return t.stages * (((a + 1023) / 1024) * 1024) + 1024 + KB * b + 1024;
+    const int a = (t.persist == 3 ? 6 : 4) * 130 * t.kc * 2, b = 9 * t.kc * t.bn * 2;
+    if (t.persist >= 2) return t.stages * (((a + 1023) / 1024) * 1024) + 1024 + KB * b + 1024;
     return t.stages * (((a + b + 1023) / 1024) * 1024) + 1024 + 1024;
 }
 
@@ -882,7 +893,7 @@ int conv_tile_candidates(int Cin, int Cout, ConvTile* out, int max)
     int k = 0;
     for (const ConvTile& t : kCompiledTiles)
         if (k < max && t.bn <= Cout && Cout % t.bn == 0 && Cin % t.kc == 0 &&
-            (t.persist != 2 || (t.bn == Cout && tile_smem(t, Cin) <= kMaxSmem)))
+            (t.persist < 2 || (t.bn == Cout && tile_smem(t, Cin) <= kMaxSmem)))
             out[k++] = t;
     return k;
 }
@@ -921,6 +932,15 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
     const TileCfg c = resolve(a.tile, a.Cin, a.Cout);
     if (a.Cout % c.bn || a.Cin % c.kc) return cudaErrorInvalidValue;
     const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    if (c.persist == 3)
+        switch (key)
+        {
+        case 32168: return launch_persistent<32, 16, 8, true, 4>(in, a, stream);
+        case 32323: return launch_persistent<32, 32, 3, true, 4>(in, a, stream);
+        case 32324: return launch_persistent<32, 32, 4, true, 4>(in, a, stream);
+        case 64323: return launch_persistent<64, 32, 3, true, 4>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
     if (c.persist == 2)
         switch (key)
         {

@@ -37,7 +37,8 @@ enum ConvEpilogue : int
 struct ConvTile
 {
     int bn, kc, stages;
-    int persist;  // 1: the persistent, warp-specialised kernel (same packing, same results)
+    int persist;  // 0: one tile per CTA; 1: the persistent, warp-specialised kernel; 2: persistent with the
+                  // weights resident in shared memory; 3: as 2 with 4-row tiles (same packing, same results)
 };
 ConvTile conv_default_tile(int Cin, int Cout);
 // The compiled tile shapes valid for a layer (Cout % bn == 0, Cin % kc == 0);

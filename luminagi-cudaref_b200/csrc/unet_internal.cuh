@@ -73,7 +73,7 @@ struct lg_unet
     int gN = 0, gH = 0, gW = 0;
     Buf dz[14], gs1, gs2, gs3, tgt;
     Buf gup;  // bilinear mode: full-resolution gradient of an upsampled concat half
-    Buf wpart, bpart;  // per-CTA partial weight / bias gradients, summed in a fixed order
+    Buf wpart, bpart, tpart;  // per-CTA partial weight / bias / tail gradients, summed in a fixed order
     // tile shapes (lg::ConvTile; zero = the default heuristic) of the 14 convs and
     // the 16 input-gradient convs, as chosen by lg_unet_autotune
     lg::ConvTile tile[14] = {}, tile_dg[16] = {};

@@ -47,8 +47,7 @@ __device__ __forceinline__ float dact(float y, float slope) { return y > 0.0f ? 
 __global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __restrict__ x, int xC, int log_hdr,
                                      const float* __restrict__ target, const float* __restrict__ tw,
                                      const float* __restrict__ tb, int N, int H, int W, float slope, float inv_numel,
-                                     bf* __restrict__ dz, float* __restrict__ dtw, float* __restrict__ dtb,
-                                     float* __restrict__ loss)
+                                     bf* __restrict__ dz, float* __restrict__ partial)
 {
     __shared__ float red[8][100];
     const int HW = H * W;
@@ -134,10 +133,22 @@ __global__ void tail_backward_kernel(const bf* __restrict__ u1, const float* __r
     {
         float t = 0.0f;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][threadIdx.x];
-        if (threadIdx.x < 96) atomicAdd(&dtw[threadIdx.x], t);
-        else if (threadIdx.x < 99) atomicAdd(&dtb[threadIdx.x - 96], t);
-        else atomicAdd(loss, t);
+        partial[(size_t)blockIdx.x * 100 + threadIdx.x] = t;  // this block's 96 + 3 + 1 sums
     }
+}
+
+// The blocks' partial sums of tail_backward_kernel added in block order:
+// 96 tail-weight and 3 tail-bias gradients (added to) and the loss sum (set).
+__global__ void tail_reduce_kernel(const float* __restrict__ partial, int blocks, float* __restrict__ dtw,
+                                   float* __restrict__ dtb, float* __restrict__ loss)
+{
+    const int i = threadIdx.x;
+    if (i >= 100) return;
+    float t = 0.0f;
+    for (int b = 0; b < blocks; ++b) t += partial[(size_t)b * 100 + i];
+    if (i < 96) dtw[i] += t;
+    else if (i < 99) dtb[i - 96] += t;
+    else *loss = t;
 }
 
 // torch.optim.Adam: m <- b1 m + (1-b1) g; v <- b2 v + (1-b2) g^2;
@@ -213,9 +224,14 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
     LG_TRY_CUDA(cudaMemsetAsync(u->loss.p, 0, sizeof(float), st));
     const long long npx = (long long)N * H * W;
     const float inv_numel = 1.0f / (float)(npx * 3);
-    tail_backward_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(
+    const int tail_blocks = (int)((npx + 255) / 256);
+    LG_TRY(u->tpart.ensure((size_t)tail_blocks * 100 * sizeof(float)));
+    tail_backward_kernel<<<(unsigned)tail_blocks, 256, 0, st>>>(
         (const bf*)u->u1.p, d_x, u->in_ch, u->log_hdr ? 1 : 0, d_t, P + u->tail_w_off, P + u->tail_b_off, N, H, W, u->slope, inv_numel,
-        (bf*)u->dz[13].p, G + u->tail_w_off, G + u->tail_b_off, (float*)u->loss.p);
+        (bf*)u->dz[13].p, (float*)u->tpart.p);
+    LG_TRY_CUDA(cudaGetLastError());
+    tail_reduce_kernel<<<1, 128, 0, st>>>((const float*)u->tpart.p, tail_blocks, G + u->tail_w_off,
+                                          G + u->tail_b_off, (float*)u->loss.p);
     LG_TRY_CUDA(cudaGetLastError());
 
     const int hs[4] = {H, H / 2, H / 4, H / 8}, ws[4] = {W, W / 2, W / 4, W / 8};
@@ -488,7 +504,7 @@ int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
     for (int i = 0; i < 30; ++i)
     {
         const int p4 = tiles[4 * i + 3];
-        if (p4 < 0 || p4 > 2) return set_error(LG_ERR_INVALID, "conv %d: kernel choice %d is not 0, 1 or 2", i, p4);
+        if (p4 < 0 || p4 > 3) return set_error(LG_ERR_INVALID, "conv %d: kernel choice %d is not 0..3", i, p4);
         ConvTile t{tiles[4 * i], tiles[4 * i + 1], tiles[4 * i + 2], p4};
         const bool back = i >= 14;
         const int cin = back ? kLayers[kDgrad[i - 14].layer].cout : kLayers[i].cin;
@@ -499,7 +515,7 @@ int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
             const int persist = t.persist;
             t = conv_default_tile(cin, cout);
             t.persist = persist;
-            ok = persist != 2;  // the resident-weights kernel is compiled for some shapes only
+            ok = persist < 2;  // the resident-weights kernels are compiled for some shapes only
         }
         ConvTile cand[32];
         const int nc = conv_tile_candidates(cin, cout, cand, 32);

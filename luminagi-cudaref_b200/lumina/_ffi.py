@@ -116,6 +116,7 @@ SIGNATURES = {
     "lg_measure_read_bandwidth": (_I, [C.c_int, C.c_int, C.c_int64, C.c_int, C.POINTER(C.c_double)]),
     "lg_unet_wait_selftest": (_I, [_P, C.c_int64]),
     "lg_renderer_set_l2_window": (_I, [_P, C.c_int]),
+    "lg_renderer_get_stack_bound": (_I, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "lg_renderer_set_top_records": (_I, [_P, C.c_int]),
     "lg_renderer_get_top_records": (_I, [_P]),
     "lg_render_sorted": (_I, [_P, C.POINTER(LgCamera), C.POINTER(LgRenderOpts), _P, _P, C.POINTER(LgRenderStats)]),

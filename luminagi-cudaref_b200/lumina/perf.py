@@ -25,6 +25,9 @@ def _events(torch):
 # where the layer has one output block and its weights fit beside the ring.
 RESIDENT_TILES = [(32, 16, 10, 2), (32, 32, 6, 2), (64, 32, 4, 2), (64, 32, 4, 2)] + [(0, 0, 0, 1)] * 7 + \
                  [(64, 32, 4, 2), (32, 32, 5, 2), (32, 32, 6, 2)]
+# The same layers with resident weights on 4-row tiles.
+ROWS4_TILES = [(32, 16, 8, 3), (32, 32, 4, 3), (64, 32, 3, 3), (64, 32, 3, 3)] + [(0, 0, 0, 1)] * 7 + \
+              [(64, 32, 3, 3), (32, 32, 3, 3), (32, 32, 4, 3)]
 
 
 def unet(a):
@@ -38,6 +41,8 @@ def unet(a):
         net.set_tiles([(0, 0, 0, 0)] * 30)
     elif a.kernel == "resident":
         net.set_tiles(RESIDENT_TILES + [(0, 0, 0, 1)] * 16)
+    elif a.kernel == "rows4":
+        net.set_tiles(ROWS4_TILES + [(0, 0, 0, 1)] * 16)
     elif a.kernel == "autotune":
         tiles = net.autotune(a.n, a.h, a.w)[:14]
     x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
@@ -72,6 +77,8 @@ def trace(a):
     rays = c["closest_rays"] + c["shadow_rays"]
     out = {"kernel": "trace", "spp": a.spp, "width": a.width, "tree": r.render_tree(), "rays": rays,
            "nodes_per_ray": c["node_fetches"] / rays, "tris_per_ray": c["tri_tests"] / rays}
+    if hasattr(r, "stack_bound"):
+        out["stack_bound"] = r.stack_bound()
     sweep = {}
     if a.l2win:
         r.set_l2_window(True)
@@ -189,7 +196,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["unet", "trace", "bvh", "batch", "membench"])
     ap.add_argument("--poses", type=int, default=50)
-    ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "autotune"],
+    ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "rows4", "autotune"],
                     help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
                          "single-block layers, or autotuned tiles")
     ap.add_argument("--n", type=int, default=1)

@@ -132,6 +132,12 @@ class Renderer:
     def leaf_quorum(self) -> int:
         return int(lib().lg_renderer_get_leaf_quorum(self._h))
 
+    def stack_bound(self):
+        """(most traversal-stack entries a ray can need over the current records, stack capacity)."""
+        b, c = C.c_int32(0), C.c_int32(0)
+        check(lib().lg_renderer_get_stack_bound(self._h, C.byref(b), C.byref(c)))
+        return int(b.value), int(c.value)
+
     def set_l2_window(self, enable: bool) -> None:
         """Persisting-L2 access window over the 4-wide BVH records (the reference's CUDAREF_L2_PIN)."""
         check(lib().lg_renderer_set_l2_window(self._h, 1 if enable else 0))

@@ -3,12 +3,13 @@
 The reference's traversal drops pushes past its 64-entry stack without a word
 (src/pathtracer.cu:142, :184).  Here every dropped push sets a fault word that
 the renderer reports as LG_ERR_DEVICE.  The test builds a caller BVH that is a
-chain of 100 binary levels (each node: one leaf, one deeper subtree), keeps
+chain of 120 binary levels (each node: one leaf, one deeper subtree), keeps
 its topology as the render tree, and aims the camera down the chain so that
 every box is entered before any triangle is hit; the traversal then needs
 about one stack entry per binary level (2-wide records) or three per 4-wide
-record, well past 64.  No access goes out of bounds: the kernel tests the
-stack depth before every push."""
+record, past the 96-entry stack.  The renderer's stack bound says so, so the
+frame runs on the checked kernel, which tests the stack depth before every
+push: no access goes out of bounds."""
 import numpy as np
 import pytest
 
@@ -17,7 +18,7 @@ from lumina._ffi import NODE_DTYPE, POINT_DTYPE, DIR_DTYPE, TRI_DTYPE, LG_ERR_DE
 
 pytestmark = pytest.mark.gpu
 
-N_CHAIN = 100
+N_CHAIN = 120
 
 
 def chain_scene(n=N_CHAIN, reverse=True):
@@ -67,6 +68,8 @@ def test_deep_chain_reports_overflow(width):
         r.set_scene_bvh(sc, nodes)
         assert r.render_tree() == "buildbvh"
         r.set_bvh_width(width)
+        bound, cap = r.stack_bound()
+        assert bound > cap, (bound, cap)
         with pytest.raises(LuminaError) as ei:
             r.render(spp=1, bounces=0)
         assert ei.value.code == LG_ERR_DEVICE and "stack overflow" in str(ei.value)
@@ -79,6 +82,18 @@ def test_deep_chain_reports_overflow(width):
         r.set_scene_bvh(sc2, nodes2)
         out = r.render(spp=1, bounces=0)
         assert out["rgb"][8, 16].any(), "the centre pixel sees the nearest triangle"
+
+
+def test_stack_bound_of_ordinary_trees_fits(box_scene, small_engine_scene):
+    """Ordinary scenes' render trees have a stack bound within the stack, so
+    their frames run on the kernel without per-push checks."""
+    for sc in (box_scene, small_engine_scene):
+        with lumina.Renderer(0) as r:
+            r.set_scene(sc)
+            for width in (4, 2):
+                r.set_bvh_width(width)
+                bound, cap = r.stack_bound()
+                assert 0 < bound <= cap, (width, bound, cap)
 
 
 def test_shallow_chain_renders_same_as_balanced_tree():

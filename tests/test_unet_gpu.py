@@ -339,7 +339,7 @@ def test_autotune_keeps_results():
     y0 = net.forward(x)
     tiles = net.autotune(n, h, w, backward=True)
     print("autotuned tiles (bn, kc, stages):", tiles)
-    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) and t[3] in (0, 1) for t in tiles)
+    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) and t[3] in (0, 1, 2, 3) for t in tiles)
     y1 = net.forward(x)
     assert np.array_equal(net.get_params(), flat)
     m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
@@ -388,29 +388,35 @@ def test_persistent_conv_kernel_is_bit_identical():
 # the layer has one output block and its weights fit beside the ring.
 RESIDENT_TILES = [(32, 16, 10, 2), (32, 32, 6, 2), (64, 32, 4, 2), (64, 32, 4, 2)] + [(0, 0, 0, 1)] * 7 + \
                  [(64, 32, 4, 2), (32, 32, 5, 2), (32, 32, 6, 2)]
+# The same layers on 4-row tiles (kernel choice 3).
+ROWS4_TILES = [(32, 16, 8, 3), (32, 32, 4, 3), (64, 32, 3, 3), (64, 32, 3, 3)] + [(0, 0, 0, 1)] * 7 + \
+              [(64, 32, 3, 3), (32, 32, 3, 3), (32, 32, 4, 3)]
 
 
 def test_resident_weight_conv_kernel_is_bit_identical():
     """The persistent kernel with the weights resident in shared memory (one
-    copy per CTA instead of one per ring stage) runs the same MMAs in the
-    same order: outputs and loss are bit-identical to the plain persistent
-    kernel's, at batch 1 and 2, with partial edge tiles."""
+    copy per CTA instead of one per ring stage), with 2- and 4-row tiles, runs
+    the same MMAs in the same order for every output row: outputs, loss and
+    gradients are bit-identical to the plain persistent kernel's, at batch 1
+    and 2, with partial tiles at the right edge."""
     flat = unet_ref.make_params(81)
-    for n, h, w in ((1, 40, 264), (2, 64, 136)):
+    for n, h, w in ((1, 40, 264), (2, 64, 136), (1, 72, 136)):
         x = np.random.default_rng(10).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
         noisy, clean = _batch(n, h, w, 13)
         dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
         outs = []
-        for tiles in ([(0, 0, 0, 1)] * 30, RESIDENT_TILES + [(0, 0, 0, 1)] * 16):
+        for tiles in ([(0, 0, 0, 1)] * 30, RESIDENT_TILES + [(0, 0, 0, 1)] * 16, ROWS4_TILES + [(0, 0, 0, 1)] * 16):
             net = lumina.UNet()
             net.set_params(flat)
             net.set_tiles(tiles)
             y = net.forward(x)
-            loss, _ = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
-            outs.append((y, loss))
+            loss, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
+            outs.append((y, loss, g))
             net.close()
-        assert np.array_equal(outs[0][0], outs[1][0])
-        assert outs[0][1] == outs[1][1]
+        for o in outs[1:]:
+            assert np.array_equal(outs[0][0], o[0])
+            assert outs[0][1] == o[1]
+            assert np.array_equal(outs[0][2], o[2])
 
 
 def test_training_is_bit_reproducible():
