@@ -15,7 +15,7 @@ counting pass) with ms/frame alongside.
             record, both 32-byte halves as loaded; 48 B per triangle test;
             8 B per leaf-table entry; as counted) over its event-timed
             duration, against the L2 read bandwidth measured in this run
-            (lg_measure_read_bandwidth: a 32 MB buffer, L2-only loads).  The
+            (lg_measure_read_bandwidth: a 64 MB buffer, L2-only loads).  The
             hot arrays (records ~22 MB, triangle records ~67 MB) stay
             L2-resident across frames: DRAM moves ~8 B per ray.  L1 and HBM
             fractions ride along.
@@ -57,22 +57,22 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 479.4 MB + 60.2 MB / 65,366,791 rays; traffic
+# of an 8-spp engine frame: 431.3 MB + 34.5 MB / 65,366,791 rays; traffic
 # scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = 539.592704e6 / 65366791
+TRACE_DRAM_BYTES_PER_RAY = (431256320 + 34534400) / 65366791
 # Bytes one traversal step loads from a BVH record: both 32-byte halves of a
 # 4-wide record (grid origin, steps, 24 one-byte planes, four links, 8 B of
 # padding), or the whole 64-byte 2-wide record.
 RECORD_BYTES = {4: 64, 2: 64}
 # Rows of the CPU sample: every CPU_ROW_STEP-th row of the frame, the same in
 # the cpu_baseline leg and the reference arm.
-CPU_ROW_STEP = 24
-# Local-memory (stack and spill) bytes per traced ray of trace_kernel, from one
-# ncu capture of an 8-spp engine frame (lmem load + store sectors x 32 B /
-# rays); the waste to cut.
-TRACE_LOCAL_BYTES_PER_RAY = None
-# L2 probe: buffer size (fits in L2) and passes.
-L2_PROBE_BYTES = 32 << 20
+CPU_ROW_STEP = 16
+# Local-memory (stack and spill) bytes per traced ray of trace_kernel, from the
+# same capture: (806.3 M load + 911.3 M store sectors) x 32 B / rays.
+TRACE_LOCAL_BYTES_PER_RAY = (806348142 + 911329462) * 32 / 65366791
+# L2 probe: buffer size and passes; 64 MB gave the highest read bandwidth of the
+# sizes tried (8-96 MB), the conservative denominator.
+L2_PROBE_BYTES = 64 << 20
 L1_PROBE_BYTES = 16 << 10
 
 
@@ -467,7 +467,8 @@ def main():
             "dram_bytes_per_ray": TRACE_DRAM_BYTES_PER_RAY, "kernel": "trace_kernel",
             "algorithmic_bytes_per_launch": algo_bytes, "algorithmic_bytes_per_ray": algo_bytes / rays,
             "kernel_ms": kernel_ms,
-            "limiter": "instruction issue, not memory (ncu: issue slots ~70% busy, L1 data pipe ~50%)"}
+            "limiter": "instruction issue, not memory (ncu: issue slots ~70% busy, L1 data pipe ~50%; "
+                       "474 warp instructions per ray)"}
     if TRACE_LOCAL_BYTES_PER_RAY is not None:
         roof["local_bytes_per_ray"] = TRACE_LOCAL_BYTES_PER_RAY
     line = {"metric": "Mrays/s (plain render; ms/frame alongside)", "value": value, "unit": "Mrays/s",

@@ -208,10 +208,13 @@ __device__ __forceinline__ void bwd_epilogue(const ConvArgs& a, float (&v)[kRows
 // block ct): the accumulator at TMEM column `tmem` holds row r at columns
 // r*BN..r*BN+BN-1; lane p = pixel x0 + p.  The calling warp reads its quarter
 // of the lanes: `warp` (0..3) selects lanes 32*warp..32*warp+31 and
-// tid = 32*warp + lane is the pixel offset.
+// tid = 32*warp + lane is the pixel offset.  With nparts > 1 several warps
+// share a quarter: part `part` takes every nparts-th 16-channel chunk, or
+// for the tail (which needs a pixel's 32 channels together) every
+// nparts-th row.
 template <int BN>
 __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, int warp, int tid, int n, int ct,
-                                              int x0, int y0)
+                                              int x0, int y0, int part = 0, int nparts = 1)
 {
     const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
     const int x = x0 + tid;
@@ -223,6 +226,7 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, 
 #pragma unroll
         for (int r = 0; r < kRows; ++r)
         {
+            if (r % nparts != part) continue;
             float v[32];
             tc::tmem_ld16(lanebase + (uint32_t)(r * BN), v);
             tc::tmem_ld16(lanebase + (uint32_t)(r * BN + 16), v + 16);
@@ -248,7 +252,7 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, 
         for (int r = 0; r < kRows; ++r)
         {
             const int y = y0 + r;
-            if (!xin || y >= a.H) continue;
+            if (r % nparts != part || !xin || y >= a.H) continue;
 #pragma unroll
             for (int k = 0; k < 3; ++k)
             {
@@ -262,7 +266,7 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, 
     else
     {
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16)
+        for (int c0 = 16 * part; c0 < BN; c0 += 16 * nparts)
         {
             float v[kRows][16];
 #pragma unroll
@@ -452,15 +456,18 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 }
 
 
-// Persistent, warp-specialised form of conv3x3_tc_kernel: one CTA per SM (two
-// for the smallest tiles) walks the output tiles in a grid-stride loop.
+// Persistent, warp-specialised form of conv3x3_tc_kernel: one CTA per SM
+// walks the output tiles in a grid-stride loop.
 //   warp 0 (one lane)  TMA loads of input halos and weight blocks into a
 //                      STAGES-deep ring (full/empty mbarriers);
 //   warp 1 (one lane)  tcgen05.mma into one of two TMEM accumulators (each two
 //                      rows x BN columns), committing the ring stage when its
 //                      MMAs retire and the accumulator when the tile is done;
-//   warps 2..5         the epilogue of tile i (tile_epilogue, each warp its
-//                      TMEM lane quarter) while tile i+1's loads and MMAs run.
+//   warps 2..9         the epilogue of tile i (tile_epilogue: two warps per
+//                      TMEM lane quarter, splitting the channel chunks, or the
+//                      rows of the tail) while tile i+1's loads and MMAs run;
+//                      eight warps hide the epilogue's load and store latency
+//                      behind one another.
 // Loads run ahead across tile boundaries; TMEM is allocated once per CTA.
 // The same packed weights, the same MMAs in the same order: results are
 // identical to conv3x3_tc_kernel's.
@@ -470,7 +477,8 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 // ROWS (2 or 4, persistent kernel only): output rows per tile; a 4-row tile
 // reads a 6-row halo for four rows of MMAs (each weight block feeds four M
 // tiles) and hands the epilogue two 2-row sub-tiles.
-constexpr int kPThreads = 192;
+constexpr int kEpiWarps = 8;
+constexpr int kPThreads = 64 + 32 * kEpiWarps;
 template <int BN, int KC, bool RESW, int ROWS = kRows>
 struct PSmem
 {
@@ -542,7 +550,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
         for (int b = 0; b < 2; ++b)
         {
             tc::mbar_init(&acc_full[b], 1);
-            tc::mbar_init(&acc_empty[b], 4);  // one arrival per epilogue warp
+            tc::mbar_init(&acc_empty[b], kEpiWarps);  // one arrival per epilogue warp
         }
         tc::mbar_init(done, 1);
         tc::mbar_init(wfull, 1);
@@ -658,7 +666,9 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
     }
     else
     {
-        const int q = warp & 3;  // the TMEM lane quarter this warp may read
+        const int q = warp & 3;                // the TMEM lane quarter this warp may read
+        const int part = (warp - 2) >> 2;      // which of the quarter's warps this is
+        constexpr int kParts = kEpiWarps / 4;
         int j = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++j)
         {
@@ -674,7 +684,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
 #pragma unroll 1
             for (int sub = 0; sub < ROWS / 2; ++sub)  // 2-row sub-tiles
                 tile_epilogue<BN>(a, tmem + (uint32_t)b * kAccCols + (uint32_t)(sub * 2 * BN), q, q * 32 + lane, n,
-                                  ct, x0, y0 + 2 * sub);
+                                  ct, x0, y0 + 2 * sub, part, kParts);
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&acc_empty[b]);
