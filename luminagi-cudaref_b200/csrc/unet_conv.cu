@@ -204,6 +204,39 @@ __device__ __forceinline__ void bwd_epilogue(const ConvArgs& a, float (&v)[kRows
     }
 }
 
+// The epilogue's per-layer constants, staged once per CTA in shared memory so
+// the epilogue reads them as 16-byte vectors instead of one global load per
+// value: bias (Cout <= 256) and the UNet tail's 3 x 32 weights and 3 biases.
+struct __align__(16) EpiConsts
+{
+    float bias[256];
+    float tw[96];
+    float tb[4];
+};
+__device__ __forceinline__ void stage_epi_consts(const ConvArgs& a, EpiConsts& ec, int tid, int nthreads)
+{
+    if (a.bias && a.epilogue <= kEpiTail)
+        for (int i = tid; i < a.Cout; i += nthreads) ec.bias[i] = a.bias[i];
+    if (a.epilogue == kEpiTail)
+    {
+        for (int i = tid; i < 96; i += nthreads) ec.tw[i] = a.tail_w[i];
+        if (tid < 3) ec.tb[tid] = a.tail_b[tid];
+    }
+}
+__device__ __forceinline__ void ld16(const float* p, float (&v)[16])  // p 16-byte aligned (shared memory)
+{
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+        const float4 t = q[i];
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+    }
+}
+
 // Epilogue of one output tile (2 rows x 128 pixels x BN channels of output
 // block ct): the accumulator at TMEM column `tmem` holds row r at columns
 // r*BN..r*BN+BN-1; lane p = pixel x0 + p.  The calling warp reads its quarter
@@ -213,8 +246,8 @@ __device__ __forceinline__ void bwd_epilogue(const ConvArgs& a, float (&v)[kRows
 // for the tail (which needs a pixel's 32 channels together) every
 // nparts-th row.
 template <int BN>
-__device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, int warp, int tid, int n, int ct,
-                                              int x0, int y0, int part = 0, int nparts = 1)
+__device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts& ec, uint32_t tmem, int warp, int tid,
+                                              int n, int ct, int x0, int y0, int part = 0, int nparts = 1)
 {
     const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
     const int x = x0 + tid;
@@ -231,7 +264,13 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, 
             tc::tmem_ld16(lanebase + (uint32_t)(r * BN), v);
             tc::tmem_ld16(lanebase + (uint32_t)(r * BN + 16), v + 16);
 #pragma unroll
-            for (int c = 0; c < 32; ++c) v[c] = bf16r(act(v[c] + __ldg(&a.bias[c]), a.slope));
+            for (int c0 = 0; c0 < 32; c0 += 16)
+            {
+                float bb[16];
+                ld16(ec.bias + c0, bb);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[c0 + j] = bf16r(act(v[c0 + j] + bb[j], a.slope));
+            }
             const int y = y0 + r;
             if (a.out && xin && y < a.H)
             {
@@ -242,9 +281,15 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, 
 #pragma unroll
             for (int k = 0; k < 3; ++k)
             {
-                float acc = __ldg(&a.tail_b[k]);
+                float acc = ec.tb[k];
 #pragma unroll
-                for (int c = 0; c < 32; ++c) acc = fmaf(__ldg(&a.tail_w[k * 32 + c]), v[c], acc);
+                for (int c0 = 0; c0 < 32; c0 += 16)
+                {
+                    float ww[16];
+                    ld16(ec.tw + k * 32 + c0, ww);
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc = fmaf(ww[j], v[c0 + j], acc);
+                }
                 o[r][k] = acc;
             }
         }
@@ -274,10 +319,12 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, uint32_t tmem, 
             const int cg = ct * BN + c0;  // layer channel of v[.][0]
             if (a.epilogue <= kEpiUpsample)
             {
+                float bb[16];
+                ld16(ec.bias + cg, bb);
 #pragma unroll
                 for (int r = 0; r < kRows; ++r)
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + __ldg(&a.bias[cg + j]), a.slope));
+                    for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + bb[j], a.slope));
             }
             const int b0 = (a.out_coff + cg) >> 3;
             if (a.epilogue >= kEpiBwdMask)
@@ -348,8 +395,10 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     uint64_t* done = empty + STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     __shared__ int s_fail;
+    __shared__ EpiConsts ec;
 
     const int tid = threadIdx.x, warp = tid >> 5;
+    stage_epi_consts(a, ec, tid, kThreads);  // visible after the __syncthreads below
     const int n_cot = a.Cout / BN;
     const int x0 = blockIdx.x * kTileX;
     const int y0 = blockIdx.y * kRows;
@@ -444,7 +493,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
     const bool got = tc::mbar_wait(done, 0);
     if (!got && a.err) atomicExch(a.err, 2);
     tc::tc_fence_after();
-    if (got && !s_fail) tile_epilogue<BN>(a, tmem, warp, tid, n, ct, x0, y0);
+    if (got && !s_fail) tile_epilogue<BN>(a, ec, tmem, warp, tid, n, ct, x0, y0);
 
     tc::tc_fence_before();
     __syncthreads();
@@ -508,8 +557,10 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(wfull + 1);
     uint8_t* wres = smem + STAGES * P::kStage + P::kBarBytes;  // RESW: KB x 9 x KC x BN weights
     __shared__ volatile int s_fail;
+    __shared__ EpiConsts ec;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    stage_epi_consts(a, ec, tid, kPThreads);  // visible after the __syncthreads below
     const int n_cot = a.Cout / BN;
     const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + ROWS - 1) / ROWS;
     const int n_tiles = tiles_x * tiles_y * a.N * n_cot;
@@ -683,8 +734,8 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
             coords(t, n, ct, x0, y0);
 #pragma unroll 1
             for (int sub = 0; sub < ROWS / 2; ++sub)  // 2-row sub-tiles
-                tile_epilogue<BN>(a, tmem + (uint32_t)b * kAccCols + (uint32_t)(sub * 2 * BN), q, q * 32 + lane, n,
-                                  ct, x0, y0 + 2 * sub, part, kParts);
+                tile_epilogue<BN>(a, ec, tmem + (uint32_t)b * kAccCols + (uint32_t)(sub * 2 * BN), q, q * 32 + lane,
+                                  n, ct, x0, y0 + 2 * sub, part, kParts);
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&acc_empty[b]);
@@ -738,9 +789,9 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// Dynamic shared memory a CTA may use on sm_100: 227 KB less 1 KB of headroom
-// for the kernel's static shared memory.
-constexpr int kMaxSmem = 226 * 1024;
+// Dynamic shared memory a CTA may use on sm_100: 227 KB less 2 KB of headroom
+// for the kernel's static shared memory (the epilogue constants, 1.4 KB).
+constexpr int kMaxSmem = 225 * 1024;
 
 template <int BN, int KC, int STAGES, bool RESW = false, int ROWS = kRows>
 cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
