@@ -368,7 +368,9 @@ int lg_unet_wait_selftest(lg_unet* u, int64_t limit_ns);
  * weights fit beside the pipeline) inside real passes at n x h x w and keeps
  * the fastest; weights are repacked to match.  tiles_out (may be NULL)
  * receives 30 (bn, kc, stages, kernel) quadruples, forward layers first.
- * The Adam state is reset. */
+ * The Adam state is reset.  Until then (or lg_unet_set_tiles) the forward
+ * convolutions use the choice this autotuner made at batch 8, 1728x864 on
+ * B200, and the input-gradient convolutions a per-shape default. */
 #define LG_UNET_TUNE_BACKWARD 1
 int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_out);
 /* Sets the 30 tile choices directly, in lg_unet_autotune's format; e.g. to
