@@ -231,6 +231,9 @@ def main(argv=None):
     ap.add_argument("--width", type=int, default=1728)
     ap.add_argument("--height", type=int, default=864)
     ap.add_argument("--checkpoint", default="")
+    ap.add_argument("--save-npz", default="",
+                    help="also write the best parameters of each recipe as <path>.<recipe>.npz (FP16, state_dict "
+                         "order, with the held-out pose indices)")
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--gbuffer", action="store_true", help="12-channel network on colour + G-buffer (train.py --gbuffer)")
     ap.add_argument("--variant", default="ref", choices=["ref", "hdr"],
@@ -265,6 +268,10 @@ def main(argv=None):
         net.set_params(best)
         if a.checkpoint:
             save_checkpoint(best, f"{a.checkpoint}.{name}.pt", in_ch, a.variant)
+        if a.save_npz:
+            np.savez_compressed(f"{a.save_npz}.{name}.npz", params=best.astype(np.float16),
+                                val_idx=np.asarray(val_idx, np.int32), poses=np.int32(a.poses), in_ch=np.int32(in_ch),
+                                variant=np.bytes_(a.variant), recipe=np.bytes_(spec))
         agg, rows = evaluate(net, frames)
         res["recipes"][name] = {"spec": spec, "train_seconds": t_train, "best_val_l1": best_val,
                                 "history_tail": hist[-3:], "eval": agg, "per_pose": rows}
