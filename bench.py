@@ -29,6 +29,10 @@ counting pass) with ms/frame alongside.
             sources for the host) with OpenMP on all host cores, on a fixed
             sample of rows (every CPU_ROW_STEP-th row; the reference arm uses
             the same rows); rays counted by the oracle on the same rows.
+  denoise   8 spp + UNet against plain 256 spp on the same frame (device
+            time), with the trained weights in lumina/data: PSNR/SSIM of both
+            and of the 8-spp input against a 1024-spp FP64 judge on an orbit
+            pose held out of training.
   ingest    scene-file load times: this library on scene.json and on the
             binary scene file, and the reference's LoadSceneJSON on the same
             JSON (host only).
@@ -70,6 +74,10 @@ CPU_ROW_STEP = 16
 # Local-memory (stack and spill) bytes per traced ray of trace_kernel, from the
 # same capture: (806.3 M load + 911.3 M store sectors) x 32 B / rays.
 TRACE_LOCAL_BYTES_PER_RAY = (806348142 + 911329462) * 32 / 65366791
+# Denoiser weights trained by this library on the engine scene (lumina.surrogate, the
+# 120-epoch recipe with 24 crops per image per epoch; FP16 copy of the best-validation
+# parameters, with the indices of the poses held out of training).
+PRETRAINED = ROOT / "luminagi-cudaref_b200" / "lumina" / "data" / "unet_engine_long.npz"
 # L2 probe: buffer size and passes; 64 MB gave the highest read bandwidth of the
 # sizes tried (8-96 MB), the conservative denominator.
 L2_PROBE_BYTES = 64 << 20
@@ -419,12 +427,17 @@ def main():
     h2d = scene.tris.nbytes + scene.mat_albedo.nbytes + scene.points.nbytes
     d2h = W * H * 3
 
-    # Headline comparison on the same frame: 8 spp + UNet denoise vs the plain 256-spp render (device time).
+    # Headline comparison: 8 spp + UNet denoise vs the plain 256-spp render (device time), and their quality
+    # against a 1024-spp FP64 judge on a pose the denoiser was not trained on.
     denoise = None
     if not args.no_denoise and args.scene == "engine":
         net = lumina.UNet()
-        rng = np.random.default_rng(0)
-        net.set_params(rng.normal(0, 0.02, net.n_params).astype(np.float32))  # cost does not depend on the values
+        trained = PRETRAINED.exists()
+        if trained:
+            z = np.load(PRETRAINED)
+            net.set_params(z["params"].astype(np.float32))
+        else:  # the cost of a forward pass does not depend on the values
+            net.set_params(np.random.default_rng(0).normal(0, 0.02, net.n_params).astype(np.float32))
         x = torch.empty((1, 3, H, W), device=f"cuda:{dev}")
         y = torch.empty_like(x)
         o8 = _ffi.LgRenderOpts(8, args.bounces, 0, 0)
@@ -453,7 +466,24 @@ def main():
         ms_p = timed(lambda: _ffi.check(_ffi.lib().lg_render_device(
             r._h, C.byref(cam), C.byref(o256), C.c_void_p(stream.cuda_stream), None, None, None)), 1)
         denoise = {"ms_8spp_plus_unet": ms_d, "ms_256spp": ms_p, "speedup": ms_p / ms_d,
-                   "weights": "random (the cost of a forward pass does not depend on their values)"}
+                   "weights": "trained (lumina/data/unet_engine_long.npz)" if trained else
+                              "random (the cost of a forward pass does not depend on their values)"}
+        if trained:
+            from lumina import surrogate as S
+            from lumina.scene import ENGINE_CENTER, orbit_poses
+            pose = int(z["val_idx"][0])
+            p_t = orbit_poses(int(z["poses"]), seed=11, center=ENGINE_CENTER)[pose]
+            vcam = scene.camera.look_at(*p_t)
+            frames = S.eval_frames(r, [vcam], 8, 256, 1024, args.bounces)
+            agg, _ = S.evaluate(net, frames)
+            denoise["quality"] = {
+                "pose": f"orbit pose {pose} of {int(z['poses'])} (held out of training)",
+                "judge": "1024 spp, FP64 accumulators", "metric": "PSNR/SSIM of the 8-bit tonemapped images",
+                "psnr_8spp": agg["noisy_psnr"], "psnr_8spp_unet": agg["denoised_psnr"],
+                "psnr_256spp": agg["clean_psnr"], "ssim_8spp": agg["noisy_ssim"],
+                "ssim_8spp_unet": agg["denoised_ssim"], "ssim_256spp": agg["clean_ssim"],
+                "gain_db_over_8spp": agg["denoised_psnr"] - agg["noisy_psnr"],
+                "db_vs_256spp": agg["denoised_psnr"] - agg["clean_psnr"]}
         net.close()
 
     traffic = TRACE_DRAM_BYTES_PER_RAY * rays

@@ -52,3 +52,16 @@ def test_bf16_emulation_is_close_to_fp32():
         a = m(torch.from_numpy(g["x"]))
         b = unet_ref.forward_bf16(m, torch.from_numpy(g["x"]))
     assert float((a - b).abs().max()) < 0.1
+
+
+def test_packaged_denoiser_weights():
+    """The trained weights shipped in the package (FP16, state_dict order)
+    match the 3-channel network's parameter count, are finite, and name the
+    orbit poses held out of their training."""
+    import pathlib
+    z = np.load(pathlib.Path(__file__).resolve().parent.parent / "luminagi-cudaref_b200" / "lumina" / "data" /
+                "unet_engine_long.npz")
+    p = z["params"].astype(np.float32)
+    assert p.shape == (1946947,) and np.isfinite(p).all() and np.abs(p).max() > 0
+    assert len(z["val_idx"]) == 5 and (0 <= z["val_idx"]).all() and (z["val_idx"] < int(z["poses"])).all()
+    assert int(z["in_ch"]) == 3 and bytes(z["variant"]) == b"ref"
