@@ -365,8 +365,13 @@ int lg_unet_wait_selftest(lg_unet* u, int64_t limit_ns);
  * per K-block, pipeline stages) with each of the kernels (0: one tile per
  * CTA; 1: persistent and warp-specialised; 2: persistent with the layer's
  * weights resident in shared memory, for layers with one output block whose
- * weights fit beside the pipeline) inside real passes at n x h x w and keeps
- * the fastest; weights are repacked to match.  tiles_out (may be NULL)
+ * weights fit beside the pipeline; 3: as 2 on 4-row tiles; 4: as 3 with the
+ * three row taps of each column tap packed side by side into one MMA's N,
+ * for 32 and 64 output channels, input tiles loaded in 8-pixel runs; 5: as 4
+ * on 8-row tiles; 6 and 7: packed row taps with the weights streamed, 4- and
+ * 8-row tiles; all give bit-identical results)
+ * inside real passes at n x h x w and keeps the fastest; weights are
+ * repacked to match.  tiles_out (may be NULL)
  * receives 30 (bn, kc, stages, kernel) quadruples, forward layers first.
  * The Adam state is reset.  Until then (or lg_unet_set_tiles) the forward
  * convolutions use the choice this autotuner made at batch 8, 1728x864 on

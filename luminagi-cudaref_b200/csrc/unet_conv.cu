@@ -56,10 +56,14 @@ TileCfg pick_cfg(int Cin, int Cout)
     return c;
 }
 
-template <int BN, int KC, int ROWS = kRows>
+// Pixels per halo row of an A tile in shared memory: 130 when the TMA box
+// starts at x0 - 1 pixel by pixel (16-byte box rows), 144 when it is loaded
+// as 18 runs of 8 pixels (128-byte box rows) from x0 - 8 (chunked view).
+constexpr int kChunkX = kTileX + 16;
+template <int BN, int KC, int ROWS = kRows, int AX = kHaloX>
 struct Smem
 {
-    static constexpr int kABytes = (ROWS + 2) * kHaloX * KC * 2;
+    static constexpr int kABytes = (ROWS + 2) * AX * KC * 2;
     static constexpr int kBBytes = 9 * KC * BN * 2;
     static constexpr int kStage = ((kABytes + kBBytes + 1023) / 1024) * 1024;
 };
@@ -523,15 +527,28 @@ __global__ void __launch_bounds__(kThreads, 1) conv3x3_tc_kernel(const __grid_co
 // RESW (layers with one output block, Cout == BN): every K-block's weights
 // are copied into shared memory once per CTA, so a ring stage holds only the
 // input halo, and more stages fit; the weights are the same for every tile.
-// ROWS (2 or 4, persistent kernel only): output rows per tile; a 4-row tile
-// reads a 6-row halo for four rows of MMAs (each weight block feeds four M
-// tiles) and hands the epilogue two 2-row sub-tiles.
+// ROWS (2, 4 or 8, persistent kernel only): output rows per tile; a 4-row
+// tile reads a 6-row halo for four rows of MMAs (each weight block feeds four
+// M tiles) and hands the epilogue two 2-row sub-tiles.
+// DYP (row taps packed into N): with BN = 32 or 64 a 128 x BN x 16 MMA is
+// bound by the tensor core reading its 4 KB A tile from shared memory, not by
+// its math.  So the weights of one column tap dx are packed with the three
+// row taps side by side along N, in the order dy = 2, 1, 0, and one MMA per
+// (halo row h, dx, K step) multiplies halo row h by all three: its N columns
+// land on the accumulators of output rows h-2, h-1, h, which lie next to
+// each other in TMEM (row r at column r * BN).  Rows outside the tile are
+// left out by narrowing N at the first and last halo rows.  Each output row
+// then receives the same products in the same order as with one MMA per tap
+// (dy outer, dx, K step inner), so results are bit-identical, from
+// ROWS + 2 MMAs per (dx, K step) instead of 3 * ROWS.  The first MMA that
+// reaches an output row (dx = 0, first K step of the first K-block) is
+// issued alone for that row so that it can overwrite instead of add.
 constexpr int kEpiWarps = 8;
 constexpr int kPThreads = 64 + 32 * kEpiWarps;
-template <int BN, int KC, bool RESW, int ROWS = kRows>
+template <int BN, int KC, bool RESW, int ROWS = kRows, int AX = kHaloX>
 struct PSmem
 {
-    using S = Smem<BN, KC, ROWS>;
+    using S = Smem<BN, KC, ROWS, AX>;
     static constexpr int kStage = RESW ? ((S::kABytes + 1023) / 1024) * 1024 : S::kStage;
     static constexpr int kBarBytes = 1024;  // mbarriers and the TMEM slot, after the ring
     // dynamic shared memory of a launch with KB K-blocks (1024 B for aligning the base)
@@ -540,12 +557,16 @@ struct PSmem
         return stages * kStage + kBarBytes + (RESW ? KB * S::kBBytes : 0) + 1024;
     }
 };
-template <int BN, int KC, int STAGES, bool RESW, int ROWS = kRows>
+template <int BN, int KC, int STAGES, bool RESW, int ROWS = kRows, bool DYP = false>
 __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
 {
-    static_assert(ROWS == 2 || ROWS == 4, "2- or 4-row tiles");
-    using S = Smem<BN, KC, ROWS>;
-    using P = PSmem<BN, KC, RESW, ROWS>;
+    static_assert(ROWS == 2 || ROWS == 4 || ROWS == 8, "2-, 4- or 8-row tiles");
+    static_assert(!DYP || 3 * BN <= 256, "row taps packed into N need 3 * BN <= 256");
+    // DYP kernels load their A tiles through the chunked view (make_map_chunked)
+    constexpr int AX = DYP ? kChunkX : kHaloX;  // pixels per halo row in shared memory
+    constexpr int AX0 = DYP ? 7 : 0;            // position of pixel x0 - 1 in a halo row
+    using S = Smem<BN, KC, ROWS, AX>;
+    using P = PSmem<BN, KC, RESW, ROWS, AX>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * P::kStage);
@@ -569,8 +590,10 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
     constexpr uint32_t kCols = 2 * kAccCols;  // two of them (a power of two >= 32 for BN >= 16)
     static_assert(kCols <= 512, "two accumulators must fit in TMEM");
     constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, BN);
-    constexpr uint32_t kLboA = (ROWS + 2) * kHaloX * 16;
-    constexpr uint32_t kLboB = BN * 16;
+    constexpr uint32_t kLboA = (ROWS + 2) * AX * 16;
+    constexpr uint32_t kLboB = (DYP ? 3 : 1) * BN * 16;
+    constexpr uint32_t kIdesc2 = tc::idesc_bf16_f32(128, DYP ? 2 * BN : BN);
+    constexpr uint32_t kIdesc3 = tc::idesc_bf16_f32(128, DYP ? 3 * BN : BN);
     // tile t -> (n, ct, y0, x0); output blocks innermost so concurrent tiles share input rows
     auto coords = [&](int t, int& n, int& ct, int& x0, int& y0) {
         ct = t % n_cot;
@@ -639,16 +662,19 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                         break;
                     }
                     uint8_t* A = smem + s * P::kStage;
+                    // x coordinate: pixel x0 - 1; for the 144-pixel rows of the DYP
+                    // kernels pixel x0 - 8, or the 8-pixel run that starts there
+                    const int ax = DYP ? (a.a_chunked ? x0 / 8 - 1 : x0 - 8) : x0 - 1;
                     if (RESW)
                     {
                         tc::mbar_expect_tx(&full[s], (uint32_t)S::kABytes);
-                        tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
+                        tc::tma_load_5d(A, &tmap, &full[s], 0, ax, y0 - 1, kb * (KC / 8), n);
                     }
                     else
                     {
                         uint8_t* B = A + S::kABytes;
                         tc::mbar_expect_tx(&full[s], (uint32_t)(S::kABytes + S::kBBytes));
-                        tc::tma_load_5d(A, &tmap, &full[s], 0, x0 - 1, y0 - 1, kb * (KC / 8), n);
+                        tc::tma_load_5d(A, &tmap, &full[s], 0, ax, y0 - 1, kb * (KC / 8), n);
                         tc::bulk_load(B, wsrc + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes, &full[s]);
                     }
                 }
@@ -684,22 +710,60 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                     const uint32_t abase = tc::smem_u32(smem + s * P::kStage);
                     const uint32_t bbase =
                         RESW ? tc::smem_u32(wres) + (uint32_t)(kb * S::kBBytes) : abase + (uint32_t)S::kABytes;
-#pragma unroll 1
-                    for (int tap = 0; tap < 9; ++tap)
+                    if (DYP)
                     {
-                        const int dy = tap / 3, dx = tap % 3;
-#pragma unroll
-                        for (int ks = 0; ks < KC / 16; ++ks)
+                        // weights of K-block kb: [dx][KC/8][dy = 2, 1, 0][BN][8]
+#pragma unroll 1
+                        for (int h = 0; h < ROWS + 2; ++h)
                         {
-                            const uint64_t bd =
-                                tc::smem_desc(bbase + (uint32_t)((tap * (KC / 8) + 2 * ks) * BN * 16), kLboB, 128);
+                            const int dmax = h < 2 ? h : 2;                        // the row taps whose output
+                            const int dmin = h - ROWS + 1 > 0 ? h - ROWS + 1 : 0;  // row h - dy is in the tile
+                            const int nb = dmax - dmin + 1;
+                            const uint32_t id = nb == 3 ? kIdesc3 : (nb == 2 ? kIdesc2 : kIdesc);
+                            const uint32_t dcol = acc + (uint32_t)((h - dmax) * BN);
+                            const bool first = kb == 0 && dmin == 0;  // output row h starts here
 #pragma unroll
-                            for (int r = 0; r < ROWS; ++r)
+                            for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                                for (int ks = 0; ks < KC / 16; ++ks)
+                                {
+                                    const uint32_t aoff =
+                                        (uint32_t)(2 * ks) * kLboA + (uint32_t)((h * AX + AX0 + dx) * 16);
+                                    const uint64_t ad = tc::smem_desc(abase + aoff, kLboA, 128);
+                                    const uint32_t plane = bbase + (uint32_t)((dx * (KC / 8) + 2 * ks) * kLboB);
+                                    const uint64_t bd =
+                                        tc::smem_desc(plane + (uint32_t)((2 - dmax) * BN * 16), kLboB, 128);
+                                    if (first && dx == 0 && ks == 0)
+                                    {
+                                        tc::mma_bf16(acc + (uint32_t)(h * BN), ad,
+                                                     tc::smem_desc(plane + 2 * BN * 16, kLboB, 128), kIdesc, 0u);
+                                        if (dmax > 0) tc::mma_bf16(dcol, ad, bd, dmax == 2 ? kIdesc2 : kIdesc, 1u);
+                                    }
+                                    else
+                                        tc::mma_bf16(dcol, ad, bd, id, 1u);
+                                }
+                        }
+                    }
+                    else
+                    {
+#pragma unroll 1
+                        for (int tap = 0; tap < 9; ++tap)
+                        {
+                            const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+                            for (int ks = 0; ks < KC / 16; ++ks)
                             {
-                                const uint32_t aoff =
-                                    (uint32_t)(2 * ks) * kLboA + (uint32_t)(((r + dy) * kHaloX + dx) * 16);
-                                const uint64_t ad = tc::smem_desc(abase + aoff, kLboA, 128);
-                                tc::mma_bf16(acc + (uint32_t)(r * BN), ad, bd, kIdesc, (kb | tap | ks) != 0 ? 1u : 0u);
+                                const uint64_t bd = tc::smem_desc(
+                                    bbase + (uint32_t)((tap * (KC / 8) + 2 * ks) * BN * 16), kLboB, 128);
+#pragma unroll
+                                for (int r = 0; r < ROWS; ++r)
+                                {
+                                    const uint32_t aoff =
+                                        (uint32_t)(2 * ks) * kLboA + (uint32_t)(((r + dy) * AX + dx) * 16);
+                                    const uint64_t ad = tc::smem_desc(abase + aoff, kLboA, 128);
+                                    tc::mma_bf16(acc + (uint32_t)(r * BN), ad, bd, kIdesc,
+                                                 (kb | tap | ks) != 0 ? 1u : 0u);
+                                }
                             }
                         }
                     }
@@ -775,13 +839,35 @@ EncodeTiledFn encode_fn()
 // 5-D map over a blocked BF16 tensor: (8 channels, W, H, C/8, N), box
 // (8, 130, 4, KC/8, 1).
 cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int KC,
-                     int halo_y = kHaloY)
+                     int halo_y = kHaloY, int box_x = kHaloX)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)(C / 8), (cuuint64_t)N};
     cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)(C / 8) * H * W * 16};
-    cuuint32_t box[5] = {8, (cuuint32_t)kHaloX, (cuuint32_t)halo_y, (cuuint32_t)(KC / 8), 1};
+    cuuint32_t box[5] = {8, (cuuint32_t)box_x, (cuuint32_t)halo_y, (cuuint32_t)(KC / 8), 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Chunked view of the same tensor: (64 = 8 pixels x 8 channels, W/8, H, C/8,
+// N), box (64, 18, halo_y, KC/8, 1).  Each box row is 128 contiguous bytes;
+// with one pixel per box row (make_map) every 16-byte row costs the TMA unit
+// a request and a 32-byte sector.  The box lands in shared memory with the
+// same pixel-major layout, 144 pixels per row from pixel x0 - 8 on.  Needs
+// W % 8 == 0 (the runs must not cross into the next row); other widths load
+// the same 144 pixels one by one (make_map with box_x = 144).
+cudaError_t make_map_chunked(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int KC, int halo_y)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    if (W % 8) return cudaErrorInvalidValue;
+    cuuint64_t dims[5] = {64, (cuuint64_t)(W / 8), (cuuint64_t)H, (cuuint64_t)(C / 8), (cuuint64_t)N};
+    cuuint64_t strides[4] = {128, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)(C / 8) * H * W * 16};
+    cuuint32_t box[5] = {64, (cuuint32_t)(kChunkX / 8), (cuuint32_t)halo_y, (cuuint32_t)(KC / 8), 1};
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)base, dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -793,17 +879,21 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
 // for the kernel's static shared memory (the epilogue constants, 1.4 KB).
 constexpr int kMaxSmem = 225 * 1024;
 
-template <int BN, int KC, int STAGES, bool RESW = false, int ROWS = kRows>
+template <int BN, int KC, int STAGES, bool RESW = false, int ROWS = kRows, bool DYP = false>
 cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
 {
     const int KB = a.Cin / KC;
     if (RESW && a.Cout != BN) return cudaErrorInvalidValue;  // one output block only
-    const int smem = PSmem<BN, KC, RESW, ROWS>::bytes(STAGES, KB);
+    const int smem = PSmem<BN, KC, RESW, ROWS, DYP ? kChunkX : kHaloX>::bytes(STAGES, KB);
     if (smem > kMaxSmem) return cudaErrorInvalidValue;
     CUtensorMap m;
-    cudaError_t e = make_map(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2);
+    ConvArgs b = a;
+    b.a_chunked = DYP && a.W % 8 == 0;
+    cudaError_t e = !DYP ? make_map(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2)
+                    : b.a_chunked ? make_map_chunked(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2)
+                                  : make_map(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2, kChunkX);
     if (e != cudaSuccess) return e;
-    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW, ROWS>;
+    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW, ROWS, DYP>;
     // The resident-weights form's smem depends on KB: size the attribute for
     // the largest launch it may see and query occupancy per launch size.
     static bool attr_done = false;
@@ -826,7 +916,7 @@ cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaSt
     if (per_sm < 1) per_sm = 1;
     const long long tiles = (long long)((a.W + kTileX - 1) / kTileX) * ((a.H + ROWS - 1) / ROWS) * a.N * (a.Cout / BN);
     const long long grid = std::min<long long>(tiles, (long long)per_sm * sm_count);
-    fn<<<(unsigned)grid, kPThreads, smem, stream>>>(m, a);
+    fn<<<(unsigned)grid, kPThreads, smem, stream>>>(m, b);
     return cudaGetLastError();
 }
 
@@ -849,20 +939,40 @@ cudaError_t launch(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stre
     return cudaGetLastError();
 }
 
-__global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real, int Cin, int BN, int KC,
+// Position i of a packed weight array -> (ct, kb, tap, kc8, j, e): output
+// block, K-block, tap (dy * 3 + dx), 8-channel plane, output channel in the
+// block, channel in the plane.  Plain layout: (ct, kb, tap, kc8, j, e),
+// innermost last.  Row taps packed into N (DYP kernels): (ct, kb, dx, kc8,
+// 2 - dy, j, e).
+__device__ __forceinline__ void packed_index(size_t r, int BN, int KC, int KB, bool dyp, int& ct, int& kb, int& tap,
+                                             int& kc8, int& j, int& e)
+{
+    e = (int)(r % 8); r /= 8;
+    j = (int)(r % BN); r /= BN;
+    if (dyp)
+    {
+        const int dyr = (int)(r % 3); r /= 3;
+        kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
+        const int dx = (int)(r % 3); r /= 3;
+        tap = (2 - dyr) * 3 + dx;
+    }
+    else
+    {
+        kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
+        tap = (int)(r % 9); r /= 9;
+    }
+    kb = (int)(r % KB); r /= KB;
+    ct = (int)r;
+}
+
+__global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real, int Cin, int BN, int KC, int dyp,
                             __nv_bfloat16* __restrict__ out, size_t total)
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
-    // i -> (ct, kb, tap, kc8, j, e), innermost last
-    size_t r = i;
-    const int e = (int)(r % 8); r /= 8;
-    const int j = (int)(r % BN); r /= BN;
-    const int kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
-    const int tap = (int)(r % 9); r /= 9;
     const int KB = Cin / KC;
-    const int kb = (int)(r % KB); r /= KB;
-    const int ct = (int)r;
+    int ct, kb, tap, kc8, j, e;
+    packed_index(i, BN, KC, KB, dyp != 0, ct, kb, tap, kc8, j, e);
     const int co = ct * BN + j;
     const int ci = kb * KC + kc8 * 8 + e;
     float v = 0.0f;
@@ -873,18 +983,13 @@ __global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real,
 // Input-gradient weights: output (ct, kb, tap, kc8, j, e) of a conv with
 // Cin' = Cout (forward) and Cout' = ci_cnt reads w[co = ci'][ci_lo + co'][2-ky][2-kx].
 __global__ void pack_dgrad_kernel(const float* __restrict__ w, int Cout, int Cin_real, int ci_lo, int ci_cnt, int BN,
-                                  int KC, __nv_bfloat16* __restrict__ out, size_t total)
+                                  int KC, int dyp, __nv_bfloat16* __restrict__ out, size_t total)
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
-    size_t r = i;
-    const int e = (int)(r % 8); r /= 8;
-    const int j = (int)(r % BN); r /= BN;
-    const int kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
-    const int tap = (int)(r % 9); r /= 9;
     const int KB = Cout / KC;
-    const int kb = (int)(r % KB); r /= KB;
-    const int ct = (int)r;
+    int ct, kb, tap, kc8, j, e;
+    packed_index(i, BN, KC, KB, dyp != 0, ct, kb, tap, kc8, j, e);
     const int cop = ct * BN + j;             // output channel of the backward conv
     const int cip = kb * KC + kc8 * 8 + e;   // its input channel = forward output channel
     const int ky = 2 - tap / 3, kx = 2 - tap % 3;
@@ -938,14 +1043,24 @@ constexpr ConvTile kCompiledTiles[] = {{32, 16, 4, 0},  {32, 32, 2, 0},  {32, 32
                                        {64, 32, 2, 1},  {64, 32, 3, 1},  {128, 16, 3, 1}, {128, 32, 2, 1},
                                        {32, 16, 10, 2}, {32, 32, 2, 2},  {32, 32, 5, 2},  {32, 32, 6, 2},
                                        {64, 32, 3, 2},  {64, 32, 4, 2},  {32, 16, 8, 3},  {32, 32, 3, 3},
-                                       {32, 32, 4, 3},  {64, 32, 3, 3}};
+                                       {32, 32, 4, 3},  {64, 32, 3, 3},  {32, 16, 7, 4},  {32, 32, 3, 4},
+                                       {64, 32, 2, 4},  {64, 32, 3, 4},  {32, 16, 4, 5},  {32, 32, 2, 5},
+                                       {64, 32, 2, 6},  {32, 32, 3, 6},  {32, 32, 2, 7}};
+
+// Kernel choices (ConvTile::persist): 0 one tile per CTA; 1 persistent; 2 resident weights; 3 resident weights,
+// 4-row tiles; 4 as 3 with the row taps packed into N (and A tiles through the chunked view); 5 the same on
+// 8-row tiles; 6 and 7: row taps packed into N with streamed weights, 4- and 8-row tiles.
+static bool tile_resident(int p) { return p >= 2 && p <= 5; }
+static int tile_rows(int p) { return (p == 5 || p == 7) ? 8 : (p == 3 || p == 4 || p == 6) ? 4 : 2; }
+static bool tile_dyp(int p) { return p >= 4; }
 
 // Shared memory of a tile shape's launch for a layer with Cin input channels.
 int tile_smem(const ConvTile& t, int Cin)
 {
     const int KB = Cin / t.kc;
-    const int a = (t.persist == 3 ? 6 : 4) * 130 * t.kc * 2, b = 9 * t.kc * t.bn * 2;
-    if (t.persist >= 2) return t.stages * (((a + 1023) / 1024) * 1024) + 1024 + KB * b + 1024;
+    const int a = (tile_rows(t.persist) + 2) * (tile_dyp(t.persist) ? kChunkX : kHaloX) * t.kc * 2,
+              b = 9 * t.kc * t.bn * 2;
+    if (tile_resident(t.persist)) return t.stages * (((a + 1023) / 1024) * 1024) + 1024 + KB * b + 1024;
     return t.stages * (((a + b + 1023) / 1024) * 1024) + 1024 + 1024;
 }
 
@@ -954,7 +1069,7 @@ int conv_tile_candidates(int Cin, int Cout, ConvTile* out, int max)
     int k = 0;
     for (const ConvTile& t : kCompiledTiles)
         if (k < max && t.bn <= Cout && Cout % t.bn == 0 && Cin % t.kc == 0 &&
-            (t.persist < 2 || (t.bn == Cout && tile_smem(t, Cin) <= kMaxSmem)))
+            (t.persist < 2 || ((t.bn == Cout || !tile_resident(t.persist)) && tile_smem(t, Cin) <= kMaxSmem)))
             out[k++] = t;
     return k;
 }
@@ -966,8 +1081,8 @@ cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin,
 {
     const TileCfg c = resolve(tile, Cin, Cout);
     const size_t total = conv_packed_elems(Cin, Cout);
-    pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, Cin, c.bn, c.kc, d_packed,
-                                                                     total);
+    pack_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, Cin, c.bn, c.kc,
+                                                                     tile_dyp(c.persist) ? 1 : 0, d_packed, total);
     return cudaGetLastError();
 }
 
@@ -976,8 +1091,8 @@ cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, in
 {
     const TileCfg c = resolve(tile, Cout, ci_cnt);
     const size_t total = conv_packed_elems(Cout, ci_cnt);
-    pack_dgrad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin_real, ci_lo, ci_cnt, c.bn,
-                                                                           c.kc, d_packed, total);
+    pack_dgrad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(
+        d_w, Cout, Cin_real, ci_lo, ci_cnt, c.bn, c.kc, tile_dyp(c.persist) ? 1 : 0, d_packed, total);
     return cudaGetLastError();
 }
 
@@ -993,6 +1108,35 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
     const TileCfg c = resolve(a.tile, a.Cin, a.Cout);
     if (a.Cout % c.bn || a.Cin % c.kc) return cudaErrorInvalidValue;
     const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    if (c.persist == 7)
+        switch (key)
+        {
+        case 32322: return launch_persistent<32, 32, 2, false, 8, true>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
+    if (c.persist == 6)
+        switch (key)
+        {
+        case 64322: return launch_persistent<64, 32, 2, false, 4, true>(in, a, stream);
+        case 32323: return launch_persistent<32, 32, 3, false, 4, true>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
+    if (c.persist == 5)
+        switch (key)
+        {
+        case 32164: return launch_persistent<32, 16, 4, true, 8, true>(in, a, stream);
+        case 32322: return launch_persistent<32, 32, 2, true, 8, true>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
+    if (c.persist == 4)
+        switch (key)
+        {
+        case 32167: return launch_persistent<32, 16, 7, true, 4, true>(in, a, stream);
+        case 32323: return launch_persistent<32, 32, 3, true, 4, true>(in, a, stream);
+        case 64322: return launch_persistent<64, 32, 2, true, 4, true>(in, a, stream);
+        case 64323: return launch_persistent<64, 32, 3, true, 4, true>(in, a, stream);
+        default: return cudaErrorInvalidValue;
+        }
     if (c.persist == 3)
         switch (key)
         {

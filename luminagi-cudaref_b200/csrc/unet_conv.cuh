@@ -71,6 +71,7 @@ struct ConvArgs
     const __nv_bfloat16* skip;   // kEpiBwdUnpool: gradient arriving through the skip connection (2x res)
     int skip_C, skip_coff;
     ConvTile tile;               // {0, 0, 0}: default; must match the tile the weights were packed with
+    int a_chunked;               // set by the launcher: the A map is the 8-pixel-run view (W % 8 == 0)
 };
 
 // Bytes of packed weights for a layer (BF16).

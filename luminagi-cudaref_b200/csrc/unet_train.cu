@@ -504,7 +504,7 @@ int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
     for (int i = 0; i < 30; ++i)
     {
         const int p4 = tiles[4 * i + 3];
-        if (p4 < 0 || p4 > 3) return set_error(LG_ERR_INVALID, "conv %d: kernel choice %d is not 0..3", i, p4);
+        if (p4 < 0 || p4 > 7) return set_error(LG_ERR_INVALID, "conv %d: kernel choice %d is not 0..7", i, p4);
         ConvTile t{tiles[4 * i], tiles[4 * i + 1], tiles[4 * i + 2], p4};
         const bool back = i >= 14;
         const int cin = back ? kLayers[kDgrad[i - 14].layer].cout : kLayers[i].cin;

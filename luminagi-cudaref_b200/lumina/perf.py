@@ -28,7 +28,13 @@ RESIDENT_TILES = [(32, 16, 10, 2), (32, 32, 6, 2), (64, 32, 4, 2), (64, 32, 4, 2
 # The same layers with resident weights on 4-row tiles.
 ROWS4_TILES = [(32, 16, 8, 3), (32, 32, 4, 3), (64, 32, 3, 3), (64, 32, 3, 3)] + [(0, 0, 0, 1)] * 7 + \
               [(64, 32, 3, 3), (32, 32, 3, 3), (32, 32, 4, 3)]
-
+# Every layer with 32 or 64 output channels with the row taps packed into N:
+# 4-row tiles (choice 4 resident weights, 6 streamed for u2a) ...
+DYP4_TILES = [(32, 16, 7, 4), (32, 32, 3, 4), (64, 32, 3, 4), (64, 32, 2, 4)] + [(0, 0, 0, 1)] * 6 + \
+             [(64, 32, 2, 6), (64, 32, 2, 4), (32, 32, 3, 4), (32, 32, 3, 4)]
+# ... and 8-row tiles for the 32-channel layers (5 resident, 7 streamed for u1a).
+DYP8_TILES = [(32, 16, 4, 5), (32, 32, 2, 5), (64, 32, 3, 4), (64, 32, 2, 4)] + [(0, 0, 0, 1)] * 6 + \
+             [(64, 32, 2, 6), (64, 32, 2, 4), (32, 32, 2, 7), (32, 32, 2, 5)]
 
 def unet(a):
     import torch
@@ -43,6 +49,10 @@ def unet(a):
         net.set_tiles(RESIDENT_TILES + [(0, 0, 0, 1)] * 16)
     elif a.kernel == "rows4":
         net.set_tiles(ROWS4_TILES + [(0, 0, 0, 1)] * 16)
+    elif a.kernel == "dyp4":
+        net.set_tiles(DYP4_TILES + [(0, 0, 0, 1)] * 16)
+    elif a.kernel == "dyp8":
+        net.set_tiles(DYP8_TILES + [(0, 0, 0, 1)] * 16)
     elif a.kernel == "autotune":
         tiles = net.autotune(a.n, a.h, a.w)[:14]
     x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
@@ -196,7 +206,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["unet", "trace", "bvh", "batch", "membench"])
     ap.add_argument("--poses", type=int, default=50)
-    ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "rows4", "autotune"],
+    ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "rows4", "dyp4", "dyp8", "autotune"],
                     help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
                          "single-block layers, or autotuned tiles")
     ap.add_argument("--n", type=int, default=1)

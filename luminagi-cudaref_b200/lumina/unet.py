@@ -134,13 +134,14 @@ class UNet:
 
     def autotune(self, n: int, h: int, w: int, backward: bool = False):
         """Times every compiled conv tile shape and kernel per layer at n x h x w and
-        keeps the fastest (lg_unet_autotune); returns 30 (bn, kc, stages, persistent)."""
+        keeps the fastest (lg_unet_autotune); returns 30 (bn, kc, stages, kernel) quadruples, kernel 0..7 as
+        include/lumina.h lists them."""
         out = np.zeros(120, np.int32)
         check(lib().lg_unet_autotune(self._h, n, h, w, 1 if backward else 0, ptr(out)))
         return [tuple(int(v) for v in out[4 * i:4 * i + 4]) for i in range(30)]
 
     def set_tiles(self, tiles) -> None:
-        """30 (bn, kc, stages, persistent) choices as autotune returns them; (0, 0, 0, 0) = default."""
+        """30 (bn, kc, stages, kernel) choices as autotune returns them; (0, 0, 0, 0) = default."""
         arr = np.ascontiguousarray(np.asarray(tiles, np.int32).reshape(120))
         check(lib().lg_unet_set_tiles(self._h, ptr(arr)))
 

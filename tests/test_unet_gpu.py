@@ -339,7 +339,7 @@ def test_autotune_keeps_results():
     y0 = net.forward(x)
     tiles = net.autotune(n, h, w, backward=True)
     print("autotuned tiles (bn, kc, stages):", tiles)
-    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) and t[3] in (0, 1, 2, 3) for t in tiles)
+    assert len(tiles) == 30 and all(t[0] in (32, 64, 128) and t[1] in (16, 32) and 0 <= t[3] <= 7 for t in tiles)
     y1 = net.forward(x)
     assert np.array_equal(net.get_params(), flat)
     m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
@@ -393,19 +393,34 @@ ROWS4_TILES = [(32, 16, 8, 3), (32, 32, 4, 3), (64, 32, 3, 3), (64, 32, 3, 3)] +
               [(64, 32, 3, 3), (32, 32, 3, 3), (32, 32, 4, 3)]
 
 
+# Row taps packed into N (kernel choices 4: resident weights, 4-row tiles; 5:
+# resident, 8-row tiles; 6 and 7: streamed weights, 4- and 8-row tiles) on
+# every conv with 32 or 64 output channels, forward (d1a .. u1b) and
+# input-gradient (in the library's order of the 16 backward convs).
+DYP4_TILES = [(32, 16, 7, 4), (32, 32, 3, 4), (64, 32, 3, 4), (64, 32, 2, 4)] + [(0, 0, 0, 1)] * 6 + \
+             [(64, 32, 2, 6), (64, 32, 2, 4), (32, 32, 3, 4), (32, 32, 3, 4)]
+DYP4_BWD = [(32, 32, 3, 4), (64, 32, 3, 4), (32, 32, 3, 4), (64, 32, 2, 4), (0, 0, 0, 1), (64, 32, 2, 4)] + \
+           [(0, 0, 0, 1)] * 7 + [(64, 32, 2, 4), (32, 32, 3, 4), (32, 32, 3, 4)]
+DYP8_TILES = [(32, 16, 4, 5), (32, 32, 2, 5), (64, 32, 2, 6), (64, 32, 2, 6)] + [(0, 0, 0, 1)] * 6 + \
+             [(64, 32, 2, 6), (64, 32, 2, 6), (32, 32, 2, 7), (32, 32, 2, 5)]
+DYP8_BWD = [(32, 32, 2, 5), (64, 32, 2, 6), (32, 32, 2, 5), (64, 32, 2, 6), (0, 0, 0, 1), (64, 32, 2, 6)] + \
+           [(0, 0, 0, 1)] * 7 + [(64, 32, 2, 6), (32, 32, 2, 7), (32, 32, 2, 5)]
+
 def test_resident_weight_conv_kernel_is_bit_identical():
     """The persistent kernel with the weights resident in shared memory (one
-    copy per CTA instead of one per ring stage), with 2- and 4-row tiles, runs
-    the same MMAs in the same order for every output row: outputs, loss and
-    gradients are bit-identical to the plain persistent kernel's, at batch 1
-    and 2, with partial tiles at the right edge."""
+    copy per CTA instead of one per ring stage), with 2-, 4- and 8-row tiles,
+    and with the three row taps of a column tap packed into one MMA's N, runs
+    the same products in the same order for every output row: outputs, loss
+    and gradients are bit-identical to the plain persistent kernel's, at
+    batch 1 and 2, with partial tiles at the right edge."""
     flat = unet_ref.make_params(81)
     for n, h, w in ((1, 40, 264), (2, 64, 136), (1, 72, 136)):
         x = np.random.default_rng(10).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
         noisy, clean = _batch(n, h, w, 13)
         dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
         outs = []
-        for tiles in ([(0, 0, 0, 1)] * 30, RESIDENT_TILES + [(0, 0, 0, 1)] * 16, ROWS4_TILES + [(0, 0, 0, 1)] * 16):
+        for tiles in ([(0, 0, 0, 1)] * 30, RESIDENT_TILES + [(0, 0, 0, 1)] * 16, ROWS4_TILES + [(0, 0, 0, 1)] * 16,
+                      DYP4_TILES + DYP4_BWD, DYP8_TILES + DYP8_BWD):
             net = lumina.UNet()
             net.set_params(flat)
             net.set_tiles(tiles)
