@@ -115,7 +115,7 @@ ConvArgs base_args(lg_unet* u, int layer, int N, int H, int W)
 typedef __nv_bfloat16 bf;
 
 // Runs the network on a device FP32 NCHW input (N x in_ch x H x W) into d_y (N x 3 x H x W).
-int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
+int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y, bool keep_u1)
 {
     if (N <= 0 || H <= 0 || W <= 0 || (H % 8) || (W % 8))
         return set_error(LG_ERR_INVALID, "UNet input must be N>0 and H, W multiples of 8 (got %dx%d)", H, W);
@@ -174,16 +174,16 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     LG_TRY(run(10, u->cat2.p, H2, W2, kEpiStore, u->t6.p, 64, 0, nullptr, 0, 0));
     LG_TRY(up(11, u->t6.p, H2, W2, u->lo11, 64, u->cat1.p, 96));
     LG_TRY(run(12, u->cat1.p, H, W, kEpiStore, u->t7.p, 32, 0, nullptr, 0, 0));
-    LG_TRY(run(13, u->t7.p, H, W, kEpiTail, u->u1.p, 32, 0, nullptr, 0, 0));
+    LG_TRY(run(13, u->t7.p, H, W, kEpiTail, keep_u1 ? u->u1.p : nullptr, 32, 0, nullptr, 0, 0));
     return LG_OK;
 }
 }  // namespace
 
 namespace lg
 {
-int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y)
+int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y, bool keep_u1)
 {
-    return forward_device_impl(u, d_x, N, H, W, d_y);
+    return forward_device_impl(u, d_x, N, H, W, d_y, keep_u1);
 }
 int unet_pack_all(lg_unet* u) { return pack_all_impl(u); }
 }  // namespace lg
@@ -289,7 +289,7 @@ int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, fl
         cudaStreamWaitEvent(u->stream, ev, 0);
         cudaEventDestroy(ev);
     }
-    LG_TRY(forward_device_impl(u, d_x, n, h, w, d_y));
+    LG_TRY(forward_device_impl(u, d_x, n, h, w, d_y, false));
     if (stream)
     {
         cudaEvent_t ev;
@@ -329,7 +329,7 @@ int lg_unet_forward(lg_unet* u, const float* x, int n, int h, int w, float* y)
     LG_TRY(u->xin.ensure(in_bytes));
     LG_TRY(u->yout.ensure(bytes));
     LG_TRY_CUDA(cudaMemcpyAsync(u->xin.p, x, in_bytes, cudaMemcpyHostToDevice, u->stream));
-    LG_TRY(forward_device_impl(u, (const float*)u->xin.p, n, h, w, (float*)u->yout.p));
+    LG_TRY(forward_device_impl(u, (const float*)u->xin.p, n, h, w, (float*)u->yout.p, false));
     LG_TRY_CUDA(cudaMemcpyAsync(y, u->yout.p, bytes, cudaMemcpyDeviceToHost, u->stream));
     LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
     int err = 0;

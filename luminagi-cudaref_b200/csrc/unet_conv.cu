@@ -260,13 +260,28 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
     {
         // BN == Cout == 32: whole pixel in this thread.
         float o[kRows][3];
+        float res[kRows][3];  // the residual input, loaded before the accumulator so the two latencies overlap
+#pragma unroll
+        for (int r = 0; r < kRows; ++r)
+        {
+            const int y = y0 + r;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                res[r][k] = (r % nparts == part && xin && y < a.H)
+                                ? a.resid[(((size_t)n * a.resid_C + k) * a.H + y) * a.W + x]
+                                : 0.0f;
+        }
 #pragma unroll
         for (int r = 0; r < kRows; ++r)
         {
             if (r % nparts != part) continue;
             float v[32];
-            tc::tmem_ld16(lanebase + (uint32_t)(r * BN), v);
-            tc::tmem_ld16(lanebase + (uint32_t)(r * BN + 16), v + 16);
+            uint32_t q0[16], q1[16];
+            tc::tmem_ld16_issue(lanebase + (uint32_t)(r * BN), q0);
+            tc::tmem_ld16_issue(lanebase + (uint32_t)(r * BN + 16), q1);
+            tc::tmem_wait_ld();
+            tc::tmem_ld16_take(q0, v);
+            tc::tmem_ld16_take(q1, v + 16);
 #pragma unroll
             for (int c0 = 0; c0 < 32; c0 += 16)
             {
@@ -305,10 +320,9 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
 #pragma unroll
             for (int k = 0; k < 3; ++k)
             {
-                const size_t pi = (((size_t)n * a.resid_C + k) * a.H + y) * a.W + x;
                 const size_t po = (((size_t)n * 3 + k) * a.H + y) * a.W + x;
-                if (a.log_hdr) a.final_out[po] = expm1f(fmaxf(log1pf(a.resid[pi]) + o[r][k], 0.0f));
-                else a.final_out[po] = fminf(fmaxf(a.resid[pi] + o[r][k], 0.0f), 1.0f);
+                if (a.log_hdr) a.final_out[po] = expm1f(fmaxf(log1pf(res[r][k]) + o[r][k], 0.0f));
+                else a.final_out[po] = fminf(fmaxf(res[r][k] + o[r][k], 0.0f), 1.0f);
             }
         }
     }
@@ -318,8 +332,14 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
         for (int c0 = 16 * part; c0 < BN; c0 += 16 * nparts)
         {
             float v[kRows][16];
+            {
+                uint32_t q[kRows][16];
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) tc::tmem_ld16(lanebase + (uint32_t)(r * BN + c0), v[r]);
+                for (int r = 0; r < kRows; ++r) tc::tmem_ld16_issue(lanebase + (uint32_t)(r * BN + c0), q[r]);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int r = 0; r < kRows; ++r) tc::tmem_ld16_take(q[r], v[r]);
+            }
             const int cg = ct * BN + c0;  // layer channel of v[.][0]
             if (a.epilogue <= kEpiUpsample)
             {
@@ -374,14 +394,13 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
                     const int y = y0 + r;
                     if (!xin || y >= a.H) continue;
                     const uint4 lo = pack8(v[r]), hi = pack8(v[r] + 8);
+                    // pixels 2x and 2x+1 are 32 contiguous bytes of a channel plane: one store each
 #pragma unroll
                     for (int i = 0; i < 2; ++i)
-#pragma unroll
-                        for (int jx = 0; jx < 2; ++jx)
-                        {
-                            *blk(a.out, a.out_C, H2, W2, n, b0, 2 * y + i, 2 * x + jx) = lo;
-                            *blk(a.out, a.out_C, H2, W2, n, b0 + 1, 2 * y + i, 2 * x + jx) = hi;
-                        }
+                    {
+                        tc::st_global_v8(blk(a.out, a.out_C, H2, W2, n, b0, 2 * y + i, 2 * x), lo, lo);
+                        tc::st_global_v8(blk(a.out, a.out_C, H2, W2, n, b0 + 1, 2 * y + i, 2 * x), hi, hi);
+                    }
                 }
             }
         }

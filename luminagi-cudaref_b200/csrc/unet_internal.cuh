@@ -88,7 +88,9 @@ namespace lg
 // Real input channels of conv `i`: the first takes the network input (padded
 // to kLayers[0].cin = 16 channels in the blocked layout), the rest are fixed.
 inline int layer_cin_real(const lg_unet* u, int i) { return i == 0 ? u->in_ch : kLayers[i].cin_real; }
-int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y);
+// keep_u1: also store u1b's activation (the tail's input), which the
+// backward pass reads; inference leaves it out (96 MB at 1728x864).
+int unet_forward_device(lg_unet* u, const float* d_x, int N, int H, int W, float* d_y, bool keep_u1 = true);
 int unet_pack_all(lg_unet* u);
 }  // namespace lg
 

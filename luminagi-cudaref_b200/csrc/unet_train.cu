@@ -426,7 +426,7 @@ int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_
         for (int rep = 0; rep < 3; ++rep)
         {
             if (backward) LG_TRY(loss_and_grads(u, (const float*)x.p, (const float*)t.p, n, h, w, nullptr));
-            else LG_TRY(unet_forward_device(u, (const float*)x.p, n, h, w, (float*)y.p));
+            else LG_TRY(unet_forward_device(u, (const float*)x.p, n, h, w, (float*)y.p, false));
             LG_TRY_CUDA(cudaStreamSynchronize(u->stream));
             float ms = 0.0f;
             LG_TRY_CUDA(cudaEventElapsedTime(&ms, u->probe_ev0, u->probe_ev1));
