@@ -40,7 +40,7 @@ def unet(a):
     import torch
 
     from .unet import UNet
-    net = UNet()
+    net = UNet(variant=a.variant)
     net.set_params(np.random.default_rng(5).normal(0, 0.02, net.n_params).astype(np.float32))
     tiles = None
     if a.kernel == "single":
@@ -69,7 +69,7 @@ def unet(a):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
     flops = 2 * 162240 * a.n * a.h * a.w
-    return {"kernel": "unet_forward", "conv": a.kernel, "n": a.n, "h": a.h, "w": a.w, "ms": ms,
+    return {"kernel": "unet_forward", "variant": a.variant, "conv": a.kernel, "n": a.n, "h": a.h, "w": a.w, "ms": ms,
             "tflops": flops / ms / 1e9, "tiles": tiles}
 
 
@@ -210,6 +210,8 @@ def main(argv=None):
                     help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
                          "single-block layers, or autotuned tiles")
     ap.add_argument("--n", type=int, default=1)
+    ap.add_argument("--variant", default="ref", choices=["ref", "hdr"],
+                    help="unet: reference network, or the HDR one (ReLU, bilinear upsampling, log1p in / expm1 out)")
     ap.add_argument("--h", type=int, default=864)
     ap.add_argument("--w", type=int, default=1728)
     ap.add_argument("--spp", type=int, default=8)
