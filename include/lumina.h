@@ -343,6 +343,20 @@ int lg_unet_forward_device(lg_unet* u, const float* d_x, int n, int h, int w, fl
  * *loss_out (may be NULL) receives the loss before the update. */
 int lg_unet_train_step(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float lr,
                        float* loss_out);
+/* The same step queued behind the work already on `stream` (the caller's
+ * CUDA stream; the batch buffers may be written there just before), with
+ * later work on `stream` ordered after it, and without waiting for the
+ * device: a training loop runs ahead of the GPU instead of stopping twice
+ * per step.  n times the batch's mean L1 loss is added to *d_loss_sum (a
+ * device float, may be NULL), so summing over an epoch's batches gives the
+ * loss summed over its images.  A wait timeout inside the step is reported
+ * by the next call that waits for the device (lg_unet_sync,
+ * lg_unet_train_step, lg_unet_loss_grad). */
+int lg_unet_train_step_async(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float lr,
+                             float* d_loss_sum, void* stream);
+/* Waits for every step queued on the network; LG_ERR_DEVICE if one of its
+ * tensor-core kernels gave up a wait. */
+int lg_unet_sync(lg_unet* u);
 /* The loss and the gradient of every parameter (host, state_dict order)
  * without updating them. */
 int lg_unet_loss_grad(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float* grads,
@@ -409,7 +423,8 @@ int lg_accum_to_f32(const float* d_accum, int n, int h, int w, float inv_spp, fl
 int lg_f32_tonemap_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream);
 /* n_crops square crops (crop x crop, all 3 channels) of FP32 NCHW images
  * (n_images x 3 x h x w) at host-given (img_idx, ys, xs) into d_out
- * (n_crops x 3 x crop x crop). */
+ * (n_crops x 3 x crop x crop).  With stream NULL the call returns when the
+ * crops are written; with a stream it only queues the copy there. */
 int lg_gather_crops(const float* d_images, int n_images, int h, int w, const int32_t* img_idx, const int32_t* ys,
                     const int32_t* xs, int n_crops, int crop, float* d_out, void* stream);
 

@@ -156,7 +156,7 @@ int lg_gather_crops(const float* d_images, int n_images, int h, int w, const int
     }
     cudaFreeAsync(d_cr, st);
     if (e != cudaSuccess) return lg::set_error(LG_ERR_CUDA, "gather_crops: %s", cudaGetErrorString(e));
-    LG_TRY_CUDA(cudaStreamSynchronize(st));
+    if (!stream) LG_TRY_CUDA(cudaStreamSynchronize(st));
     return LG_OK;
 }
 

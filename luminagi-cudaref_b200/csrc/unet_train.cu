@@ -359,6 +359,12 @@ int adam_step(lg_unet* u, float lr)
     return LG_OK;
 }
 
+// *dst += *sum * scale (one thread): the batch loss into a caller's device accumulator.
+__global__ void loss_add_kernel(const float* __restrict__ sum, float scale, float* __restrict__ dst)
+{
+    *dst += *sum * scale;
+}
+
 int check_err(lg_unet* u)
 {
     int err = 0;
@@ -381,6 +387,36 @@ int lg_unet_train_step(lg_unet* u, const float* d_x, const float* d_target, int 
     LG_TRY(check_err(u));
     if (loss_out) *loss_out = loss;
     return LG_OK;
+}
+
+int lg_unet_train_step_async(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float lr,
+                             float* d_loss_sum, void* stream)
+{
+    if (!u || !d_x || !d_target) return set_error(LG_ERR_INVALID, "NULL argument");
+    cudaEvent_t ev;
+    LG_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaEventRecord(ev, (cudaStream_t)stream);
+    cudaStreamWaitEvent(u->stream, ev, 0);
+    int rc = loss_and_grads(u, d_x, d_target, n, h, w, nullptr);
+    if (rc == LG_OK && d_loss_sum)
+    {
+        // u->loss holds the summed |difference| of this batch; the mean times n
+        const float inv_numel = 1.0f / (float)((long long)n * h * w * 3);  // as loss_and_grads scales it
+        loss_add_kernel<<<1, 1, 0, u->stream>>>((const float*)u->loss.p, inv_numel * (float)n, d_loss_sum);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = set_error(LG_ERR_CUDA, "loss: %s", cudaGetErrorString(e));
+    }
+    if (rc == LG_OK) rc = adam_step(u, lr);
+    cudaEventRecord(ev, u->stream);
+    cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+    cudaEventDestroy(ev);
+    return rc;
+}
+
+int lg_unet_sync(lg_unet* u)
+{
+    if (!u) return set_error(LG_ERR_INVALID, "NULL argument");
+    return check_err(u);
 }
 
 int lg_unet_loss_grad(lg_unet* u, const float* d_x, const float* d_target, int n, int h, int w, float* grads_host,

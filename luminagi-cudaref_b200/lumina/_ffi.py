@@ -133,6 +133,8 @@ SIGNATURES = {
     "lg_unet_forward": (_I, [_P, _P, _I, _I, _I, _P]),
     "lg_unet_forward_device": (_I, [_P, _P, _I, _I, _I, _P, _P]),
     "lg_unet_train_step": (_I, [_P, _P, _P, _I, _I, _I, C.c_float, C.POINTER(C.c_float)]),
+    "lg_unet_train_step_async": (_I, [_P, _P, _P, _I, _I, _I, C.c_float, _P, _P]),
+    "lg_unet_sync": (_I, [_P]),
     "lg_unet_loss_grad": (_I, [_P, _P, _P, _I, _I, _I, _P, C.POINTER(C.c_float)]),
     "lg_unet_adam_apply": (_I, [_P, C.c_float]),
     "lg_unet_adam_reset": (_I, [_P]),

@@ -95,41 +95,62 @@ def make_dataset(r: Renderer, cams, noisy_spp: int, clean_spp: int, bounces: int
     return noisy, clean
 
 
-def gather(images, idx, ys, xs, crop):
+def gather(images, idx, ys, xs, crop, out=None, stream: int = 0):
     """Crops (all channels) of FP32 NCHW images; C a multiple of 3: a C-channel
-    image is gathered as C/3 consecutive 3-channel images."""
+    image is gathered as C/3 consecutive 3-channel images.  With a stream
+    handle the copy is only queued there."""
     torch = _torch()
     n = len(idx)
     I, Cc, Hh, Ww = images.shape
     g = Cc // 3
-    out = torch.empty((n, Cc, crop, crop), device="cuda")
+    if out is None:
+        out = torch.empty((n, Cc, crop, crop), device="cuda")
     a = lambda v: np.ascontiguousarray(v, np.int32)
     ii = a((np.asarray(idx, np.int64)[:, None] * g + np.arange(g)[None, :]).reshape(-1))
     yy, xx = a(np.repeat(ys, g)), a(np.repeat(xs, g))
     _ffi.check(_ffi.lib().lg_gather_crops(C.c_void_p(images.data_ptr()), I * g, Hh, Ww, _ffi.ptr(ii), _ffi.ptr(yy),
-                                          _ffi.ptr(xx), n * g, crop, C.c_void_p(out.data_ptr()), None))
+                                          _ffi.ptr(xx), n * g, crop, C.c_void_p(out.data_ptr()),
+                                          C.c_void_p(stream) if stream else None))
     return out
 
 
 def train(net: UNet, noisy, clean, train_idx, val_idx, epochs=120, batch=16, crop=128, lr=1e-4, crops_per_image=1,
           seed=42, log=print):
-    """ml/train.py:184-217: returns (best params, history)."""
+    """ml/train.py:184-217: returns (best params, history).
+
+    The batches of an epoch are queued without waiting for the GPU: crops are
+    gathered into one pair of buffers on a stream of this loop, and each
+    step (lg_unet_train_step_async) is ordered on that stream, so the next
+    gather waits for the step that reads the buffers.  The training loss is
+    summed on the device and read once per epoch; validation (synchronous)
+    follows, as in the reference loop."""
+    torch = _torch()
     rng = np.random.RandomState(seed)
     H, W = noisy.shape[2], noisy.shape[3]
     best, best_val, hist = None, float("inf"), []
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        xbuf = torch.empty((batch, noisy.shape[1], crop, crop), device="cuda")
+        tbuf = torch.empty((batch, clean.shape[1], crop, crop), device="cuda")
+        loss_sum = torch.zeros(1, device="cuda")
     for ep in range(epochs):
         order = np.repeat(np.asarray(train_idx), crops_per_image)
         rng.shuffle(order)
         ys = rng.randint(0, H - crop + 1, len(order))
         xs = rng.randint(0, W - crop + 1, len(order))
-        tl, seen = 0.0, 0
-        for b0 in range(0, len(order), batch):
-            sl = slice(b0, b0 + batch)
-            xb = gather(noisy, order[sl], ys[sl], xs[sl], crop)
-            tb = gather(clean, order[sl], ys[sl], xs[sl], crop)
-            n = xb.shape[0]
-            tl += net.train_step(xb.data_ptr(), tb.data_ptr(), n, crop, crop, lr) * n
-            seen += n
+        seen = 0
+        with torch.cuda.stream(stream):
+            loss_sum.zero_()
+            for b0 in range(0, len(order), batch):
+                sl = slice(b0, b0 + batch)
+                n = len(order[sl])
+                xb = gather(noisy, order[sl], ys[sl], xs[sl], crop, xbuf[:n], sh)
+                tb = gather(clean, order[sl], ys[sl], xs[sl], crop, tbuf[:n], sh)
+                net.train_step_async(xb.data_ptr(), tb.data_ptr(), n, crop, crop, lr, loss_sum.data_ptr(), sh)
+                seen += n
+            tl = float(loss_sum.item())
+        net.sync()
         vy = rng.randint(0, H - crop + 1, len(val_idx))
         vx = rng.randint(0, W - crop + 1, len(val_idx))
         xv = gather(noisy, val_idx, vy, vx, crop)

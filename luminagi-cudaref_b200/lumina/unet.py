@@ -118,6 +118,18 @@ class UNet:
         check(lib().lg_unet_train_step(self._h, C.c_void_p(d_x), C.c_void_p(d_target), n, h, w, lr, C.byref(loss)))
         return float(loss.value)
 
+    def train_step_async(self, d_x: int, d_target: int, n: int, h: int, w: int, lr: float, d_loss_sum: int = 0,
+                         stream: int = 0) -> None:
+        """The same step queued on `stream` (a CUDA stream handle) without waiting for the device; n x the
+        batch's mean loss is added to the device float at d_loss_sum (0: none).  See sync()."""
+        check(lib().lg_unet_train_step_async(self._h, C.c_void_p(d_x), C.c_void_p(d_target), n, h, w, lr,
+                                             C.c_void_p(d_loss_sum) if d_loss_sum else None,
+                                             C.c_void_p(stream) if stream else None))
+
+    def sync(self) -> None:
+        """Waits for the queued steps; raises if a tensor-core kernel gave up a wait."""
+        check(lib().lg_unet_sync(self._h))
+
     def loss_grad(self, d_x: int, d_target: int, n: int, h: int, w: int):
         """(loss, flat FP32 gradient) without updating the parameters."""
         g = np.zeros(self.n_params, np.float32)

@@ -434,6 +434,35 @@ def test_resident_weight_conv_kernel_is_bit_identical():
             assert np.array_equal(outs[0][2], o[2])
 
 
+def test_async_train_step_matches_sync():
+    """lg_unet_train_step_async queues the same step on the caller's stream
+    without waiting: after lg_unet_sync the parameters are bit-identical to
+    those of the synchronous steps, and the device loss sum is the sum of n x
+    the losses those steps returned."""
+    flat = unet_ref.make_params(83)
+    n, h, w = 3, 32, 48
+    batches = [_batch(n, h, w, 20 + k) for k in range(3)]
+    dev = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in batches]
+    net = lumina.UNet()
+    net.set_params(flat)
+    losses = [net.train_step(dx.data_ptr(), dt.data_ptr(), n, h, w, 1e-3) for dx, dt in dev]
+    p_sync = net.get_params()
+    net.close()
+    net = lumina.UNet()
+    net.set_params(flat)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        loss_sum = torch.zeros(1, device="cuda")
+        for dx, dt in dev:
+            net.train_step_async(dx.data_ptr(), dt.data_ptr(), n, h, w, 1e-3, loss_sum.data_ptr(), s.cuda_stream)
+        total = float(loss_sum.item())
+    net.sync()
+    p_async = net.get_params()
+    net.close()
+    assert np.array_equal(p_sync, p_async)
+    assert abs(total - n * sum(losses)) <= 1e-5 * abs(total)
+
+
 def test_training_is_bit_reproducible():
     """Weight and bias gradients are reduced from per-CTA partials in a fixed
     order (no floating-point atomics), so the same batch gives the same
