@@ -54,6 +54,8 @@ int ensure_acts(lg_unet* u, int N, int H, int W)
     if (u->aN == N && u->aH == H && u->aW == W) return LG_OK;
     const size_t px = (size_t)N * H * W, b2 = sizeof(__nv_bfloat16);
     LG_TRY(u->x0.ensure(px * 16 * b2));
+    // channels past in_ch stay zero: the input conversion writes only the blocks that hold input channels
+    LG_TRY_CUDA(cudaMemsetAsync(u->x0.p, 0, px * 16 * b2, u->stream));
     LG_TRY(u->t1.ensure(px * 32 * b2));
     LG_TRY(u->cat1.ensure(px * 96 * b2));
     LG_TRY(u->p1.ensure(px / 4 * 32 * b2));
@@ -123,7 +125,7 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     LG_TRY(ensure_acts(u, N, H, W));
     cudaStream_t st = u->stream;
     LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), st));
-    LG_TRY_CUDA(to_blocked_bf16(d_x, N, u->in_ch, H, W, (bf*)u->x0.p, 16, st, u->log_hdr));
+    LG_TRY_CUDA(to_blocked_bf16(d_x, N, u->in_ch, H, W, (bf*)u->x0.p, 16, st, u->log_hdr, true));
     const int H2 = H / 2, W2 = W / 2, H4 = H / 4, W4 = W / 4, H8 = H / 8, W8 = W / 8;
     auto run = [&](int layer, const void* in, int h, int w, int epi, void* out, int out_c, int out_coff, void* out2,
                    int out2_c, int out2_coff) -> int {

@@ -1018,22 +1018,28 @@ __global__ void pack_dgrad_kernel(const float* __restrict__ w, int Cout, int Cin
     out[i] = __float2bfloat16_rn(v);
 }
 
+// One thread per (image, 8-channel block, pixel) of the first nb blocks:
+// reads the block's channels from their NCHW planes (consecutive threads,
+// consecutive pixels of a plane) and writes the pixel's 16 bytes.
 __global__ void to_blocked_kernel(const float* __restrict__ x, int N, int C, int H, int W,
-                                  __nv_bfloat16* __restrict__ out, int Cpad, int log1p_in)
+                                  __nv_bfloat16* __restrict__ out, int Cpad, int nb, int log1p_in)
 {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over N * Cpad * H * W
-    const size_t total = (size_t)N * Cpad * H * W;
-    if (i >= total) return;
-    size_t r = i;
-    const int e = (int)(r % 8); r /= 8;
-    const int xx = (int)(r % W); r /= W;
-    const int y = (int)(r % H); r /= H;
-    const int b = (int)(r % (Cpad / 8)); r /= (Cpad / 8);
-    const int n = (int)r;
-    const int c = b * 8 + e;
-    float v = c < C ? x[(((size_t)n * C + c) * H + y) * W + xx] : 0.0f;
-    if (log1p_in) v = log1pf(v);
-    out[i] = __float2bfloat16_rn(v);
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over N * nb * H * W
+    const size_t HW = (size_t)H * W;
+    if (i >= (size_t)N * nb * HW) return;
+    const size_t p = i % HW;
+    const int b = (int)((i / HW) % nb);
+    const int n = (int)(i / (HW * nb));
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e)
+    {
+        const int c = b * 8 + e;
+        float t = c < C ? x[((size_t)n * C + c) * HW + p] : 0.0f;
+        if (log1p_in) t = log1pf(t);
+        v[e] = t;
+    }
+    reinterpret_cast<uint4*>(out)[((size_t)n * (Cpad / 8) + b) * HW + p] = pack8(v);
 }
 
 __global__ void from_blocked_kernel(const __nv_bfloat16* __restrict__ in, int N, int C, int H, int W,
@@ -1204,10 +1210,12 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
 }
 
 cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,
-                            cudaStream_t stream, bool log1p_in)
+                            cudaStream_t stream, bool log1p_in, bool skip_zero_blocks)
 {
-    const size_t total = (size_t)N * Cpad * H * W;
-    to_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(x, N, C, H, W, out, Cpad, log1p_in ? 1 : 0);
+    const int nb = skip_zero_blocks ? (C + 7) / 8 : Cpad / 8;
+    const size_t total = (size_t)N * nb * H * W;
+    to_blocked_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(x, N, C, H, W, out, Cpad, nb,
+                                                                         log1p_in ? 1 : 0);
     return cudaGetLastError();
 }
 

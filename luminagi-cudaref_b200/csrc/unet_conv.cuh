@@ -99,8 +99,10 @@ cudaError_t launch_wait_probe(int* err, unsigned long long limit_ns, cudaStream_
 
 // FP32 NCHW (C channels) -> blocked BF16 with Cpad channels (zero padded);
 // log1p_in applies log1p to every value first (the HDR variant's input).
+// skip_zero_blocks: leave the 8-channel blocks past channel C untouched (the
+// caller keeps them zero).
 cudaError_t to_blocked_bf16(const float* x, int N, int C, int H, int W, __nv_bfloat16* out, int Cpad,
-                            cudaStream_t stream, bool log1p_in = false);
+                            cudaStream_t stream, bool log1p_in = false, bool skip_zero_blocks = false);
 
 // Bilinear 2x upsampling (F.interpolate(scale_factor=2, mode="bilinear",
 // align_corners=False)) of a blocked BF16 tensor N x C x h x w into channels
