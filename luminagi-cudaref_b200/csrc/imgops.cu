@@ -18,55 +18,57 @@
 
 namespace
 {
-__global__ void rgb8_to_f32_kernel(const uint8_t* __restrict__ in, long long n, int H, int W,
-                                   float* __restrict__ out)
+// The four conversions below run one thread per pixel, grid (ceil(H*W / 256),
+// n): the pixel's three HWC values and its three NCHW plane entries, with no
+// 64-bit divisions in the index math.
+__global__ void rgb8_to_f32_kernel(const uint8_t* __restrict__ in, long long HW, float* __restrict__ out)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over n*3*H*W (NCHW)
-    const long long HW = (long long)H * W;
-    if (i >= n * 3 * HW) return;
-    const long long img = i / (3 * HW), r = i % (3 * HW);
-    const int c = (int)(r / HW);
-    const long long p = r % HW;
-    out[i] = (float)in[(img * HW + p) * 3 + c] / 255.0f;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= HW) return;
+    const long long img = blockIdx.y;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[(img * 3 + c) * HW + p] = (float)in[(img * HW + p) * 3 + c] / 255.0f;
 }
 
-__global__ void f32_to_rgb8_kernel(const float* __restrict__ in, long long n, int H, int W, uint8_t* __restrict__ out)
+__global__ void f32_to_rgb8_kernel(const float* __restrict__ in, long long HW, uint8_t* __restrict__ out)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over n*H*W*3 (HWC)
-    const long long HW = (long long)H * W;
-    if (i >= n * HW * 3) return;
-    const int c = (int)(i % 3);
-    const long long px = i / 3;
-    const long long img = px / HW, p = px % HW;
-    const float v = fminf(fmaxf(in[(img * 3 + c) * HW + p], 0.0f), 1.0f);
-    out[i] = (uint8_t)(v * 255.0f + 0.5f);
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= HW) return;
+    const long long img = blockIdx.y;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+        const float v = fminf(fmaxf(in[(img * 3 + c) * HW + p], 0.0f), 1.0f);
+        out[(img * HW + p) * 3 + c] = (uint8_t)(v * 255.0f + 0.5f);
+    }
 }
 
 // accum (HWC sums over spp) * inv_spp -> FP32 NCHW linear radiance.
-__global__ void accum_to_f32_kernel(const float* __restrict__ acc, long long n, int H, int W, float inv_spp,
-                                    float* __restrict__ out)
+__global__ void accum_to_f32_kernel(const float* __restrict__ acc, long long HW, float inv_spp, float* __restrict__ out)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over n*3*H*W (NCHW)
-    const long long HW = (long long)H * W;
-    if (i >= n * 3 * HW) return;
-    const long long img = i / (3 * HW), r = i % (3 * HW);
-    const int c = (int)(r / HW);
-    const long long p = r % HW;
-    out[i] = acc[(img * HW + p) * 3 + c] * inv_spp;
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= HW) return;
+    const long long img = blockIdx.y;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[(img * 3 + c) * HW + p] = acc[(img * HW + p) * 3 + c] * inv_spp;
 }
 
 // FP32 NCHW linear radiance -> HWC u8 with tonemap_kernel's formula.
-__global__ void f32_tonemap_kernel(const float* __restrict__ in, long long n, int H, int W, uint8_t* __restrict__ out)
+__global__ void f32_tonemap_kernel(const float* __restrict__ in, long long HW, uint8_t* __restrict__ out)
 {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over n*H*W*3 (HWC)
-    const long long HW = (long long)H * W;
-    if (i >= n * HW * 3) return;
-    const int c = (int)(i % 3);
-    const long long px = i / 3;
-    const long long img = px / HW, p = px % HW;
-    const float v = sqrtf(fmaxf(0.0f, fminf(in[(img * 3 + c) * HW + p], 1.0f)));
-    out[i] = (uint8_t)(v * 255.0f);
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= HW) return;
+    const long long img = blockIdx.y;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+    {
+        const float v = sqrtf(fmaxf(0.0f, fminf(in[(img * 3 + c) * HW + p], 1.0f)));
+        out[(img * HW + p) * 3 + c] = (uint8_t)(v * 255.0f);
+    }
 }
+
+// Grid of the per-pixel conversions.
+dim3 px_grid(long long HW, int n) { return dim3((unsigned)((HW + 255) / 256), (unsigned)n); }
 
 struct Crop
 {
@@ -93,9 +95,9 @@ extern "C" {
 int lg_rgb8_to_f32(const uint8_t* d_rgb, int n, int h, int w, float* d_out, void* stream)
 {
     if (!d_rgb || !d_out || n < 0 || h <= 0 || w <= 0) return lg::set_error(LG_ERR_INVALID, "bad argument");
-    const long long total = (long long)n * 3 * h * w;
-    if (total == 0) return LG_OK;
-    rgb8_to_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_rgb, n, h, w, d_out);
+    if (n == 0) return LG_OK;
+    if (n > 65535) return lg::set_error(LG_ERR_INVALID, "at most 65535 images per call");
+    rgb8_to_f32_kernel<<<px_grid((long long)h * w, n), 256, 0, (cudaStream_t)stream>>>(d_rgb, (long long)h * w, d_out);
     LG_TRY_CUDA(cudaGetLastError());
     return LG_OK;
 }
@@ -103,9 +105,9 @@ int lg_rgb8_to_f32(const uint8_t* d_rgb, int n, int h, int w, float* d_out, void
 int lg_f32_to_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream)
 {
     if (!d_rgb || !d_in || n < 0 || h <= 0 || w <= 0) return lg::set_error(LG_ERR_INVALID, "bad argument");
-    const long long total = (long long)n * 3 * h * w;
-    if (total == 0) return LG_OK;
-    f32_to_rgb8_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_in, n, h, w, d_rgb);
+    if (n == 0) return LG_OK;
+    if (n > 65535) return lg::set_error(LG_ERR_INVALID, "at most 65535 images per call");
+    f32_to_rgb8_kernel<<<px_grid((long long)h * w, n), 256, 0, (cudaStream_t)stream>>>(d_in, (long long)h * w, d_rgb);
     LG_TRY_CUDA(cudaGetLastError());
     return LG_OK;
 }
@@ -113,10 +115,10 @@ int lg_f32_to_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void*
 int lg_accum_to_f32(const float* d_accum, int n, int h, int w, float inv_spp, float* d_out, void* stream)
 {
     if (!d_accum || !d_out || n < 0 || h <= 0 || w <= 0) return lg::set_error(LG_ERR_INVALID, "bad argument");
-    const long long total = (long long)n * 3 * h * w;
-    if (total == 0) return LG_OK;
-    accum_to_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_accum, n, h, w, inv_spp,
-                                                                                           d_out);
+    if (n == 0) return LG_OK;
+    if (n > 65535) return lg::set_error(LG_ERR_INVALID, "at most 65535 images per call");
+    accum_to_f32_kernel<<<px_grid((long long)h * w, n), 256, 0, (cudaStream_t)stream>>>(d_accum, (long long)h * w,
+                                                                                        inv_spp, d_out);
     LG_TRY_CUDA(cudaGetLastError());
     return LG_OK;
 }
@@ -124,9 +126,9 @@ int lg_accum_to_f32(const float* d_accum, int n, int h, int w, float inv_spp, fl
 int lg_f32_tonemap_rgb8(const float* d_in, int n, int h, int w, uint8_t* d_rgb, void* stream)
 {
     if (!d_rgb || !d_in || n < 0 || h <= 0 || w <= 0) return lg::set_error(LG_ERR_INVALID, "bad argument");
-    const long long total = (long long)n * 3 * h * w;
-    if (total == 0) return LG_OK;
-    f32_tonemap_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(d_in, n, h, w, d_rgb);
+    if (n == 0) return LG_OK;
+    if (n > 65535) return lg::set_error(LG_ERR_INVALID, "at most 65535 images per call");
+    f32_tonemap_kernel<<<px_grid((long long)h * w, n), 256, 0, (cudaStream_t)stream>>>(d_in, (long long)h * w, d_rgb);
     LG_TRY_CUDA(cudaGetLastError());
     return LG_OK;
 }

@@ -51,6 +51,14 @@ __device__ __forceinline__ const uint4* at(const __nv_bfloat16* base, int C, int
     return reinterpret_cast<const uint4*>(base + ((((size_t)n * (C >> 3) + b) * H + y) * W + x) * 8);
 }
 
+// 32 bytes to global memory in one store (address 32-byte aligned).
+__device__ __forceinline__ void tc_st_v8(void* p, uint4 a, uint4 b)
+{
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
+                 "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                 : "memory");
+}
+
 // Source rows (i0, i1) and the weight of i1 for output index d of an axis of size n.
 __device__ __forceinline__ void src_axis(int d, int n, int& i0, int& i1, float& l1)
 {
@@ -74,29 +82,44 @@ __device__ __forceinline__ void src_axis(int d, int n, int& i0, int& i1, float& 
     }
 }
 
-__global__ void up2_kernel(const __nv_bfloat16* __restrict__ in, int N, int C, int h, int w,
-                           __nv_bfloat16* __restrict__ out, int out_C, int coff)
+// Grid (ceil(w / 128), 2h, N * C/8), 128 threads: a thread writes the output
+// pixel pair (2i, 2i+1) of row Y, 8 channels, from the source columns
+// i-1, i, i+1 of the two source rows (6 loads for 2 outputs, one 32-byte
+// store); 32-bit index math from the grid, no divisions.
+__global__ void __launch_bounds__(128) up2_kernel(const __nv_bfloat16* __restrict__ in, int N, int C, int h, int w,
+                                                  __nv_bfloat16* __restrict__ out, int out_C, int coff)
 {
+    const int i = blockIdx.x * 128 + threadIdx.x;
+    if (i >= w) return;
     const int H = 2 * h, W = 2 * w, CB = C >> 3;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over N * CB * H * W
-    if (i >= (long long)N * CB * H * W) return;
-    const int X = (int)(i % W);
-    const int Y = (int)((i / W) % H);
-    const int b = (int)((i / ((long long)W * H)) % CB);
-    const int n = (int)(i / ((long long)W * H * CB));
-    int y0, y1, x0, x1;
-    float ly, lx;
+    const int Y = blockIdx.y;
+    const int n = blockIdx.z / CB, b = blockIdx.z % CB;
+    int y0, y1;
+    float ly;
     src_axis(Y, h, y0, y1, ly);
-    src_axis(X, w, x0, x1, lx);
-    float a[8], bb[8], c[8], d[8], o[8];
-    unpack(__ldg(at(in, C, h, w, n, b, y0, x0)), a);
-    unpack(__ldg(at(in, C, h, w, n, b, y0, x1)), bb);
-    unpack(__ldg(at(in, C, h, w, n, b, y1, x0)), c);
-    unpack(__ldg(at(in, C, h, w, n, b, y1, x1)), d);
-    const float hy = 1.0f - ly, hx = 1.0f - lx;
+    const float hy = 1.0f - ly;
+    // output 2i reads columns (i-1, i) with weight 0.75 on i (column 0 alone at i = 0);
+    // output 2i+1 reads (i, i+1) with weight 0.25 on i+1 (column w-1 alone at the end)
+    int xa0, xa1, xb0, xb1;
+    float la, lb;
+    src_axis(2 * i, w, xa0, xa1, la);
+    src_axis(2 * i + 1, w, xb0, xb1, lb);
+    const float ha = 1.0f - la, hb = 1.0f - lb;
+    float p0[8], q0[8], p1[8], q1[8], r0[8], r1[8], o[8], o2[8];
+    unpack(__ldg(at(in, C, h, w, n, b, y0, xa0)), p0);  // row y0: columns xa0 (= i-1 or 0), i, xb1 (= i+1 or w-1)
+    unpack(__ldg(at(in, C, h, w, n, b, y0, xa1)), q0);
+    unpack(__ldg(at(in, C, h, w, n, b, y0, xb1)), r0);
+    unpack(__ldg(at(in, C, h, w, n, b, y1, xa0)), p1);
+    unpack(__ldg(at(in, C, h, w, n, b, y1, xa1)), q1);
+    unpack(__ldg(at(in, C, h, w, n, b, y1, xb1)), r1);
+    // xa1 == xb0 == i: the pair's shared column
 #pragma unroll
-    for (int k = 0; k < 8; ++k) o[k] = hy * (hx * a[k] + lx * bb[k]) + ly * (hx * c[k] + lx * d[k]);
-    *reinterpret_cast<uint4*>(out + ((((size_t)n * (out_C >> 3) + (coff >> 3) + b) * H + Y) * W + X) * 8) = pack(o);
+    for (int k = 0; k < 8; ++k)
+    {
+        o[k] = hy * (ha * p0[k] + la * q0[k]) + ly * (ha * p1[k] + la * q1[k]);
+        o2[k] = hy * (hb * q0[k] + lb * r0[k]) + ly * (hb * q1[k] + lb * r1[k]);
+    }
+    tc_st_v8(out + ((((size_t)n * (out_C >> 3) + (coff >> 3) + b) * H + Y) * W + 2 * i) * 8, pack(o), pack(o2));
 }
 
 // Outputs of one axis feeding input i (size n): up to 4 indices and weights.
@@ -112,17 +135,17 @@ __device__ __forceinline__ int taps_axis(int i, int n, int* idx, float* wt)
     return k;
 }
 
-__global__ void up2_adjoint_kernel(const __nv_bfloat16* __restrict__ g_hi, int N, int C, int h, int w,
-                                   const __nv_bfloat16* __restrict__ ref, float slope,
-                                   __nv_bfloat16* __restrict__ g_lo)
+// Grid (ceil(w / 128), h, N * C/8), 128 threads: one low-resolution pixel
+// (8 channels) per thread.
+__global__ void __launch_bounds__(128) up2_adjoint_kernel(const __nv_bfloat16* __restrict__ g_hi, int N, int C, int h,
+                                                          int w, const __nv_bfloat16* __restrict__ ref, float slope,
+                                                          __nv_bfloat16* __restrict__ g_lo)
 {
+    const int x = blockIdx.x * 128 + threadIdx.x;
+    if (x >= w) return;
     const int H = 2 * h, W = 2 * w, CB = C >> 3;
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // over N * CB * h * w
-    if (i >= (long long)N * CB * h * w) return;
-    const int x = (int)(i % w);
-    const int y = (int)((i / w) % h);
-    const int b = (int)((i / ((long long)w * h)) % CB);
-    const int n = (int)(i / ((long long)w * h * CB));
+    const int y = blockIdx.y;
+    const int n = blockIdx.z / CB, b = blockIdx.z % CB;
     int iy[4], ix[4];
     float wy[4], wx[4];
     const int ny = taps_axis(y, h, iy, wy), nx = taps_axis(x, w, ix, wx);
@@ -148,8 +171,9 @@ cudaError_t bilinear_up2(const __nv_bfloat16* in, int N, int C, int h, int w, __
                          int coff, cudaStream_t stream)
 {
     if (N <= 0 || C <= 0 || h <= 0 || w <= 0 || (C % 8) || (coff % 8) || coff + C > out_C) return cudaErrorInvalidValue;
-    const long long total = (long long)N * (C >> 3) * (2 * h) * (2 * w);
-    up2_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(in, N, C, h, w, out, out_C, coff);
+    if (2 * h > 65535 || (long long)N * (C >> 3) > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((unsigned)((w + 127) / 128), (unsigned)(2 * h), (unsigned)(N * (C >> 3)));
+    up2_kernel<<<grid, 128, 0, stream>>>(in, N, C, h, w, out, out_C, coff);
     return cudaGetLastError();
 }
 
@@ -157,8 +181,9 @@ cudaError_t bilinear_up2_adjoint(const __nv_bfloat16* g_hi, int N, int C, int h,
                                  float slope, __nv_bfloat16* g_lo, cudaStream_t stream)
 {
     if (N <= 0 || C <= 0 || h <= 0 || w <= 0 || (C % 8)) return cudaErrorInvalidValue;
-    const long long total = (long long)N * (C >> 3) * h * w;
-    up2_adjoint_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(g_hi, N, C, h, w, ref, slope, g_lo);
+    if (h > 65535 || (long long)N * (C >> 3) > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((unsigned)((w + 127) / 128), (unsigned)h, (unsigned)(N * (C >> 3)));
+    up2_adjoint_kernel<<<grid, 128, 0, stream>>>(g_hi, N, C, h, w, ref, slope, g_lo);
     return cudaGetLastError();
 }
 }  // namespace lg
