@@ -10,8 +10,16 @@
 // row ky and all three kx taps: the X box is 130 pixels wide and tap kx reads
 // it 16*kx bytes further on, accumulating into three TMEM tiles.  Each CTA
 // sums a chunk of image rows and stores its partial dW in a scratch slice of
-// its own; a second pass adds the chunks' partials to dW in chunk order, so
+// its own; a second pass adds the chunks' partials to dW in a fixed order, so
 // gradients (and training) are bit-reproducible.
+// A K-step is 128 pixels: one 128-pixel row segment for layers wider than 64
+// pixels; for narrower ones (the deep levels of training crops) R rows of Wp
+// pixels (Wp = W rounded up to 16, R * Wp <= 128) with one MMA per 16 pixels
+// of a row, so the step is not mostly zero padding.
+// Layers with 32 output channels (KYP) fill M with the three kernel rows
+// instead of zeros: the A tile stacks dZ rows y+1, y, y-1 (ky = 0, 1, 2) of
+// channels 0..31 against X row y, so one CTA and one B tile serve all three
+// kernel rows; TMEM lane 32 * ky + co holds dW[co][.][ky][.].
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -28,27 +36,47 @@ namespace lg
 {
 namespace
 {
-constexpr int kPix = 128;         // pixels per K-chunk (one row segment)
-constexpr int kXHalo = kPix + 2;
+constexpr int kPix = 128;         // pixels per K-step
 constexpr int kThreads = 128;
 constexpr int kStages = 3;
+constexpr int kMaxRowPix = 144;   // the largest R * (Wp + 2) of a step (R = 8, Wp = 16)
+
+// Rows and pixels per row of a K-step for width W.
+__host__ __device__ inline void step_shape(int W, int& R, int& Wp)
+{
+    if (W > 64)
+    {
+        R = 1;
+        Wp = kPix;
+        return;
+    }
+    Wp = (W + 15) / 16 * 16;
+    R = kPix / Wp;
+}
 
 template <int BNW>
 struct WSmem
 {
-    static constexpr int kABytes = 16 * kPix * 16;          // 16 channel blocks (M = 128) x 128 px
-    static constexpr int kBBytes = (BNW / 8) * kXHalo * 16;
-    static constexpr int kStage = ((kABytes + kBBytes + 1023) / 1024) * 1024;
+    static constexpr int kABytes = 16 * kPix * 16;  // 16 channel blocks (M = 128) x 128 px
+    static constexpr int kMaxStage = ((kABytes + (BNW / 8) * kMaxRowPix * 16 + 1023) / 1024) * 1024;
+    // B: BNW/8 channel blocks x R rows x (Wp + 2) pixels
+    __host__ __device__ static int stage(int R, int Wp)
+    {
+        return ((kABytes + (BNW / 8) * R * (Wp + 2) * 16 + 1023) / 1024) * 1024;
+    }
 };
 
-template <int BNW>
+template <int BNW, bool KYP>
 __global__ void __launch_bounds__(kThreads, 1)
     wgrad_kernel(const __grid_constant__ CUtensorMap map_dz, const __grid_constant__ CUtensorMap map_x, WgradArgs a)
 {
     using S = WSmem<BNW>;
+    int R, Wp;
+    step_shape(a.W, R, Wp);
+    const int kStage = S::stage(R, Wp);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * S::kStage);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStage);
     uint64_t* empty = full + kStages;
     uint64_t* done = empty + kStages;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
@@ -56,22 +84,25 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const int tid = threadIdx.x, warp = tid >> 5;
     const int n_cit = a.Cin / BNW;
-    const int ky = blockIdx.y / n_cit;
+    const int ky = KYP ? 0 : blockIdx.y / n_cit;  // KYP: all three
     const int ci0 = (blockIdx.y % n_cit) * BNW;
     const int co0 = blockIdx.z * 128;
-    const int rows = a.N * a.H;
-    const int r0 = blockIdx.x * a.rows_per_cta;
-    const int r1 = min(rows, r0 + a.rows_per_cta);
-    const int xsegs = (a.W + kPix - 1) / kPix;
-    const int steps = (r1 - r0) * xsegs;
+    const int gpi = (a.H + R - 1) / R;  // row groups per image
+    const int groups = a.N * gpi;
+    const int g0 = blockIdx.x * a.rows_per_cta;  // this CTA's row groups
+    const int g1 = min(groups, g0 + a.rows_per_cta);
+    const int xsegs = (a.W + Wp - 1) / Wp;
+    const int steps = (g1 - g0) * xsegs;
     const int co_blocks = min(16, (a.Cout - co0) / 8);  // channel blocks loaded; the rest stay zero
     constexpr uint32_t kCols = (3 * BNW <= 32) ? 32 : (3 * BNW <= 64) ? 64 : (3 * BNW <= 128) ? 128 : (3 * BNW <= 256) ? 256 : 512;
     // M = 128, N = BNW, both operands MN-major.
     constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, BNW) | (1u << 15) | (1u << 16);
-    const uint32_t a_bytes = (uint32_t)(co_blocks * kPix * 16);
+    const uint32_t a_bytes = (uint32_t)((KYP ? 12 : co_blocks) * R * Wp * 16);
+    const uint32_t b_bytes = (uint32_t)((BNW / 8) * R * (Wp + 2) * 16);
+    const uint32_t a_sbo = (uint32_t)(R * Wp * 16), b_sbo = (uint32_t)(R * (Wp + 2) * 16);  // channel-block strides
 
     // Zero the A buffers once: channel blocks beyond Cout are never written by TMA.
-    for (int i = tid; i < kStages * S::kStage / 16; i += kThreads)
+    for (int i = tid; i < kStages * kStage / 16; i += kThreads)
         reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
     tc::fence_proxy_async();
     if (warp == 0)
@@ -98,14 +129,24 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (tid == 0 && steps > 0)
     {
         auto issue = [&](int s, int step) {
-            const int r = r0 + step / xsegs;
-            const int x0 = (step % xsegs) * kPix;
-            const int n = r / a.H, y = r % a.H;
-            uint8_t* A = smem + s * S::kStage;
+            const int g = g0 + step / xsegs;
+            const int x0 = (step % xsegs) * Wp;
+            const int n = g / gpi, y = (g % gpi) * R;
+            uint8_t* A = smem + s * kStage;
             uint8_t* B = A + S::kABytes;
-            tc::mbar_expect_tx(&full[s], a_bytes + (uint32_t)S::kBBytes);
-            tc::tma_load_5d(A, &map_dz, &full[s], 0, x0, y, co0 / 8, n);
-            tc::tma_load_5d(B, &map_x, &full[s], 0, x0 - 1, y + ky - 1, ci0 / 8, n);
+            tc::mbar_expect_tx(&full[s], a_bytes + b_bytes);
+            if (KYP)
+            {
+                // M blocks 4 * k .. 4 * k + 3: dZ rows y + 1 - k against X rows y (kernel row k)
+                for (int k = 0; k < 3; ++k)
+                    tc::tma_load_5d(A + k * 4 * R * Wp * 16, &map_dz, &full[s], 0, x0, y + 1 - k, 0, n);
+                tc::tma_load_5d(B, &map_x, &full[s], 0, x0 - 1, y, ci0 / 8, n);
+            }
+            else
+            {
+                tc::tma_load_5d(A, &map_dz, &full[s], 0, x0, y, co0 / 8, n);
+                tc::tma_load_5d(B, &map_x, &full[s], 0, x0 - 1, y + ky - 1, ci0 / 8, n);
+            }
         };
         const int pre = steps < kStages ? steps : kStages;
         for (int s = 0; s < pre; ++s) issue(s, s);
@@ -115,17 +156,19 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int s = step % kStages;
             if (!tc::mbar_wait(&full[s], (uint32_t)((step / kStages) & 1))) { ok = false; break; }
             tc::tc_fence_after();
-            const uint32_t abase = tc::smem_u32(smem + s * S::kStage);
+            const uint32_t abase = tc::smem_u32(smem + s * kStage);
             const uint32_t bbase = abase + S::kABytes;
-#pragma unroll
+#pragma unroll 1
             for (int dx = 0; dx < 3; ++dx)
-#pragma unroll
-                for (int ks = 0; ks < kPix / 16; ++ks)
-                {
-                    const uint64_t ad = tc::smem_desc(abase + (uint32_t)(ks * 16 * 16), 128, kPix * 16);
-                    const uint64_t bd = tc::smem_desc(bbase + (uint32_t)((ks * 16 + dx) * 16), 128, kXHalo * 16);
-                    tc::mma_bf16(tmem + (uint32_t)(dx * BNW), ad, bd, kIdesc, (step | ks) != 0 ? 1u : 0u);
-                }
+#pragma unroll 1
+                for (int r = 0; r < R; ++r)
+                    for (int ks = 0; ks < Wp / 16; ++ks)
+                    {
+                        const uint64_t ad = tc::smem_desc(abase + (uint32_t)((r * Wp + ks * 16) * 16), 128, a_sbo);
+                        const uint64_t bd =
+                            tc::smem_desc(bbase + (uint32_t)((r * (Wp + 2) + ks * 16 + dx) * 16), 128, b_sbo);
+                        tc::mma_bf16(tmem + (uint32_t)(dx * BNW), ad, bd, kIdesc, (step | r | ks) != 0 ? 1u : 0u);
+                    }
             tc::mma_commit(&empty[s]);
             if (step >= 1)
             {
@@ -146,9 +189,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::mma_commit(done);
     }
     __syncwarp();
-    // This CTA's slice of the scratch: chunk blockIdx.x of [chunk][Cout][Cin_real][3][3].
+    // This CTA's slice of the scratch: chunk blockIdx.x of [chunk][ky][kx][Cin_real][Cout], output channels
+    // innermost so that a warp's 32 lanes (32 output channels) store 128 contiguous bytes.
     float* part = a.partial + (size_t)blockIdx.x * a.Cout * a.Cin_real * 9;
-    const int co = co0 + tid;  // TMEM lane = output channel
+    // TMEM lane = output channel; with KYP, lane 32 * k + co is kernel row k
+    const int co = KYP ? (tid & 31) : co0 + tid;
+    const int kyo = KYP ? (tid >> 5) : ky;
     bool have = false;
     if (steps > 0)
     {
@@ -170,13 +216,13 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int j = 0; j < 16; ++j) v[j] = 0.0f;  // an empty chunk (or a failed one) adds zeros
             }
-            if (co < a.Cout)
+            if (co < a.Cout && kyo < 3)
             {
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
                 {
                     const int ci = ci0 + c0 + j;
-                    if (ci < a.Cin_real) part[(((size_t)co * a.Cin_real + ci) * 3 + ky) * 3 + dx] = v[j];
+                    if (ci < a.Cin_real) part[((size_t)(kyo * 3 + dx) * a.Cin_real + ci) * a.Cout + co] = v[j];
                 }
             }
         }
@@ -206,13 +252,14 @@ EncodeTiledFn encode_fn()
     return fn;
 }
 
-cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int box_x, int box_cb)
+cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, int H, int W, int box_x, int box_y,
+                     int box_cb)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     cuuint64_t dims[5] = {8, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)(C / 8), (cuuint64_t)N};
     cuuint64_t strides[4] = {16, (cuuint64_t)W * 16, (cuuint64_t)H * W * 16, (cuuint64_t)(C / 8) * H * W * 16};
-    cuuint32_t box[5] = {8, (cuuint32_t)box_x, 1, (cuuint32_t)box_cb, 1};
+    cuuint32_t box[5] = {8, (cuuint32_t)box_x, (cuuint32_t)box_y, (cuuint32_t)box_cb, 1};
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)base, dims, strides, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -220,24 +267,47 @@ cudaError_t make_map(CUtensorMap* m, const __nv_bfloat16* base, int N, int C, in
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-// dw[e] += partial[0][e] + partial[1][e] + ... in chunk order.
-__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int chunks, size_t n, float* __restrict__ dw)
+// dw[co][ci][ky][kx] += the chunks' partials of that weight, in a fixed
+// order: a block takes 32 consecutive partial entries ([ky][kx][ci][co]
+// order, so reads are coalesced) and splits the chunks into 8 consecutive
+// slices, one warp each; the slice sums are then added in slice order.
+__global__ void __launch_bounds__(256) wgrad_reduce_kernel(const float* __restrict__ partial, int chunks, int Cout,
+                                                           int Cin_real, float* __restrict__ dw)
 {
-    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    __shared__ float t[8][32];
+    const size_t n = (size_t)Cout * Cin_real * 9;
+    const int lane = threadIdx.x & 31, slice = threadIdx.x >> 5;
+    const size_t e = (size_t)blockIdx.x * 32 + lane;
+    const int per = (chunks + 7) / 8;
+    const int c0 = slice * per, c1 = min(chunks, c0 + per);
+    float s = 0.0f;
+    if (e < n)
+        for (int c = c0; c < c1; ++c) s += partial[(size_t)c * n + e];
+    t[slice][lane] = s;
+    __syncthreads();
+    if (slice == 0 && e < n)
     {
-        float s = 0.0f;
-        for (int c = 0; c < chunks; ++c) s += partial[(size_t)c * n + e];
-        dw[e] += s;
+        float tot = t[0][lane];
+#pragma unroll
+        for (int k = 1; k < 8; ++k) tot += t[k][lane];
+        const int co = (int)(e % Cout);
+        const size_t r = e / Cout;
+        const int ci = (int)(r % Cin_real), tap = (int)(r / Cin_real);  // tap = ky * 3 + kx
+        dw[((size_t)co * Cin_real + ci) * 9 + tap] += tot;
     }
 }
 
-// Row chunks of a launch: about two CTAs per SM over the (ky, input block,
-// output block) grid, at most one per image row.
-int wgrad_chunks(int N, int H, int Cout, int Cin, int bnw, int sm_count, int* rows_per_cta)
+// Chunks of a launch: about two CTAs per SM over the (ky, input block,
+// output block) grid, at most one per row group (R rows of the K-step shape
+// for width W; W = 0 counts single rows, an upper bound for sizing scratch).
+int wgrad_chunks(int N, int H, int W, int Cout, int Cin, int bnw, int sm_count, int* rows_per_cta)
 {
     const int cot = (Cout + 127) / 128, cit = Cin / bnw;
-    const int rows = N * H;
-    int chunks = (2 * sm_count) / (3 * cit * cot);
+    const int kys = Cout == 32 ? 1 : 3;  // CTAs per (input block, output block): one with the kernel rows in M
+    int R = 1, Wp = kPix;
+    if (W > 0) step_shape(W, R, Wp);
+    const int rows = N * ((H + R - 1) / R);
+    int chunks = (2 * sm_count) / (kys * cit * cot);
     if (chunks < 1) chunks = 1;
     if (chunks > rows) chunks = rows;
     const int rpc = (rows + chunks - 1) / chunks;
@@ -247,33 +317,35 @@ int wgrad_chunks(int N, int H, int Cout, int Cin, int bnw, int sm_count, int* ro
 
 int wgrad_bnw(int Cin) { return Cin % 128 == 0 ? 128 : Cin % 64 == 0 ? 64 : Cin % 32 == 0 ? 32 : 16; }
 
-template <int BNW>
+template <int BNW, bool KYP>
 cudaError_t launch_w(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
                      cudaStream_t stream)
 {
+    int R, Wp;
+    step_shape(a.W, R, Wp);
     CUtensorMap mdz, mx;
-    cudaError_t e = make_map(&mdz, dz, a.N, a.Cout, a.H, a.W, kPix, a.Cout / 8 < 16 ? a.Cout / 8 : 16);
+    cudaError_t e = make_map(&mdz, dz, a.N, a.Cout, a.H, a.W, Wp, R, a.Cout / 8 < 16 ? a.Cout / 8 : 16);
     if (e != cudaSuccess) return e;
-    e = make_map(&mx, x, a.N, a.Cin, a.H, a.W, kXHalo, BNW / 8);
+    e = make_map(&mx, x, a.N, a.Cin, a.H, a.W, Wp + 2, R, BNW / 8);
     if (e != cudaSuccess) return e;
-    const int smem = kStages * WSmem<BNW>::kStage + 1024 + 256;
+    const int smem_max = kStages * WSmem<BNW>::kMaxStage + 1024 + 256;
+    const int smem = kStages * WSmem<BNW>::stage(R, Wp) + 1024 + 256;
     static bool attr = false;
     if (!attr)
     {
-        e = cudaFuncSetAttribute(wgrad_kernel<BNW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = cudaFuncSetAttribute(wgrad_kernel<BNW, KYP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max);
         if (e != cudaSuccess) return e;
         attr = true;
     }
     WgradArgs b = a;
     const int cot = (a.Cout + 127) / 128, cit = a.Cin / BNW;
-    const int chunks = wgrad_chunks(a.N, a.H, a.Cout, a.Cin, BNW, sm_count, &b.rows_per_cta);
-    dim3 grid(chunks, 3 * cit, cot);
-    wgrad_kernel<BNW><<<grid, kThreads, smem, stream>>>(mdz, mx, b);
+    const int chunks = wgrad_chunks(a.N, a.H, a.W, a.Cout, a.Cin, BNW, sm_count, &b.rows_per_cta);
+    dim3 grid(chunks, (KYP ? 1 : 3) * cit, cot);
+    wgrad_kernel<BNW, KYP><<<grid, kThreads, smem, stream>>>(mdz, mx, b);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t n = (size_t)a.Cout * a.Cin_real * 9;
-    wgrad_reduce_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 1184), 256, 0, stream>>>(b.partial, chunks, n,
-                                                                                               a.dw);
+    wgrad_reduce_kernel<<<(unsigned)((n + 31) / 32), 256, 0, stream>>>(b.partial, chunks, a.Cout, a.Cin_real, a.dw);
     return cudaGetLastError();
 }
 
@@ -330,7 +402,7 @@ __global__ void bias_reduce_kernel(const float* __restrict__ partial, int C, flo
 
 size_t conv3x3_wgrad_partial_floats(int N, int H, int Cout, int Cin, int Cin_real, int sm_count)
 {
-    const int chunks = wgrad_chunks(N, H, Cout, Cin, wgrad_bnw(Cin), sm_count, nullptr);
+    const int chunks = wgrad_chunks(N, H, 0, Cout, Cin, wgrad_bnw(Cin), sm_count, nullptr);
     return (size_t)chunks * Cout * Cin_real * 9;
 }
 
@@ -339,12 +411,20 @@ cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const
 {
     if (a.Cout % 32 || a.Cin % 16 || !a.partial) return cudaErrorInvalidValue;
     const int bnw = wgrad_bnw(a.Cin);
+    if (a.Cout == 32)  // the three kernel rows share M
+        switch (bnw)
+        {
+        case 128: return launch_w<128, true>(dz, x, a, sm_count, stream);
+        case 64: return launch_w<64, true>(dz, x, a, sm_count, stream);
+        case 32: return launch_w<32, true>(dz, x, a, sm_count, stream);
+        default: return launch_w<16, true>(dz, x, a, sm_count, stream);
+        }
     switch (bnw)
     {
-    case 128: return launch_w<128>(dz, x, a, sm_count, stream);
-    case 64: return launch_w<64>(dz, x, a, sm_count, stream);
-    case 32: return launch_w<32>(dz, x, a, sm_count, stream);
-    default: return launch_w<16>(dz, x, a, sm_count, stream);
+    case 128: return launch_w<128, false>(dz, x, a, sm_count, stream);
+    case 64: return launch_w<64, false>(dz, x, a, sm_count, stream);
+    case 32: return launch_w<32, false>(dz, x, a, sm_count, stream);
+    default: return launch_w<16, false>(dz, x, a, sm_count, stream);
     }
 }
 

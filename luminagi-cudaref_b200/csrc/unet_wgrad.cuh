@@ -11,11 +11,11 @@ struct WgradArgs
     int Cout;       // channels of dZ (multiple of 32)
     int Cin;        // channels of the blocked input X (multiple of 16)
     int Cin_real;   // channels that have weights (<= Cin)
-    int rows_per_cta;  // set by the launcher
+    int rows_per_cta;  // set by the launcher: row groups (of the K-step's rows) per CTA
     float* dw;      // [Cout][Cin_real][3][3], added to
     int* err;
     // Scratch of conv3x3_wgrad_partial_floats() floats: each CTA stores its
-    // partial sums there and one pass adds them to dw in chunk order, so the
+    // partial sums there and one pass adds them to dw in a fixed order, so the
     // gradient does not depend on the order the CTAs finish in.
     float* partial;
 };
