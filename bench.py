@@ -61,19 +61,19 @@ import numpy as np  # noqa: E402
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # DRAM bytes (read + write) per traced ray of trace_kernel, from one ncu capture
-# of an 8-spp engine frame: 431.3 MB + 34.5 MB / 65,366,791 rays; traffic
+# of an 8-spp engine frame: 427.7 MB + 37.8 MB / 65,366,791 rays; traffic
 # scales with rays.
-TRACE_DRAM_BYTES_PER_RAY = (431256320 + 34534400) / 65366791
+TRACE_DRAM_BYTES_PER_RAY = (427703296 + 37808384) / 65366791
 # Bytes one traversal step loads from a BVH record: both 32-byte halves of a
-# 4-wide record (grid origin, steps, 24 one-byte planes, four links, 8 B of
-# padding), or the whole 64-byte 2-wide record.
+# 4-wide record (grid origin, steps, 24 one-byte planes, four links), or the
+# whole 64-byte 2-wide record.
 RECORD_BYTES = {4: 64, 2: 64}
 # Rows of the CPU sample: every CPU_ROW_STEP-th row of the frame, the same in
 # the cpu_baseline leg and the reference arm.
 CPU_ROW_STEP = 16
 # Local-memory (stack and spill) bytes per traced ray of trace_kernel, from the
-# same capture: (806.3 M load + 911.3 M store sectors) x 32 B / rays.
-TRACE_LOCAL_BYTES_PER_RAY = (806348142 + 911329462) * 32 / 65366791
+# same capture: (806.4 M load + 911.3 M store sectors) x 32 B / rays.
+TRACE_LOCAL_BYTES_PER_RAY = (806358764 + 911343284) * 32 / 65366791
 # Denoiser weights trained by this library on the engine scene (lumina.surrogate, the
 # 120-epoch recipe with 24 crops per image per epoch; FP16 copy of the best-validation
 # parameters, with the indices of the poses held out of training).
@@ -497,8 +497,8 @@ def main():
             "dram_bytes_per_ray": TRACE_DRAM_BYTES_PER_RAY, "kernel": "trace_kernel",
             "algorithmic_bytes_per_launch": algo_bytes, "algorithmic_bytes_per_ray": algo_bytes / rays,
             "kernel_ms": kernel_ms,
-            "limiter": "instruction issue, not memory (ncu: issue slots ~70% busy, L1 data pipe ~50%; "
-                       "474 warp instructions per ray)"}
+            "limiter": "instruction issue, not memory (ncu: issue slots 71% busy at 16 of 32 lanes active, "
+                       "L1 data pipe 53%; 455 warp instructions per ray)"}
     if TRACE_LOCAL_BYTES_PER_RAY is not None:
         roof["local_bytes_per_ray"] = TRACE_LOCAL_BYTES_PER_RAY
     line = {"metric": "Mrays/s (plain render; ms/frame alongside)", "value": value, "unit": "Mrays/s",
