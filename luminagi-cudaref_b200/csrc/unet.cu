@@ -249,6 +249,7 @@ void lg_unet_destroy(lg_unet* u)
     for (auto& b : u->dz) b.release();
     if (u->probe_ev0) cudaEventDestroy(u->probe_ev0);
     if (u->probe_ev1) cudaEventDestroy(u->probe_ev1);
+    if (u->order_ev) cudaEventDestroy(u->order_ev);
     if (u->stream) cudaStreamDestroy(u->stream);
     delete u;
 }

@@ -81,6 +81,7 @@ struct lg_unet
     // or of the backward (probe_dgrad); -1 = none
     int probe_layer = -1, probe_dgrad = -1;
     cudaEvent_t probe_ev0 = nullptr, probe_ev1 = nullptr;
+    cudaEvent_t order_ev = nullptr;  // lg_unet_train_step_async: orders the caller's stream and the network's
 };
 
 namespace lg

@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "tc_ptx.cuh"
 #include "unet_conv.cuh"
 
 namespace lg
@@ -49,14 +50,6 @@ __device__ __forceinline__ uint4 pack(const float* v)
 __device__ __forceinline__ const uint4* at(const __nv_bfloat16* base, int C, int H, int W, int n, int b, int y, int x)
 {
     return reinterpret_cast<const uint4*>(base + ((((size_t)n * (C >> 3) + b) * H + y) * W + x) * 8);
-}
-
-// 32 bytes to global memory in one store (address 32-byte aligned).
-__device__ __forceinline__ void tc_st_v8(void* p, uint4 a, uint4 b)
-{
-    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "r"(a.x), "r"(a.y), "r"(a.z),
-                 "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
-                 : "memory");
 }
 
 // Source rows (i0, i1) and the weight of i1 for output index d of an axis of size n.
@@ -119,7 +112,8 @@ __global__ void __launch_bounds__(128) up2_kernel(const __nv_bfloat16* __restric
         o[k] = hy * (ha * p0[k] + la * q0[k]) + ly * (ha * p1[k] + la * q1[k]);
         o2[k] = hy * (hb * q0[k] + lb * r0[k]) + ly * (hb * q1[k] + lb * r1[k]);
     }
-    tc_st_v8(out + ((((size_t)n * (out_C >> 3) + (coff >> 3) + b) * H + Y) * W + 2 * i) * 8, pack(o), pack(o2));
+    // 2i is even and W = 2w, so the pair starts on a 32-byte boundary
+    tc::st_global_v8(out + ((((size_t)n * (out_C >> 3) + (coff >> 3) + b) * H + Y) * W + 2 * i) * 8, pack(o), pack(o2));
 }
 
 // Outputs of one axis feeding input i (size n): up to 4 indices and weights.

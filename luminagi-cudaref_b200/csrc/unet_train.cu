@@ -393,10 +393,10 @@ int lg_unet_train_step_async(lg_unet* u, const float* d_x, const float* d_target
                              float* d_loss_sum, void* stream)
 {
     if (!u || !d_x || !d_target) return set_error(LG_ERR_INVALID, "NULL argument");
-    cudaEvent_t ev;
-    LG_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    cudaEventRecord(ev, (cudaStream_t)stream);
-    cudaStreamWaitEvent(u->stream, ev, 0);
+    if (!u->order_ev) LG_TRY_CUDA(cudaEventCreateWithFlags(&u->order_ev, cudaEventDisableTiming));
+    cudaEvent_t ev = u->order_ev;
+    LG_TRY_CUDA(cudaEventRecord(ev, (cudaStream_t)stream));
+    LG_TRY_CUDA(cudaStreamWaitEvent(u->stream, ev, 0));
     int rc = loss_and_grads(u, d_x, d_target, n, h, w, nullptr);
     if (rc == LG_OK && d_loss_sum)
     {
@@ -407,9 +407,10 @@ int lg_unet_train_step_async(lg_unet* u, const float* d_x, const float* d_target
         if (e != cudaSuccess) rc = set_error(LG_ERR_CUDA, "loss: %s", cudaGetErrorString(e));
     }
     if (rc == LG_OK) rc = adam_step(u, lr);
-    cudaEventRecord(ev, u->stream);
-    cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
-    cudaEventDestroy(ev);
+    // later work on the caller's stream waits for this step (also after an error, for what was queued)
+    const cudaError_t e1 = cudaEventRecord(ev, u->stream);
+    const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent((cudaStream_t)stream, ev, 0) : e1;
+    if (rc == LG_OK && e2 != cudaSuccess) rc = set_error(LG_ERR_CUDA, "stream order: %s", cudaGetErrorString(e2));
     return rc;
 }
 
