@@ -32,7 +32,9 @@ counting pass) with ms/frame alongside.
   denoise   8 spp + UNet against plain 256 spp on the same frame (device
             time), with the trained weights in lumina/data: PSNR/SSIM of both
             and of the 8-spp input against a 1024-spp FP64 judge on an orbit
-            pose held out of training.
+            pose held out of training; and the denoiser alone (reference and
+            HDR networks, batch 1 and 8) in TFLOP/s against the dense BF16
+            peak.
   ingest    scene-file load times: this library on scene.json and on the
             binary scene file, and the reference's LoadSceneJSON on the same
             JSON (host only).
@@ -71,6 +73,8 @@ RECORD_BYTES = {4: 64, 2: 64}
 # Rows of the CPU sample: every CPU_ROW_STEP-th row of the frame, the same in
 # the cpu_baseline leg and the reference arm.
 CPU_ROW_STEP = 16
+# Multiply-adds per output pixel of the denoiser (14 3x3 convolutions and the 1x1 tail; ml/train.py's UNet).
+UNET_MAC_PER_PIXEL = 162240
 # Local-memory (stack and spill) bytes per traced ray of trace_kernel, from the
 # same capture: (806.4 M load + 911.3 M store sectors) x 32 B / rays.
 TRACE_LOCAL_BYTES_PER_RAY = (806358764 + 911343284) * 32 / 65366791
@@ -485,6 +489,23 @@ def main():
                 "gain_db_over_8spp": agg["denoised_psnr"] - agg["noisy_psnr"],
                 "db_vs_256spp": agg["denoised_psnr"] - agg["clean_psnr"]}
         net.close()
+
+        # The denoiser alone against the dense BF16 peak (configuration 4): the reference network and the HDR one
+        # (ReLU, bilinear upsampling, log1p in / expm1 out) at batch 1 and 8, 1728x864, inputs already on the device.
+        def unet_rate(variant, n):
+            m = lumina.UNet(variant=variant)
+            m.set_params(np.random.default_rng(1).normal(0, 0.02, m.n_params).astype(np.float32))
+            xb = torch.rand((n, 3, H, W), device=f"cuda:{dev}")
+            yb = torch.empty_like(xb)
+            ms = timed(lambda: m.forward_device(xb.data_ptr(), n, H, W, yb.data_ptr(), stream.cuda_stream), 10)
+            m.close()
+            tf = 2 * UNET_MAC_PER_PIXEL * n * H * W / ms / 1e9
+            return {"ms": ms, "tflops": tf, "frac": tf / peaks["bf16_tflops"]}
+
+        denoise["unet"] = {"flop_per_pixel": 2 * UNET_MAC_PER_PIXEL, "peak_tflops": peaks["bf16_tflops"],
+                           "peak_source": f"{peak_kind} dense BF16 GEMM, burst",
+                           "ref": {"batch1": unet_rate("ref", 1), "batch8": unet_rate("ref", 8)},
+                           "hdr": {"batch1": unet_rate("hdr", 1), "batch8": unet_rate("hdr", 8)}}
 
     traffic = TRACE_DRAM_BYTES_PER_RAY * rays
     roof = {"bound": "l2", "achieved": achieved, "peak": l2_gbs.value, "unit": "GB/s",
