@@ -350,7 +350,7 @@ struct PathState
     uint32_t rng;
     int px, py, k, n_this, bounce, li;  // li: -1 camera/bounce ray in flight, >= 0 shadow ray of light li
     unsigned pixel;                     // index of the pixel's first accumulator value
-    int job, max_bounces;               // batched launches: the frame this item belongs to
+    int job;                            // batched launches: the frame this item belongs to
 };
 
 // Frame of a global work item in a batched launch: the last job whose
@@ -505,7 +505,6 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
                         tiles_x = b.tiles_x;
                         spp = b.spp;
                         sbase = b.sample_base;
-                        st.max_bounces = b.max_bounces;
                     }
                     const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
                     const unsigned j = (unsigned)(item & 31ull);
@@ -547,7 +546,9 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceMinBlocks) trace_kernel(D
         if (active && tdone)
         {
             const DevCam& c = kBatch ? job.jobs[st.job].cam : cam;
-            if (advance<kAcc64>(st, s, c, kBatch ? st.max_bounces : job.max_bounces, q.tri, q.t, q.u, q.v))
+            // batched: the frame's bounce limit is read from the job table (one register less than keeping it)
+            const int max_b = kBatch ? job.jobs[st.job].max_bounces : job.max_bounces;
+            if (advance<kAcc64>(st, s, c, max_b, q.tri, q.t, q.u, q.v))
             {
                 trav_begin<kCount>(q, root, st.tmax, st.li >= 0, cnt);
                 tdone = false;
