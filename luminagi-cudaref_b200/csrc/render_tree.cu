@@ -65,9 +65,13 @@ __device__ __forceinline__ int block_excl_scan(int v, int* warp_sums, int& total
     __syncthreads();
     return before + x - v;
 }
-__global__ void scan_local_kernel(const int* __restrict__ in, int n, int* __restrict__ out, int* __restrict__ sums)
+// n: element count, or (dn != null) read from device memory, at most the
+// elements the grid covers.
+__global__ void scan_local_kernel(const int* __restrict__ in, int n, const int* __restrict__ dn, int* __restrict__ out,
+                                  int* __restrict__ sums)
 {
     __shared__ int ws[kTB / 32];
+    if (dn) n = *dn;
     const int i = blockIdx.x * kTB + threadIdx.x;
     int total;
     const int e = block_excl_scan(i < n ? in[i] : 0, ws, total);
@@ -92,8 +96,9 @@ __global__ void scan_sums_kernel(int* __restrict__ sums, int nb, int* __restrict
     }
     if (threadIdx.x == 0 && grand_total) *grand_total = carry;
 }
-__global__ void scan_add_kernel(int* __restrict__ out, int n, const int* __restrict__ sums)
+__global__ void scan_add_kernel(int* __restrict__ out, int n, const int* __restrict__ dn, const int* __restrict__ sums)
 {
+    if (dn) n = *dn;
     const int i = blockIdx.x * kTB + threadIdx.x;
     if (i < n) out[i] += sums[blockIdx.x];
 }
@@ -102,9 +107,19 @@ cudaError_t excl_scan(const int* in, int n, int* out, int* sums, int* total, cud
 {
     const int nb = (n + kTB - 1) / kTB;
     if (n <= 0) return cudaMemsetAsync(total, 0, sizeof(int), st);
-    scan_local_kernel<<<nb, kTB, 0, st>>>(in, n, out, sums);
+    scan_local_kernel<<<nb, kTB, 0, st>>>(in, n, nullptr, out, sums);
     scan_sums_kernel<<<1, kTB, 0, st>>>(sums, nb, total);
-    scan_add_kernel<<<nb, kTB, 0, st>>>(out, n, sums);
+    scan_add_kernel<<<nb, kTB, 0, st>>>(out, n, nullptr, sums);
+    return cudaGetLastError();
+}
+// The same over *dn elements (device memory), with a grid for n_max >= *dn.
+cudaError_t excl_scan_dev(const int* in, const int* dn, int n_max, int* out, int* sums, int* total, cudaStream_t st)
+{
+    const int nb = (n_max + kTB - 1) / kTB;
+    if (n_max <= 0) return cudaMemsetAsync(total, 0, sizeof(int), st);
+    scan_local_kernel<<<nb, kTB, 0, st>>>(in, 0, dn, out, sums);
+    scan_sums_kernel<<<1, kTB, 0, st>>>(sums, nb, total);
+    scan_add_kernel<<<nb, kTB, 0, st>>>(out, 0, dn, sums);
     return cudaGetLastError();
 }
 
@@ -222,9 +237,13 @@ __global__ void init_tri_clusters_kernel(const lg_triangle* __restrict__ tris, i
     cbox[t] = b;
 }
 // Nearest neighbour within +-kRadius positions by union surface area; ties -> lower position.
-__global__ void __launch_bounds__(kTB) nn_kernel(const Box* __restrict__ cbox, int c, int* __restrict__ nn)
+// The clustering round's kernels read the cluster count c from device memory
+// (the round loop checks it on the host only every few rounds).
+__global__ void __launch_bounds__(kTB) nn_kernel(const Box* __restrict__ cbox, const int* __restrict__ dc,
+                                                 int* __restrict__ nn)
 {
     __shared__ Box sb[kTB + 2 * kRadius];
+    const int c = *dc;
     const int base = blockIdx.x * kTB - kRadius;
     for (int j = threadIdx.x; j < kTB + 2 * kRadius; j += kTB)
     {
@@ -250,8 +269,10 @@ __global__ void __launch_bounds__(kTB) nn_kernel(const Box* __restrict__ cbox, i
     }
     nn[i] = bj;
 }
-__global__ void merge_flags_kernel(const int* __restrict__ nn, int c, int* __restrict__ mflag, int* __restrict__ kflag)
+__global__ void merge_flags_kernel(const int* __restrict__ nn, const int* __restrict__ dc, int* __restrict__ mflag,
+                                   int* __restrict__ kflag)
 {
+    const int c = *dc;
     const int i = blockIdx.x * kTB + threadIdx.x;
     if (i >= c) return;
     const int j = nn[i];
@@ -259,10 +280,11 @@ __global__ void merge_flags_kernel(const int* __restrict__ nn, int c, int* __res
     mflag[i] = (mutual && i < j) ? 1 : 0;   // i owns the merged node
     kflag[i] = (mutual && i > j) ? 0 : 1;   // j's partner disappears
 }
-__global__ void merge_kernel(const int* __restrict__ nn, int c, const int* __restrict__ mflag,
-                             const int* __restrict__ midx, int node_base, int* __restrict__ cid,
+__global__ void merge_kernel(const int* __restrict__ nn, const int* __restrict__ dstate,
+                             const int* __restrict__ mflag, const int* __restrict__ midx, int* __restrict__ cid,
                              Box* __restrict__ cbox, lg_bvh_node* __restrict__ tn)
 {
+    const int c = dstate[0], node_base = dstate[1];
     const int i = blockIdx.x * kTB + threadIdx.x;
     if (i >= c || !mflag[i]) return;
     const int j = nn[i];
@@ -279,14 +301,24 @@ __global__ void merge_kernel(const int* __restrict__ nn, int c, const int* __res
     cid[i] = id;
     cbox[i] = b;
 }
-__global__ void compact_kernel(const int* __restrict__ kflag, const int* __restrict__ kpos, int c,
+__global__ void compact_kernel(const int* __restrict__ kflag, const int* __restrict__ kpos, const int* __restrict__ dc,
                                const int* __restrict__ cid, const Box* __restrict__ cbox, int* __restrict__ cid2,
                                Box* __restrict__ cbox2)
 {
+    const int c = *dc;
     const int i = blockIdx.x * kTB + threadIdx.x;
     if (i >= c || !kflag[i]) return;
     cid2[kpos[i]] = cid[i];
     cbox2[kpos[i]] = cbox[i];
+}
+
+// End of a clustering round: state = {c, next node id, error}; totals = {merges, kept clusters}.  A round that
+// merges nothing while more than one cluster is left marks the error (rounds after the last merge are no-ops).
+__global__ void round_end_kernel(int* __restrict__ state, const int* __restrict__ totals)
+{
+    if (state[0] > 1 && totals[0] == 0) state[2] = 1;
+    state[1] += totals[0];
+    state[0] = totals[1];
 }
 
 struct Scratch
@@ -381,26 +413,33 @@ int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, const lg_triangle
             LG_TRY_CUDA(cudaStreamSynchronize(st));
             if (c != L) return set_error(LG_ERR_INVALID, "render tree: %d leaves by range start, %d expected", c, L);
         }
-        int next_id = L;
-        while (c > 1)
+        // Rounds run kRoundsPerCheck at a time on a device-held count, grids sized by the last count read back (an
+        // upper bound: rounds only merge); the host reads the state between groups.
+        constexpr int kRoundsPerCheck = 8;
+        int* state = totals + 8;  // {c, next node id, error}
+        int hstate[3] = {c, L, 0};
+        LG_TRY_CUDA(cudaMemcpyAsync(state, hstate, sizeof(hstate), cudaMemcpyHostToDevice, st));
+        while (hstate[0] > 1)
         {
-            const int gc = (c + kTB - 1) / kTB;
-            nn_kernel<<<gc, kTB, 0, st>>>(cbox, c, nn);
-            merge_flags_kernel<<<gc, kTB, 0, st>>>(nn, c, mflag, kflag);
-            LG_TRY_CUDA(excl_scan(mflag, c, midx, sums, totals, st));
-            LG_TRY_CUDA(excl_scan(kflag, c, kpos, sums, totals + 1, st));
-            merge_kernel<<<gc, kTB, 0, st>>>(nn, c, mflag, midx, next_id, cid, cbox, tn);
-            compact_kernel<<<gc, kTB, 0, st>>>(kflag, kpos, c, cid, cbox, cid2, cbox2);
-            LG_TRY_CUDA(cudaGetLastError());
-            int tot[2] = {0, 0};
-            LG_TRY_CUDA(cudaMemcpyAsync(tot, totals, sizeof(tot), cudaMemcpyDeviceToHost, st));
+            const int gc = (hstate[0] + kTB - 1) / kTB;
+            for (int k = 0; k < kRoundsPerCheck; ++k)
+            {
+                nn_kernel<<<gc, kTB, 0, st>>>(cbox, state, nn);
+                merge_flags_kernel<<<gc, kTB, 0, st>>>(nn, state, mflag, kflag);
+                LG_TRY_CUDA(excl_scan_dev(mflag, state, hstate[0], midx, sums, totals, st));
+                LG_TRY_CUDA(excl_scan_dev(kflag, state, hstate[0], kpos, sums, totals + 1, st));
+                merge_kernel<<<gc, kTB, 0, st>>>(nn, state, mflag, midx, cid, cbox, tn);
+                compact_kernel<<<gc, kTB, 0, st>>>(kflag, kpos, state, cid, cbox, cid2, cbox2);
+                round_end_kernel<<<1, 1, 0, st>>>(state, totals);
+                LG_TRY_CUDA(cudaGetLastError());
+                int* ti = cid; cid = cid2; cid2 = ti;
+                Box* tb = cbox; cbox = cbox2; cbox2 = tb;
+            }
+            LG_TRY_CUDA(cudaMemcpyAsync(hstate, state, sizeof(hstate), cudaMemcpyDeviceToHost, st));
             LG_TRY_CUDA(cudaStreamSynchronize(st));
-            if (tot[0] == 0) return set_error(LG_ERR_DEVICE, "render tree: a clustering round merged nothing");
-            next_id += tot[0];
-            c = tot[1];
-            int* ti = cid; cid = cid2; cid2 = ti;
-            Box* tb = cbox; cbox = cbox2; cbox2 = tb;
+            if (hstate[2]) return set_error(LG_ERR_DEVICE, "render tree: a clustering round merged nothing");
         }
+        const int next_id = hstate[1];
         if (next_id != n_nodes) return set_error(LG_ERR_DEVICE, "render tree: %d nodes, %d expected", next_id, n_nodes);
         LG_TRY_CUDA(cudaMemcpyAsync(&root, cid, sizeof(int), cudaMemcpyDeviceToHost, st));
         LG_TRY_CUDA(cudaStreamSynchronize(st));

@@ -101,13 +101,26 @@ def test_accum64_and_batch(box_scene):
 
 
 def test_bad_material_index_is_rejected(box_scene):
-    sc = lumina.Scene(box_scene.camera, box_scene.sun, box_scene.tris.copy(), box_scene.mat_albedo,
-                      box_scene.mat_emissive, box_scene.points)
-    sc.tris["material"][5] = 99
+    """Material indices are checked on the device after the upload: the first
+    bad triangle is reported, the renderer is left without a scene, and a
+    valid scene set afterwards renders as usual (both set-up entry points)."""
+    def bad(tris):
+        sc = lumina.Scene(box_scene.camera, box_scene.sun, tris.copy(), box_scene.mat_albedo, box_scene.mat_emissive,
+                          box_scene.points)
+        sc.tris["material"][5] = 99
+        sc.tris["material"][7] = -1
+        return sc
+
+    nodes, bvh_tris = O.ref_build_bvh(box_scene.tris.copy())
     with lumina.Renderer(0) as r:
-        with pytest.raises(lumina.LuminaError) as e:
-            r.set_scene(sc)
-        assert e.value.code == -1
+        for setup in (lambda: r.set_scene(bad(box_scene.tris)), lambda: r.set_scene_bvh(bad(bvh_tris), nodes)):
+            with pytest.raises(lumina.LuminaError) as e:
+                setup()
+            assert e.value.code == -1 and "triangle 5 has material 99" in str(e.value)
+            black = r.render(spp=1, bounces=0)["rgb"]
+            assert not black.any()  # no scene: every pixel misses
+        r.set_scene(box_scene)
+        assert r.render(spp=1, bounces=0)["rgb"].any()
 
 
 @pytest.mark.parametrize("width", [2, 4])
