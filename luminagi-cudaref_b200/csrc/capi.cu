@@ -1185,7 +1185,7 @@ int lg_render_sorted(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
     LG_TRY(ensure_frame(r, cam->width, cam->height, false));
     const int npix = cam->width * cam->height;
     const long long nval = (long long)npix * 3;
-    LG_TRY(r->wf_scratch.reserve(wavefront_scratch_bytes(npix)));
+    LG_TRY(r->wf_scratch.reserve(wavefront_scratch_bytes(npix, r->n_points + 1)));
     LG_TRY_CUDA(cudaMemsetAsync(r->accum.p, 0, (size_t)nval * sizeof(float), r->stream));
     if (r->counting) LG_TRY_CUDA(cudaMemsetAsync(r->counters.p, 0, sizeof(RenderCounters), r->stream));
     LG_TRY_CUDA(cudaEventRecord(r->ev0, r->stream));
@@ -1200,6 +1200,10 @@ int lg_render_sorted(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
         job.watertight = r->watertight;
         job.accum = r->accum.as<float>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
+        job.sm_count = r->sm_count;
+        job.refill = r->trace_refill;
+        job.quorum = r->trace_quorum;
+        job.stack_safe = stack_safe(r);
         LG_TRY_CUDA(launch_wavefront_frame(dev_scene(r), make_dev_cam(*cam), job, r->wf_scratch.p,
                                            r->wf_scratch.bytes, r->stream));
     }
