@@ -1201,7 +1201,7 @@ int lg_render_sorted(lg_renderer* r, const lg_camera* cam, const lg_render_opts*
         job.accum = r->accum.as<float>();
         job.counters = r->counting ? r->counters.as<RenderCounters>() : nullptr;
         job.sm_count = r->sm_count;
-        job.refill = r->trace_refill;
+        job.refill = 8;  // ray-list traversals: refill at 8 idle lanes (64-spp engine frame: 4 and 16 are 2-4% slower)
         job.quorum = r->trace_quorum;
         job.stack_safe = stack_safe(r);
         LG_TRY_CUDA(launch_wavefront_frame(dev_scene(r), make_dev_cam(*cam), job, r->wf_scratch.p,

@@ -27,7 +27,7 @@ struct WavefrontJob
     RenderCounters* counters;  // optional: counts rays and record/triangle visits (one-thread-per-ray launches)
     // the staged launches (when not counting): persistent traversal grid and schedule
     int sm_count;
-    int refill;                // idle lanes of a warp that trigger a refill from the ray list, 1..32
+    int refill;                // idle lanes of a warp that trigger a refill from the ray list, 1..32 (8)
     int quorum;                // leaf postponement quorum, as for the persistent trace kernel
     bool stack_safe;           // the records' stack bound fits: traversal without push checks
 };
