@@ -185,6 +185,65 @@ def batch(a):
     return out
 
 
+def train(a):
+    """UNet training steps at n x h x w (random crops stand in: the cost does not depend on the values): the
+    synchronous step (lg_unet_train_step) and the queued one (lg_unet_train_step_async), wall time per step."""
+    import time
+
+    import torch
+
+    from .unet import UNet
+    net = UNet(variant=a.variant)
+    net.set_params(np.random.default_rng(5).normal(0, 0.02, net.n_params).astype(np.float32))
+    x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
+    t = torch.rand((a.n, 3, a.h, a.w), device="cuda")
+    out = {"kernel": "unet_train_step", "variant": a.variant, "n": a.n, "h": a.h, "w": a.w}
+    for _ in range(3):
+        net.train_step(x.data_ptr(), t.data_ptr(), a.n, a.h, a.w, 1e-4)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.reps):
+        net.train_step(x.data_ptr(), t.data_ptr(), a.n, a.h, a.w, 1e-4)
+    torch.cuda.synchronize()
+    out["sync_ms"] = (time.perf_counter() - t0) / a.reps * 1e3
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        t0 = time.perf_counter()
+        for _ in range(a.reps):
+            net.train_step_async(x.data_ptr(), t.data_ptr(), a.n, a.h, a.w, 1e-4, 0, s.cuda_stream)
+        s.synchronize()
+        out["async_ms"] = (time.perf_counter() - t0) / a.reps * 1e3
+    net.sync()
+    net.close()
+    return out
+
+
+def setup(a):
+    """lg_renderer_set_scene on the engine scene from pinned host memory (upload, device LBVH, render tree,
+    records), wall time per call."""
+    import time
+
+    import torch
+
+    from . import _ffi
+    from .render import Renderer
+    from .scene import Scene, engine_scene
+    sc = engine_scene(seed=7)
+    pinned = torch.empty(sc.tris.nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+    pinned[:] = sc.tris.view(np.uint8).ravel()
+    scp = Scene(sc.camera, sc.sun, pinned.view(_ffi.TRI_DTYPE), sc.mat_albedo, sc.mat_emissive, sc.points)
+    r = Renderer(0)
+    r.set_scene(scp)
+    ms = []
+    for _ in range(a.reps):
+        t0 = time.perf_counter()
+        r.set_scene(scp)
+        torch.cuda.synchronize()
+        ms.append((time.perf_counter() - t0) * 1e3)
+    r.close()
+    return {"kernel": "set_scene", "triangles": sc.n_tris, "ms": ms}
+
+
 def membench(a):
     """Read bandwidth of the L2 (buffers of 8-96 MB, L2-only loads) and of L1
     (every block re-reading a 16 KB region), lg_measure_read_bandwidth."""
@@ -204,7 +263,7 @@ def membench(a):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["unet", "trace", "bvh", "batch", "membench"])
+    ap.add_argument("what", choices=["unet", "trace", "bvh", "batch", "membench", "train", "setup"])
     ap.add_argument("--poses", type=int, default=50)
     ap.add_argument("--kernel", default="default", choices=["default", "single", "resident", "rows4", "dyp4", "dyp8", "autotune"],
                     help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
@@ -225,7 +284,8 @@ def main(argv=None):
     ap.add_argument("--tune", type=int, default=1, help="batch: autotune the launch and schedule first (1/0)")
     ap.add_argument("--tree", default="ploc_tris", choices=["ploc", "buildbvh", "ploc_tris"], help="trace: render tree")
     a = ap.parse_args(argv)
-    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch, "membench": membench}[a.what](a)))
+    print(json.dumps({"unet": unet, "trace": trace, "bvh": bvh, "batch": batch, "membench": membench, "train": train,
+                      "setup": setup}[a.what](a)))
 
 
 if __name__ == "__main__":
