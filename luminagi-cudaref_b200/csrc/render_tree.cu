@@ -65,13 +65,9 @@ __device__ __forceinline__ int block_excl_scan(int v, int* warp_sums, int& total
     __syncthreads();
     return before + x - v;
 }
-// n: element count, or (dn != null) read from device memory, at most the
-// elements the grid covers.
-__global__ void scan_local_kernel(const int* __restrict__ in, int n, const int* __restrict__ dn, int* __restrict__ out,
-                                  int* __restrict__ sums)
+__global__ void scan_local_kernel(const int* __restrict__ in, int n, int* __restrict__ out, int* __restrict__ sums)
 {
     __shared__ int ws[kTB / 32];
-    if (dn) n = *dn;
     const int i = blockIdx.x * kTB + threadIdx.x;
     int total;
     const int e = block_excl_scan(i < n ? in[i] : 0, ws, total);
@@ -96,9 +92,8 @@ __global__ void scan_sums_kernel(int* __restrict__ sums, int nb, int* __restrict
     }
     if (threadIdx.x == 0 && grand_total) *grand_total = carry;
 }
-__global__ void scan_add_kernel(int* __restrict__ out, int n, const int* __restrict__ dn, const int* __restrict__ sums)
+__global__ void scan_add_kernel(int* __restrict__ out, int n, const int* __restrict__ sums)
 {
-    if (dn) n = *dn;
     const int i = blockIdx.x * kTB + threadIdx.x;
     if (i < n) out[i] += sums[blockIdx.x];
 }
@@ -107,22 +102,11 @@ cudaError_t excl_scan(const int* in, int n, int* out, int* sums, int* total, cud
 {
     const int nb = (n + kTB - 1) / kTB;
     if (n <= 0) return cudaMemsetAsync(total, 0, sizeof(int), st);
-    scan_local_kernel<<<nb, kTB, 0, st>>>(in, n, nullptr, out, sums);
+    scan_local_kernel<<<nb, kTB, 0, st>>>(in, n, out, sums);
     scan_sums_kernel<<<1, kTB, 0, st>>>(sums, nb, total);
-    scan_add_kernel<<<nb, kTB, 0, st>>>(out, n, nullptr, sums);
+    scan_add_kernel<<<nb, kTB, 0, st>>>(out, n, sums);
     return cudaGetLastError();
 }
-// The same over *dn elements (device memory), with a grid for n_max >= *dn.
-cudaError_t excl_scan_dev(const int* in, const int* dn, int n_max, int* out, int* sums, int* total, cudaStream_t st)
-{
-    const int nb = (n_max + kTB - 1) / kTB;
-    if (n_max <= 0) return cudaMemsetAsync(total, 0, sizeof(int), st);
-    scan_local_kernel<<<nb, kTB, 0, st>>>(in, 0, dn, out, sums);
-    scan_sums_kernel<<<1, kTB, 0, st>>>(sums, nb, total);
-    scan_add_kernel<<<nb, kTB, 0, st>>>(out, 0, dn, sums);
-    return cudaGetLastError();
-}
-
 // ---- depth order ----
 __global__ void parent_of_kernel(const lg_bvh_node* __restrict__ nodes, int n, int* __restrict__ parent)
 {
@@ -269,56 +253,112 @@ __global__ void __launch_bounds__(kTB) nn_kernel(const Box* __restrict__ cbox, c
     }
     nn[i] = bj;
 }
-__global__ void merge_flags_kernel(const int* __restrict__ nn, const int* __restrict__ dc, int* __restrict__ mflag,
-                                   int* __restrict__ kflag)
+// A clustering round in four launches: nn_kernel, round_flags_kernel (merge
+// and keep flags and their block-local exclusive scans), round_sums_kernel
+// (one block: the block offsets, and the next round's state), and
+// round_apply_kernel (merge and compact).  State {c, next node id, error}
+// is double-buffered, cur -> nxt, so no launch reads a value its round
+// changes.  The integer scans give the same positions as the three-kernel
+// scans, so the tree does not change.
+__global__ void round_flags_kernel(const int* __restrict__ nn, const int* __restrict__ cur, int* __restrict__ mflag,
+                                   int* __restrict__ kflag, int* __restrict__ midx, int* __restrict__ kpos,
+                                   int* __restrict__ msums, int* __restrict__ ksums)
 {
-    const int c = *dc;
+    __shared__ int ws[kTB / 32];
+    const int c = cur[0];
+    const int i = blockIdx.x * kTB + threadIdx.x;
+    int m = 0, k = 0;
+    if (i < c)
+    {
+        const int j = nn[i];
+        const bool mutual = j >= 0 && nn[j] == i;
+        m = (mutual && i < j) ? 1 : 0;  // i owns the merged node
+        k = (mutual && i > j) ? 0 : 1;  // j's partner disappears
+        mflag[i] = m;
+        kflag[i] = k;
+    }
+    int tm, tk;
+    const int em = block_excl_scan(m, ws, tm);
+    const int ek = block_excl_scan(k, ws, tk);
+    if (i < c)
+    {
+        midx[i] = em;
+        kpos[i] = ek;
+    }
+    if (threadIdx.x == 0)
+    {
+        msums[blockIdx.x] = tm;
+        ksums[blockIdx.x] = tk;
+    }
+}
+__global__ void round_sums_kernel(int* __restrict__ msums, int* __restrict__ ksums, int nb, const int* __restrict__ cur,
+                                  int* __restrict__ nxt)
+{
+    __shared__ int ws[kTB / 32];
+    __shared__ int carry[2];
+    if (threadIdx.x < 2) carry[threadIdx.x] = 0;
+    __syncthreads();
+    for (int b = 0; b < nb; b += kTB)
+    {
+        const int i = b + threadIdx.x;
+        int tm, tk;
+        const int em = block_excl_scan(i < nb ? msums[i] : 0, ws, tm);
+        const int ek = block_excl_scan(i < nb ? ksums[i] : 0, ws, tk);
+        if (i < nb)
+        {
+            msums[i] = carry[0] + em;
+            ksums[i] = carry[1] + ek;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            carry[0] += tm;
+            carry[1] += tk;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        const int merges = carry[0];
+        nxt[2] = cur[2] | ((cur[0] > 1 && merges == 0) ? 1 : 0);
+        nxt[1] = cur[1] + merges;
+        nxt[0] = carry[1];
+    }
+}
+__global__ void round_apply_kernel(const int* __restrict__ nn, const int* __restrict__ cur,
+                                   const int* __restrict__ mflag, const int* __restrict__ kflag,
+                                   const int* __restrict__ midx, const int* __restrict__ kpos,
+                                   const int* __restrict__ msums, const int* __restrict__ ksums, int* __restrict__ cid,
+                                   Box* __restrict__ cbox, lg_bvh_node* __restrict__ tn, int* __restrict__ cid2,
+                                   Box* __restrict__ cbox2)
+{
+    const int c = cur[0], node_base = cur[1];
     const int i = blockIdx.x * kTB + threadIdx.x;
     if (i >= c) return;
-    const int j = nn[i];
-    const bool mutual = j >= 0 && nn[j] == i;
-    mflag[i] = (mutual && i < j) ? 1 : 0;   // i owns the merged node
-    kflag[i] = (mutual && i > j) ? 0 : 1;   // j's partner disappears
-}
-__global__ void merge_kernel(const int* __restrict__ nn, const int* __restrict__ dstate,
-                             const int* __restrict__ mflag, const int* __restrict__ midx, int* __restrict__ cid,
-                             Box* __restrict__ cbox, lg_bvh_node* __restrict__ tn)
-{
-    const int c = dstate[0], node_base = dstate[1];
-    const int i = blockIdx.x * kTB + threadIdx.x;
-    if (i >= c || !mflag[i]) return;
-    const int j = nn[i];
-    const int id = node_base + midx[i];
-    const Box b = join(cbox[i], cbox[j]);
-    lg_bvh_node nd;
-    nd.bbMin[0] = b.lo.x; nd.bbMin[1] = b.lo.y; nd.bbMin[2] = b.lo.z;
-    nd.bbMax[0] = b.hi.x; nd.bbMax[1] = b.hi.y; nd.bbMax[2] = b.hi.z;
-    nd.left = cid[i];
-    nd.right = cid[j];
-    nd.firstTri = -1;
-    nd.triCount = 0;
-    tn[id] = nd;
-    cid[i] = id;
-    cbox[i] = b;
-}
-__global__ void compact_kernel(const int* __restrict__ kflag, const int* __restrict__ kpos, const int* __restrict__ dc,
-                               const int* __restrict__ cid, const Box* __restrict__ cbox, int* __restrict__ cid2,
-                               Box* __restrict__ cbox2)
-{
-    const int c = *dc;
-    const int i = blockIdx.x * kTB + threadIdx.x;
-    if (i >= c || !kflag[i]) return;
-    cid2[kpos[i]] = cid[i];
-    cbox2[kpos[i]] = cbox[i];
-}
-
-// End of a clustering round: state = {c, next node id, error}; totals = {merges, kept clusters}.  A round that
-// merges nothing while more than one cluster is left marks the error (rounds after the last merge are no-ops).
-__global__ void round_end_kernel(int* __restrict__ state, const int* __restrict__ totals)
-{
-    if (state[0] > 1 && totals[0] == 0) state[2] = 1;
-    state[1] += totals[0];
-    state[0] = totals[1];
+    int id = cid[i];
+    Box b = cbox[i];
+    if (mflag[i])
+    {
+        // merge with the mutual nearest neighbour j > i (j keeps nothing and writes nothing this round)
+        const int j = nn[i];
+        id = node_base + msums[blockIdx.x] + midx[i];
+        const Box bj = cbox[j];
+        b = join(b, bj);
+        lg_bvh_node nd;
+        nd.bbMin[0] = b.lo.x; nd.bbMin[1] = b.lo.y; nd.bbMin[2] = b.lo.z;
+        nd.bbMax[0] = b.hi.x; nd.bbMax[1] = b.hi.y; nd.bbMax[2] = b.hi.z;
+        nd.left = cid[i];
+        nd.right = cid[j];
+        nd.firstTri = -1;
+        nd.triCount = 0;
+        tn[id] = nd;
+    }
+    if (kflag[i])
+    {
+        const int pos = ksums[blockIdx.x] + kpos[i];
+        cid2[pos] = id;
+        cbox2[pos] = b;
+    }
 }
 
 struct Scratch
@@ -353,7 +393,7 @@ size_t render_tree_scratch_bytes(int n_nodes, int n_tris)
     b += 3 * a256(t * 4);                       // leaf_at, flag, pos
     b += 2 * (a256(L * 4) + a256(L * sizeof(Box)));  // cluster arrays (double buffered)
     b += 5 * a256(L * 4);                       // nn, mflag, midx, kflag, kpos
-    b += a256((L / kTB + 2) * 4) + 256;         // block sums, totals
+    b += a256(2 * (L / kTB + 2) * 4) + 256;     // block sums (merge and keep flags), totals
     return b + 1024;
 }
 
@@ -392,7 +432,7 @@ int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, const lg_triangle
         int* midx = s.take<int>((size_t)L);
         int* kflag = s.take<int>((size_t)L);
         int* kpos = s.take<int>((size_t)L);
-        int* sums = s.take<int>((size_t)t / kTB + 2);
+        int* sums = s.take<int>(2 * ((size_t)t / kTB + 2));
         int* totals = s.take<int>(64);
         if (!sums || !totals) return set_error(LG_ERR_CAPACITY, "render tree: scratch too small");
         int c = 0;
@@ -416,26 +456,29 @@ int build_render_tree(const lg_bvh_node* d_nodes, int n_nodes, const lg_triangle
         // Rounds run kRoundsPerCheck at a time on a device-held count, grids sized by the last count read back (an
         // upper bound: rounds only merge); the host reads the state between groups.
         constexpr int kRoundsPerCheck = 8;
-        int* state = totals + 8;  // {c, next node id, error}
+        int* sbuf[2] = {totals + 8, totals + 16};  // double-buffered state {c, next node id, error}
+        int* ksums = sums + ((size_t)t / kTB + 2);  // the keep flags' block sums beside the merge flags'
+        int cur = 0;
         int hstate[3] = {c, L, 0};
-        LG_TRY_CUDA(cudaMemcpyAsync(state, hstate, sizeof(hstate), cudaMemcpyHostToDevice, st));
+        LG_TRY_CUDA(cudaMemcpyAsync(sbuf[0], hstate, sizeof(hstate), cudaMemcpyHostToDevice, st));
         while (hstate[0] > 1)
         {
             const int gc = (hstate[0] + kTB - 1) / kTB;
             for (int k = 0; k < kRoundsPerCheck; ++k)
             {
-                nn_kernel<<<gc, kTB, 0, st>>>(cbox, state, nn);
-                merge_flags_kernel<<<gc, kTB, 0, st>>>(nn, state, mflag, kflag);
-                LG_TRY_CUDA(excl_scan_dev(mflag, state, hstate[0], midx, sums, totals, st));
-                LG_TRY_CUDA(excl_scan_dev(kflag, state, hstate[0], kpos, sums, totals + 1, st));
-                merge_kernel<<<gc, kTB, 0, st>>>(nn, state, mflag, midx, cid, cbox, tn);
-                compact_kernel<<<gc, kTB, 0, st>>>(kflag, kpos, state, cid, cbox, cid2, cbox2);
-                round_end_kernel<<<1, 1, 0, st>>>(state, totals);
+                const int* sc = sbuf[cur];
+                int* sn = sbuf[cur ^ 1];
+                nn_kernel<<<gc, kTB, 0, st>>>(cbox, sc, nn);
+                round_flags_kernel<<<gc, kTB, 0, st>>>(nn, sc, mflag, kflag, midx, kpos, sums, ksums);
+                round_sums_kernel<<<1, kTB, 0, st>>>(sums, ksums, gc, sc, sn);
+                round_apply_kernel<<<gc, kTB, 0, st>>>(nn, sc, mflag, kflag, midx, kpos, sums, ksums, cid, cbox, tn,
+                                                       cid2, cbox2);
                 LG_TRY_CUDA(cudaGetLastError());
                 int* ti = cid; cid = cid2; cid2 = ti;
                 Box* tb = cbox; cbox = cbox2; cbox2 = tb;
+                cur ^= 1;
             }
-            LG_TRY_CUDA(cudaMemcpyAsync(hstate, state, sizeof(hstate), cudaMemcpyDeviceToHost, st));
+            LG_TRY_CUDA(cudaMemcpyAsync(hstate, sbuf[cur], sizeof(hstate), cudaMemcpyDeviceToHost, st));
             LG_TRY_CUDA(cudaStreamSynchronize(st));
             if (hstate[2]) return set_error(LG_ERR_DEVICE, "render tree: a clustering round merged nothing");
         }
