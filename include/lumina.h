@@ -161,7 +161,11 @@ typedef struct {
 int lg_renderer_create(int device, lg_renderer** out);
 void lg_renderer_destroy(lg_renderer* r);
 /* Upload a scene and build its BVH on the device (triangles are reordered on
- * the device; host arrays are not modified). */
+ * the device; host arrays are not modified).  Every triangle's material index
+ * must lie in [0, n_mats): it is checked on the device after the upload, and
+ * a bad one returns LG_ERR_INVALID naming the first such triangle, with the
+ * renderer left without a scene (renders then miss everywhere) until the
+ * next successful call.  The same holds for lg_renderer_set_scene_bvh. */
 int lg_renderer_set_scene(lg_renderer* r, const lg_scene_desc* scene);
 /* Upload a scene whose triangles are already in BVH order with its node array. */
 int lg_renderer_set_scene_bvh(lg_renderer* r, const lg_scene_desc* scene, const lg_bvh_node* nodes, int32_t n_nodes);
