@@ -206,6 +206,9 @@ __global__ void __launch_bounds__(kWfThreads) wf_bounce_kernel(DevScene s, int n
 // leaf at a time (warp_step, leaves postponed) and take the next ray of
 // the list as soon as enough lanes are free, with no shading in between.
 constexpr int kWfListThreads = 256;
+// The staged bounce keeps a shadow ray, a contribution and a flag per (light, ray): 52 bytes per light and pixel.
+// Scenes with more lights than this trace their bounces one ray per thread instead.
+constexpr int kWfStagedLights = 8;
 
 // Ray i of a traversal list.  Closest hits (kAny false): the sorted ray
 // rays_in[order[i]], its origin and direction through make_ray as
@@ -501,7 +504,9 @@ cudaError_t staged_bounce(const DevScene& s, const WavefrontJob& job, int n, con
 
 size_t wavefront_scratch_bytes(int n_pixels, int n_lights)
 {
-    const size_t n = (size_t)(n_pixels > 0 ? n_pixels : 1), nl = (size_t)(n_lights > 0 ? n_lights : 1);
+    const size_t n = (size_t)(n_pixels > 0 ? n_pixels : 1);
+    // scenes with more lights than kWfStagedLights run the one-thread-per-ray bounce and need no per-light buffers
+    const size_t nl = (n_lights > kWfStagedLights) ? 0 : (size_t)(n_lights > 0 ? n_lights : 1);
     const size_t a = 256;
     auto up = [&](size_t b) { return (b + a - 1) / a * a; };
     return 2 * up(n * sizeof(WfRay)) + 5 * up(n * sizeof(uint32_t)) + up(radix_sort_scratch_bytes(n)) +
@@ -516,6 +521,8 @@ cudaError_t launch_wavefront_frame(const DevScene& s, const DevCam& cam, const W
     if (n <= 0 || job.spp <= 0) return cudaSuccess;
     const int nl = s.n_points + 1;
     if (scratch_bytes < wavefront_scratch_bytes(n, nl)) return cudaErrorInvalidValue;
+    const bool staged = !job.counters && nl <= kWfStagedLights;
+    const size_t snl = staged ? (size_t)nl : 0;  // per-light buffers only for the staged launch
     const size_t a = 256;
     auto up = [&](size_t b) { return (b + a - 1) / a * a; };
     char* p = (char*)(((uintptr_t)scratch + a - 1) & ~(uintptr_t)(a - 1));
@@ -533,10 +540,10 @@ cudaError_t launch_wavefront_frame(const DevScene& s, const DevCam& cam, const W
     Staged sb;
     sb.hit = (int4*)p; p += up((size_t)n * sizeof(int4));
     sb.surf = (float4*)p; p += up(3 * (size_t)n * sizeof(float4));
-    sb.so = (float4*)p; p += up((size_t)nl * n * sizeof(float4));
-    sb.sd = (float4*)p; p += up((size_t)nl * n * sizeof(float4));
-    sb.sc = (float4*)p; p += up((size_t)nl * n * sizeof(float4));
-    sb.occ = (int*)p; p += up((size_t)nl * n * sizeof(int));
+    sb.so = (float4*)p; p += up(snl * n * sizeof(float4));
+    sb.sd = (float4*)p; p += up(snl * n * sizeof(float4));
+    sb.sc = (float4*)p; p += up(snl * n * sizeof(float4));
+    sb.occ = (int*)p; p += up(snl * n * sizeof(int));
     sb.work = (unsigned long long*)p;
     const int blocks = (n + kWfThreads - 1) / kWfThreads;
     cudaError_t e = cudaSuccess;
@@ -549,11 +556,12 @@ cudaError_t launch_wavefront_frame(const DevScene& s, const DevCam& cam, const W
         for (int b = 0; b <= job.max_bounces && e == cudaSuccess; ++b)
         {
             const bool last = b == job.max_bounces;
-            // counting runs the one-thread-per-ray launch, which counts as it traverses
-            e = job.counters ? bounce(s, job.width, job.watertight, true, n, rays[cur], slots[cur], job.accum,
-                                      rays[cur ^ 1], keys[cur ^ 1], slots[cur ^ 1], rng, last, job.counters, st)
-                             : staged_bounce(s, job, n, rays[cur], slots[cur], rays[cur ^ 1], keys[cur ^ 1],
-                                             slots[cur ^ 1], rng, last, sb, st);
+            // counting runs the one-thread-per-ray launch, which counts as it traverses; so do scenes with many
+            // lights (the staged launch's per-light buffers grow with them)
+            e = staged ? staged_bounce(s, job, n, rays[cur], slots[cur], rays[cur ^ 1], keys[cur ^ 1], slots[cur ^ 1], rng,
+                                       last, sb, st)
+                       : bounce(s, job.width, job.watertight, job.counters != nullptr, n, rays[cur], slots[cur],
+                                job.accum, rays[cur ^ 1], keys[cur ^ 1], slots[cur ^ 1], rng, last, job.counters, st);
             if (last || e != cudaSuccess) break;
             if (job.sort) e = radix_sort_pairs(keys[cur ^ 1], slots[cur ^ 1], (size_t)n, 0, 32, rs, st);
             cur ^= 1;

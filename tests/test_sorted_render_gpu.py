@@ -117,6 +117,22 @@ def test_staged_bounces_match_one_thread_per_ray(small_engine_scene, wt):
             assert match_fraction(a, b) >= 0.999
 
 
+def test_many_lights_trace_one_ray_per_thread(box_scene):
+    """Scenes with more than 8 lights (the sun and the point lights) keep the
+    one-thread-per-ray bounce, which needs no per-light buffers: the frame
+    renders and matches the counting launch bit for bit (same kernel)."""
+    pts = np.concatenate([box_scene.points] * 9)
+    sc = lumina.Scene(box_scene.camera, box_scene.sun, box_scene.tris, box_scene.mat_albedo, box_scene.mat_emissive,
+                      pts)
+    with lumina.Renderer(0) as r:
+        r.set_scene(sc)
+        b = r.render_sorted(spp=2, bounces=1)["accum"]
+        r.set_counting(True)
+        a = r.render_sorted(spp=2, bounces=1)
+    assert a["shadow_rays"] > 0 and b.any()
+    assert np.array_equal(a["accum"], b)
+
+
 def _png(path):
     from PIL import Image
     return np.asarray(Image.open(path).convert("RGB"))
