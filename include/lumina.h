@@ -401,6 +401,16 @@ int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_
  * the kernel p selects (0: one tile per CTA, 1: persistent; 2 only with an
  * explicit shape compiled for it). */
 int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles);
+/* Folded upsampling (on by default): in inference passes of a network with
+ * nearest upsampling, u3a, u2a and u1a read the upsampled half of their input
+ * as the lower level's output repeated along x only, and sum the row taps
+ * that meet the same low-resolution row (even output rows: ky1 + ky2, odd:
+ * ky0 + ky1), where their tile has that form (kernel choices 6 and 7 with at
+ * most 64 output channels per CTA).  Same network function; the folded
+ * weights are rounded to BF16 after the sum, so outputs differ from the
+ * unfolded pass by BF16 rounding.  Training passes never fold.  on = 0 turns
+ * it off (e.g. to compare against the unfolded pass). */
+int lg_unet_set_fold_upsampling(lg_unet* u, int on);
 /* One 3x3 convolution layer on device buffers in the channel-blocked BF16
  * layout ((n*C/8 + c/8)*H + y)*W + x)*8 + c%8: epilogue 0 writes act(conv+b)
  * into channels [out_coff, out_coff+cout) of d_out (and, if d_out2, the 2x2

@@ -83,15 +83,33 @@ int ensure_acts(lg_unet* u, int N, int H, int W)
     return LG_OK;
 }
 
+// Upsampled channels at the front of decoder conv i's input (u3a, u2a, u1a: cat(up, skip)); 0 otherwise.
+int up_channels(int i) { return (i == 8 || i == 10 || i == 12) ? kLayers[i].cin - kLayers[i].cout : 0; }
+
+// Whether decoder conv i runs its folded-upsampling form in inference: nearest upsampling and a tile that has one.
+bool folds(const lg_unet* u, int i)
+{
+    return u->fold_up && !u->bilinear && up_channels(i) > 0 &&
+           conv_tile_folds(u->tile[i], kLayers[i].cin, kLayers[i].cout, up_channels(i));
+}
+
 int pack_all_impl(lg_unet* u)
 {
     if (u->packed_ok) return LG_OK;
     for (int i = 0; i < 14; ++i)
     {
         const LayerDef& L = kLayers[i];
+        const float* w = (const float*)u->params.p + u->w_off[i];
         LG_TRY(u->packed[i].ensure(conv_packed_elems(L.cin, L.cout) * sizeof(__nv_bfloat16)));
-        LG_TRY_CUDA(conv_pack_weights((const float*)u->params.p + u->w_off[i], L.cout, layer_cin_real(u, i), L.cin,
-                                      (__nv_bfloat16*)u->packed[i].p, u->stream, u->tile[i]));
+        LG_TRY_CUDA(conv_pack_weights(w, L.cout, layer_cin_real(u, i), L.cin, (__nv_bfloat16*)u->packed[i].p,
+                                      u->stream, u->tile[i]));
+        if (folds(u, i))
+        {
+            const int uc = up_channels(i);
+            LG_TRY(u->packed_fold[i].ensure(conv_packed_elems_folded(L.cin, L.cout, uc) * sizeof(__nv_bfloat16)));
+            LG_TRY_CUDA(conv_pack_weights_folded(w, L.cout, L.cin, uc, (__nv_bfloat16*)u->packed_fold[i].p,
+                                                 u->stream, u->tile[i]));
+        }
     }
     u->packed_ok = true;
     return LG_OK;
@@ -127,9 +145,18 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     LG_TRY_CUDA(cudaMemsetAsync(u->err.p, 0, sizeof(int), st));
     LG_TRY_CUDA(to_blocked_bf16(d_x, N, u->in_ch, H, W, (bf*)u->x0.p, 16, st, u->log_hdr, true));
     const int H2 = H / 2, W2 = W / 2, H4 = H / 4, W4 = W / 4, H8 = H / 8, W8 = W / 8;
+    // inference with nearest upsampling: u3a, u2a, u1a fold their upsampled inputs where their tiles allow
+    const bool fold = !keep_u1;
     auto run = [&](int layer, const void* in, int h, int w, int epi, void* out, int out_c, int out_coff, void* out2,
-                   int out2_c, int out2_coff) -> int {
+                   int out2_c, int out2_coff, const void* up_h = nullptr, int x_only = 0) -> int {
         ConvArgs a = base_args(u, layer, N, h, w);
+        a.up_x_only = x_only;
+        if (up_h)
+        {
+            a.up_h = (const bf*)up_h;
+            a.up_C = up_channels(layer);
+            a.wpack = (const bf*)u->packed_fold[layer].p;
+        }
         a.epilogue = epi;
         a.out = (bf*)out;
         a.out_C = out_c;
@@ -163,19 +190,28 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     // The conv before each upsampling writes its output 2x upsampled into the
     // first channels of the next level's concat buffer: nearest copies in its
     // epilogue, or (bilinear) a stored low-resolution result and a resampling pass.
-    auto up = [&](int layer, const void* in, int h, int w, Buf& lo, int c, void* cat, int cat_c) -> int {
+    // With folding, the conv before the upsampling writes its output upsampled along x only (uh, h x 2w) and
+    // the next level's first conv reads it there instead of the concat buffer's upsampled half.
+    const size_t px = (size_t)N * H * W;
+    if (fold && folds(u, 8)) LG_TRY(u->uh3.ensure(px / 32 * 256 * sizeof(bf)));
+    if (fold && folds(u, 10)) LG_TRY(u->uh2.ensure(px / 8 * 128 * sizeof(bf)));
+    if (fold && folds(u, 12)) LG_TRY(u->uh1.ensure(px / 2 * 64 * sizeof(bf)));
+    auto up = [&](int layer, const void* in, int h, int w, Buf& lo, int c, void* cat, int cat_c, Buf& uh) -> int {
+        if (fold && folds(u, layer + 1))
+            return run(layer, in, h, w, kEpiUpsample, uh.p, c, 0, nullptr, 0, 0, nullptr, 1);
         if (!u->bilinear) return run(layer, in, h, w, kEpiUpsample, cat, cat_c, 0, nullptr, 0, 0);
         LG_TRY(run(layer, in, h, w, kEpiStore, lo.p, c, 0, nullptr, 0, 0));
         LG_TRY_CUDA(bilinear_up2((const bf*)lo.p, N, c, h, w, (bf*)cat, cat_c, 0, st));
         return LG_OK;
     };
-    LG_TRY(up(7, u->t4.p, H8, W8, u->lo7, 256, u->cat3.p, 384));
+    LG_TRY(up(7, u->t4.p, H8, W8, u->lo7, 256, u->cat3.p, 384, u->uh3));
     // decoder
-    LG_TRY(run(8, u->cat3.p, H4, W4, kEpiStore, u->t5.p, 128, 0, nullptr, 0, 0));
-    LG_TRY(up(9, u->t5.p, H4, W4, u->lo9, 128, u->cat2.p, 192));
-    LG_TRY(run(10, u->cat2.p, H2, W2, kEpiStore, u->t6.p, 64, 0, nullptr, 0, 0));
-    LG_TRY(up(11, u->t6.p, H2, W2, u->lo11, 64, u->cat1.p, 96));
-    LG_TRY(run(12, u->cat1.p, H, W, kEpiStore, u->t7.p, 32, 0, nullptr, 0, 0));
+    auto uh_of = [&](int layer, Buf& uh) -> const void* { return fold && folds(u, layer) ? uh.p : nullptr; };
+    LG_TRY(run(8, u->cat3.p, H4, W4, kEpiStore, u->t5.p, 128, 0, nullptr, 0, 0, uh_of(8, u->uh3)));
+    LG_TRY(up(9, u->t5.p, H4, W4, u->lo9, 128, u->cat2.p, 192, u->uh2));
+    LG_TRY(run(10, u->cat2.p, H2, W2, kEpiStore, u->t6.p, 64, 0, nullptr, 0, 0, uh_of(10, u->uh2)));
+    LG_TRY(up(11, u->t6.p, H2, W2, u->lo11, 64, u->cat1.p, 96, u->uh1));
+    LG_TRY(run(12, u->cat1.p, H, W, kEpiStore, u->t7.p, 32, 0, nullptr, 0, 0, uh_of(12, u->uh1)));
     LG_TRY(run(13, u->t7.p, H, W, kEpiTail, keep_u1 ? u->u1.p : nullptr, 32, 0, nullptr, 0, 0));
     return LG_OK;
 }
@@ -243,8 +279,10 @@ void lg_unet_destroy(lg_unet* u)
     for (auto& b : u->packed) b.release();
     for (Buf* b : {&u->x0, &u->t1, &u->cat1, &u->p1, &u->t2, &u->cat2, &u->p2, &u->t3, &u->cat3, &u->p3, &u->t4,
                    &u->t5, &u->t6, &u->t7, &u->u1, &u->xin, &u->yout, &u->err, &u->grads, &u->adam_m, &u->adam_v,
-                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt, &u->lo7, &u->lo9, &u->lo11, &u->gup, &u->wpart, &u->bpart, &u->tpart})
+                   &u->loss, &u->gs1, &u->gs2, &u->gs3, &u->tgt, &u->lo7, &u->lo9, &u->lo11, &u->gup, &u->wpart, &u->bpart, &u->tpart,
+                   &u->uh1, &u->uh2, &u->uh3})
         b->release();
+    for (auto& b : u->packed_fold) b.release();
     for (auto& b : u->packed_dg) b.release();
     for (auto& b : u->dz) b.release();
     if (u->probe_ev0) cudaEventDestroy(u->probe_ev0);

@@ -385,9 +385,10 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
                     }
                 }
             }
-            else  // kEpiUpsample: nearest 2x into a 2H x 2W buffer
+            else  // kEpiUpsample: nearest 2x into a 2H x 2W buffer (H x 2W with up_x_only)
             {
-                const int H2 = a.H * 2, W2 = a.W * 2;
+                const int ry = a.up_x_only ? 1 : 2;
+                const int H2 = a.H * ry, W2 = a.W * 2;
 #pragma unroll
                 for (int r = 0; r < kRows; ++r)
                 {
@@ -395,11 +396,10 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
                     if (!xin || y >= a.H) continue;
                     const uint4 lo = pack8(v[r]), hi = pack8(v[r] + 8);
                     // pixels 2x and 2x+1 are 32 contiguous bytes of a channel plane: one store each
-#pragma unroll
-                    for (int i = 0; i < 2; ++i)
+                    for (int i = 0; i < ry; ++i)
                     {
-                        tc::st_global_v8(blk(a.out, a.out_C, H2, W2, n, b0, 2 * y + i, 2 * x), lo, lo);
-                        tc::st_global_v8(blk(a.out, a.out_C, H2, W2, n, b0 + 1, 2 * y + i, 2 * x), hi, hi);
+                        tc::st_global_v8(blk(a.out, a.out_C, H2, W2, n, b0, ry * y + i, 2 * x), lo, lo);
+                        tc::st_global_v8(blk(a.out, a.out_C, H2, W2, n, b0 + 1, ry * y + i, 2 * x), hi, hi);
                     }
                 }
             }
@@ -576,11 +576,26 @@ struct PSmem
         return stages * kStage + kBarBytes + (RESW ? KB * S::kBBytes : 0) + 1024;
     }
 };
-template <int BN, int KC, int STAGES, bool RESW, int ROWS = kRows, bool DYP = false>
-__global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __grid_constant__ CUtensorMap tmap, ConvArgs a)
+// Folded upsampling (VUP): the first up_C input channels are the nearest 2x
+// upsampling of a low-resolution tensor, read as up_h (upsampled along x
+// only, H/2 rows).  Output row y reads upsampled rows y-1, y, y+1, which are
+// low-resolution rows (y-1)/2, y/2, (y+1)/2: two distinct rows, so the row
+// taps fold per parity (even y = 2r: ky0 on row r-1, ky1+ky2 on row r; odd
+// y = 2r+1: ky0+ky1 on row r, ky2 on row r+1).  Low-resolution row h then
+// reaches the four consecutive output rows 2h-1 .. 2h+2 with weights ky2,
+// ky1+ky2, ky0+ky1, ky0: one MMA with N = 4*BN per (row, column tap, K
+// step), over ROWS/2 + 2 low-resolution rows instead of ROWS + 2 upsampled
+// ones (two thirds of the MMA work, half the rows loaded).  The skip
+// channels' K-blocks run first, as in the DYP kernel, so every output row
+// is initialised before the folded ones accumulate.
+template <int BN, int KC, int STAGES, bool RESW, int ROWS = kRows, bool DYP = false, bool VUP = false>
+__global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __grid_constant__ CUtensorMap tmap,
+                                                                      const __grid_constant__ CUtensorMap tmap2,
+                                                                      ConvArgs a)
 {
     static_assert(ROWS == 2 || ROWS == 4 || ROWS == 8, "2-, 4- or 8-row tiles");
     static_assert(!DYP || 3 * BN <= 256, "row taps packed into N need 3 * BN <= 256");
+    static_assert(!VUP || (DYP && !RESW && ROWS >= 4 && 4 * BN <= 256), "folded upsampling: streamed DYP, 4*BN <= 256");
     // DYP kernels load their A tiles through the chunked view (make_map_chunked)
     constexpr int AX = DYP ? kChunkX : kHaloX;  // pixels per halo row in shared memory
     constexpr int AX0 = DYP ? 7 : 0;            // position of pixel x0 - 1 in a halo row
@@ -605,6 +620,12 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
     const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + ROWS - 1) / ROWS;
     const int n_tiles = tiles_x * tiles_y * a.N * n_cot;
     const int KB = a.Cin / KC;
+    const int KBS = VUP ? (a.Cin - a.up_C) / KC : KB;  // K-blocks of `in` (the skip channels, with VUP)
+    constexpr int kRowsU = ROWS / 2 + 2;                 // VUP: low-resolution rows of a tile
+    constexpr uint32_t kAUBytes = (uint32_t)(kRowsU * AX * KC * 2), kBUBytes = (uint32_t)(12 * KC * BN * 2);
+    static_assert(!VUP || kAUBytes + kBUBytes <= (uint32_t)P::kStage, "a folded K-block must fit a stage");
+    constexpr uint32_t kLboAU = kRowsU * AX * 16, kLboBU = 4 * BN * 16;
+    constexpr uint32_t kIdesc4 = tc::idesc_bf16_f32(128, VUP ? 4 * BN : BN);
     constexpr uint32_t kAccCols = ROWS * BN;   // one accumulator: ROWS rows x BN FP32 columns
     constexpr uint32_t kCols = 2 * kAccCols;  // two of them (a power of two >= 32 for BN >= 16)
     static_assert(kCols <= 512, "two accumulators must fit in TMEM");
@@ -671,7 +692,8 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
             {
                 int n, ct, x0, y0;
                 coords(t, n, ct, x0, y0);
-                const __nv_bfloat16* wsrc = a.wpack + (size_t)ct * KB * (9 * KC * BN);
+                const __nv_bfloat16* wsrc =
+                    a.wpack + (size_t)ct * (KBS * (9 * KC * BN) + (KB - KBS) * (12 * KC * BN));
                 for (int kb = 0; kb < KB; ++kb, ++it)
                 {
                     const int s = it % STAGES, u = it / STAGES;
@@ -684,7 +706,16 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                     // x coordinate: pixel x0 - 1; for the 144-pixel rows of the DYP
                     // kernels pixel x0 - 8, or the 8-pixel run that starts there
                     const int ax = DYP ? (a.a_chunked ? x0 / 8 - 1 : x0 - 8) : x0 - 1;
-                    if (RESW)
+                    if (VUP && kb >= KBS)
+                    {
+                        // low-resolution rows y0/2 - 1 .. y0/2 + ROWS/2 of up_h, then the K-block's folded weights
+                        uint8_t* B = A + kAUBytes;
+                        tc::mbar_expect_tx(&full[s], kAUBytes + kBUBytes);
+                        tc::tma_load_5d(A, &tmap2, &full[s], 0, ax, y0 / 2 - 1, (kb - KBS) * (KC / 8), n);
+                        tc::bulk_load(B, wsrc + (size_t)KBS * (9 * KC * BN) + (size_t)(kb - KBS) * (12 * KC * BN),
+                                      kBUBytes, &full[s]);
+                    }
+                    else if (RESW)
                     {
                         tc::mbar_expect_tx(&full[s], (uint32_t)S::kABytes);
                         tc::tma_load_5d(A, &tmap, &full[s], 0, ax, y0 - 1, kb * (KC / 8), n);
@@ -693,7 +724,7 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                     {
                         uint8_t* B = A + S::kABytes;
                         tc::mbar_expect_tx(&full[s], (uint32_t)(S::kABytes + S::kBBytes));
-                        tc::tma_load_5d(A, &tmap, &full[s], 0, ax, y0 - 1, kb * (KC / 8), n);
+                        tc::tma_load_5d(A, &tmap, &full[s], 0, ax, y0 - 1, (VUP ? a.up_C / 8 : 0) + kb * (KC / 8), n);
                         tc::bulk_load(B, wsrc + (size_t)kb * (9 * KC * BN), (uint32_t)S::kBBytes, &full[s]);
                     }
                 }
@@ -729,7 +760,35 @@ __global__ void __launch_bounds__(kPThreads, 1) conv3x3_tc_persistent(const __gr
                     const uint32_t abase = tc::smem_u32(smem + s * P::kStage);
                     const uint32_t bbase =
                         RESW ? tc::smem_u32(wres) + (uint32_t)(kb * S::kBBytes) : abase + (uint32_t)S::kABytes;
-                    if (DYP)
+                    if (VUP && kb >= KBS)
+                    {
+                        // folded K-block: weights [dx][KC/8][ky2 | ky1+ky2 | ky0+ky1 | ky0][BN][8]; low-resolution
+                        // row h of the tile reaches output rows 2h-3+s (slot s) of those inside the tile
+                        const uint32_t ubase = abase + kAUBytes;
+#pragma unroll 1
+                        for (int h = 0; h < kRowsU; ++h)
+                        {
+                            const int smin = h == 0 ? 3 : (h == 1 ? 1 : 0);
+                            const int smax = ROWS + 2 - 2 * h < 3 ? ROWS + 2 - 2 * h : 3;
+                            const int nb = smax - smin + 1;
+                            const uint32_t id = nb == 4 ? kIdesc4 : nb == 3 ? kIdesc3 : (nb == 2 ? kIdesc2 : kIdesc);
+                            const uint32_t dcol = acc + (uint32_t)((2 * h - 3 + smin) * BN);
+#pragma unroll
+                            for (int dx = 0; dx < 3; ++dx)
+#pragma unroll
+                                for (int ks = 0; ks < KC / 16; ++ks)
+                                {
+                                    const uint32_t aoff =
+                                        (uint32_t)(2 * ks) * kLboAU + (uint32_t)((h * AX + AX0 + dx) * 16);
+                                    const uint64_t ad = tc::smem_desc(abase + aoff, kLboAU, 128);
+                                    const uint32_t plane = ubase + (uint32_t)((dx * (KC / 8) + 2 * ks) * kLboBU);
+                                    const uint64_t bd =
+                                        tc::smem_desc(plane + (uint32_t)(smin * BN * 16), kLboBU, 128);
+                                    tc::mma_bf16(dcol, ad, bd, id, 1u);
+                                }
+                        }
+                    }
+                    else if (DYP)
                     {
                         // weights of K-block kb: [dx][KC/8][dy = 2, 1, 0][BN][8]
 #pragma unroll 1
@@ -898,21 +957,31 @@ cudaError_t make_map_chunked(CUtensorMap* m, const __nv_bfloat16* base, int N, i
 // for the kernel's static shared memory (the epilogue constants, 1.4 KB).
 constexpr int kMaxSmem = 225 * 1024;
 
-template <int BN, int KC, int STAGES, bool RESW = false, int ROWS = kRows, bool DYP = false>
+template <int BN, int KC, int STAGES, bool RESW = false, int ROWS = kRows, bool DYP = false, bool VUP = false>
 cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
 {
     const int KB = a.Cin / KC;
     if (RESW && a.Cout != BN) return cudaErrorInvalidValue;  // one output block only
+    if (VUP != (a.up_C > 0)) return cudaErrorInvalidValue;
+    // folded upsampling: both parts whole K-blocks, at least one skip K-block first, even rows
+    if (VUP && (!a.up_h || a.up_C % KC || a.Cin - a.up_C < KC || (a.H & 1))) return cudaErrorInvalidValue;
     const int smem = PSmem<BN, KC, RESW, ROWS, DYP ? kChunkX : kHaloX>::bytes(STAGES, KB);
     if (smem > kMaxSmem) return cudaErrorInvalidValue;
-    CUtensorMap m;
+    CUtensorMap m, m2;
     ConvArgs b = a;
     b.a_chunked = DYP && a.W % 8 == 0;
     cudaError_t e = !DYP ? make_map(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2)
                     : b.a_chunked ? make_map_chunked(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2)
                                   : make_map(&m, in, a.N, a.Cin, a.H, a.W, KC, ROWS + 2, kChunkX);
     if (e != cudaSuccess) return e;
-    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW, ROWS, DYP>;
+    m2 = m;
+    if (VUP)
+    {
+        e = b.a_chunked ? make_map_chunked(&m2, a.up_h, a.N, a.up_C, a.H / 2, a.W, KC, ROWS / 2 + 2)
+                        : make_map(&m2, a.up_h, a.N, a.up_C, a.H / 2, a.W, KC, ROWS / 2 + 2, kChunkX);
+        if (e != cudaSuccess) return e;
+    }
+    auto fn = conv3x3_tc_persistent<BN, KC, STAGES, RESW, ROWS, DYP, VUP>;
     // The resident-weights form's smem depends on KB: size the attribute for
     // the largest launch it may see and query occupancy per launch size.
     static bool attr_done = false;
@@ -935,7 +1004,7 @@ cudaError_t launch_persistent(const __nv_bfloat16* in, const ConvArgs& a, cudaSt
     if (per_sm < 1) per_sm = 1;
     const long long tiles = (long long)((a.W + kTileX - 1) / kTileX) * ((a.H + ROWS - 1) / ROWS) * a.N * (a.Cout / BN);
     const long long grid = std::min<long long>(tiles, (long long)per_sm * sm_count);
-    fn<<<(unsigned)grid, kPThreads, smem, stream>>>(m, b);
+    fn<<<(unsigned)grid, kPThreads, smem, stream>>>(m, m2, b);
     return cudaGetLastError();
 }
 
@@ -996,6 +1065,45 @@ __global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real,
     const int ci = kb * KC + kc8 * 8 + e;
     float v = 0.0f;
     if (ci < Cin_real) v = w[(((size_t)co * Cin_real + ci) * 3 + tap / 3) * 3 + tap % 3];
+    out[i] = __float2bfloat16_rn(v);
+}
+
+// Folded-upsampling weights (conv_pack_weights_folded): per output block,
+// the skip channels up_C..Cin-1 in the DYP layout, then the upsampled
+// channels 0..up_C-1 as (kb, dx, kc8, slot, j, e) with the four folded row
+// taps of output rows 2h-1 .. 2h+2: ky2, ky1 + ky2, ky0 + ky1, ky0 (summed in
+// FP32, rounded once).
+__global__ void pack_folded_kernel(const float* __restrict__ w, int Cout, int Cin, int up_C, int BN, int KC,
+                                   __nv_bfloat16* __restrict__ out, size_t total)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int KBS = (Cin - up_C) / KC;
+    const size_t skip_elems = (size_t)KBS * 9 * KC * BN;
+    const size_t per_ct = skip_elems + (size_t)(up_C / KC) * 12 * KC * BN;
+    const int ct = (int)(i / per_ct);
+    size_t r = i % per_ct;
+    float v;
+    if (r < skip_elems)
+    {
+        int ct0, kb, tap, kc8, j, e;
+        packed_index(r, BN, KC, KBS, true, ct0, kb, tap, kc8, j, e);
+        const int co = ct * BN + j, ci = up_C + kb * KC + kc8 * 8 + e;
+        v = w[(((size_t)co * Cin + ci) * 3 + tap / 3) * 3 + tap % 3];
+    }
+    else
+    {
+        r -= skip_elems;
+        const int e = (int)(r % 8); r /= 8;
+        const int j = (int)(r % BN); r /= BN;
+        const int slot = (int)(r % 4); r /= 4;
+        const int kc8 = (int)(r % (KC / 8)); r /= (KC / 8);
+        const int dx = (int)(r % 3); r /= 3;
+        const int kb = (int)r;
+        const int co = ct * BN + j, ci = kb * KC + kc8 * 8 + e;
+        const float* wk = w + ((size_t)co * Cin + ci) * 9 + dx;  // wk[3 * ky]
+        v = slot == 0 ? wk[6] : slot == 1 ? wk[3] + wk[6] : slot == 2 ? wk[0] + wk[3] : wk[0];
+    }
     out[i] = __float2bfloat16_rn(v);
 }
 
@@ -1111,6 +1219,31 @@ cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin,
     return cudaGetLastError();
 }
 
+size_t conv_packed_elems_folded(int Cin, int Cout, int up_C)
+{
+    return (size_t)9 * (Cin - up_C) * Cout + (size_t)12 * up_C * Cout;
+}
+
+bool conv_tile_folds(ConvTile tile, int Cin, int Cout, int up_C)
+{
+    const TileCfg c = resolve(tile, Cin, Cout);
+    const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    const bool compiled = (c.persist == 7 && key == 32322) || (c.persist == 6 && (key == 64322 || key == 32323));
+    return compiled && up_C > 0 && up_C % c.kc == 0 && Cin - up_C >= c.kc && (Cin - up_C) % c.kc == 0 &&
+           Cout % c.bn == 0;
+}
+
+cudaError_t conv_pack_weights_folded(const float* d_w, int Cout, int Cin, int up_C, __nv_bfloat16* d_packed,
+                                     cudaStream_t stream, ConvTile tile)
+{
+    if (!conv_tile_folds(tile, Cin, Cout, up_C)) return cudaErrorInvalidValue;
+    const TileCfg c = resolve(tile, Cin, Cout);
+    const size_t total = conv_packed_elems_folded(Cin, Cout, up_C);
+    pack_folded_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin, up_C, c.bn, c.kc,
+                                                                            d_packed, total);
+    return cudaGetLastError();
+}
+
 cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
                                     __nv_bfloat16* d_packed, cudaStream_t stream, ConvTile tile)
 {
@@ -1133,6 +1266,13 @@ cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStre
     const TileCfg c = resolve(a.tile, a.Cin, a.Cout);
     if (a.Cout % c.bn || a.Cin % c.kc) return cudaErrorInvalidValue;
     const int key = c.bn * 1000 + c.kc * 10 + c.stages;
+    if (a.up_C > 0)
+    {
+        if (!conv_tile_folds(c, a.Cin, a.Cout, a.up_C)) return cudaErrorInvalidValue;
+        if (c.persist == 7) return launch_persistent<32, 32, 2, false, 8, true, true>(in, a, stream);
+        if (key == 64322) return launch_persistent<64, 32, 2, false, 4, true, true>(in, a, stream);
+        return launch_persistent<32, 32, 3, false, 4, true, true>(in, a, stream);
+    }
     if (c.persist == 7)
         switch (key)
         {

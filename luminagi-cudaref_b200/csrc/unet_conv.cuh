@@ -20,7 +20,7 @@ namespace lg
 enum ConvEpilogue : int
 {
     kEpiStore = 0,     // act(acc + bias) -> out (and, if out2, 2x2 max-pooled -> out2)
-    kEpiUpsample = 1,  // act(acc + bias) -> out at 2x resolution (nearest, 4 copies)
+    kEpiUpsample = 1,  // act(acc + bias) -> out at 2x resolution (nearest, 4 copies; 2 along x with up_x_only)
     kEpiTail = 2,      // act(acc + bias) -> out (optional); 1x1 conv to 3 + residual + clamp -> final (FP32 NCHW)
                        // (log_hdr: residual on log1p(input), out = expm1(max(y, 0)))
     // Backward (input-gradient) epilogues; no bias is added.
@@ -72,10 +72,28 @@ struct ConvArgs
     int skip_C, skip_coff;
     ConvTile tile;               // {0, 0, 0}: default; must match the tile the weights were packed with
     int a_chunked;               // set by the launcher: the A map is the 8-pixel-run view (W % 8 == 0)
+    // Folded upsampling (inference form of a decoder conv whose input is cat([up2(lo), skip]) with nearest
+    // 2x upsampling): with up_C > 0 the first up_C input channels are read from up_h, the low-resolution
+    // tensor upsampled along x only (blocked, N x up_C x H/2 x W), and the row taps are folded per output-row
+    // parity (conv_pack_weights_folded); the skip channels are read from `in` (channels up_C..Cin-1).
+    const __nv_bfloat16* up_h;
+    int up_C;
+    int up_x_only;               // kEpiUpsample: write the 2x-along-x copy only (out is N x out_C x H x 2W)
 };
 
 // Bytes of packed weights for a layer (BF16).
 size_t conv_packed_elems(int Cin, int Cout);
+// The same for the folded-upsampling form (ConvArgs::up_C): the up_C upsampled channels carry four
+// folded row taps per column tap instead of three.
+size_t conv_packed_elems_folded(int Cin, int Cout, int up_C);
+// Whether a tile has a folded-upsampling form (the packed-row-tap kernels with streamed weights, BN <= 64).
+bool conv_tile_folds(ConvTile tile, int Cin, int Cout, int up_C);
+// Packs w[Cout][Cin][3][3] for the folded form: per output block the skip channels' K-blocks (row taps
+// packed into N, as conv_pack_weights with the same tile) and then the upsampled channels' K-blocks with the
+// row taps summed per output-row parity: [dx][KC/8][ky2 | ky1+ky2 | ky0+ky1 | ky0][BN][8], the four
+// output rows 2h-1 .. 2h+2 that low-resolution row h reaches.
+cudaError_t conv_pack_weights_folded(const float* d_w, int Cout, int Cin, int up_C, __nv_bfloat16* d_packed,
+                                     cudaStream_t stream, ConvTile tile);
 // Packs PyTorch-layout FP32 weights w[Cout][Cin_real][3][3] into the layout
 // the kernel streams (input channels beyond Cin_real are zero).
 cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,

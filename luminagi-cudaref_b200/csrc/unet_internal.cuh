@@ -64,6 +64,12 @@ struct lg_unet
     int aN = 0, aH = 0, aW = 0;
     Buf x0, t1, cat1, p1, t2, cat2, p2, t3, cat3, p3, t4, t5, t6, t7, u1, xin, yout, err;
     Buf lo7, lo9, lo11;  // bilinear mode: low-resolution outputs of the convs before each upsampling
+    // Inference with nearest upsampling: u3a, u2a and u1a read the upsampled half of their input as the
+    // lower level's output upsampled along x only (uh3, uh2, uh1) and fold their row taps per output-row
+    // parity (packed_fold); fold_up = false keeps the 2x2-copied concat halves.
+    bool fold_up = true;
+    Buf packed_fold[14];
+    Buf uh1, uh2, uh3;
     // training state
     int sm_count = 148;
     Buf grads, adam_m, adam_v, loss;

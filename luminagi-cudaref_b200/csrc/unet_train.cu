@@ -534,6 +534,14 @@ int lg_unet_autotune(lg_unet* u, int n, int h, int w, int flags, int32_t* tiles_
     return rc;
 }
 
+int lg_unet_set_fold_upsampling(lg_unet* u, int on)
+{
+    if (!u) return set_error(LG_ERR_INVALID, "NULL argument");
+    u->fold_up = on != 0;
+    u->packed_ok = false;  // the folded weights are packed with the others
+    return LG_OK;
+}
+
 int lg_unet_set_tiles(lg_unet* u, const int32_t* tiles)
 {
     if (!u || !tiles) return set_error(LG_ERR_INVALID, "NULL argument");

@@ -140,6 +140,7 @@ SIGNATURES = {
     "lg_unet_adam_reset": (_I, [_P]),
     "lg_unet_autotune": (_I, [_P, _I, _I, _I, _I, _P]),
     "lg_unet_set_tiles": (_I, [_P, _P]),
+    "lg_unet_set_fold_upsampling": (_I, [_P, _I]),
     "lg_conv3x3_device": (_I, [_P, _I, _I, _I, _I, _P, _I, _P, _I, C.c_float, _I, _P, _I, _I, _P, _I, _I, _P]),
     "lg_to_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _I, _P]),
     "lg_from_blocked_bf16": (_I, [_P, _I, _I, _I, _I, _P, _P]),

@@ -1,6 +1,6 @@
 """Device-timed micro-benchmarks of the library's kernels.
 
-    python -m lumina.perf unet  [--n 1] [--h 864] [--w 1728] [--reps 10] [--kernel default|single|autotune]
+    python -m lumina.perf unet  [--n 1] [--h 864] [--w 1728] [--reps 10] [--kernel default|single|autotune] [--fold 1|0]
     python -m lumina.perf trace [--spp 8] [--bounces 2] [--width 4] [--reps 2]
     python -m lumina.perf bvh   [--reps 5]
     python -m lumina.perf batch [--poses 50] [--spp 8] [--bounces 2]
@@ -53,7 +53,8 @@ def unet(a):
         net.set_tiles(DYP4_TILES + [(0, 0, 0, 1)] * 16)
     elif a.kernel == "dyp8":
         net.set_tiles(DYP8_TILES + [(0, 0, 0, 1)] * 16)
-    elif a.kernel == "autotune":
+    net.set_fold_upsampling(bool(a.fold))
+    if a.kernel == "autotune":
         tiles = net.autotune(a.n, a.h, a.w)[:14]
     x = torch.rand((a.n, 3, a.h, a.w), device="cuda")
     y = torch.empty_like(x)
@@ -69,8 +70,8 @@ def unet(a):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / a.reps
     flops = 2 * 162240 * a.n * a.h * a.w
-    return {"kernel": "unet_forward", "variant": a.variant, "conv": a.kernel, "n": a.n, "h": a.h, "w": a.w, "ms": ms,
-            "tflops": flops / ms / 1e9, "tiles": tiles}
+    return {"kernel": "unet_forward", "variant": a.variant, "conv": a.kernel, "fold": a.fold, "n": a.n, "h": a.h,
+            "w": a.w, "ms": ms, "tflops": flops / ms / 1e9, "tiles": tiles}
 
 
 def trace(a):
@@ -269,6 +270,7 @@ def main(argv=None):
                     help="unet: default tiles, the one-tile-per-CTA conv kernel, resident weights for the "
                          "single-block layers, or autotuned tiles")
     ap.add_argument("--n", type=int, default=1)
+    ap.add_argument("--fold", type=int, default=1, help="unet: folded upsampling in u3a/u2a/u1a (1/0)")
     ap.add_argument("--variant", default="ref", choices=["ref", "hdr"],
                     help="unet: reference network, or the HDR one (ReLU, bilinear upsampling, log1p in / expm1 out)")
     ap.add_argument("--h", type=int, default=864)

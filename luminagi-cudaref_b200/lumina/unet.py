@@ -157,6 +157,11 @@ class UNet:
         arr = np.ascontiguousarray(np.asarray(tiles, np.int32).reshape(120))
         check(lib().lg_unet_set_tiles(self._h, ptr(arr)))
 
+    def set_fold_upsampling(self, on: bool) -> None:
+        """Inference passes of u3a, u2a, u1a on the x-only upsampled lower level with row taps summed per
+        output-row parity (lg_unet_set_fold_upsampling; on by default, nearest upsampling only)."""
+        check(lib().lg_unet_set_fold_upsampling(self._h, 1 if on else 0))
+
     def denoise_hdr(self, radiance: np.ndarray) -> np.ndarray:
         """HDR variant: (H,W,3) FP32 linear radiance -> (H,W,3), edge-padded to multiples of 8."""
         assert self.variant == "hdr" and self.in_ch == 3

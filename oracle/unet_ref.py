@@ -118,10 +118,19 @@ def flat_params(model: nn.Module) -> np.ndarray:
     return np.concatenate([v.detach().cpu().float().numpy().ravel() for v in model.state_dict().values()])
 
 
-def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32) -> torch.Tensor:
+def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32, fold=()) -> torch.Tensor:
     """The network with BF16 rounding where the tensor-core kernels round;
     everything else in `dtype` (float64 gives the accumulation-order noise
-    floor of the FP32 version)."""
+    floor of the FP32 version).
+
+    fold: names of the decoder blocks ("u3", "u2", "u1") whose first conv runs
+    the library's folded-upsampling form.  Nearest upsampling repeats each
+    row, so an even output row 2r reads low-resolution rows r-1 (tap ky0) and
+    r (ky1 + ky2), an odd row 2r+1 rows r (ky0 + ky1) and r+1 (ky2); the
+    library sums those taps of the upsampled channels in FP32 and rounds the
+    sum to BF16 once.  Here: the conv over the upsampled input with those
+    rounded weights, even output rows from one weight set and odd rows from
+    the other (exact, since rows 2r and 2r+1 of the input are equal)."""
     s = model.slope
 
     def _q(t):
@@ -135,8 +144,20 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32) -> torch.
     def conv(block_conv, t):
         return F.conv2d(_q(t), _q(block_conv.weight.to(dtype)), block_conv.bias.to(dtype), padding=1)
 
-    def block(b, t):
-        t = _q(F.leaky_relu(conv(b.net[0], t), s))
+    def conv_folded(block_conv, t, up_c):
+        w = block_conv.weight.to(dtype)
+        u = w[:, :up_c]
+        we, wo = _q(w), _q(w)
+        we[:, :up_c, 0], we[:, :up_c, 1], we[:, :up_c, 2] = _q(u[:, :, 0]), _q(u[:, :, 1] + u[:, :, 2]), 0.0
+        wo[:, :up_c, 0], wo[:, :up_c, 1], wo[:, :up_c, 2] = _q(u[:, :, 0] + u[:, :, 1]), 0.0, _q(u[:, :, 2])
+        b = block_conv.bias.to(dtype)
+        y = F.conv2d(_q(t), we, b, padding=1)
+        y[:, :, 1::2] = F.conv2d(_q(t), wo, b, padding=1)[:, :, 1::2]
+        return y
+
+    def block(b, t, name=None, up_c=0):
+        first = conv_folded(b.net[0], t, up_c) if name in fold else conv(b.net[0], t)
+        t = _q(F.leaky_relu(first, s))
         return _q(F.leaky_relu(conv(b.net[2], t), s))
 
     pool = lambda t: F.max_pool2d(t, 2)
@@ -148,9 +169,11 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32) -> torch.
     d2 = block(model.d2, pool(d1))
     d3 = block(model.d3, pool(d2))
     d4 = block(model.d4, pool(d3))
-    u3 = block(model.u3, torch.cat([up(d4), d3], 1))
-    u2 = block(model.u2, torch.cat([up(u3), d2], 1))
-    u1 = block(model.u1, torch.cat([up(u2), d1], 1))
+    if hdr:
+        fold = ()  # bilinear upsampling does not repeat rows
+    u3 = block(model.u3, torch.cat([up(d4), d3], 1), "u3", d4.shape[1])
+    u2 = block(model.u2, torch.cat([up(u3), d2], 1), "u2", u3.shape[1])
+    u1 = block(model.u1, torch.cat([up(u2), d1], 1), "u1", u2.shape[1])
     tail = F.conv2d(u1, model.tail.weight.to(dtype), model.tail.bias.to(dtype))
     if hdr:
         return torch.expm1(torch.clamp(x[:, :3] + tail, min=0.0))

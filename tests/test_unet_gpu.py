@@ -99,19 +99,35 @@ def test_conv_upsample_epilogue():
     assert close_frac(got, ref) >= 0.999
 
 
+# Decoder blocks whose first conv folds its upsampled input in inference (default tiles: all three).
+FOLD_ALL = ("u3", "u2", "u1")
+
+
+def _folded_blocks(tiles):
+    """The blocks lg_unet folds for a tile list (kernel choices 6 and 7 with the compiled shapes)."""
+    def folds(t):
+        return (t[3] == 7 and tuple(t[:3]) == (32, 32, 2)) or (t[3] == 6 and tuple(t[:3]) in ((64, 32, 2), (32, 32, 3)))
+    return tuple(b for b, i in (("u3", 8), ("u2", 10), ("u1", 12)) if folds(tiles[i]))
+
+
+@pytest.mark.parametrize("fold", [True, False])
 @pytest.mark.parametrize("n,h,w,in_ch", [(2, 32, 48, 3), (1, 64, 136, 3), (2, 32, 48, 12)])
-def test_unet_forward_matches_torch(n, h, w, in_ch):
+def test_unet_forward_matches_torch(n, h, w, in_ch, fold):
+    """Inference forward against the BF16-emulated restatement (same roundings, FP32 sums), with the
+    folded-upsampling form of u3a/u2a/u1a (default) and without; and against plain FP32."""
     flat = unet_ref.make_params(77, unet_ref.UNetRef(in_ch=in_ch))
     net = lumina.UNet(in_ch=in_ch)
     net.set_params(flat)
+    net.set_fold_upsampling(fold)
     assert np.array_equal(net.get_params(), flat)
     x = np.random.default_rng(3).uniform(0, 1, (n, in_ch, h, w)).astype(np.float32)
     y = net.forward(x)
     assert y.shape == (n, 3, h, w)
     m = unet_ref.load_flat(unet_ref.UNetRef(in_ch=in_ch).eval(), flat)
+    fb = FOLD_ALL if fold else ()
     with torch.no_grad():
-        ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x)).numpy()
-        ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64).numpy()
+        ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x), fold=fb).numpy()
+        ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64, fold=fb).numpy()
         ref_f = m(torch.from_numpy(x)).numpy()
     err_q = np.abs(y - ref_q)
     err_f = np.abs(y - ref_f)
@@ -257,7 +273,7 @@ def test_denoise_rgb8_gbuffer_variant():
     x = F.pad(torch.from_numpy(x), (0, 5, 0, 4), mode="replicate")
     m = unet_ref.load_flat(unet_ref.UNetRef(in_ch=12).eval(), flat)
     with torch.no_grad():
-        y = unet_ref.forward_bf16(m, x)[0, :, :20, :27].numpy().transpose(1, 2, 0)
+        y = unet_ref.forward_bf16(m, x, fold=FOLD_ALL)[0, :, :20, :27].numpy().transpose(1, 2, 0)
     ref = (np.clip(y, 0, 1) * 255.0 + 0.5).astype(np.uint8)
     diff = np.abs(got.astype(int) - ref.astype(int))
     assert diff.max() <= 6 and np.mean(diff <= 1) > 0.95
@@ -343,11 +359,11 @@ def test_autotune_keeps_results():
     y1 = net.forward(x)
     assert np.array_equal(net.get_params(), flat)
     m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
-    with torch.no_grad():
-        ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x)).numpy()
-        ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64).numpy()
-    floor = np.abs(ref_q - ref_q64)
-    for y in (y0, y1):
+    for y, fb in ((y0, FOLD_ALL), (y1, _folded_blocks(tiles))):
+        with torch.no_grad():
+            ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x), fold=fb).numpy()
+            ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64, fold=fb).numpy()
+        floor = np.abs(ref_q - ref_q64)
         err = np.abs(y - ref_q)
         assert err.mean() <= 2.0 * floor.mean() + 1e-4 and err.max() <= 2.0 * floor.max() + 2e-3
     noisy, clean = _batch(n, h, w, 4)
@@ -424,6 +440,7 @@ def test_resident_weight_conv_kernel_is_bit_identical():
             net = lumina.UNet()
             net.set_params(flat)
             net.set_tiles(tiles)
+            net.set_fold_upsampling(False)  # the folded form rounds its summed weights: compared elsewhere
             y = net.forward(x)
             loss, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
             outs.append((y, loss, g))
@@ -433,6 +450,43 @@ def test_resident_weight_conv_kernel_is_bit_identical():
             assert outs[0][1] == o[1]
             assert np.array_equal(outs[0][2], o[2])
 
+
+
+# Both folded-upsampling shapes per decoder level: u3a (64, 32, 2, 6); u2a and u1a (32, 32, 3, 6) here,
+# (64, 32, 2, 6) and (32, 32, 2, 7) in the default tiles.
+FOLD_B_TILES = [(32, 16, 4, 5), (32, 32, 3, 4), (64, 32, 2, 4), (64, 32, 2, 4)] + [(64, 32, 2, 6)] * 6 + \
+               [(32, 32, 3, 6), (64, 32, 2, 4), (32, 32, 3, 6), (32, 32, 3, 4)]
+
+
+@pytest.mark.parametrize("n,h,w", [(1, 40, 264), (2, 64, 136), (1, 72, 136)])
+def test_folded_upsampling_matches_restatement(n, h, w):
+    """u3a/u2a/u1a in their folded-upsampling form (x-only upsampled lower level, row taps summed per
+    output-row parity): each folded kernel shape against the BF16-emulated restatement of that form, at
+    sizes with partial row tiles at the bottom, widths whose deeper levels are not multiples of 8 (the
+    pixel-by-pixel input view), and batch 2; and close to the unfolded pass."""
+    flat = unet_ref.make_params(83)
+    m = unet_ref.load_flat(unet_ref.UNetRef().eval(), flat)
+    x = np.random.default_rng(12).uniform(0, 1, (n, 3, h, w)).astype(np.float32)
+    with torch.no_grad():
+        ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x), fold=FOLD_ALL).numpy()
+        ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64, fold=FOLD_ALL).numpy()
+    floor = np.abs(ref_q - ref_q64)
+    for tiles in (None, FOLD_B_TILES + [(0, 0, 0, 1)] * 16):
+        net = lumina.UNet()
+        net.set_params(flat)
+        if tiles is not None:
+            net.set_tiles(tiles)
+            assert _folded_blocks(tiles) == FOLD_ALL
+        y = net.forward(x)
+        err = np.abs(y - ref_q)
+        print(f"folded {n}x{h}x{w}: max {err.max():.2e} mean {err.mean():.2e} "
+              f"(floor max {floor.max():.2e} mean {floor.mean():.2e})")
+        assert err.mean() <= 2.0 * floor.mean() + 1e-4
+        assert err.max() <= 2.0 * floor.max() + 2e-3
+        net.set_fold_upsampling(False)
+        y_plain = net.forward(x)
+        assert np.abs(y - y_plain).max() < 0.05 and np.abs(y - y_plain).mean() < 2e-3
+        net.close()
 
 def test_async_train_step_matches_sync():
     """lg_unet_train_step_async queues the same step on the caller's stream
