@@ -122,7 +122,7 @@ int lg_build_bvh_device(const lg_triangle* d_tris, int32_t n_tris, lg_bvh_node* 
  * scratch is a fixed array in device memory that the library holds on every
  * GPU that loads it, so at most LG_NOALLOC_MAX_TRIS triangles are accepted
  * (larger inputs return LG_ERR_CAPACITY).  The first call on a device looks
- * up the array's address for that device; make it before any stream capture.
+ * up the array's address for that device.
  * Under lazy module loading (CUDA's default since 12.2) that first call is
  * also when the array is loaded and its 14 MB are taken from the device, so
  * a host that reserves all device memory for its own allocator should make
