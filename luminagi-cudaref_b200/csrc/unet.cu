@@ -93,25 +93,38 @@ bool folds(const lg_unet* u, int i)
            conv_tile_folds(u->tile[i], kLayers[i].cin, kLayers[i].cout, up_channels(i));
 }
 
+// The 14 convs' packed weights, in one launch (they are repacked after every Adam step).
 int pack_all_impl(lg_unet* u)
 {
     if (u->packed_ok) return LG_OK;
+    ConvPackJob jobs[14];
     for (int i = 0; i < 14; ++i)
     {
         const LayerDef& L = kLayers[i];
-        const float* w = (const float*)u->params.p + u->w_off[i];
         LG_TRY(u->packed[i].ensure(conv_packed_elems(L.cin, L.cout) * sizeof(__nv_bfloat16)));
-        LG_TRY_CUDA(conv_pack_weights(w, L.cout, layer_cin_real(u, i), L.cin, (__nv_bfloat16*)u->packed[i].p,
-                                      u->stream, u->tile[i]));
-        if (folds(u, i))
-        {
-            const int uc = up_channels(i);
-            LG_TRY(u->packed_fold[i].ensure(conv_packed_elems_folded(L.cin, L.cout, uc) * sizeof(__nv_bfloat16)));
-            LG_TRY_CUDA(conv_pack_weights_folded(w, L.cout, L.cin, uc, (__nv_bfloat16*)u->packed_fold[i].p,
-                                                 u->stream, u->tile[i]));
-        }
+        jobs[i] = conv_pack_job((const float*)u->params.p + u->w_off[i], L.cout, layer_cin_real(u, i), L.cin,
+                                (__nv_bfloat16*)u->packed[i].p, u->tile[i]);
     }
+    LG_TRY_CUDA(conv_pack_many(jobs, 14, u->stream));
     u->packed_ok = true;
+    u->packed_fold_ok = false;
+    return LG_OK;
+}
+
+// The folded-upsampling weights of u3a/u2a/u1a, packed on the first inference pass that needs them.
+int pack_fold_impl(lg_unet* u)
+{
+    if (u->packed_fold_ok) return LG_OK;
+    for (int i = 0; i < 14; ++i)
+    {
+        if (!folds(u, i)) continue;
+        const LayerDef& L = kLayers[i];
+        const int uc = up_channels(i);
+        LG_TRY(u->packed_fold[i].ensure(conv_packed_elems_folded(L.cin, L.cout, uc) * sizeof(__nv_bfloat16)));
+        LG_TRY_CUDA(conv_pack_weights_folded((const float*)u->params.p + u->w_off[i], L.cout, L.cin, uc,
+                                             (__nv_bfloat16*)u->packed_fold[i].p, u->stream, u->tile[i]));
+    }
+    u->packed_fold_ok = true;
     return LG_OK;
 }
 
@@ -147,6 +160,7 @@ int forward_device_impl(lg_unet* u, const float* d_x, int N, int H, int W, float
     const int H2 = H / 2, W2 = W / 2, H4 = H / 4, W4 = W / 4, H8 = H / 8, W8 = W / 8;
     // inference with nearest upsampling: u3a, u2a, u1a fold their upsampled inputs where their tiles allow
     const bool fold = !keep_u1;
+    if (fold) LG_TRY(pack_fold_impl(u));
     auto run = [&](int layer, const void* in, int h, int w, int epi, void* out, int out_c, int out_coff, void* out2,
                    int out2_c, int out2_coff, const void* up_h = nullptr, int x_only = 0) -> int {
         ConvArgs a = base_args(u, layer, N, h, w);

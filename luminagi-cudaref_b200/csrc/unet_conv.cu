@@ -1053,19 +1053,60 @@ __device__ __forceinline__ void packed_index(size_t r, int BN, int KC, int KB, b
     ct = (int)r;
 }
 
+// Packed forward weight at position i (packed_index layout).
+__device__ __forceinline__ float pack_value(const float* __restrict__ w, size_t i, int Cin_real, int Cin, int BN,
+                                            int KC, bool dyp)
+{
+    const int KB = Cin / KC;
+    int ct, kb, tap, kc8, j, e;
+    packed_index(i, BN, KC, KB, dyp, ct, kb, tap, kc8, j, e);
+    const int co = ct * BN + j;
+    const int ci = kb * KC + kc8 * 8 + e;
+    return ci < Cin_real ? w[(((size_t)co * Cin_real + ci) * 3 + tap / 3) * 3 + tap % 3] : 0.0f;
+}
+
+// Input-gradient weight at position i: output (ct, kb, tap, kc8, j, e) of a conv with Cin' = Cout (forward)
+// and Cout' = ci_cnt reads w[co = ci'][ci_lo + co'][2-ky][2-kx].
+__device__ __forceinline__ float pack_dgrad_value(const float* __restrict__ w, size_t i, int Cout, int Cin_real,
+                                                  int ci_lo, int ci_cnt, int BN, int KC, bool dyp)
+{
+    const int KB = Cout / KC;
+    int ct, kb, tap, kc8, j, e;
+    packed_index(i, BN, KC, KB, dyp, ct, kb, tap, kc8, j, e);
+    const int cop = ct * BN + j;            // output channel of the backward conv
+    const int cip = kb * KC + kc8 * 8 + e;  // its input channel = forward output channel
+    const int ky = 2 - tap / 3, kx = 2 - tap % 3;
+    const int ci = ci_lo + cop;
+    return (cop < ci_cnt && ci < Cin_real) ? w[(((size_t)cip * Cin_real + ci) * 3 + ky) * 3 + kx] : 0.0f;
+}
+
 __global__ void pack_kernel(const float* __restrict__ w, int Cout, int Cin_real, int Cin, int BN, int KC, int dyp,
                             __nv_bfloat16* __restrict__ out, size_t total)
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
-    const int KB = Cin / KC;
-    int ct, kb, tap, kc8, j, e;
-    packed_index(i, BN, KC, KB, dyp != 0, ct, kb, tap, kc8, j, e);
-    const int co = ct * BN + j;
-    const int ci = kb * KC + kc8 * 8 + e;
-    float v = 0.0f;
-    if (ci < Cin_real) v = w[(((size_t)co * Cin_real + ci) * 3 + tap / 3) * 3 + tap % 3];
-    out[i] = __float2bfloat16_rn(v);
+    out[i] = __float2bfloat16_rn(pack_value(w, i, Cin_real, Cin, BN, KC, dyp != 0));
+}
+
+// Every layer of a ConvPackJob list in one launch: thread i packs position i - begin of the job whose
+// [begin, begin + elems) range holds i, with the single-layer kernels' arithmetic (identical bits).
+struct PackTable
+{
+    ConvPackJob job[kMaxPackJobs];
+    size_t begin[kMaxPackJobs + 1];
+    int n;
+};
+__global__ void pack_many_kernel(const __grid_constant__ PackTable t)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t.begin[t.n]) return;
+    int k = 0;
+    while (i >= t.begin[k + 1]) ++k;
+    const ConvPackJob& j = t.job[k];
+    const size_t r = i - t.begin[k];
+    const float v = j.dgrad ? pack_dgrad_value(j.w, r, j.Cout, j.Cin_real, j.ci_lo, j.ci_cnt, j.bn, j.kc, j.dyp != 0)
+                            : pack_value(j.w, r, j.Cin_real, j.Cin, j.bn, j.kc, j.dyp != 0);
+    j.out[r] = __float2bfloat16_rn(v);
 }
 
 // Folded-upsampling weights (conv_pack_weights_folded): per output block,
@@ -1114,16 +1155,7 @@ __global__ void pack_dgrad_kernel(const float* __restrict__ w, int Cout, int Cin
 {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
-    const int KB = Cout / KC;
-    int ct, kb, tap, kc8, j, e;
-    packed_index(i, BN, KC, KB, dyp != 0, ct, kb, tap, kc8, j, e);
-    const int cop = ct * BN + j;             // output channel of the backward conv
-    const int cip = kb * KC + kc8 * 8 + e;   // its input channel = forward output channel
-    const int ky = 2 - tap / 3, kx = 2 - tap % 3;
-    const int ci = ci_lo + cop;
-    float v = 0.0f;
-    if (cop < ci_cnt && ci < Cin_real) v = w[(((size_t)cip * Cin_real + ci) * 3 + ky) * 3 + kx];
-    out[i] = __float2bfloat16_rn(v);
+    out[i] = __float2bfloat16_rn(pack_dgrad_value(w, i, Cout, Cin_real, ci_lo, ci_cnt, BN, KC, dyp != 0));
 }
 
 // One thread per (image, 8-channel block, pixel) of the first nb blocks:
@@ -1241,6 +1273,58 @@ cudaError_t conv_pack_weights_folded(const float* d_w, int Cout, int Cin, int up
     const size_t total = conv_packed_elems_folded(Cin, Cout, up_C);
     pack_folded_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(d_w, Cout, Cin, up_C, c.bn, c.kc,
                                                                             d_packed, total);
+    return cudaGetLastError();
+}
+
+ConvPackJob conv_pack_job(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed, ConvTile tile)
+{
+    const TileCfg c = resolve(tile, Cin, Cout);
+    ConvPackJob j{};
+    j.w = d_w;
+    j.out = d_packed;
+    j.elems = conv_packed_elems(Cin, Cout);
+    j.Cout = Cout;
+    j.Cin_real = Cin_real;
+    j.Cin = Cin;
+    j.bn = c.bn;
+    j.kc = c.kc;
+    j.dyp = tile_dyp(c.persist) ? 1 : 0;
+    return j;
+}
+
+ConvPackJob conv_pack_job_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
+                                __nv_bfloat16* d_packed, ConvTile tile)
+{
+    const TileCfg c = resolve(tile, Cout, ci_cnt);
+    ConvPackJob j{};
+    j.w = d_w;
+    j.out = d_packed;
+    j.elems = conv_packed_elems(Cout, ci_cnt);
+    j.Cout = Cout;
+    j.Cin_real = Cin_real;
+    j.bn = c.bn;
+    j.kc = c.kc;
+    j.dyp = tile_dyp(c.persist) ? 1 : 0;
+    j.dgrad = 1;
+    j.ci_lo = ci_lo;
+    j.ci_cnt = ci_cnt;
+    return j;
+}
+
+cudaError_t conv_pack_many(const ConvPackJob* jobs, int n, cudaStream_t stream)
+{
+    if (n < 0 || n > kMaxPackJobs) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    PackTable t{};
+    t.n = n;
+    t.begin[0] = 0;
+    for (int k = 0; k < n; ++k)
+    {
+        t.job[k] = jobs[k];
+        t.begin[k + 1] = t.begin[k] + jobs[k].elems;
+    }
+    const size_t total = t.begin[n];
+    pack_many_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(t);
     return cudaGetLastError();
 }
 

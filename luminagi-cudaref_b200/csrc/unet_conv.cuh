@@ -99,6 +99,22 @@ cudaError_t conv_pack_weights_folded(const float* d_w, int Cout, int Cin, int up
 cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
                               cudaStream_t stream, ConvTile tile = ConvTile{0, 0, 0});
 
+// One layer's packing in a batched launch (conv_pack_many): the arguments of conv_pack_weights (dgrad = 0) or
+// conv_pack_weights_dgrad (dgrad = 1), resolved to the tile's (BN, KC) and layout.
+struct ConvPackJob
+{
+    const float* w;
+    __nv_bfloat16* out;
+    size_t elems;
+    int Cout, Cin_real, Cin, bn, kc, dyp, dgrad, ci_lo, ci_cnt;
+};
+constexpr int kMaxPackJobs = 16;
+ConvPackJob conv_pack_job(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed, ConvTile tile);
+ConvPackJob conv_pack_job_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
+                                __nv_bfloat16* d_packed, ConvTile tile);
+// Packs up to kMaxPackJobs layers in one launch; the same bits as one conv_pack_weights[_dgrad] call per job.
+cudaError_t conv_pack_many(const ConvPackJob* jobs, int n, cudaStream_t stream);
+
 // Packs the input-gradient weights of a forward conv w[Cout][Cin_real][3][3]:
 // w'[ci][co][ky][kx] = w[co][ci][2-ky][2-kx] for ci in [ci_lo, ci_lo+ci_cnt),
 // as a convolution with Cin' = Cout input and ci_cnt output channels.

@@ -69,6 +69,7 @@ struct lg_unet
     // parity (packed_fold); fold_up = false keeps the 2x2-copied concat halves.
     bool fold_up = true;
     Buf packed_fold[14];
+    bool packed_fold_ok = false;  // reset whenever the plain weights are repacked
     Buf uh1, uh2, uh3;
     // training state
     int sm_count = 148;

@@ -195,17 +195,21 @@ int ensure_train(lg_unet* u, int N, int H, int W)
     return LG_OK;
 }
 
+// The 16 input-gradient convs' packed weights, in one launch.
 int pack_dgrad(lg_unet* u)
 {
     if (u->packed_dg_ok) return LG_OK;
+    ConvPackJob jobs[16];
     for (int k = 0; k < 16; ++k)
     {
         const DgradDef& d = kDgrad[k];
         const LayerDef& L = kLayers[d.layer];
         LG_TRY(u->packed_dg[k].ensure(conv_packed_elems(L.cout, d.ci_cnt) * sizeof(bf)));
-        LG_TRY_CUDA(conv_pack_weights_dgrad((const float*)u->params.p + u->w_off[d.layer], L.cout, layer_cin_real(u, d.layer), d.ci_lo,
-                                            d.ci_cnt, (bf*)u->packed_dg[k].p, u->stream, u->tile_dg[k]));
+        jobs[k] = conv_pack_job_dgrad((const float*)u->params.p + u->w_off[d.layer], L.cout,
+                                      layer_cin_real(u, d.layer), d.ci_lo, d.ci_cnt, (bf*)u->packed_dg[k].p,
+                                      u->tile_dg[k]);
     }
+    LG_TRY_CUDA(conv_pack_many(jobs, 16, u->stream));
     u->packed_dg_ok = true;
     return LG_OK;
 }
@@ -252,11 +256,8 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
         a.err = (int*)u->err.p;
         LG_TRY(u->wpart.ensure(conv3x3_wgrad_partial_floats(N, a.H, a.Cout, a.Cin, a.Cin_real, u->sm_count) *
                                sizeof(float)));
-        LG_TRY(u->bpart.ensure(conv_bias_grad_partial_floats(a.Cout) * sizeof(float)));
         a.partial = (float*)u->wpart.p;
         LG_TRY_CUDA(conv3x3_wgrad((const bf*)u->dz[L].p, (const bf*)in_of[L], a, u->sm_count, st));
-        LG_TRY_CUDA(conv_bias_grad((const bf*)u->dz[L].p, N, kLayers[L].cout, hs[lv], ws[lv], G + u->b_off[L],
-                                   (float*)u->bpart.p, st));
         return LG_OK;
     };
     auto dgrad = [&](int k, void* out, int out_c, const void* ref, int ref_c, int ref_coff, const void* skip,
@@ -332,6 +333,17 @@ int loss_and_grads(lg_unet* u, const float* d_x, const float* d_t, int N, int H,
     LG_TRY(wgrad(1));
     LG_TRY(dgrad(15, u->dz[0].p, 32, u->t1.p, 32, 0, nullptr, 0));
     LG_TRY(wgrad(0));
+    // every layer's bias gradient from its kept dZ, in one batched pass (the same sums as one pass per layer)
+    BiasGradJob bj[14];
+    int bias_c = 0;
+    for (int L = 0; L < 14; ++L)
+    {
+        const int lv = lv_out[L];
+        bj[L] = BiasGradJob{(const bf*)u->dz[L].p, G + u->b_off[L], N, kLayers[L].cout, hs[lv] * ws[lv]};
+        bias_c += kLayers[L].cout;
+    }
+    LG_TRY(u->bpart.ensure(conv_bias_grad_partial_floats(bias_c) * sizeof(float)));
+    LG_TRY_CUDA(conv_bias_grad_many(bj, 14, (float*)u->bpart.p, st));
     if (loss_host)
     {
         float s = 0.0f;
@@ -538,7 +550,7 @@ int lg_unet_set_fold_upsampling(lg_unet* u, int on)
 {
     if (!u) return set_error(LG_ERR_INVALID, "NULL argument");
     u->fold_up = on != 0;
-    u->packed_ok = false;  // the folded weights are packed with the others
+    u->packed_fold_ok = false;  // which layers fold has changed
     return LG_OK;
 }
 

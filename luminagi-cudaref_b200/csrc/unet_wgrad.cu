@@ -350,15 +350,15 @@ cudaError_t launch_w(const __nv_bfloat16* dz, const __nv_bfloat16* x, const Wgra
 }
 
 constexpr int kBiasBlocks = 64;  // blocks per 8-channel group; each writes its own partial
-__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW,
-                                 float* __restrict__ partial)
+// Block `chunk` of 8-channel group cb of dz (N x C x HW, blocked BF16): the sum of its pixels p = chunk*256 + t,
+// stepping by kBiasBlocks*256, per thread, then over the warps in order, into out[0..7].
+__device__ __forceinline__ void bias_block_sum(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW, int cb,
+                                               int chunk, float* __restrict__ out)
 {
     __shared__ float warp_sum[8][8];
-    // block (c-block, chunk): 8 channels of a range of pixels
-    const int cb = blockIdx.y;
     float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const size_t pixels = (size_t)N * HW;
-    for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += (size_t)gridDim.x * blockDim.x)
+    for (size_t p = (size_t)chunk * blockDim.x + threadIdx.x; p < pixels; p += (size_t)kBiasBlocks * blockDim.x)
     {
         const size_t n = p / HW, q = p % HW;
         const uint4 u = __ldg(reinterpret_cast<const uint4*>(dz + ((n * (C / 8) + cb) * HW + q) * 8));
@@ -384,8 +384,45 @@ __global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, in
     {
         float s = 0.0f;
         for (int w = 0; w < 8; ++w) s += warp_sum[w][threadIdx.x];  // warps in order
-        partial[((size_t)cb * kBiasBlocks + blockIdx.x) * 8 + threadIdx.x] = s;
+        out[threadIdx.x] = s;
     }
+}
+// grid (kBiasBlocks, C/8), 256 threads
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW,
+                                 float* __restrict__ partial)
+{
+    bias_block_sum(dz, N, C, HW, blockIdx.y, blockIdx.x, partial + ((size_t)blockIdx.y * kBiasBlocks + blockIdx.x) * 8);
+}
+
+// Several layers' bias gradients: blockIdx.y runs over every layer's 8-channel groups (group g of the whole
+// list belongs to the job k with gbegin[k] <= g < gbegin[k+1]); the partials of group g are where a
+// single-layer launch would put them, offset by the groups before it.
+struct BiasTable
+{
+    BiasGradJob job[kMaxBiasJobs];
+    int gbegin[kMaxBiasJobs + 1];  // 8-channel groups before job k
+    int n;
+};
+__global__ void bias_grad_many_kernel(const __grid_constant__ BiasTable t, float* __restrict__ partial)
+{
+    const int g = blockIdx.y;
+    int k = 0;
+    while (g >= t.gbegin[k + 1]) ++k;
+    const BiasGradJob& j = t.job[k];
+    bias_block_sum(j.dz, j.N, j.C, j.HW, g - t.gbegin[k], blockIdx.x,
+                   partial + ((size_t)g * kBiasBlocks + blockIdx.x) * 8);
+}
+// db[c] += the kBiasBlocks partials of channel c, in block order, for every job's channels.
+__global__ void bias_reduce_many_kernel(const __grid_constant__ BiasTable t, const float* __restrict__ partial)
+{
+    const int gc = blockIdx.x * blockDim.x + threadIdx.x;  // channel in the whole list
+    if (gc >= 8 * t.gbegin[t.n]) return;
+    int k = 0;
+    while (gc >= 8 * t.gbegin[k + 1]) ++k;
+    const int g = gc >> 3, i = gc & 7;
+    float s = 0.0f;
+    for (int b = 0; b < kBiasBlocks; ++b) s += partial[((size_t)g * kBiasBlocks + b) * 8 + i];
+    t.job[k].db[gc - 8 * t.gbegin[k]] += s;
 }
 
 // db[c] += the kBiasBlocks partials of channel c, in block order.
@@ -429,6 +466,25 @@ cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const
 }
 
 size_t conv_bias_grad_partial_floats(int C) { return (size_t)(C / 8) * kBiasBlocks * 8; }
+
+cudaError_t conv_bias_grad_many(const BiasGradJob* jobs, int n, float* partial, cudaStream_t stream)
+{
+    if (n < 0 || n > kMaxBiasJobs || !partial) return cudaErrorInvalidValue;
+    if (n == 0) return cudaSuccess;
+    BiasTable t{};
+    t.n = n;
+    for (int k = 0; k < n; ++k)
+    {
+        if (jobs[k].C % 8) return cudaErrorInvalidValue;
+        t.job[k] = jobs[k];
+        t.gbegin[k + 1] = t.gbegin[k] + jobs[k].C / 8;
+    }
+    bias_grad_many_kernel<<<dim3(kBiasBlocks, t.gbegin[n]), 256, 0, stream>>>(t, partial);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    bias_reduce_many_kernel<<<(8 * t.gbegin[n] + 255) / 256, 256, 0, stream>>>(t, partial);
+    return cudaGetLastError();
+}
 
 cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, float* partial,
                            cudaStream_t stream)
