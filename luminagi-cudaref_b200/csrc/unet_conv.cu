@@ -343,12 +343,14 @@ __device__ __forceinline__ void tile_epilogue(const ConvArgs& a, const EpiConsts
             const int cg = ct * BN + c0;  // layer channel of v[.][0]
             if (a.epilogue <= kEpiUpsample)
             {
+                // stored through pack8, which rounds to BF16 once; the 2x2 max of the pooled output commutes
+                // with that (monotonic) rounding, so no separate rounding step is needed here
                 float bb[16];
                 ld16(ec.bias + cg, bb);
 #pragma unroll
                 for (int r = 0; r < kRows; ++r)
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[r][j] = bf16r(act(v[r][j] + bb[j], a.slope));
+                    for (int j = 0; j < 16; ++j) v[r][j] = act(v[r][j] + bb[j], a.slope);
             }
             const int b0 = (a.out_coff + cg) >> 3;
             if (a.epilogue >= kEpiBwdMask)
