@@ -75,6 +75,15 @@ def test_conv_layer_matches_torch(cin_real, cin, cout, n, h, w):
     ref = q(F.leaky_relu(F.conv2d(q(x), q(wt), b, padding=1), 0.1))
     assert close_frac(got, ref) >= 0.999
     assert float((got - ref).abs().max()) < 0.05
+    # The error of the BF16 result against the FP64 host conv of the unrounded operands (the precision
+    # statement): BF16 inputs, weights and output each carry up to 2^-9 relative rounding.
+    ref64 = F.leaky_relu(F.conv2d(x.cpu().double(), wt.cpu().double(), b.cpu().double(), padding=1), 0.1)
+    err = (got.cpu().double() - ref64).abs()
+    rel_mean = float(err.mean() / ref64.abs().mean())
+    rel_max = float(err.max() / ref64.abs().max())
+    print(f"conv {cin_real}->{cout} at {n}x{h}x{w} vs FP64: mean |err| / mean |y| = {rel_mean:.2e}, "
+          f"max |err| / max |y| = {rel_max:.2e}")
+    assert rel_mean < 2.0 ** -7 and rel_max < 2.0 ** -5
     untouched = unblock(out, n, out_c, h, w)[:, :coff]
     assert float(untouched.abs().max()) == 0.0
     if pool:
@@ -114,7 +123,8 @@ def _folded_blocks(tiles):
 @pytest.mark.parametrize("n,h,w,in_ch", [(2, 32, 48, 3), (1, 64, 136, 3), (2, 32, 48, 12)])
 def test_unet_forward_matches_torch(n, h, w, in_ch, fold):
     """Inference forward against the BF16-emulated restatement (same roundings, FP32 sums), with the
-    folded-upsampling form of u3a/u2a/u1a (default) and without; and against plain FP32."""
+    folded-upsampling form of u3a/u2a/u1a (default) and without; and against the plain network in FP32 and
+    in FP64 (the host oracle of the precision statement)."""
     flat = unet_ref.make_params(77, unet_ref.UNetRef(in_ch=in_ch))
     net = lumina.UNet(in_ch=in_ch)
     net.set_params(flat)
@@ -129,14 +139,17 @@ def test_unet_forward_matches_torch(n, h, w, in_ch, fold):
         ref_q = unet_ref.forward_bf16(m, torch.from_numpy(x), fold=fb).numpy()
         ref_q64 = unet_ref.forward_bf16(m, torch.from_numpy(x), torch.float64, fold=fb).numpy()
         ref_f = m(torch.from_numpy(x)).numpy()
+        ref_64 = m.double()(torch.from_numpy(x).double()).numpy()  # FP64 host network, unrounded weights
     err_q = np.abs(y - ref_q)
     err_f = np.abs(y - ref_f)
+    err_64 = np.abs(y - ref_64)
     # Noise floor: the same BF16-rounded network summed in FP32 vs FP64 already
     # differs this much (a different summation order flips BF16 roundings).
     floor = np.abs(ref_q - ref_q64)
-    print(f"UNet {n}x{h}x{w}: vs BF16-emulated max {err_q.max():.2e} mean {err_q.mean():.2e} "
+    print(f"UNet {n}x{h}x{w} fold={fold}: vs BF16-emulated max {err_q.max():.2e} mean {err_q.mean():.2e} "
           f"(floor max {floor.max():.2e} mean {floor.mean():.2e}); vs FP32 max {err_f.max():.2e} "
-          f"mean {err_f.mean():.2e}")
+          f"mean {err_f.mean():.2e}; vs FP64 max {err_64.max():.2e} mean {err_64.mean():.2e}")
+    assert err_64.mean() < 5e-3 and err_64.max() < 0.1
     assert err_q.mean() <= 2.0 * floor.mean() + 1e-4
     assert err_q.max() <= 2.0 * floor.max() + 2e-3
     assert err_f.mean() < 5e-3 and err_f.max() < 0.1
