@@ -261,6 +261,32 @@ def test_engine_full_frame_vs_reference_gpu():
     assert frac >= 0.999
 
 
+def test_engine_converged_image_vs_reference_1024spp():
+    """The converged engine frame (1,050,972 triangles, 1728x864, 1024 spp, 2
+    bounces) against the reference accumulate_kernel's own 1024-spp image on
+    the same BVH: PSNR of the 8-bit tonemapped images as the reference's
+    tools/diff.py:25-29 computes it, and of the linear FP32 radiance (peak of
+    the reference image as the data range)."""
+    if not O.ref_available():
+        pytest.skip("reference oracle not built")
+    from lumina.metrics import psnr
+    sc = lumina.engine_scene(seed=7)
+    nodes, tris, _ = lumina.build_bvh(sc.tris)
+    spp = 1024
+    ours = render_ours(sc, nodes, tris, spp, 2, width=4)
+    ref_acc, ref_rgb, ref_ms = O.ref_render_gpu(sc, nodes, tris, spp, 2)
+    p8 = psnr(ours["rgb"], ref_rgb)
+    lin_o, lin_r = ours["accum"] / spp, ref_acc / spp
+    p_lin = psnr(lin_o, lin_r, data_range=float(lin_r.max()))
+    frac = match_fraction(ours["accum"], ref_acc)
+    diff8 = np.abs(ours["rgb"].astype(int) - ref_rgb.astype(int))
+    print(f"engine frame {spp} spp vs the reference's {spp}-spp image: PSNR 8-bit {p8:.2f} dB "
+          f"({int((diff8 > 0).sum())} of {diff8.size} values differ, max {int(diff8.max())}), linear {p_lin:.2f} dB, "
+          f"{frac * 100:.4f}% of pixels within 1e-3; ours {ours['kernel_ms']:.1f} ms, reference kernel {ref_ms:.1f} ms")
+    assert frac >= 0.999
+    assert p8 >= 60.0 and p_lin >= 60.0
+
+
 def _dfs_order(nodes):
     """The same tree with its records in depth-first preorder (links remapped)."""
     order, stack = [], [0]
