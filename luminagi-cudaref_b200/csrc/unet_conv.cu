@@ -1152,13 +1152,6 @@ __global__ void pack_folded_kernel(const float* __restrict__ w, int Cout, int Ci
 
 // Input-gradient weights: output (ct, kb, tap, kc8, j, e) of a conv with
 // Cin' = Cout (forward) and Cout' = ci_cnt reads w[co = ci'][ci_lo + co'][2-ky][2-kx].
-__global__ void pack_dgrad_kernel(const float* __restrict__ w, int Cout, int Cin_real, int ci_lo, int ci_cnt, int BN,
-                                  int KC, int dyp, __nv_bfloat16* __restrict__ out, size_t total)
-{
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
-    out[i] = __float2bfloat16_rn(pack_dgrad_value(w, i, Cout, Cin_real, ci_lo, ci_cnt, BN, KC, dyp != 0));
-}
 
 // One thread per (image, 8-channel block, pixel) of the first nb blocks:
 // reads the block's channels from their NCHW planes (consecutive threads,
@@ -1330,15 +1323,6 @@ cudaError_t conv_pack_many(const ConvPackJob* jobs, int n, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
-                                    __nv_bfloat16* d_packed, cudaStream_t stream, ConvTile tile)
-{
-    const TileCfg c = resolve(tile, Cout, ci_cnt);
-    const size_t total = conv_packed_elems(Cout, ci_cnt);
-    pack_dgrad_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(
-        d_w, Cout, Cin_real, ci_lo, ci_cnt, c.bn, c.kc, tile_dyp(c.persist) ? 1 : 0, d_packed, total);
-    return cudaGetLastError();
-}
 
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream)
 {

@@ -99,8 +99,10 @@ cudaError_t conv_pack_weights_folded(const float* d_w, int Cout, int Cin, int up
 cudaError_t conv_pack_weights(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed,
                               cudaStream_t stream, ConvTile tile = ConvTile{0, 0, 0});
 
-// One layer's packing in a batched launch (conv_pack_many): the arguments of conv_pack_weights (dgrad = 0) or
-// conv_pack_weights_dgrad (dgrad = 1), resolved to the tile's (BN, KC) and layout.
+// One layer's packing in a batched launch (conv_pack_many): the arguments of conv_pack_weights (dgrad = 0), or
+// (dgrad = 1) a forward conv's input-gradient weights w'[ci][co][ky][kx] = w[co][ci][2-ky][2-kx] for ci in
+// [ci_lo, ci_lo+ci_cnt), packed as a convolution with Cin' = Cout input and ci_cnt output channels; resolved to
+// the tile's (BN, KC) and layout.
 struct ConvPackJob
 {
     const float* w;
@@ -112,14 +114,8 @@ constexpr int kMaxPackJobs = 16;
 ConvPackJob conv_pack_job(const float* d_w, int Cout, int Cin_real, int Cin, __nv_bfloat16* d_packed, ConvTile tile);
 ConvPackJob conv_pack_job_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
                                 __nv_bfloat16* d_packed, ConvTile tile);
-// Packs up to kMaxPackJobs layers in one launch; the same bits as one conv_pack_weights[_dgrad] call per job.
+// Packs up to kMaxPackJobs layers in one launch (forward jobs: the same bits as one conv_pack_weights call each).
 cudaError_t conv_pack_many(const ConvPackJob* jobs, int n, cudaStream_t stream);
-
-// Packs the input-gradient weights of a forward conv w[Cout][Cin_real][3][3]:
-// w'[ci][co][ky][kx] = w[co][ci][2-ky][2-kx] for ci in [ci_lo, ci_lo+ci_cnt),
-// as a convolution with Cin' = Cout input and ci_cnt output channels.
-cudaError_t conv_pack_weights_dgrad(const float* d_w, int Cout, int Cin_real, int ci_lo, int ci_cnt,
-                                    __nv_bfloat16* d_packed, cudaStream_t stream, ConvTile tile = ConvTile{0, 0, 0});
 
 // Launches the convolution reading `in` (blocked BF16, N x Cin x H x W).
 cudaError_t conv3x3_forward(const __nv_bfloat16* in, const ConvArgs& a, cudaStream_t stream);

@@ -387,16 +387,10 @@ __device__ __forceinline__ void bias_block_sum(const __nv_bfloat16* __restrict__
         out[threadIdx.x] = s;
     }
 }
-// grid (kBiasBlocks, C/8), 256 threads
-__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, int N, int C, int HW,
-                                 float* __restrict__ partial)
-{
-    bias_block_sum(dz, N, C, HW, blockIdx.y, blockIdx.x, partial + ((size_t)blockIdx.y * kBiasBlocks + blockIdx.x) * 8);
-}
 
 // Several layers' bias gradients: blockIdx.y runs over every layer's 8-channel groups (group g of the whole
-// list belongs to the job k with gbegin[k] <= g < gbegin[k+1]); the partials of group g are where a
-// single-layer launch would put them, offset by the groups before it.
+// list belongs to the job k with gbegin[k] <= g < gbegin[k+1]); block (chunk, g) writes the 8 partials
+// partial[(g * kBiasBlocks + chunk) * 8 ..].
 struct BiasTable
 {
     BiasGradJob job[kMaxBiasJobs];
@@ -425,16 +419,6 @@ __global__ void bias_reduce_many_kernel(const __grid_constant__ BiasTable t, con
     t.job[k].db[gc - 8 * t.gbegin[k]] += s;
 }
 
-// db[c] += the kBiasBlocks partials of channel c, in block order.
-__global__ void bias_reduce_kernel(const float* __restrict__ partial, int C, float* __restrict__ db)
-{
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= C) return;
-    const int cb = c >> 3, i = c & 7;
-    float s = 0.0f;
-    for (int b = 0; b < kBiasBlocks; ++b) s += partial[((size_t)cb * kBiasBlocks + b) * 8 + i];
-    db[c] += s;
-}
 }  // namespace
 
 size_t conv3x3_wgrad_partial_floats(int N, int H, int Cout, int Cin, int Cin_real, int sm_count)
@@ -486,15 +470,4 @@ cudaError_t conv_bias_grad_many(const BiasGradJob* jobs, int n, float* partial, 
     return cudaGetLastError();
 }
 
-cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, float* partial,
-                           cudaStream_t stream)
-{
-    if (!partial || C % 8) return cudaErrorInvalidValue;
-    dim3 grid(kBiasBlocks, C / 8);
-    bias_grad_kernel<<<grid, 256, 0, stream>>>(dz, N, C, H * W, partial);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    bias_reduce_kernel<<<(C + 255) / 256, 256, 0, stream>>>(partial, C, db);
-    return cudaGetLastError();
-}
 }  // namespace lg

@@ -25,7 +25,7 @@ size_t conv3x3_wgrad_partial_floats(int N, int H, int Cout, int Cin, int Cin_rea
 // dW += sum over pixels of dZ (x) shifted X; both blocked BF16 at N x C x H x W.
 cudaError_t conv3x3_wgrad(const __nv_bfloat16* dz, const __nv_bfloat16* x, const WgradArgs& a, int sm_count,
                           cudaStream_t stream);
-// Floats of scratch conv_bias_grad needs for C channels.
+// Floats of scratch conv_bias_grad_many needs for C channels in all.
 size_t conv_bias_grad_partial_floats(int C);
 // One layer's bias gradient in a batched launch: db[c] += sum over the N x HW pixels of dz (blocked BF16).
 struct BiasGradJob
@@ -35,10 +35,8 @@ struct BiasGradJob
     int N, C, HW;
 };
 constexpr int kMaxBiasJobs = 16;
-// Up to kMaxBiasJobs layers in two launches, with the same partials and summation order as one
-// conv_bias_grad per job (identical bits); partial holds conv_bias_grad_partial_floats(sum of C) floats.
+// Up to kMaxBiasJobs layers in two launches, each channel's sum in a fixed order: kBiasBlocks block partials,
+// each over a fixed pixel stride and its warps in order, then the partials in block order; partial holds
+// conv_bias_grad_partial_floats(sum of C) floats.
 cudaError_t conv_bias_grad_many(const BiasGradJob* jobs, int n, float* partial, cudaStream_t stream);
-// db += sum over pixels of dZ, summed in a fixed order through `partial`.
-cudaError_t conv_bias_grad(const __nv_bfloat16* dz, int N, int C, int H, int W, float* db, float* partial,
-                           cudaStream_t stream);
 }  // namespace lg
