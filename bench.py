@@ -112,6 +112,8 @@ def parse_args():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the reference kernels on this GPU (ref_gpu, sorted)")
     ap.add_argument("--no-ingest", action="store_true", help="skip the scene-file load timing")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched orbit-pose frames (one graph-replayed launch against one launch per pose)")
     return ap.parse_args()
 
 
@@ -308,6 +310,29 @@ def reference_designs_on_gpu(scene, spp, bounces, ours_kernel_ms, r):
                   "what": "RenderSceneCUDASorted semantics (per-sample seeding, rays sorted by direction "
                           "between bounces, no Russian roulette); the reference's sorted kernels vs lg_render_sorted"}
     return ref_gpu, sorted_cmp
+
+
+def batched_poses(r, scene, bounces, poses_8=50, poses_256=4):
+    """Orbit poses of the engine scene (radius 15-25 m, height 2-8 m, looking at
+    the scene centre; the 50 poses the denoiser's data come from) rendered in one
+    persistent trace launch replayed from a CUDA graph (lg_render_batch) against
+    one launch per pose (lg_render), device time per frame.  8 spp over all 50
+    poses; 256 spp over the first `poses_256` of them (the per-frame cost does
+    not depend on how many poses share the launch, and 50 such frames would take
+    almost a minute).  The batched time includes the graph's accumulator clears
+    and per-frame tonemaps; the separate one is the trace kernel alone."""
+    from lumina.scene import ENGINE_CENTER, orbit_poses
+    poses = orbit_poses(50, seed=11, center=ENGINE_CENTER)
+    out = {"what": "orbit poses in one graph-replayed persistent launch vs one launch per pose, device ms per frame"}
+    for spp, n in ((8, poses_8), (256, poses_256)):
+        cams = [scene.camera.look_at(p, t) for p, t in poses[:n]]
+        r.render_batch(cams, [spp] * n, [bounces] * n)  # the first call captures the graph
+        _, ms = r.render_batch(cams, [spp] * n, [bounces] * n)
+        sep = [r.render(camera=c, spp=spp, bounces=bounces, accum=False, rgb=False)["kernel_ms"] for c in cams]
+        b, s = float(ms.sum()) / n, float(np.sum(sep)) / n
+        out[f"spp{spp}"] = {"poses": n, "bounces": bounces, "batch_ms_per_frame": b, "separate_ms_per_frame": s,
+                            "speedup": s / b}
+    return out
 
 
 def main():
@@ -542,6 +567,8 @@ def main():
                 line["sorted"] = sorted_cmp
         except Exception as e:  # the oracle libraries are test infrastructure; report, don't fail
             line["ref_gpu"] = {"error": str(e)}
+    if rank == 0 and world == 1 and not args.no_batched and args.scene == "engine":
+        line["batched"] = batched_poses(r, scene, args.bounces)
     if rank == 0 and world == 1 and not args.no_ingest:
         line["ingest"] = ingest_timing(scene, with_reference=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

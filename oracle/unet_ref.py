@@ -118,7 +118,7 @@ def flat_params(model: nn.Module) -> np.ndarray:
     return np.concatenate([v.detach().cpu().float().numpy().ravel() for v in model.state_dict().values()])
 
 
-def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32, fold=()) -> torch.Tensor:
+def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32, fold=(), log_out=False) -> torch.Tensor:
     """The network with BF16 rounding where the tensor-core kernels round;
     everything else in `dtype` (float64 gives the accumulation-order noise
     floor of the FP32 version).
@@ -130,7 +130,10 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32, fold=()) 
     library sums those taps of the upsampled channels in FP32 and rounds the
     sum to BF16 once.  Here: the conv over the upsampled input with those
     rounded weights, even output rows from one weight set and odd rows from
-    the other (exact, since rows 2r and 2r+1 of the input are equal)."""
+    the other (exact, since rows 2r and 2r+1 of the input are equal).
+
+    log_out: for the hdr variant, return the log-space output max(log1p(x) +
+    tail, 0) that hdr_loss compares with log1p(target), not its expm1."""
     s = model.slope
 
     def _q(t):
@@ -176,5 +179,6 @@ def forward_bf16(model: UNetRef, x: torch.Tensor, dtype=torch.float32, fold=()) 
     u1 = block(model.u1, torch.cat([up(u2), d1], 1), "u1", u2.shape[1])
     tail = F.conv2d(u1, model.tail.weight.to(dtype), model.tail.bias.to(dtype))
     if hdr:
-        return torch.expm1(torch.clamp(x[:, :3] + tail, min=0.0))
+        y = torch.clamp(x[:, :3] + tail, min=0.0)
+        return y if log_out else torch.expm1(y)
     return torch.clamp(x[:, :3] + tail, 0.0, 1.0)

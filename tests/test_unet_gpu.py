@@ -357,6 +357,47 @@ def test_unet_hdr_variant_gradients_match_torch_autograd():
     assert losses[-1] < 0.8 * losses[0], losses[::5]
 
 
+def _hdr_grads_bf16(flat, noisy, clean, dtype):
+    """Autograd of the HDR loss (L1 in log1p space) through the BF16-emulated
+    restatement in `dtype`, flat in parameter order."""
+    m = unet_ref.load_flat(unet_ref.UNetRef(variant="hdr"), flat).to(dtype)
+    y = unet_ref.forward_bf16(m, torch.from_numpy(noisy), dtype=dtype, log_out=True)
+    F.l1_loss(y, torch.log1p(torch.from_numpy(clean).to(dtype))).backward()
+    return np.concatenate([p.grad.double().numpy().ravel() for p in m.parameters()]), \
+        [(k, p.numel()) for k, p in m.named_parameters()]
+
+
+def test_unet_hdr_gradients_match_bf16_emulated_autograd():
+    """HDR variant: the kernels' gradients vs autograd through the BF16-emulated
+    restatement in FP64, per tensor within 3x the FP32-vs-FP64 emulation
+    floor + 1% relative L2, cosine above 0.998 (the bar of the reference
+    variant's test above)."""
+    flat = unet_ref.make_params(24, unet_ref.UNetRef(variant="hdr"))
+    net = lumina.UNet(variant="hdr")
+    net.set_params(flat)
+    n, h, w = 2, 32, 48
+    noisy, clean = _hdr_batch(n, h, w, 8)
+    dx, dt = torch.from_numpy(noisy).cuda(), torch.from_numpy(clean).cuda()
+    _, g = net.loss_grad(dx.data_ptr(), dt.data_ptr(), n, h, w)
+    g64, names = _hdr_grads_bf16(flat, noisy, clean, torch.float64)
+    g32, _ = _hdr_grads_bf16(flat, noisy, clean, torch.float32)
+
+    def err(a, b):
+        return (float(np.dot(a, b) / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30)),
+                float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-30)))
+
+    off, worst = 0, []
+    for k, cnt in names:
+        sl = slice(off, off + cnt)
+        off += cnt
+        (cos, rel), (_, frel) = err(g[sl].astype(np.float64), g64[sl]), err(g32[sl], g64[sl])
+        worst.append((rel - 3 * frel, cos, rel, frel, k))
+    worst.sort(reverse=True)
+    print("HDR worst tensors (excess, cos, rel, FP32 floor rel):", worst[:4])
+    for _, cos, rel, frel, k in worst:
+        assert cos > 0.998 and rel <= 3 * frel + 0.01, (k, cos, rel, frel)
+
+
 def test_autotune_keeps_results():
     """lg_unet_autotune picks per-layer tile shapes by timing; the network's
     output and gradients must stay within the same bars against torch."""
