@@ -38,6 +38,9 @@ counting pass) with ms/frame alongside.
   ingest    scene-file load times: this library on scene.json and on the
             binary scene file, and the reference's LoadSceneJSON on the same
             JSON (host only).
+  batched   the 50 orbit poses of the engine scene in one graph-replayed
+            persistent launch (lg_render_batch) against one launch per pose,
+            device ms per frame, at 8 spp (all 50) and 256 spp (the first 4).
 
 --impl reference times only that CPU path (the reference renderer has no
 other CPU path) on the same rows, over the reference's own BuildBVH, and
