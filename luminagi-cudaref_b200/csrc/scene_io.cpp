@@ -234,6 +234,20 @@ struct Cursor
         }
         te = p;
     }
+    // nlohmann::json rejects a number whose double is not finite (an
+    // exponent past 1e308, or an integer of more than 308 digits that it
+    // reads as a double) with this error, wherever the number stands.
+    [[noreturn]] static void overflow(const char* tb, const char* te)
+    {
+        throw ParseError{"[json.exception.out_of_range.406] number overflow parsing '" + std::string(tb, te) + "'"};
+    }
+    // The overflow check of a number that is not converted (a skipped value).
+    static void check_finite(const char* tb, const char* te)
+    {
+        if (te - tb < 300 && !std::memchr(tb, 'e', (size_t)(te - tb)) && !std::memchr(tb, 'E', (size_t)(te - tb)))
+            return;  // under 300 characters without an exponent: below 1e300
+        if (!std::isfinite(std::strtod(std::string(tb, te).c_str(), nullptr))) overflow(tb, te);
+    }
     // nlohmann get<float>(): integer -> (float)int64, real -> (float)strtod.
     float real()
     {
@@ -260,6 +274,7 @@ struct Cursor
         auto r = std::from_chars(tb, te, d);
         if (r.ec == std::errc::result_out_of_range) d = std::strtod(std::string(tb, te).c_str(), nullptr);
         else if (r.ec != std::errc()) fail("bad number");
+        if (!std::isfinite(d)) overflow(tb, te);
         return (float)d;
     }
     // nlohmann get<int>(): integer -> (int)int64, real -> (int)double.
@@ -274,8 +289,12 @@ struct Cursor
             int64_t v;
             auto r = std::from_chars(tb, te, v);
             if (r.ec == std::errc()) return (int)v;
+            uint64_t u;  // nlohmann keeps integers up to 2^64 - 1 as unsigned
+            r = std::from_chars(tb, te, u);
+            if (r.ec == std::errc()) return (int)u;
         }
         double d = std::strtod(std::string(tb, te).c_str(), nullptr);
+        if (!std::isfinite(d)) overflow(tb, te);
         return (int)d;
     }
     // Skips one value.  When starts != null and the value is an array, the
@@ -339,6 +358,7 @@ struct Cursor
         const char *tb, *te;
         bool is_int;
         number_token(tb, te, is_int);
+        check_finite(tb, te);
     }
 };
 

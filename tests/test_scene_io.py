@@ -282,3 +282,101 @@ def test_split_parse_fuzz_matches_serial(tmp_path):
         assert res[0] == res[1], (trial, res[0][0], res[1][0])
         outcomes.add(res[0][0])
     assert outcomes == {"ok", "err"}
+
+
+def _number_tokens(n, seed):
+    """JSON real tokens of many forms: %.9g coordinates (the writers' form),
+    short and long digit strings, leading and trailing zeros, exponents inside
+    and outside 1e+-22, more than 19 significant digits, signed zeros,
+    subnormal and overflowing floats, and decimal halfway points between
+    adjacent floats (where a second rounding would show)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        k = rng.integers(0, 10)
+        x = float(rng.standard_normal() * 10.0 ** rng.integers(-8, 9))
+        if k == 0:
+            out.append("%.9g" % x)
+        elif k == 1:
+            out.append("%.17g" % x)
+        elif k == 2:
+            out.append("%.*f" % (int(rng.integers(1, 12)), x))
+        elif k == 3:
+            out.append("%.*e" % (int(rng.integers(0, 20)), x * 10.0 ** rng.integers(-40, 40)))
+        elif k == 4:  # 20 to 30 significant digits
+            d = str(rng.integers(1, 10)) + "".join(str(v) for v in rng.integers(0, 10, int(rng.integers(19, 30))))
+            out.append(("-" if x < 0 else "") + d[:3] + "." + d[3:])
+        elif k == 5:  # leading zeros in the fraction, trailing zeros after it
+            out.append("%s0.%s%d%s" % ("-" if x < 0 else "", "0" * int(rng.integers(0, 25)),
+                                       int(rng.integers(1, 10**6)), "0" * int(rng.integers(0, 15))))
+        elif k == 6:
+            out.append(rng.choice(["0.0", "-0.0", "-0.000e5", "0e-400", "1e-46", "1.4e-45", "7e-46",
+                                   "3.4028235e38", "3.5e38", "1e39", "-1e300", "1.17549435e-38", "123456789012345678.5",
+                                   "9007199254740993.0", "9007199254740992.0", "4.9406564584124654e-324"]))
+        elif k == 7:  # halfway between two adjacent floats, printed exactly
+            f = np.float32(x)
+            g = np.nextafter(f, np.float32(np.inf))
+            out.append("%.20e" % ((float(f) + float(g)) / 2))
+        elif k == 8:
+            out.append("%de%d" % (int(rng.integers(-999, 1000)), int(rng.integers(-30, 31))))
+        else:
+            out.append("%.*fE+%d" % (int(rng.integers(0, 6)), x, int(rng.integers(0, 25))))
+    return out
+
+
+def test_real_tokens_convert_as_strtod_then_float(tmp_path):
+    """Every real token converts to the float nearest the correctly rounded
+    double (nlohmann::json's strtod then get<float>): Python's float() is the
+    correctly rounded double, numpy narrows it to float as a C cast does."""
+    toks = _number_tokens(24 * 3000, 5)
+    n = len(toks) // 24
+    head = ('{"version": 1, "camera": {"pos": [0,0,1], "camera_to_world": [1,0,0,0,0,1,0,0,0,0,1,0,0,0,1,1],'
+            ' "fov_y_deg": 60, "aspect": 2, "near": 0.1, "far": 100, "image_width": 64, "image_height": 32},'
+            ' "sun": {"direction": [0,0,-1], "color": [1,1,1], "intensity": 1}, "lights": [],'
+            ' "materials": [{"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]}], "triangles": [\n')
+    parts = []
+    for i in range(n):
+        t = toks[24 * i:24 * i + 24]
+        parts.append('{"v": [[%s,%s,%s],[%s,%s,%s],[%s,%s,%s]], "n": [[%s,%s,%s],[%s,%s,%s],[%s,%s,%s]], '
+                     '"uv": [[%s,%s],[%s,%s],[%s,%s]], "mat": 0}' % tuple(t))
+    p = tmp_path / "numbers.json"
+    p.write_text(head + ",\n".join(parts) + "\n]}\n")
+    with np.errstate(over="ignore"):
+        want = np.array([np.float32(float(s)) for s in toks[:24 * n]], np.float32)
+    s = lumina.Scene.load_json(p, threads=1)
+    got = s.tris.view(np.float32).reshape(n, 25)[:, :24].ravel()
+    bad = np.flatnonzero(got.view(np.uint32) != want.view(np.uint32))
+    assert bad.size == 0, [(toks[i], got[i], want[i]) for i in bad[:8]]
+    if O.ref_available():
+        ref = O.ref_load_scene(str(p))["tris"]
+        assert ref.tobytes() == s.tris.tobytes()
+
+
+@pytest.mark.parametrize("where,token", [("coordinate", "-1e400"), ("coordinate", "1" + "0" * 309),
+                                         ("material index", "2e308"), ("skipped value", "1.5E+999")])
+def test_number_overflow_rejected_as_reference(tmp_path, where, token):
+    """A number whose double is not finite fails the load, with nlohmann's
+    message, as the reference's LoadSceneJSON does (its parser rejects it
+    wherever it stands); 3.5e38, finite as a double, loads as float inf."""
+    tri = {"coordinate": '{"v": [[0,0,%s],[1,0,0],[0,1,0]], "n": [[0,0,1],[0,0,1],[0,0,1]], '
+                         '"uv": [[0,0],[1,0],[0,1]], "mat": 0}' % token,
+           "material index": '{"v": [[0,0,0],[1,0,0],[0,1,0]], "n": [[0,0,1],[0,0,1],[0,0,1]], '
+                             '"uv": [[0,0],[1,0],[0,1]], "mat": %s}' % token,
+           "skipped value": '{"v": [[0,0,0],[1,0,0],[0,1,0]], "n": [[0,0,1],[0,0,1],[0,0,1]], '
+                            '"uv": [[0,0],[1,0],[0,1]], "mat": 0, "extra": %s}' % token}[where]
+    head = ('{"version": 1, "camera": {"pos": [0,0,1], "camera_to_world": [1,0,0,0,0,1,0,0,0,0,1,0,0,0,1,1],'
+            ' "fov_y_deg": 60, "aspect": 2, "near": 0.1, "far": 100, "image_width": 64, "image_height": 32},'
+            ' "sun": {"direction": [0,0,-1], "color": [1,1,1], "intensity": 1}, "lights": [],'
+            ' "materials": [{"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]}], "triangles": [\n')
+    p = tmp_path / "overflow.json"
+    p.write_text(head + tri + "\n]}\n")
+    r = subprocess.run([str(_ffi.CLI_PATH), str(p), "--spp", "1"],
+                       capture_output=True, text=True)
+    want = "[scene] JSON parse error: [json.exception.out_of_range.406] number overflow parsing '%s'" % token
+    assert r.returncode == 2 and want in r.stderr, r.stderr
+    if O.ref_available():
+        assert O.ref_load_scene(str(p)) is None
+    p.write_text(head + tri.replace(token, "3.5e38") + "\n]}\n")
+    if where == "coordinate":
+        s = lumina.Scene.load_json(p)
+        assert np.isinf(s.tris["v"][0][0][2])
