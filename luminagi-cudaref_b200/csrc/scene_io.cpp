@@ -165,6 +165,33 @@ struct Cursor
         }
         return v;
     }
+    // A multi-byte UTF-8 sequence whose lead byte b0 was just read: the
+    // well-formed sequences of RFC 3629 (no overlong forms, no UTF-16
+    // surrogates, nothing above U+10FFFF), which nlohmann::json's lexer
+    // accepts and no others.  Appends the sequence to s.
+    void utf8_tail(unsigned char b0, std::string& s)
+    {
+        int n;
+        unsigned char lo = 0x80, hi = 0xBF;  // range of the second byte
+        if (b0 >= 0xC2 && b0 <= 0xDF) n = 1;
+        else if (b0 == 0xE0) { n = 2; lo = 0xA0; }
+        else if (b0 >= 0xE1 && b0 <= 0xEC) n = 2;
+        else if (b0 == 0xED) { n = 2; hi = 0x9F; }
+        else if (b0 >= 0xEE && b0 <= 0xEF) n = 2;
+        else if (b0 == 0xF0) { n = 3; lo = 0x90; }
+        else if (b0 >= 0xF1 && b0 <= 0xF3) n = 3;
+        else if (b0 == 0xF4) { n = 3; hi = 0x8F; }
+        else { --p; fail("ill-formed UTF-8 byte"); }
+        s += (char)b0;
+        for (int i = 0; i < n; ++i)
+        {
+            if (p >= end) fail("unterminated string");
+            const unsigned char b = (unsigned char)*p;
+            if (b < (i ? 0x80 : lo) || b > (i ? 0xBF : hi)) fail("ill-formed UTF-8 byte");
+            s += (char)b;
+            ++p;
+        }
+    }
     std::string string()
     {
         expect('"');
@@ -175,6 +202,7 @@ struct Cursor
             char c = *p++;
             if (c == '"') break;
             if ((unsigned char)c < 0x20) fail("control character in string");
+            if ((unsigned char)c >= 0x80) { utf8_tail((unsigned char)c, s); continue; }
             if (c != '\\') { s += c; continue; }
             if (p >= end) fail("unterminated escape");
             char e = *p++;

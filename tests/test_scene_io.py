@@ -380,3 +380,46 @@ def test_number_overflow_rejected_as_reference(tmp_path, where, token):
     if where == "coordinate":
         s = lumina.Scene.load_json(p)
         assert np.isinf(s.tris["v"][0][0][2])
+
+
+_UTF8_CASES = [  # (bytes inside a string, well-formed per RFC 3629)
+    (b"caf\xc3\xa9", True), (b"\xe2\x82\xac", True), (b"\xf0\x9f\x98\x80", True), (b"\xef\xbf\xbf", True),
+    (b"\xf4\x8f\xbf\xbf", True), (b"\xed\x9f\xbf", True), (b"\xee\x80\x80", True), (b"\xe0\xa0\x80", True),
+    (b"\xc0\x80", False), (b"\xc1\xbf", False), (b"\xe0\x80\x80", False), (b"\xe0\x9f\xbf", False),
+    (b"\xed\xa0\x80", False), (b"\xed\xbf\xbf", False), (b"\xf0\x8f\xbf\xbf", False), (b"\xf4\x90\x80\x80", False),
+    (b"\xf5\x80\x80\x80", False), (b"\xf8\x88\x80\x80\x80", False), (b"\xff", False), (b"\x80", False),
+    (b"\xbf", False), (b"\xe2\x82", False), (b"\xe2\x28\xa1", False), (b"\xc3", False), (b"\xf0\x9f\x98", False),
+]
+
+
+@pytest.mark.parametrize("where", ["texture path", "skipped member"])
+@pytest.mark.parametrize("seq,ok", _UTF8_CASES)
+def test_string_utf8_accepted_as_reference(tmp_path, where, seq, ok):
+    """Strings accept exactly the well-formed UTF-8 sequences, as nlohmann's
+    lexer does (the reference's loader fails on the others); an accepted
+    sequence reaches the texture path byte for byte."""
+    tex = b'"tex/a' + seq + b'b.png"'
+    mat = b'{"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]' + (b', "diffuse_tex": ' + tex if where ==
+                                                              "texture path" else b"") + b"}"
+    doc = (b'{"version": 1, "camera": {"pos": [0,0,1], "camera_to_world": [1,0,0,0,0,1,0,0,0,0,1,0,0,0,1,1],'
+           b' "fov_y_deg": 60, "aspect": 2, "near": 0.1, "far": 100, "image_width": 64, "image_height": 32},'
+           b' "sun": {"direction": [0,0,-1], "color": [1,1,1], "intensity": 1}, "lights": [],'
+           + (b' "note": ' + tex + b"," if where == "skipped member" else b"")
+           + b' "materials": [' + mat + b'], "triangles": [{"v": [[0,0,0],[1,0,0],[0,1,0]],'
+           b' "n": [[0,0,1],[0,0,1],[0,0,1]], "uv": [[0,0],[1,0],[0,1]], "mat": 0}]}\n')
+    p = tmp_path / "utf8.json"
+    p.write_bytes(doc)
+    import ctypes as C
+    h = C.c_void_p()
+    rc = _ffi.lib().lg_scene_load_json(str(p).encode(), 0, 1, C.byref(h))
+    assert (rc == 0) == ok, _ffi.lib().lg_last_error()
+    if ok:
+        try:
+            if where == "texture path":
+                assert _ffi.lib().lg_scene_texture(h, 0) == b"tex/a" + seq + b"b.png"
+        finally:
+            _ffi.lib().lg_scene_destroy(h)
+    else:
+        assert b"ill-formed UTF-8" in _ffi.lib().lg_last_error() or b"unterminated" in _ffi.lib().lg_last_error()
+    if O.ref_available():
+        assert (O.ref_load_scene(str(p)) is not None) == ok
