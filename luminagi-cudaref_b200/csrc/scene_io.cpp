@@ -14,6 +14,11 @@
 // parallel from those offsets.  Where the
 // reference lets nlohmann throw out of LoadSceneJSON on a missing key (the
 // process terminates), this loader prints "[scene] ..." and returns false.
+// Which documents load follows the reference's nlohmann::json read with
+// `f >> j`: a leading UTF-8 byte-order mark is skipped, nothing after the
+// top-level object is read, members the schema does not use are checked for
+// syntax as they are skipped, strings must be well-formed UTF-8, and a number
+// whose double overflows fails the load.
 // A file that begins with the binary scene magic ("LGSCENE1", layout below)
 // is read as a binary scene instead: same content, no text parsing.
 #include <algorithm>
@@ -226,6 +231,7 @@ struct Cursor
                     if (lo < 0xDC00 || lo > 0xDFFF) fail("bad surrogate pair");
                     cp = 0x10000 + ((cp - 0xD800) << 10) + (lo - 0xDC00);
                 }
+                else if (cp >= 0xDC00 && cp <= 0xDFFF) fail("unpaired surrogate");
                 put_utf8(s, cp);
                 break;
             }
@@ -325,10 +331,79 @@ struct Cursor
         if (!std::isfinite(d)) overflow(tb, te);
         return (int)d;
     }
+    // Skips one value, checking its syntax as nlohmann's parser does (an
+    // explicit stack of the open containers, so nesting depth is unbounded).
+    void skip_checked()
+    {
+        std::vector<char> open;
+        for (;;)
+        {
+            const char c = peek();
+            if (c == '{' || c == '[')
+            {
+                ++p;
+                if (peek() == (c == '{' ? '}' : ']')) ++p;
+                else
+                {
+                    open.push_back(c);
+                    if (c == '{')
+                    {
+                        string();
+                        expect(':');
+                    }
+                    continue;
+                }
+            }
+            else scalar();
+            // after a value: close containers, or go on to the next member or element
+            for (;;)
+            {
+                if (open.empty()) return;
+                const char d = peek();
+                if (d == ',')
+                {
+                    ++p;
+                    if (open.back() == '{')
+                    {
+                        string();
+                        expect(':');
+                    }
+                    break;
+                }
+                if (d == (open.back() == '{' ? '}' : ']'))
+                {
+                    ++p;
+                    open.pop_back();
+                    continue;
+                }
+                fail(open.back() == '{' ? "expected ',' or '}'" : "expected ',' or ']'");
+            }
+        }
+    }
+    // A string, literal or number (checked for overflow).
+    void scalar()
+    {
+        const char c = peek();
+        if (c == '"') { string(); return; }
+        if (c == 't') { if (!literal("true")) fail("bad literal"); return; }
+        if (c == 'f') { if (!literal("false")) fail("bad literal"); return; }
+        if (c == 'n') { if (!literal("null")) fail("bad literal"); return; }
+        const char *tb, *te;
+        bool is_int;
+        number_token(tb, te, is_int);
+        check_finite(tb, te);
+    }
     // Skips one value.  When starts != null and the value is an array, the
-    // offset of each element is appended (used for the triangle array).
+    // offset of each element is appended (used for the triangle array, whose
+    // elements are then parsed, and so checked, one by one); any other value
+    // is checked as it is skipped.
     void skip(std::vector<const char*>* starts = nullptr)
     {
+        if (!starts)
+        {
+            skip_checked();
+            return;
+        }
         char c = peek();
         if (c == '{' || c == '[')
         {
@@ -379,14 +454,7 @@ struct Cursor
             p = q;
             return;
         }
-        if (c == '"') { string(); return; }
-        if (c == 't') { if (!literal("true")) fail("bad literal"); return; }
-        if (c == 'f') { if (!literal("false")) fail("bad literal"); return; }
-        if (c == 'n') { if (!literal("null")) fail("bad literal"); return; }
-        const char *tb, *te;
-        bool is_int;
-        number_token(tb, te, is_int);
-        check_finite(tb, te);
+        scalar();
     }
 };
 
@@ -576,6 +644,8 @@ bool parse_triangles_speculative(Cursor& c, std::vector<Triangle>& out, int nt)
 std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
 {
     Cursor c{data, data, data + size};
+    // nlohmann's lexer skips a UTF-8 byte-order mark at the start of the input.
+    if (size >= 3 && std::memcmp(data, "\xEF\xBB\xBF", 3) == 0) c.p += 3;
     try
     {
         Span sv, sc, ss, sl, sm, st;
@@ -603,8 +673,8 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
             v.skip(s == &st ? &tri_starts : nullptr);
             if (s) { s->p = b; s->end = v.p; }
         });
-        c.ws();
-        if (c.p != c.end) c.fail("trailing characters");
+        // LoadSceneJSON reads the file with `f >> j` (scene_loader.cpp:38), a
+        // non-strict parse: what follows the top-level object is not read.
 
         // "version" via j.value("version", 0): absent or not a number -> 0.
         int version = 0;
@@ -744,6 +814,9 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
                         Cursor tc{data, tri_starts[i], st.end};
                         if (tc.peek() != '{') tc.fail("triangle must be an object");
                         parse_triangle(tc, out.triangles[i]);
+                        // the scan recorded starts only after commas: the element must end
+                        // where the next one's comma (or the array's ']') follows
+                        if (tc.peek() != (i + 1 < n ? ',' : ']')) tc.fail("expected ',' or ']'");
                     }
                 }
                 catch (const ParseError& pe) { errs[(size_t)w] = pe.msg; }

@@ -423,3 +423,79 @@ def test_string_utf8_accepted_as_reference(tmp_path, where, seq, ok):
         assert b"ill-formed UTF-8" in _ffi.lib().lg_last_error() or b"unterminated" in _ffi.lib().lg_last_error()
     if O.ref_available():
         assert (O.ref_load_scene(str(p)) is not None) == ok
+
+
+_CAM = ('"camera": {"pos": [0,0,1], "camera_to_world": [1,0,0,0,0,1,0,0,0,0,1,0,0,0,1,1], "fov_y_deg": 60,'
+        ' "aspect": 2, "near": 0.1, "far": 100, "image_width": 64, "image_height": 32}')
+_SUN = '"sun": {"direction": [0,0,-1], "color": [1,1,1], "intensity": 1}'
+_MAT = '"materials": [{"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]}]'
+_TRI = '{"v": [[0,0,0],[1,0,0],[0,1,0]], "n": [[0,0,1],[0,0,1],[0,0,1]], "uv": [[0,0],[1,0],[0,1]], "mat": 0}'
+
+
+def _doc(tris=_TRI, extra="", head=b"", tail=b""):
+    body = '{"version": 1, %s, %s, "lights": [], %s%s, "triangles": [%s]}' % (_CAM, _SUN, _MAT, extra, tris)
+    return head + body.encode() + tail
+
+
+def _many(n, sep=", "):
+    return sep.join([_TRI] * n)
+
+
+# (name, document, the reference's LoadSceneJSON accepts it)
+_DOCS = [
+    ("plain", _doc(), True),
+    ("byte-order mark", _doc(head=b"\xef\xbb\xbf"), True),
+    ("text after the object (f >> j reads one value)", _doc(tail=b" x {"), True),
+    ("second object after the first", _doc(tail=b" {}"), True),
+    ("duplicate triangles key: last wins", _doc()[:-1] + b', "triangles": []}', True),
+    ("lone low surrogate escape", _doc(extra=', "x": "\\udc00"'), False),
+    ("lone high surrogate escape", _doc(extra=', "x": "\\ud800x"'), False),
+    ("escaped NUL", _doc(extra=', "x": "\\u0000"'), True),
+    ("form feed as whitespace", _doc(extra=',\f"x": 1'), False),
+    ("skipped member: empty array element", _doc(extra=', "x": [1,,2]'), False),
+    ("skipped member: missing colon", _doc(extra=', "x": {"a" 1}'), False),
+    ("skipped member: trailing comma", _doc(extra=', "x": [1,2,]'), False),
+    ("skipped member: bad literal", _doc(extra=', "x": [tru]'), False),
+    ("skipped member: mismatched bracket", _doc(extra=', "x": {"a": [1}'), False),
+    ("skipped member: 5,000 levels deep", _doc(extra=', "x": ' + "[" * 5000 + "]" * 5000), True),
+    ("triangles: missing comma", _doc(_TRI + " " + _TRI), False),
+    ("triangles: trailing comma", _doc(_TRI + ","), False),
+    ("triangles: double comma", _doc(_TRI + ",," + _TRI), False),
+    ("triangle with a malformed extra member", _doc(_TRI.replace('"mat": 0', '"mat": 0, "q": [1 2]')), False),
+    ("triangle with a nested extra member", _doc(_TRI.replace('"mat": 0', '"mat": 0, "q": {"z": [1, "s", null]}')),
+     True),
+    ("lights: trailing comma", _doc().replace(b'"lights": []', b'"lights": [1,]'), False),
+    ("30,000 triangles", _doc(_many(30000)), True),
+    ("30,000 triangles, missing comma in the middle", _doc(_many(15000) + " " + _many(15000)), False),
+    ("30,000 triangles, trailing comma", _doc(_many(30000) + ","), False),
+    ("30,000 triangles, malformed extra member in the middle",
+     _doc(_many(15000) + ", " + _TRI.replace('"mat": 0', '"mat": 0, "q": [1,,2]') + ", " + _many(15000)), False),
+    ("30,000 triangles, element-like text inside a string",
+     _doc(_many(15000) + ", " + _TRI.replace('"mat": 0', '"mat": 0, "q": "}, {\\"v\\": ["') + ", " + _many(15000)),
+     True),
+]
+
+
+@pytest.mark.parametrize("name,doc,ok", _DOCS, ids=[d[0] for d in _DOCS])
+def test_document_accepted_as_reference(tmp_path, name, doc, ok):
+    """Which documents load: the reference's LoadSceneJSON (nlohmann's
+    non-strict `f >> j`, scene_loader.cpp:38) decides, on the serial path and
+    on the parallel triangle parse (30,000 triangles span several 1 MB
+    shares)."""
+    import ctypes as C
+    p = tmp_path / "doc.json"
+    p.write_bytes(doc)
+    for threads in (1, 8):
+        h = C.c_void_p()
+        rc = _ffi.lib().lg_scene_load_json(str(p).encode(), 0, threads, C.byref(h))
+        if rc == 0:
+            _ffi.lib().lg_scene_destroy(h)
+        assert (rc == 0) == ok, (threads, _ffi.lib().lg_last_error())
+    if ok:
+        s = lumina.Scene.load_json(p)
+        assert s.n_tris == (0 if "duplicate" in name else doc.count(b'"mat": 0'))
+    if O.ref_available():
+        r = O.ref_load_scene(str(p))
+        assert (r is not None) == ok
+        if ok:
+            assert r["tris"].tobytes() == s.tris.tobytes()
