@@ -490,6 +490,50 @@ void for_elements(Cursor& c, F&& fn)
     }
 }
 
+// Where an object stands for the lights, materials or triangles array, the
+// reference's range-for over the json value visits the object's values in the
+// order its std::map keeps them: by key, compared byte by byte, with the last
+// of equal keys kept.  Returns the start of each such value; `c` ends after
+// the object.
+std::vector<const char*> object_values_in_key_order(Cursor& c)
+{
+    std::vector<std::pair<std::string, const char*>> m;
+    for_members(c, [&](const std::string& k, Cursor& v) {
+        v.ws();
+        m.emplace_back(k, v.p);
+        v.skip();
+    });
+    std::stable_sort(m.begin(), m.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<const char*> out;
+    for (size_t i = 0; i < m.size(); ++i)
+        if (i + 1 == m.size() || m[i + 1].first != m[i].first) out.push_back(m[i].second);
+    return out;
+}
+// The elements of a lights or materials value as the reference's range-for
+// visits them: an array's elements, an object's values in key order, none for
+// null.
+template <class F>
+void for_values(Cursor& c, F&& fn)
+{
+    const char ch = c.peek();
+    if (ch == 'n')
+    {
+        if (!c.literal("null")) c.fail("bad literal");
+        return;
+    }
+    if (ch != '{')
+    {
+        for_elements(c, fn);
+        return;
+    }
+    const std::vector<const char*> vals = object_values_in_key_order(c);
+    for (const char* v : vals)
+    {
+        Cursor e{c.beg, v, c.end};
+        fn(e);
+    }
+}
+
 // Reads a JSON array of exactly `n` numbers (the reference reads j[0..n-1];
 // extra elements are ignored, missing ones are an error).
 void read_floats(Cursor& c, float* out, int n)
@@ -727,7 +771,7 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
         if (!sl.present()) missing("lights");
         {
             Cursor v{data, sl.p, sl.end};
-            for_elements(v, [&](Cursor& e) {
+            for_values(v, [&](Cursor& e) {
                 // Members may come in any order: collect, then interpret by type.
                 std::string type;
                 bool htype = false, hdir = false, hcol = false, hint = false, hpos = false, hrad = false;
@@ -776,7 +820,7 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
         if (!sm.present()) missing("materials");
         {
             Cursor v{data, sm.p, sm.end};
-            for_elements(v, [&](Cursor& e) {
+            for_values(v, [&](Cursor& e) {
                 Material m;
                 bool ha = false, he = false;
                 for_members(e, [&](const std::string& k, Cursor& f) {
@@ -798,7 +842,16 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
         if (!tris_parsed)
         {
             Cursor v{data, st.p, st.end};
-            if (v.peek() != '[') v.fail("triangles must be an array");
+            // an object's values in key order, or none for null, as for lights and materials
+            const char tc0 = v.peek();
+            const bool tri_object = tc0 == '{' || tc0 == 'n';
+            if (tc0 == '{') tri_starts = object_values_in_key_order(v);
+            else if (tc0 == 'n')
+            {
+                if (!v.literal("null")) v.fail("bad literal");
+                tri_starts.clear();
+            }
+            else if (tc0 != '[') v.fail("triangles must be an array");
             const size_t n = tri_starts.size();
             size_triangles(out.triangles, n);
             int nt = nt_all;
@@ -816,7 +869,7 @@ std::string parse_scene(const char* data, size_t size, Scene& out, int threads)
                         parse_triangle(tc, out.triangles[i]);
                         // the scan recorded starts only after commas: the element must end
                         // where the next one's comma (or the array's ']') follows
-                        if (tc.peek() != (i + 1 < n ? ',' : ']')) tc.fail("expected ',' or ']'");
+                        if (!tri_object && tc.peek() != (i + 1 < n ? ',' : ']')) tc.fail("expected ',' or ']'");
                     }
                 }
                 catch (const ParseError& pe) { errs[(size_t)w] = pe.msg; }

@@ -499,3 +499,50 @@ def test_document_accepted_as_reference(tmp_path, name, doc, ok):
         assert (r is not None) == ok
         if ok:
             assert r["tris"].tobytes() == s.tris.tobytes()
+
+
+_PL = '{"type": "point", "pos": [0,0,3], "color": [1,1,1], "intensity": %d, "radius": 10}'
+_T_AT = lambda z: _TRI.replace("[0,0,0],[1,0,0]", "[0,0,%d],[1,0,0]" % z)
+
+
+def _doc_with(lights="[]", mats=None, tris=None):
+    mats = mats if mats is not None else '[{"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]}]'
+    tris = tris if tris is not None else "[" + _TRI + "]"
+    return ('{"version": 1, %s, %s, "lights": %s, "materials": %s, "triangles": %s}'
+            % (_CAM, _SUN, lights, mats, tris)).encode()
+
+
+# (name, document, point intensities, material albedo reds, first-vertex z per triangle), as the reference loads them
+_VALUE_FORMS = [
+    ("lights as an object: values in key order", _doc_with('{"b": %s, "a": %s}' % (_PL % 5, _PL % 7)),
+     [7, 5], [0.5], [0]),
+    ("lights object with duplicate keys: the last kept", _doc_with('{"b": %s, "b": %s, "B": %s}' % (_PL % 5, _PL % 7, _PL % 3)),
+     [3, 7], [0.5], [0]),
+    ("lights null", _doc_with("null"), [], [0.5], [0]),
+    ("materials as an object, keys compared as bytes",
+     _doc_with(mats='{"z": {"albedo": [0.5,0.5,0.5], "emissive": [0,0,0]}, "\\u00e9": {"albedo": [0.25,0.2,0.3],'
+                    ' "emissive": [0,0,0]}, "a": {"albedo": [0.75,0.7,0.7], "emissive": [0,0,0]}}'),
+     [], [0.75, 0.5, 0.25], [0]),
+    ("materials null", _doc_with(mats="null"), [], [], [0]),
+    ("triangles as an object", _doc_with(tris='{"t2": %s, "t10": %s, "t1": %s}' % (_T_AT(2), _T_AT(10), _T_AT(1))),
+     [], [0.5], [1, 10, 2]),
+    ("triangles null", _doc_with(tris="null"), [], [0.5], []),
+]
+
+
+@pytest.mark.parametrize("name,doc,points,reds,zs", _VALUE_FORMS, ids=[v[0] for v in _VALUE_FORMS])
+def test_lights_materials_triangles_objects_and_null_as_reference(tmp_path, name, doc, points, reds, zs):
+    """The reference's range-for over `j.at("lights")` (and materials,
+    triangles) visits an object's values in its std::map's key order, keeping
+    the last of duplicate keys, and nothing for null; this loader does the
+    same."""
+    p = tmp_path / "forms.json"
+    p.write_bytes(doc)
+    s = lumina.Scene.load_json(p)
+    assert s.points["intensity"].tolist() == points
+    assert s.mat_albedo[:, 0].tolist() == reds
+    assert s.tris["v"][:, 0, 2].tolist() == zs
+    if O.ref_available():
+        r = O.ref_load_scene(str(p))
+        assert r["tris"].tobytes() == s.tris.tobytes() and r["points"].tobytes() == s.points.tobytes()
+        assert r["albedo"].tobytes() == s.mat_albedo.tobytes()
